@@ -1,0 +1,122 @@
+// Shared device/host helpers for the acoustic-substep kernels.
+//
+// Device layout of every field (all six cube tiles in one allocation):
+//   3-D  double f[6][nk][nj][ni]   ni = nj = n + 2*halo + 1, nk = npz + 1
+//   2-D  double g[6][nj][ni]       (metric terms, surface fields)
+//   1-D  double c[nk]              (per-level constants)
+// i is the fastest index so that a warp reads 32 consecutive i points.
+// Index (t, i, j, k) uses the reference's storage indices (compute domain
+// starts at i = j = halo).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/fv3core_b200.h"
+
+namespace fv3b {
+
+struct Dims {
+  int n, h, nz;
+  int ni, nj, nk;
+  long long sj, sk, st;  // 3-D strides (i stride is 1)
+  long long st2;         // 2-D tile stride (j stride is ni)
+  int isc, iec, jsc, jec;  // compute domain (inclusive), storage indices
+};
+
+inline Dims make_dims(const fv3b_grid_dims* g) {
+  Dims d;
+  d.n = g->npx;
+  d.h = g->n_halo;
+  d.nz = g->npz;
+  d.ni = d.n + 2 * d.h + 1;
+  d.nj = d.ni;
+  d.nk = d.nz + 1;
+  d.sj = d.ni;
+  d.sk = (long long)d.ni * d.nj;
+  d.st = d.sk * d.nk;
+  d.st2 = (long long)d.ni * d.nj;
+  d.isc = d.h;
+  d.iec = d.h + d.n - 1;
+  d.jsc = d.h;
+  d.jec = d.h + d.n - 1;
+  return d;
+}
+
+__host__ __device__ __forceinline__ long long idx3(const Dims& d, int t, int i, int j, int k) {
+  return t * d.st + k * d.sk + j * d.sj + i;
+}
+__host__ __device__ __forceinline__ long long idx2(const Dims& d, int t, int i, int j) {
+  return t * d.st2 + (long long)j * d.ni + i;
+}
+
+// Box of storage indices [i0, i1) x [j0, j1) x [k0, k1), all six tiles.
+struct Box {
+  int i0, i1, j0, j1, k0, k1;
+};
+
+// Launch f(t, i, j, k) over a box: x covers i (warp-contiguous), y covers j,
+// z covers (tile, k).
+template <typename F>
+__global__ void box_kernel(Box b, F f) {
+  int i = b.i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  int j = b.j0 + blockIdx.y * blockDim.y + threadIdx.y;
+  int nkb = b.k1 - b.k0;
+  int t = blockIdx.z / nkb;
+  int k = b.k0 + blockIdx.z % nkb;
+  if (i < b.i1 && j < b.j1) f(t, i, j, k);
+}
+
+template <typename F>
+cudaError_t launch_box(const Box& b, cudaStream_t s, F f) {
+  int ni = b.i1 - b.i0, nj = b.j1 - b.j0, nk = b.k1 - b.k0;
+  if (ni <= 0 || nj <= 0 || nk <= 0) return cudaSuccess;
+  dim3 block(32, 4, 1);
+  dim3 grid((ni + 31) / 32, (nj + 3) / 4, 6 * nk);
+  box_kernel<<<grid, block, 0, s>>>(b, f);
+  return cudaGetLastError();
+}
+
+// Launch f(t, i, j) over the columns of a 2-D box (all six tiles).
+template <typename F>
+__global__ void column_kernel(int i0, int i1, int j0, int j1, F f) {
+  int ncol_i = i1 - i0;
+  int ncol = ncol_i * (j1 - j0);
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  int t = blockIdx.y;
+  if (c >= ncol) return;
+  int i = i0 + c % ncol_i;
+  int j = j0 + c / ncol_i;
+  f(t, i, j);
+}
+
+template <typename F>
+cudaError_t launch_columns(int i0, int i1, int j0, int j1, cudaStream_t s, F f, int block = 128) {
+  int ncol = (i1 - i0) * (j1 - j0);
+  if (ncol <= 0) return cudaSuccess;
+  dim3 grid((ncol + block - 1) / block, 6, 1);
+  column_kernel<<<grid, block, 0, s>>>(i0, i1, j0, j1, f);
+  return cudaGetLastError();
+}
+
+void set_last_error(const char* where, cudaError_t e);
+void set_last_error_msg(const char* msg);
+
+}  // namespace fv3b
+
+#define FV3B_CHECK(call)                                  \
+  do {                                                    \
+    cudaError_t _e = (call);                              \
+    if (_e != cudaSuccess) {                              \
+      fv3b::set_last_error(__func__, _e);                 \
+      return FV3B_ERR_CUDA;                               \
+    }                                                     \
+  } while (0)
+
+#define FV3B_REQUIRE(cond, msg)                           \
+  do {                                                    \
+    if (!(cond)) {                                        \
+      fv3b::set_last_error_msg(msg);                      \
+      return FV3B_ERR_ARGUMENT;                           \
+    }                                                     \
+  } while (0)

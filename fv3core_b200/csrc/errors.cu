@@ -1,0 +1,20 @@
+// Last-error bookkeeping for the C ABI (thread-local, no allocation).
+#include <stdio.h>
+#include <string.h>
+
+#include "common.cuh"
+
+namespace {
+thread_local char g_last_error[512] = "";
+}
+
+namespace fv3b {
+void set_last_error(const char* where, cudaError_t e) {
+  snprintf(g_last_error, sizeof(g_last_error), "%s: %s (%s)", where, cudaGetErrorName(e),
+           cudaGetErrorString(e));
+}
+void set_last_error_msg(const char* msg) { snprintf(g_last_error, sizeof(g_last_error), "%s", msg); }
+}  // namespace fv3b
+
+extern "C" const char* fv3b_last_error(void) { return g_last_error; }
+extern "C" const char* fv3b_version(void) { return "fv3core_b200 0.1.0 sm_100a"; }

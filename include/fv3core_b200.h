@@ -1,0 +1,66 @@
+/*
+ * fv3core_b200 — C ABI of the B200-native acoustic substep.
+ *
+ * Every entry point replaces one stencil class (or class method) of the
+ * reference, fv3core, whose Python interface is cited beside it.  The
+ * reference runs one cube tile per MPI rank; here all six tiles live in one
+ * device allocation and every call advances all of them.
+ *
+ * Memory layout (device pointers, FP64 unless stated):
+ *   3-D field   double[6][npz+1][n+2h+1][n+2h+1]   (i fastest)
+ *   2-D field   double[6][n+2h+1][n+2h+1]
+ *   1-D field   double[npz+1]
+ * Index (i, j) in a field is the reference's storage index: the compute
+ * domain of a tile is i, j in [h, h+n) (cell centres) or [h, h+n] (edges).
+ *
+ * All calls are asynchronous on the given CUDA stream (cudaStream_t passed
+ * as void*), allocate nothing, and return 0 on success or an FV3B_ERR_*
+ * code; fv3b_last_error() describes the last failure of the calling thread.
+ */
+#ifndef FV3CORE_B200_H
+#define FV3CORE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  FV3B_OK = 0,
+  FV3B_ERR_ARGUMENT = 1,    /* bad size, null pointer or unsupported option */
+  FV3B_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  FV3B_ERR_UNSUPPORTED = 3, /* configuration the reference also rejects */
+  FV3B_ERR_TIMEOUT = 4      /* a bounded device wait gave up */
+};
+
+typedef struct fv3b_grid_dims {
+  int32_t npx;    /* compute cells along a tile edge (n) */
+  int32_t n_halo; /* halo width h (3) */
+  int32_t npz;    /* number of layers */
+  int32_t reserved;
+} fv3b_grid_dims;
+
+/* Description of the last error raised on the calling host thread. */
+const char* fv3b_last_error(void);
+
+/* Library version string. */
+const char* fv3b_version(void);
+
+/*
+ * RiemannSolverC.__call__  (fv3core/stencils/riem_solver_c.py:106-165,
+ * with Sim1Solver, fv3core/stencils/sim1_solver.py:11-175).
+ * Columns i, j in [h-1, h+n] of all tiles, interface levels 0..npz.
+ * In: cappa, hs (2-D), ws (2-D), ptc, q_con, delpc, w3.  In/out: gz
+ * (heights in, geopotential out).  Out: pef.
+ */
+int fv3b_riem_solver_c(const fv3b_grid_dims* dims, double dt2, double ptop, double p_fac,
+                       const double* cappa, const double* hs, const double* ws,
+                       const double* ptc, const double* q_con, const double* delpc,
+                       double* gz, double* pef, const double* w3, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FV3CORE_B200_H */

@@ -1,0 +1,107 @@
+"""Deterministic test cases shared by the golden-fixture generator (which runs
+the reference here) and the parity tests (which run the oracle and the CUDA
+path, on any machine).
+
+Every case is built from the package's grid and baroclinic-wave generators
+plus seeded perturbations, so only outputs need to be stored as fixtures.
+Arrays are numpy FP64 in the reference's index order: 3-D fields
+``[6, n+2h+1, n+2h+1, nz+1]``, 2-D ``[6, n+2h+1, n+2h+1]``.
+"""
+import functools
+
+import numpy as np
+
+from fv3core_b200 import constants as C
+from fv3core_b200.grid import CubedSphereGrid
+from fv3core_b200.initial_state import baroclinic_state
+
+HALO = 3
+
+
+@functools.lru_cache(maxsize=8)
+def grid_for(n):
+    return CubedSphereGrid(n, HALO)
+
+
+def base_state(n, nz, seed):
+    return baroclinic_state(grid_for(n), nz, seed=seed)
+
+
+def heights(st, nz):
+    """Interface heights (m) from delz and the surface height, as the
+    reference's ``set_gz`` (dyn_core.py:80-85) builds them."""
+    zs = st["phis"] / C.GRAV
+    gz = np.zeros_like(st["delz"])
+    gz[..., nz] = zs
+    for k in range(nz - 1, -1, -1):
+        gz[..., k] = gz[..., k + 1] - st["delz"][..., k]
+    return gz
+
+
+def riem_solver_c_case(n=12, nz=16, seed=11):
+    st = base_state(n, nz, seed)
+    rng = np.random.default_rng(seed + 1000)
+    shp = st["delp"].shape
+    gz = heights(st, nz)
+    case = {
+        "dt2": 18.75,
+        "ptop": st["ptop"],
+        "p_fac": 0.05,
+        "cappa": st["cappa"].copy(),
+        "hs": st["phis"].copy(),
+        "ws": 0.05 * rng.standard_normal(shp[:3]),
+        "ptc": st["pt"] * (1.0 + 1e-3 * rng.standard_normal(shp)),
+        "q_con": st["q_con"].copy(),
+        "delpc": st["delp"] * (1.0 + 1e-3 * rng.standard_normal(shp)),
+        "gz": gz * (1.0 + 1e-5 * rng.standard_normal(shp)),
+        "pef": np.zeros(shp),
+        "w3": 0.1 * rng.standard_normal(shp),
+    }
+    return case
+
+
+CASES = {
+    "riem_solver_c": riem_solver_c_case,
+}
+
+
+def metric_namespace(n, tile):
+    """One tile's metric arrays as attributes (oracle input)."""
+    import types
+
+    g = grid_for(n)
+    ns = types.SimpleNamespace()
+    for name, val in vars(g).items():
+        if isinstance(val, np.ndarray) and val.ndim == 3 and val.shape[0] == 6:
+            setattr(ns, name, val[tile])
+    for name in ("edge_w", "edge_e", "edge_s", "edge_n"):
+        setattr(ns, name, getattr(g, name)[tile])
+    ns.da_min, ns.da_min_c = g.da_min, g.da_min_c
+    return ns
+
+
+def c_sw_case(n=12, nz=6, seed=21):
+    st = base_state(n, nz, seed)
+    rng = np.random.default_rng(seed + 1000)
+    shp = st["delp"].shape
+    r = lambda scale: scale * rng.standard_normal(shp)
+    case = {
+        "dt2": 18.75,
+        "delp": st["delp"].copy(),
+        "pt": st["pt"].copy(),
+        "u": st["u"].copy(),
+        "v": st["v"].copy(),
+        "w": r(0.2),
+        "uc": r(5.0),
+        "vc": r(5.0),
+        "ua": r(5.0),
+        "va": r(5.0),
+        "ut": r(5.0),
+        "vt": r(5.0),
+        "divgd": r(1e-5),
+        "omga": r(0.1),
+    }
+    return case
+
+
+CASES["c_sw"] = c_sw_case

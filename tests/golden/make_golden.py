@@ -1,0 +1,94 @@
+"""Generate golden fixtures by running the reference's own stencil classes.
+
+Run here (needs the reference checkout at /root/reference)::
+
+    python tests/golden/make_golden.py [case ...]
+
+For each case in ``cases.py`` the inputs are rebuilt deterministically, the
+reference class runs tile by tile (or, for the full substep, six tiles in
+lock step with a threaded halo exchange), and the outputs are stored in
+``tests/golden/<case>.npz`` restricted to the points the reference defines.
+"""
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+sys.path.insert(0, HERE)
+
+import cases  # noqa: E402
+import reference_runner as rr  # noqa: E402
+
+
+def run_riem_solver_c(case, n, nz):
+    from fv3core.stencils.riem_solver_c import RiemannSolverC
+
+    grid = cases.grid_for(n)
+    out = {"pef": np.zeros_like(case["pef"]), "gz": np.zeros_like(case["gz"])}
+    for t in range(6):
+        tr = rr.TileReference(grid, t, nz)
+        rs = RiemannSolverC(tr.stencil_factory, p_fac=case["p_fac"])
+        S = rr.storage
+        pef = S(case["pef"][t])
+        gz = S(case["gz"][t])
+        rs(
+            case["dt2"],
+            S(case["cappa"][t]),
+            case["ptop"],
+            S(case["hs"][t], origin=(3, 3)),
+            S(case["ws"][t], origin=(3, 3)),
+            S(case["ptc"][t]),
+            S(case["q_con"][t]),
+            S(case["delpc"][t]),
+            gz,
+            pef,
+            S(case["w3"][t]),
+        )
+        out["pef"][t] = pef
+        out["gz"][t] = gz
+    h = 3
+    sl = (slice(None), slice(h - 1, h + n + 1), slice(h - 1, h + n + 1), slice(0, nz + 1))
+    return {k: v[sl] for k, v in out.items()}, {"region": "is-1:ie+2, js-1:je+2, 0:nz+1"}
+
+
+def run_c_sw(case, n, nz):
+    from fv3core.stencils.c_sw import CGridShallowWaterDynamics
+
+    grid = cases.grid_for(n)
+    names = ["delp", "pt", "u", "v", "w", "uc", "vc", "ua", "va", "ut", "vt", "divgd", "omga"]
+    out = {k: np.zeros_like(case["delp"]) for k in names + ["delpc", "ptc"]}
+    for t in range(6):
+        tr = rr.TileReference(grid, t, nz)
+        csw = CGridShallowWaterDynamics(tr.stencil_factory, tr.grid_data, False, 0, 3)
+        st = {k: rr.storage(case[k][t]) for k in names}
+        delpc, ptc = csw(*[st[k] for k in names], case["dt2"])
+        for k in names:
+            out[k][t] = st[k]
+        out["delpc"][t] = delpc
+        out["ptc"][t] = ptc
+    return out, {"region": "full storage"}
+
+
+RUNNERS = {
+    "c_sw": (run_c_sw, dict(n=12, nz=6, seed=21)),
+    "riem_solver_c": (run_riem_solver_c, dict(n=12, nz=16, seed=11)),
+}
+
+
+def main(names):
+    rr.import_reference()
+    for name in names or list(RUNNERS):
+        fn, kw = RUNNERS[name]
+        t0 = time.time()
+        case = cases.CASES[name](**kw)
+        outputs, meta = fn(case, kw["n"], kw["nz"])
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, **outputs, **{f"meta_{k}": v for k, v in meta.items()}, **{f"arg_{k}": v for k, v in kw.items()})
+        print(f"{name}: {time.time() - t0:.1f}s -> {path} ({os.path.getsize(path) / 1e3:.0f} kB)")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])
