@@ -32,6 +32,11 @@ SIGNATURES = {
     "fv3b_riem_solver_c": [D, D, D, P, P, P, P, P, P, P, P, P, P],
 }
 
+# entry points whose first argument is the context (fv3b_ctx*)
+CTX_SIGNATURES = {
+    "fv3b_c_sw": [P, P, P, P, P, P, P, P, P, P, P, P, P, D, ctypes.c_int, P, P, P],
+}
+
 
 def lib():
     global _lib
@@ -45,8 +50,14 @@ def lib():
         L.fv3b_last_error.restype = ctypes.c_char_p
         L.fv3b_version.restype = ctypes.c_char_p
         for name, args in SIGNATURES.items():
+            if args is None:
+                continue
             fn = getattr(L, name)
             fn.argtypes = [ctypes.POINTER(GridDims)] + args
+            fn.restype = ctypes.c_int
+        for name, args in CTX_SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = [ctypes.c_void_p] + args
             fn.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -59,5 +70,14 @@ def call(name, dims, *args):
         raise ERRORS.get(rc, RuntimeError)(f"{name} failed ({rc}): {msg}")
 
 
+def call_ctx(name, ctx, *args):
+    rc = getattr(lib(), name)(ctx, *args)
+    if rc != 0:
+        msg = lib().fv3b_last_error().decode()
+        raise ERRORS.get(rc, RuntimeError)(f"{name} failed ({rc}): {msg}")
+
+
 def exported_symbols():
-    return ["fv3b_last_error", "fv3b_version"] + list(SIGNATURES)
+    return ["fv3b_last_error", "fv3b_version", "fv3b_ctx_create", "fv3b_ctx_destroy"] + [
+        k for k, v in SIGNATURES.items() if v is not None
+    ] + list(CTX_SIGNATURES)

@@ -1,0 +1,41 @@
+// Context: grid sizes, metric pointers, device workspace.
+#include <new>
+
+#include "ctx.cuh"
+
+using namespace fv3b;
+
+extern "C" int fv3b_ctx_create(const fv3b_grid_dims* dims, const fv3b_metrics* metrics, fv3b_ctx** out) {
+  FV3B_REQUIRE(dims && metrics && out, "fv3b_ctx_create: null argument");
+  FV3B_REQUIRE(dims->npx >= 4 && dims->n_halo == 3 && dims->npz >= 2 && dims->npz < 127,
+               "fv3b_ctx_create: need npx >= 4, n_halo == 3, 2 <= npz < 127");
+  fv3b_ctx* c = new (std::nothrow) fv3b_ctx();
+  FV3B_REQUIRE(c != nullptr, "fv3b_ctx_create: out of host memory");
+  c->d = make_dims(dims);
+  c->m = *metrics;
+  size_t n3 = (size_t)c->d.st * 6;
+  cudaError_t e = cudaMalloc((void**)&c->ws_base, n3 * sizeof(double) * NWS);
+  if (e != cudaSuccess) {
+    delete c;
+    set_last_error("fv3b_ctx_create", e);
+    return FV3B_ERR_CUDA;
+  }
+  for (int i = 0; i < NWS; ++i) c->ws[i] = c->ws_base + n3 * i;
+  e = cudaMemset(c->ws_base, 0, n3 * sizeof(double) * NWS);
+  if (e != cudaSuccess) {
+    cudaFree(c->ws_base);
+    delete c;
+    set_last_error("fv3b_ctx_create", e);
+    return FV3B_ERR_CUDA;
+  }
+  *out = c;
+  return FV3B_OK;
+}
+
+extern "C" int fv3b_ctx_destroy(fv3b_ctx* ctx) {
+  if (!ctx) return FV3B_OK;
+  cudaError_t e = cudaFree(ctx->ws_base);
+  delete ctx;
+  FV3B_CHECK(e);
+  return FV3B_OK;
+}

@@ -185,6 +185,7 @@ class CubedSphereGrid:
         cos_sg[4] = _cos_angle(mn, p11, 2 * mn - C)
         cos_sg[5] = _cos_angle(C, me, mn)
         sin_sg = {k: np.minimum(1.0, np.sqrt(np.maximum(0.0, 1.0 - v * v))) for k, v in cos_sg.items()}
+        self._corner_fix(cos_sg, sin_sg)
         for k in range(1, 6):
             setattr(self, f"cos_sg{k}", pad2(cos_sg[k]))
             setattr(self, f"sin_sg{k}", pad2(sin_sg[k]))
@@ -269,6 +270,36 @@ class CubedSphereGrid:
         self.da_max = float(area[:, hs:he, hs:he].max())
         self.da_min_c = float(area_c[:, hs : he + 1, hs : he + 1].min())
         self.da_max_c = float(area_c[:, hs : he + 1, hs : he + 1].max())
+
+    def _corner_fix(self, cos_sg, sin_sg):
+        """Angles in the 3x3 cube-corner halo blocks, which have no cell of
+        their own on the sphere, follow FV3's convention
+        (fv3core/grid/geometry.py:430-512): the block is filled with
+        sin = 1e-8, cos = 1e8, then the edge angles facing the adjacent edge
+        halos are rotated in from those halo cells."""
+        h = self.halo
+        N = cos_sg[1].shape[1]  # cell-centred extent n + 2h
+        for arrs, fill in ((sin_sg, 1.0e-8), (cos_sg, 1.0e8)):
+            for k in range(1, 6):
+                a = arrs[k]
+                a[:, :h, :h] = fill
+                a[:, :h, N - h :] = fill
+                a[:, N - h :, :h] = fill
+                a[:, N - h :, N - h :] = fill
+            sg1, sg2, sg3, sg4 = arrs[1], arrs[2], arrs[3], arrs[4]
+            for a in range(h):
+                # south-west
+                sg3[:, h - 1, a] = sg2[:, a, h]
+                sg4[:, a, h - 1] = sg1[:, h, a]
+                # north-west
+                sg2[:, a, N - h] = sg1[:, h, N - 1 - a]
+                sg3[:, h - 1, N - 1 - a] = sg4[:, a, N - 1 - h]
+                # south-east
+                sg1[:, N - h, a] = sg2[:, N - 1 - a, h]
+                sg4[:, N - 1 - a, h - 1] = sg3[:, N - 1 - h, a]
+                # north-east
+                sg1[:, N - h, N - 1 - a] = sg4[:, N - 1 - a, N - 1 - h]
+                sg2[:, N - 1 - a, N - h] = sg3[:, N - 1 - h, N - 1 - a]
 
     def _edge_factors(self, C):
         """1-D A->B interpolation weights along the four tile edges; entries

@@ -41,6 +41,49 @@ typedef struct fv3b_grid_dims {
   int32_t reserved;
 } fv3b_grid_dims;
 
+/*
+ * Grid metric terms (device pointers, owned by the caller, read only).
+ * 2-D fields are [6][n+2h+1][n+2h+1]; the four edge factors are
+ * [6][n+1] (index = position along the tile edge).  Replaces the reference's
+ * GridData / DampingCoefficients containers (fv3core/utils/grid.py:475-799)
+ * plus the legacy spec.grid fields the hot path reads (fC, f0, agrid, bgrid,
+ * edge_*, divg_*).
+ */
+typedef struct fv3b_metrics {
+  const double *dx, *dy, *dxa, *dya, *dxc, *dyc;
+  const double *rdx, *rdy, *rdxa, *rdya, *rdxc, *rdyc;
+  const double *area, *rarea, *rarea_c;
+  const double *sin_sg1, *sin_sg2, *sin_sg3, *sin_sg4;
+  const double *cos_sg1, *cos_sg2, *cos_sg3, *cos_sg4;
+  const double *cosa, *cosa_u, *cosa_v, *cosa_s, *sina_u, *sina_v;
+  const double *rsina, *rsin_u, *rsin_v, *rsin2;
+  const double *del6_u, *del6_v, *divg_u, *divg_v;
+  const double *fC, *f0;
+  const double *agrid1, *agrid2, *bgrid1, *bgrid2;
+  const double *edge_w, *edge_e, *edge_s, *edge_n;
+  double da_min, da_min_c;
+} fv3b_metrics;
+
+/* Opaque context: grid sizes, metric pointers and the device workspace
+ * (scratch fields) of the stage kernels.  Created once per grid; stage calls
+ * allocate nothing. */
+typedef struct fv3b_ctx fv3b_ctx;
+
+/* Allocates the workspace (cudaMalloc) on the current device. */
+int fv3b_ctx_create(const fv3b_grid_dims* dims, const fv3b_metrics* metrics, fv3b_ctx** out);
+int fv3b_ctx_destroy(fv3b_ctx* ctx);
+
+/*
+ * CGridShallowWaterDynamics.__call__ (fv3core/stencils/c_sw.py:534-659)
+ * including DGrid2AGrid2CGridVectors (fv3core/stencils/d2a2c_vect.py:543-651)
+ * and divergence_corner when nord > 0.
+ * In: u, v.  In/out: delp, pt, w (cube-corner halos are filled, as in the
+ * reference), uc, vc, ua, va, ut, vt, divgd, omga.  Out: delpc, ptc.
+ */
+int fv3b_c_sw(fv3b_ctx* ctx, double* delp, double* pt, const double* u, const double* v, double* w,
+              double* uc, double* vc, double* ua, double* va, double* ut, double* vt, double* divgd,
+              double* omga, double dt2, int nord, double* delpc, double* ptc, void* stream);
+
 /* Description of the last error raised on the calling host thread. */
 const char* fv3b_last_error(void);
 

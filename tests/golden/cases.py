@@ -105,3 +105,51 @@ def c_sw_case(n=12, nz=6, seed=21):
 
 
 CASES["c_sw"] = c_sw_case
+
+
+# D-grid shallow-water namelist of the baroclinic-wave configuration
+# (examples/wrapped/config/baroclinic.yml in the reference)
+DSW_CONFIG = dict(
+    dddmp=0.5, d2_bg=0.0, d2_bg_k1=0.2, d2_bg_k2=0.1, d4_bg=0.15, ke_bg=0.0, nord=3, n_sponge=48,
+    grid_type=0, d_ext=0.0, hord_dp=6, hord_tm=6, hord_mt=6, hord_vt=6, do_f3d=False, do_skeb=False,
+    d_con=1.0, vtdm4=0.06, inline_q=False, convert_ke=False, do_vort_damp=True, hydrostatic=False,
+)
+
+
+def d_sw_case(n=12, nz=8, seed=31):
+    st = base_state(n, nz, seed)
+    rng = np.random.default_rng(seed + 1000)
+    shp = st["delp"].shape
+    r = lambda scale: scale * rng.standard_normal(shp)
+    gz = heights(st, nz)
+    case = {
+        "dt": 37.5,
+        "delpc": st["delp"] * (1.0 + 1e-3 * rng.standard_normal(shp)),
+        "delp": st["delp"].copy(),
+        "ptc": st["pt"] * (1.0 + 1e-3 * rng.standard_normal(shp)),
+        "pt": st["pt"].copy(),
+        "u": st["u"].copy(),
+        "v": st["v"].copy(),
+        "w": r(0.2),
+        "uc": st["u"] * 0.9 + r(1.0),
+        "vc": st["v"] * 0.9 + r(1.0),
+        "ua": r(10.0),
+        "va": r(10.0),
+        "divgd": r(1e-5),
+        "mfx": r(1e3),
+        "mfy": r(1e3),
+        "cx": r(0.05),
+        "cy": r(0.05),
+        "crx": r(0.05),
+        "cry": r(0.05),
+        "xfx": r(1e3),
+        "yfx": r(1e3),
+        "q_con": st["q_con"].copy(),
+        "zh": gz,
+        "heat_source": r(1e-3),
+        "diss_est": r(1e-3),
+    }
+    return case
+
+
+CASES["d_sw"] = d_sw_case

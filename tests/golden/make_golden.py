@@ -72,7 +72,32 @@ def run_c_sw(case, n, nz):
     return out, {"region": "full storage"}
 
 
+DSW_ARGS = ["delpc", "delp", "ptc", "pt", "u", "v", "w", "uc", "vc", "ua", "va", "divgd", "mfx", "mfy",
+            "cx", "cy", "crx", "cry", "xfx", "yfx", "q_con", "zh", "heat_source", "diss_est"]
+
+
+def run_d_sw(case, n, nz):
+    from fv3core._config import DGridShallowWaterLagrangianDynamicsConfig
+    from fv3core.stencils import d_sw
+
+    grid = cases.grid_for(n)
+    cfg = DGridShallowWaterLagrangianDynamicsConfig(**cases.DSW_CONFIG)
+    out = {k: np.zeros_like(case["delp"]) for k in DSW_ARGS}
+    for t in range(6):
+        tr = rr.TileReference(grid, t, nz)
+        col = d_sw.get_column_namelist(cfg, nz)
+        dsw = d_sw.DGridShallowWaterLagrangianDynamics(
+            tr.stencil_factory, tr.grid_data, tr.damping_coefficients, col, False, False, cfg
+        )
+        st = {k: rr.storage(case[k][t]) for k in DSW_ARGS}
+        dsw(*[st[k] for k in DSW_ARGS], case["dt"])
+        for k in DSW_ARGS:
+            out[k][t] = st[k]
+    return out, {"region": "full storage"}
+
+
 RUNNERS = {
+    "d_sw": (run_d_sw, dict(n=12, nz=8, seed=31)),
     "c_sw": (run_c_sw, dict(n=12, nz=6, seed=21)),
     "riem_solver_c": (run_riem_solver_c, dict(n=12, nz=16, seed=11)),
 }

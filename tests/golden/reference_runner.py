@@ -45,6 +45,11 @@ def storage(arr, origin=(3, 3, 0)):
     return st
 
 
+class _LegacyGrid:
+    """Stand-in for the reference's global ``spec.grid`` (hashable by identity,
+    as fv3core caches axis offsets per grid object)."""
+
+
 class TileReference:
     """Reference objects (grid data, stencil factory, legacy ``spec.grid``)
     for one tile of a ``CubedSphereGrid``."""
@@ -115,7 +120,7 @@ class TileReference:
             del6_u=ij("del6_u"), del6_v=ij("del6_v"), da_min=g.da_min, da_min_c=g.da_min_c
         )
         m = n + 2 * h + 1
-        legacy = types.SimpleNamespace()
+        legacy = _LegacyGrid()
         legacy.fC = ij("fC")
         legacy.f0 = ij("f0")
         legacy.npz = nz
@@ -146,6 +151,7 @@ class TileReference:
         self.legacy = legacy
         self.spec = spec
         self.grid_indexing = GridIndexing((n, n, nz), h, True, True, True, True)
+        legacy.axis_offsets = self.grid_indexing.axis_offsets
         self.stencil_factory = StencilFactory(StencilConfig("numpy", False, False), self.grid_indexing)
 
     def activate(self):

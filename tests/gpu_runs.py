@@ -1,0 +1,34 @@
+"""Run CUDA stages through the package's drop-in classes (shared by tests)."""
+import functools
+
+import numpy as np
+
+import cases
+
+
+@functools.lru_cache(maxsize=4)
+def device_grid(n, nz):
+    from fv3core_b200.grid_data import GridData
+    from fv3core_b200.stencil import StencilConfig, StencilFactory
+
+    gd = GridData(cases.grid_for(n), nz)
+    sf = StencilFactory(StencilConfig(), gd.grid_indexing)
+    return gd, sf
+
+
+def run_c_sw(case, n, nz, nord=3):
+    import torch
+
+    from fv3core_b200.stencils.c_sw import CGridShallowWaterDynamics
+    from fv3core_b200.storage import to_device, to_host
+
+    gd, sf = device_grid(n, nz)
+    csw = CGridShallowWaterDynamics(sf, gd, False, 0, nord)
+    names = ["delp", "pt", "u", "v", "w", "uc", "vc", "ua", "va", "ut", "vt", "divgd", "omga"]
+    dev = {k: to_device(case[k]) for k in names}
+    delpc, ptc = csw(*[dev[k] for k in names], case["dt2"])
+    torch.cuda.synchronize()
+    out = {k: to_host(dev[k]) for k in names}
+    out["delpc"] = to_host(delpc)
+    out["ptc"] = to_host(ptc)
+    return out

@@ -22,3 +22,26 @@ def max_rel_err(computed, ref, near_zero=1e-18):
     if np.any(np.isnan(err)):
         return float("inf")
     return float(err.max()) if err.size else 0.0
+
+
+def parity_err(computed, ref, near_zero_frac=1e-6):
+    """Relative error used for CUDA-vs-oracle parity: the translate-test
+    metric 2|a-b|/(|a|+|b|), except that points where the reference value is
+    smaller than ``near_zero_frac`` times the field's largest magnitude are
+    measured against that magnitude floor instead (values crossing zero carry
+    cancellation error of order the field's scale times machine epsilon,
+    which a pointwise relative measure would amplify without bound).
+    NaN must coincide with NaN."""
+    a = np.asarray(computed, dtype=np.float64)
+    b = np.asarray(ref, dtype=np.float64)
+    nan_a, nan_b = np.isnan(a), np.isnan(b)
+    if np.any(nan_a != nan_b):
+        return float("inf")
+    a = np.where(nan_a, 0.0, a)
+    b = np.where(nan_b, 0.0, b)
+    scale = float(np.max(np.abs(b))) if b.size else 0.0
+    if scale == 0.0:
+        return float(np.max(np.abs(a))) if a.size else 0.0
+    floor = near_zero_frac * scale
+    denom = np.maximum(0.5 * (np.abs(a) + np.abs(b)), floor)
+    return float(np.max(np.abs(a - b) / denom))

@@ -1,0 +1,54 @@
+"""Run oracle stages over all six tiles of a case (shared by tests)."""
+import numpy as np
+
+import cases
+from oracle._util import Tile
+
+
+def run_c_sw(case, n, nz):
+    from oracle.c_sw import c_sw
+
+    names = ["delp", "pt", "u", "v", "w", "uc", "vc", "ua", "va", "ut", "vt", "divgd", "omga"]
+    out = {k: np.array(case[k], copy=True) for k in names}
+    out["delpc"] = np.zeros_like(out["delp"])
+    out["ptc"] = np.zeros_like(out["delp"])
+    g = cases.grid_for(n)
+    for t in range(6):
+        ns = cases.metric_namespace(n, t)
+        arrs = {k: out[k][t] for k in names}
+        with np.errstate(all="ignore"):
+            delpc, ptc = c_sw(Tile(n, nz), ns, g.fC[t], *[arrs[k] for k in names], case["dt2"])
+        out["delpc"][t] = delpc
+        out["ptc"][t] = ptc
+    return out
+
+
+def run_riem_solver_c(case, n, nz):
+    from oracle.riem_solver_c import riem_solver_c
+
+    out = {k: (np.array(v, copy=True) if isinstance(v, np.ndarray) else v) for k, v in case.items()}
+    for t in range(6):
+        riem_solver_c(
+            out["dt2"], out["cappa"][t], out["ptop"], out["hs"][t], out["ws"][t], out["ptc"][t],
+            out["q_con"][t], out["delpc"][t], out["gz"][t], out["pef"][t], out["w3"][t], out["p_fac"], n, nz,
+        )
+    return out
+
+
+DSW_ARGS = ["delpc", "delp", "ptc", "pt", "u", "v", "w", "uc", "vc", "ua", "va", "divgd", "mfx", "mfy",
+            "cx", "cy", "crx", "cry", "xfx", "yfx", "q_con", "zh", "heat_source", "diss_est"]
+
+
+def run_d_sw(case, n, nz, states=None):
+    from oracle.d_sw import DSWState, d_sw
+
+    out = {k: np.array(case[k], copy=True) for k in DSW_ARGS}
+    g = cases.grid_for(n)
+    for t in range(6):
+        T = Tile(n, nz)
+        ns = cases.metric_namespace(n, t)
+        st = DSWState(T, ns, cases.DSW_CONFIG) if states is None else states[t]
+        arrs = {k: out[k][t] for k in DSW_ARGS}
+        with np.errstate(all="ignore"):
+            d_sw(T, ns, g.f0[t], st, cases.DSW_CONFIG, *[arrs[k] for k in DSW_ARGS], case["dt"])
+    return out
