@@ -35,7 +35,19 @@ SIGNATURES = {
 # entry points whose first argument is the context (fv3b_ctx*)
 CTX_SIGNATURES = {
     "fv3b_c_sw": [P, P, P, P, P, P, P, P, P, P, P, P, P, D, ctypes.c_int, P, P, P],
+    "fv3b_d_sw_setup": [P],
+    "fv3b_d_sw": [P] * 24 + [D, P],
 }
+
+
+class DswConfig(ctypes.Structure):
+    _fields_ = [(n, D) for n in ("dddmp", "d2_bg", "d2_bg_k1", "d2_bg_k2", "d4_bg", "ke_bg", "d_con", "vtdm4", "d_ext")] + [
+        (n, I32)
+        for n in (
+            "nord", "n_sponge", "grid_type", "hord_dp", "hord_tm", "hord_mt", "hord_vt",
+            "do_vort_damp", "hydrostatic", "do_f3d", "do_skeb", "inline_q", "convert_ke",
+        )
+    ]
 
 
 def lib():

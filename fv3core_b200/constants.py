@@ -17,3 +17,5 @@ CV_AIR = CP_AIR - RDGAS
 RDG = -RDGAS / GRAV
 CNST_0P20 = 0.2
 ZVIR = RVGAS / RDGAS - 1
+RGRAV = 1.0 / GRAV
+SDAY = 86400.0

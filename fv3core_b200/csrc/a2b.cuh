@@ -1,0 +1,178 @@
+// Fourth-order A-grid to B-grid interpolation (fv3core/stencils/a2b_ord4.py,
+// AGrid2BGridFourthOrder.__call__ 606-676) on levels [k0, k1), three passes:
+// corner/edge values, PPM volume means, interior interpolation.
+#pragma once
+#include "ctx.cuh"
+#include "stencil.cuh"
+
+namespace fv3b {
+
+namespace a2b {
+constexpr double C1 = 2.0 / 3.0, C2 = -1.0 / 6.0;
+constexpr double B1 = 7.0 / 12.0, B2 = -1.0 / 12.0;
+constexpr double A1 = 9.0 / 16.0, A2 = -1.0 / 16.0;
+
+// great_circle_dist / extrap_corner (a2b_ord4.py:38-57)
+__device__ __forceinline__ double gcd(double p1a, double p1b, double p2a, double p2b) {
+  double sb = sin((p1b - p2b) / 2.0);
+  double sa = sin((p1a - p2a) / 2.0);
+  double tb = sb * sb, ta = sa * sa;
+  return asin(sqrt(tb + cos(p1b) * cos(p2b) * ta)) * 2.0;
+}
+__device__ __forceinline__ double extrap(double p0a, double p0b, double p1a, double p1b, double p2a, double p2b,
+                                         double qa, double qb) {
+  double x1 = gcd(p1a, p1b, p0a, p0b);
+  double x2 = gcd(p2a, p2b, p0a, p0b);
+  return qa + x1 / (x2 - x1) * (qa - qb);
+}
+
+// ppm_volume_mean edge formulas (a2b_ord4.py:340-451) along one axis; L(o)
+// reads qin at offset o, G(o) the A-grid spacing.
+template <typename L, typename Gs>
+__device__ __forceinline__ double vm_edge1(const L& q, const Gs& g) {
+  double g_in = g(1) / g(0), g_ou = g(-2) / g(-1);
+  return 0.5 * (((2.0 + g_in) * q(0) - q(1)) / (1.0 + g_in) + ((2.0 + g_ou) * q(-1) - q(-2)) / (1.0 + g_ou));
+}
+template <typename L, typename Gs>
+__device__ __forceinline__ double vm_edge2(const L& q, const Gs& g) {
+  double g_in = g(0) / g(-1), g_ou = g(-3) / g(-2);
+  double left = 0.5 * (((2.0 + g_in) * q(-1) - q(0)) / (1.0 + g_in) + ((2.0 + g_ou) * q(-2) - q(-3)) / (1.0 + g_ou));
+  double right = B2 * (q(-1) + q(2)) + B1 * (q(0) + q(1));
+  return (3.0 * (g_in * q(-1) + q(0)) - (g_in * left + right)) / (2.0 + 2.0 * g_in);
+}
+template <typename L, typename Gs>
+__device__ __forceinline__ double vm_edge3(const L& q, const Gs& g) {
+  double g_in = g(-2) / g(-1), g_ou = g(1) / g(0);
+  return 0.5 * (((2.0 + g_in) * q(-1) - q(-2)) / (1.0 + g_in) + ((2.0 + g_ou) * q(0) - q(1)) / (1.0 + g_ou));
+}
+template <typename L, typename Gs>
+__device__ __forceinline__ double vm_edge4(const L& q, const Gs& g) {
+  double g_in = g(-1) / g(0), g_ou = g(2) / g(1);
+  double right = 0.5 * (((2.0 + g_in) * q(0) - q(-1)) / (1.0 + g_in) + ((2.0 + g_ou) * q(1) - q(2)) / (1.0 + g_ou));
+  double left = B2 * (q(-3) + q(0)) + B1 * (q(-2) + q(-1));
+  return (3.0 * (q(-1) + g_in * q(0)) - (g_in * right + left)) / (2.0 + 2.0 * g_in);
+}
+template <typename L, typename Gs>
+__device__ __forceinline__ double volume_mean(const L& q, const Gs& g, int pos, int s, int e) {
+  // statement order of ppm_volume_mean_x: general, s, s+1, e+1, e
+  if (pos == e) return vm_edge4(q, g);
+  if (pos == e + 1) return vm_edge3(q, g);
+  if (pos == s + 1) return vm_edge2(q, g);
+  if (pos == s) return vm_edge1(q, g);
+  return B2 * (q(-2) + q(1)) + B1 * (q(-1) + q(0));
+}
+}  // namespace a2b
+
+template <int AXIS>
+struct A2BLine {
+  const double* p;
+  long long base, step;
+  __device__ __forceinline__ double operator()(int o) const { return p[base + o * step]; }
+};
+
+inline cudaError_t a2b_ord4(const Dims d, const fv3b_metrics g, double* qin, double* qout, double* qx, double* qy,
+                            double* edges, int k0, int k1, cudaStream_t st, bool replace = false) {
+  using namespace a2b;
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, h = d.h, n = d.n;
+  cudaError_t err;
+  if (k1 <= k0) return cudaSuccess;
+  // corners (a2b_ord4.py:60-235, 616-654) and edges (313-336, 678-695)
+  err = launch_box(Box{s, e + 2, js, je + 2, k0, k1}, st, [=] __device__(int t, int i, int j, int k) {
+    PT_SETUP(d, t, k);
+    bool wcol = i == s, ecol = i == e + 1, srow = j == js, nrow = j == je + 1;
+    if (!(wcol || ecol || srow || nrow)) return;
+    double v;
+    if ((wcol || ecol) && (srow || nrow)) {
+      // offsets (near, far) of the three extrapolations; the reference's
+      // _nw/_se stencils run at the (ie+1, js) / (is, je+1) corners
+      int o[3][4];
+      if (wcol && srow) {
+        int oo[3][4] = {{0, 0, 1, 1}, {-1, 0, -2, 1}, {0, -1, 1, -2}};
+        memcpy(o, oo, sizeof(o));
+      } else if (ecol && srow) {
+        int oo[3][4] = {{-1, 0, -2, 1}, {-1, -1, -2, -2}, {0, 0, 1, 1}};
+        memcpy(o, oo, sizeof(o));
+      } else if (ecol && nrow) {
+        int oo[3][4] = {{-1, -1, -2, -2}, {0, -1, 1, -2}, {-1, 0, -2, 1}};
+        memcpy(o, oo, sizeof(o));
+      } else {
+        int oo[3][4] = {{0, -1, 1, -2}, {-1, -1, -2, -2}, {0, 0, 1, 1}};
+        memcpy(o, oo, sizeof(o));
+      }
+      double b1 = F2(g.bgrid1, i, j), b2 = F2(g.bgrid2, i, j);
+      double ec[3];
+      for (int m = 0; m < 3; ++m) {
+        int i1 = i + o[m][0], j1 = j + o[m][1], i2 = i + o[m][2], j2 = j + o[m][3];
+        ec[m] = extrap(b1, b2, F2(g.agrid1, i1, j1), F2(g.agrid2, i1, j1), F2(g.agrid1, i2, j2),
+                       F2(g.agrid2, i2, j2), F3(qin, i1, j1), F3(qin, i2, j2));
+      }
+      v = (ec[0] + ec[1] + ec[2]) * (1.0 / 3.0);
+    } else if (wcol || ecol) {
+      const double* ef = wcol ? g.edge_w : g.edge_e;
+      double wgt = ef[t * (n + 1) + (j - h)];
+      auto q2 = [&](int jj) {
+        return (F3(qin, i - 1, jj) * F2(g.dxa, i, jj) + F3(qin, i, jj) * F2(g.dxa, i - 1, jj)) /
+               (F2(g.dxa, i - 1, jj) + F2(g.dxa, i, jj));
+      };
+      v = wgt * q2(j - 1) + (1.0 - wgt) * q2(j);
+    } else {
+      const double* ef = srow ? g.edge_s : g.edge_n;
+      double wgt = ef[t * (n + 1) + (i - h)];
+      auto q1 = [&](int ii) {
+        return (F3(qin, ii, j - 1) * F2(g.dya, ii, j) + F3(qin, ii, j) * F2(g.dya, ii, j - 1)) /
+               (F2(g.dya, ii, j - 1) + F2(g.dya, ii, j));
+      };
+      v = wgt * q1(i - 1) + (1.0 - wgt) * q1(i);
+    }
+    W3(qout, i, j) = v;
+    W3(edges, i, j) = v;
+  });
+  if (err != cudaSuccess) return err;
+  // ppm_volume_mean_x on [is, ie+1] x [js-2, je+2], _y on [is-2, ie+2] x [js, je+1]
+  err = launch_box(Box{s - 2, e + 3, js - 2, je + 3, k0, k1}, st, [=] __device__(int t, int i, int j, int k) {
+    PT_SETUP(d, t, k);
+    long long b = idx3(d, t, i, j, k);
+    long long b2 = idx2(d, t, i, j);
+    if (i >= s && i < e + 2) {
+      A2BLine<0> q{qin, b, 1};
+      A2BLine<0> gx{g.dxa, b2, 1};
+      W3(qx, i, j) = volume_mean(q, gx, i, s, e);
+    }
+    if (j >= js && j < je + 2) {
+      A2BLine<1> q{qin, b, d.sj};
+      A2BLine<1> gy{g.dya, b2, (long long)d.ni};
+      W3(qy, i, j) = volume_mean(q, gy, j, js, je);
+    }
+  });
+  if (err != cudaSuccess) return err;
+  // a2b_interpolation (a2b_ord4.py:286-310) on interior cell corners
+  err = launch_box(Box{s + 1, e + 1, js + 1, je + 1, k0, k1}, st, [=] __device__(int t, int i, int j, int k) {
+    PT_SETUP(d, t, k);
+    double qxx = A2 * (F3(qx, i, j - 2) + F3(qx, i, j + 1)) + A1 * (F3(qx, i, j - 1) + F3(qx, i, j));
+    double qyy = A2 * (F3(qy, i - 2, j) + F3(qy, i + 1, j)) + A1 * (F3(qy, i - 1, j) + F3(qy, i, j));
+    if (j == js + 1) {
+      double up = A2 * (F3(qx, i, j - 1) + F3(qx, i, j + 2)) + A1 * (F3(qx, i, j) + F3(qx, i, j + 1));
+      qxx = C1 * (F3(qx, i, j - 1) + F3(qx, i, j)) + C2 * (F3(edges, i, j - 1) + up);
+    }
+    if (j == je) {
+      double lo = A2 * (F3(qx, i, j - 3) + F3(qx, i, j)) + A1 * (F3(qx, i, j - 2) + F3(qx, i, j - 1));
+      qxx = C1 * (F3(qx, i, j - 1) + F3(qx, i, j)) + C2 * (F3(edges, i, j + 1) + lo);
+    }
+    if (i == s + 1) {
+      double right = A2 * (F3(qy, i - 1, j) + F3(qy, i + 2, j)) + A1 * (F3(qy, i, j) + F3(qy, i + 1, j));
+      qyy = C1 * (F3(qy, i - 1, j) + F3(qy, i, j)) + C2 * (F3(edges, i - 1, j) + right);
+    }
+    if (i == e) {
+      double left = A2 * (F3(qy, i - 3, j) + F3(qy, i, j)) + A1 * (F3(qy, i - 2, j) + F3(qy, i - 1, j));
+      qyy = C1 * (F3(qy, i - 1, j) + F3(qy, i, j)) + C2 * (F3(edges, i + 1, j) + left);
+    }
+    W3(qout, i, j) = 0.5 * (qxx + qyy);
+  });
+  if (err != cudaSuccess || !replace) return err;
+  return launch_box(Box{s, e + 2, js, je + 2, k0, k1}, st, [=] __device__(int t, int i, int j, int k) {
+    PT_SETUP(d, t, k);
+    W3(qin, i, j) = F3(qout, i, j);
+  });
+}
+
+}  // namespace fv3b

@@ -13,42 +13,9 @@
 #include <stdint.h>
 
 #include "../../include/fv3core_b200.h"
+#include "dims.h"
 
 namespace fv3b {
-
-struct Dims {
-  int n, h, nz;
-  int ni, nj, nk;
-  long long sj, sk, st;  // 3-D strides (i stride is 1)
-  long long st2;         // 2-D tile stride (j stride is ni)
-  int isc, iec, jsc, jec;  // compute domain (inclusive), storage indices
-};
-
-inline Dims make_dims(const fv3b_grid_dims* g) {
-  Dims d;
-  d.n = g->npx;
-  d.h = g->n_halo;
-  d.nz = g->npz;
-  d.ni = d.n + 2 * d.h + 1;
-  d.nj = d.ni;
-  d.nk = d.nz + 1;
-  d.sj = d.ni;
-  d.sk = (long long)d.ni * d.nj;
-  d.st = d.sk * d.nk;
-  d.st2 = (long long)d.ni * d.nj;
-  d.isc = d.h;
-  d.iec = d.h + d.n - 1;
-  d.jsc = d.h;
-  d.jec = d.h + d.n - 1;
-  return d;
-}
-
-__host__ __device__ __forceinline__ long long idx3(const Dims& d, int t, int i, int j, int k) {
-  return t * d.st + k * d.sk + j * d.sj + i;
-}
-__host__ __device__ __forceinline__ long long idx2(const Dims& d, int t, int i, int j) {
-  return t * d.st2 + (long long)j * d.ni + i;
-}
 
 // Box of storage indices [i0, i1) x [j0, j1) x [k0, k1), all six tiles.
 struct Box {

@@ -21,6 +21,13 @@ extern "C" int fv3b_ctx_create(const fv3b_grid_dims* dims, const fv3b_metrics* m
     return FV3B_ERR_CUDA;
   }
   for (int i = 0; i < NWS; ++i) c->ws[i] = c->ws_base + n3 * i;
+  e = cudaMalloc((void**)&c->col, sizeof(double) * NCOL * MAXLEV);
+  if (e != cudaSuccess) {
+    cudaFree(c->ws_base);
+    delete c;
+    set_last_error("fv3b_ctx_create", e);
+    return FV3B_ERR_CUDA;
+  }
   e = cudaMemset(c->ws_base, 0, n3 * sizeof(double) * NWS);
   if (e != cudaSuccess) {
     cudaFree(c->ws_base);
@@ -35,7 +42,9 @@ extern "C" int fv3b_ctx_create(const fv3b_grid_dims* dims, const fv3b_metrics* m
 extern "C" int fv3b_ctx_destroy(fv3b_ctx* ctx) {
   if (!ctx) return FV3B_OK;
   cudaError_t e = cudaFree(ctx->ws_base);
+  cudaError_t e2 = cudaFree(ctx->col);
   delete ctx;
+  if (e == cudaSuccess) e = e2;
   FV3B_CHECK(e);
   return FV3B_OK;
 }

@@ -1,0 +1,276 @@
+// Piecewise-parabolic fluxes, the 2-D finite-volume transport and del-n
+// flux damping, shared by the D-grid stages.
+//
+// References: fv3core/stencils/xppm.py, yppm.py, ppm.py (PPM flux),
+// xtp_u.py / ytp_v.py (wind self-advection), fvtp2d.py (Lin-Rood 2-D
+// transport), delnflux.py (del-n damping).  The y-direction code is the
+// x-direction code with the roles of i and j exchanged (an AXIS template
+// parameter); the statement order of the reference is kept so that FP64
+// results agree to rounding.
+#pragma once
+#include "corners.cuh"
+#include "ctx.cuh"
+#include "stencil.cuh"
+
+namespace fv3b {
+
+// ppm.py:8-20
+constexpr double PPM_C1 = -2.0 / 14.0, PPM_C2 = 11.0 / 14.0, PPM_C3 = 5.0 / 14.0;
+constexpr double PPM_P1 = 7.0 / 12.0, PPM_P2 = -1.0 / 12.0;
+
+// Accessor of a 3-D field along one axis through point (i, j) of level k:
+// at(o) = f[i + o, j] (AXIS 0) or f[i, j + o] (AXIS 1).
+template <int AXIS>
+struct Line3 {
+  const double* p;
+  long long base;  // index of (i, j, k)
+  long long step;  // 1 or sj
+  __device__ __forceinline__ double operator()(int o) const { return p[base + o * step]; }
+};
+
+template <int AXIS>
+struct Line2 {
+  const double* p;
+  long long base;
+  long long step;
+  __device__ __forceinline__ double operator()(int o) const { return p[base + o * step]; }
+};
+
+template <int AXIS>
+__device__ __forceinline__ Line3<AXIS> line3(const Dims& d, const double* p, int t, int i, int j, int k) {
+  return Line3<AXIS>{p, idx3(d, t, i, j, k), AXIS == 0 ? 1LL : d.sj};
+}
+template <int AXIS>
+__device__ __forceinline__ Line2<AXIS> line2(const Dims& d, const double* p, int t, int i, int j) {
+  return Line2<AXIS>{p, idx2(d, t, i, j), AXIS == 0 ? 1LL : (long long)d.ni};
+}
+
+// compute_al (xppm.py:148-181) for the cell at offset o of the line; pos is
+// the absolute index (along AXIS) of offset 0, s/e the compute bounds.
+template <typename Q, typename A>
+__device__ __forceinline__ double ppm_al(const Q& q, const A& dxa, int o, int pos, int s, int e) {
+  int ii = pos + o;
+  if (ii == s + 1 || ii == e + 2) return PPM_C3 * q(o - 1) + PPM_C2 * q(o) + PPM_C1 * q(o + 1);
+  if (ii == s || ii == e + 1)
+    return 0.5 * (((2.0 * dxa(o - 1) + dxa(o - 2)) * q(o - 1) - dxa(o - 1) * q(o - 2)) / (dxa(o - 2) + dxa(o - 1)) +
+                  ((2.0 * dxa(o) + dxa(o + 1)) * q(o) - dxa(o) * q(o + 1)) / (dxa(o) + dxa(o + 1)));
+  if (ii == s - 1 || ii == e) return PPM_C1 * q(o - 2) + PPM_C2 * q(o - 1) + PPM_C3 * q(o);
+  return PPM_P1 * (q(o - 1) + q(o)) + PPM_P2 * (q(o - 2) + q(o + 1));
+}
+
+__device__ __forceinline__ bool ppm_smooth(double bl, double b0, double br, int mord) {
+  if (mord == 5) return bl * br < 0;
+  return (3.0 * fabs(b0)) < fabs(bl - br);
+}
+
+// Mean of q advected through the interface at offset 0 (between cells -1
+// and 0) for Courant number c: get_flux (xppm.py:65-72) with fx1_fn,
+// get_advection_mask and apply_flux (xppm.py:19-61).
+template <typename Q, typename A>
+__device__ __forceinline__ double ppm_flux(const Q& q, const A& dxa, double c, int pos, int s, int e, int mord) {
+  double alm = ppm_al(q, dxa, -1, pos, s, e);
+  double al0 = ppm_al(q, dxa, 0, pos, s, e);
+  double alp = ppm_al(q, dxa, 1, pos, s, e);
+  double qm = q(-1), q0 = q(0);
+  double blm = alm - qm, brm = al0 - qm, b0m = blm + brm;
+  double bl0 = al0 - q0, br0 = alp - q0, b00 = bl0 + br0;
+  double mask = (ppm_smooth(blm, b0m, brm, mord) || ppm_smooth(bl0, b00, br0, mord)) ? 1.0 : 0.0;
+  double fx1 = c > 0.0 ? (1.0 - c) * (brm - c * b0m) : (1.0 + c) * (bl0 + c * b00);
+  return c > 0.0 ? qm + fx1 * mask : q0 + fx1 * mask;
+}
+
+// Scratch and options of one FiniteVolumeTransport call.
+struct FvTp2dArgs {
+  const double* q_base;   // field (x-corner-copied in place)
+  const double* q_y;      // y-corner-copied copy
+  const double* crx;
+  const double* cry;
+  const double* xfx;
+  const double* yfx;
+  const double* x_unit;   // x_mass_flux or xfx
+  const double* y_unit;
+  double* fx;
+  double* fy;
+  int hord;
+  double* fx_mean;
+  double* fy_mean;
+  double* q_adv_x;
+  double* q_adv_y;
+};
+
+// FiniteVolumeTransport.__call__ (fvtp2d.py:249-362) without the damping
+// step; three passes: inner PPM, q_i/q_j, outer PPM + final fluxes.
+inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a, cudaStream_t st) {
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nk = d.nk;
+  const int full = d.ni - 1;
+  const int ord_in = a.hord == 10 ? 8 : a.hord;
+  const int mord_in = ord_in < 0 ? -ord_in : ord_in;
+  const int mord_out = a.hord < 0 ? -a.hord : a.hord;
+  cudaError_t err;
+  // inner PPM: fy_mean on [is-3, ie+4] x [js, je+1], fx_mean on [is, ie+1] x [js-3, je+4]
+  err = launch_box(Box{s - 3, e + 5, js - 3, je + 5, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
+    if (i >= s - 3 && i < e + 5 && j >= js && j < je + 2) {
+      auto q = line3<1>(d, a.q_y, t, i, j, k);
+      auto dya = line2<1>(d, g.dya, t, i, j);
+      a.fy_mean[idx3(d, t, i, j, k)] = ppm_flux(q, dya, a.cry[idx3(d, t, i, j, k)], j, js, je, mord_in);
+    }
+    if (i >= s && i < e + 2 && j >= js - 3 && j < je + 5) {
+      auto q = line3<0>(d, a.q_base, t, i, j, k);
+      auto dxa = line2<0>(d, g.dxa, t, i, j);
+      a.fx_mean[idx3(d, t, i, j, k)] = ppm_flux(q, dxa, a.crx[idx3(d, t, i, j, k)], i, s, e, mord_in);
+    }
+  });
+  if (err != cudaSuccess) return err;
+  // q_i (fvtp2d.py:33-47) on [0, n+6) x [js, je+4), q_j (50-60) on [is, ie+4) x [0, n+6)
+  err = launch_box(Box{0, full, 0, full, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
+    PT_SETUP(d, t, k);
+    double area = F2(g.area, i, j);
+    if (j >= js && j < je + 4) {
+      double fyy0 = F3(a.yfx, i, j) * F3(a.fy_mean, i, j);
+      double fyy1 = F3(a.yfx, i, j + 1) * F3(a.fy_mean, i, j + 1);
+      W3(a.q_adv_y, i, j) =
+          (F3(a.q_y, i, j) * area + fyy0 - fyy1) / (area + F3(a.yfx, i, j) - F3(a.yfx, i, j + 1));
+    }
+    if (i >= s && i < e + 4) {
+      double fx10 = F3(a.xfx, i, j) * F3(a.fx_mean, i, j);
+      double fx11 = F3(a.xfx, i + 1, j) * F3(a.fx_mean, i + 1, j);
+      double awx = area + F3(a.xfx, i, j) - F3(a.xfx, i + 1, j);
+      W3(a.q_adv_x, i, j) = (F3(a.q_base, i, j) * area + fx10 - fx11) / awx;
+    }
+  });
+  if (err != cudaSuccess) return err;
+  // outer PPM and final_fluxes (fvtp2d.py:63-93) on [is, ie+1] x [js, je+1]
+  return launch_box(Box{s, e + 2, js, je + 2, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
+    long long o = idx3(d, t, i, j, k);
+    if (j <= je) {
+      auto q = line3<0>(d, a.q_adv_y, t, i, j, k);
+      auto dxa = line2<0>(d, g.dxa, t, i, j);
+      double xo = ppm_flux(q, dxa, a.crx[o], i, s, e, mord_out);
+      a.fx[o] = 0.5 * (xo + a.fx_mean[o]) * a.x_unit[o];
+    }
+    if (i <= e) {
+      auto q = line3<1>(d, a.q_adv_x, t, i, j, k);
+      auto dya = line2<1>(d, g.dya, t, i, j);
+      double yo = ppm_flux(q, dya, a.cry[o], j, js, je, mord_out);
+      a.fy[o] = 0.5 * (yo + a.fy_mean[o]) * a.y_unit[o];
+    }
+  });
+}
+
+// Per-level damping column on the device: nord band value and damp.
+struct DelnCol {
+  const double* nord;  // [nk] per-level nord (band value, see nord_at)
+  const double* damp;  // [nk]
+};
+
+// nord of level k: the reference folds the column into bands k = 0, 1, 2, 3+
+// (delnflux.py intervals with externals nord0..nord3).
+__device__ __forceinline__ int nord_at(const double* nord, int k) { return (int)nord[k < 3 ? k : 3]; }
+
+// DelnFluxNoSG.__call__ (delnflux.py:1156-1207): del-n diffusive fluxes of q
+// into fx2/fy2 using d2 as scratch.  Corner copies of d2 are applied on read
+// (a point of a corner block reads its copy source), which gives the values
+// the reference reads after copying the corners in place.
+inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const double* q, double* fx2, double* fy2,
+                                 DelnCol col, double* d2, bool mass_weighted, int nmax, cudaStream_t st) {
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = d.nz;
+  cudaError_t err;
+  // d2_damp_interval / copy_stencil_interval
+  err = launch_box(Box{s - 1 - nmax, e + 2 + nmax, js - 1 - nmax, je + 2 + nmax, 0, nz}, st,
+                   [=] __device__(int t, int i, int j, int k) {
+                     PT_SETUP(d, t, k);
+                     int nk_ = nord_at(col.nord, k);
+                     bool in0 = i >= s - 1 && i < e + 2 && j >= js - 1 && j < je + 2;
+                     if (nk_ > 0 || in0) W3(d2, i, j) = mass_weighted ? F3(q, i, j) : col.damp[k] * F3(q, i, j);
+                   });
+  if (err != cudaSuccess) return err;
+  auto flux_pass = [&](int nt, bool first) {
+    // first pass: fx_calc_stencil_nord / fy_calc_stencil_nord (all levels);
+    // later passes: fx/fy_calc_stencil_column (levels with nord > 0)
+    int lo = first ? nmax : nt;
+    return launch_box(Box{s - lo, e + 2 + lo, js - lo, je + 2 + lo, 0, nz}, st,
+                      [=] __device__(int t, int i, int j, int k) {
+                        PT_SETUP(d, t, k);
+                        int nk_ = nord_at(col.nord, k);
+                        if (!first && nk_ == 0) return;
+                        bool corners = nk_ > 0;
+                        auto d2x = [&](int ii, int jj) {
+                          int si, sj;
+                          if (corners && copy_corner_x(d, ii, jj, si, sj)) return F3(d2, si, sj);
+                          return F3(d2, ii, jj);
+                        };
+                        auto d2y = [&](int ii, int jj) {
+                          int si, sj;
+                          if (corners && copy_corner_y(d, ii, jj, si, sj)) return F3(d2, si, sj);
+                          return F3(d2, ii, jj);
+                        };
+                        bool fx_in, fy_in;
+                        if (nk_ > 0) {
+                          fx_in = i >= s - lo && i < e + 2 + lo && j >= js - lo && j < je + 1 + lo;
+                          fy_in = i >= s - lo && i < e + 1 + lo && j >= js - lo && j < je + 2 + lo;
+                        } else {
+                          fx_in = i >= s && i < e + 2 && j >= js && j < je + 1;
+                          fy_in = i >= s && i < e + 1 && j >= js && j < je + 2;
+                        }
+                        if (fx_in) {
+                          double v = F2(g.del6_v, i, j) * (d2x(i - 1, j) - d2x(i, j));
+                          W3(fx2, i, j) = first ? v : -v;
+                        }
+                        if (fy_in) {
+                          double v = F2(g.del6_u, i, j) * (d2y(i, j - 1) - d2y(i, j));
+                          W3(fy2, i, j) = first ? v : -v;
+                        }
+                      });
+  };
+  err = flux_pass(nmax, true);
+  if (err != cudaSuccess) return err;
+  for (int n = 0; n < nmax; ++n) {
+    int nt = nmax - 1 - n;
+    // d2_highorder_stencil (delnflux.py:159-181)
+    err = launch_box(Box{s - nt - 1, e + nt + 2, js - nt - 1, je + nt + 2, 0, nz}, st,
+                     [=] __device__(int t, int i, int j, int k) {
+                       PT_SETUP(d, t, k);
+                       if (nord_at(col.nord, k) == 0) return;
+                       W3(d2, i, j) = (F3(fx2, i, j) - F3(fx2, i + 1, j) + F3(fy2, i, j) - F3(fy2, i, j + 1)) *
+                                      F2(g.rarea, i, j);
+                     });
+    if (err != cudaSuccess) return err;
+    err = flux_pass(nt, false);
+    if (err != cudaSuccess) return err;
+  }
+  return cudaSuccess;
+}
+
+// DelnFlux.__call__ (delnflux.py:963-998): damped fluxes added to fx, fy on
+// the cell corners of the compute domain.
+inline cudaError_t delnflux(const Dims d, const fv3b_metrics g, const double* q, double* fx, double* fy, DelnCol col,
+                           const double* mass, double* fx2, double* fy2, double* d2, int nmax, cudaStream_t st) {
+  cudaError_t err = delnflux_nosg(d, g, q, fx2, fy2, col, d2, mass != nullptr, nmax, st);
+  if (err != cudaSuccess) return err;
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
+  return launch_box(Box{s, e + 2, js, je + 2, 0, d.nz}, st, [=] __device__(int t, int i, int j, int k) {
+    PT_SETUP(d, t, k);
+    if (mass == nullptr) {
+      W3(fx, i, j) = F3(fx, i, j) + F3(fx2, i, j);
+      W3(fy, i, j) = F3(fy, i, j) + F3(fy2, i, j);
+    } else {
+      double dk = col.damp[k];
+      W3(fx, i, j) = F3(fx, i, j) + 0.5 * dk * (F3(mass, i - 1, j) + F3(mass, i, j)) * F3(fx2, i, j);
+      W3(fy, i, j) = F3(fy, i, j) + 0.5 * dk * (F3(mass, i, j - 1) + F3(mass, i, j)) * F3(fy2, i, j);
+    }
+  });
+}
+
+// CopyCornersXY on dims (X, Y, Z_INTERFACE) (corners.py:64-117): q gets its
+// x-differenceable corners in place, qy becomes the y-differenceable copy.
+inline cudaError_t copy_corners_xy(const Dims d, double* q, double* qy, cudaStream_t st) {
+  const int full = d.ni - 1;
+  return launch_box(Box{0, full, 0, full, 0, d.nk}, st, [=] __device__(int t, int i, int j, int k) {
+    PT_SETUP(d, t, k);
+    int si, sj;
+    W3(qy, i, j) = copy_corner_y(d, i, j, si, sj) ? F3(q, si, sj) : F3(q, i, j);
+    if (copy_corner_x(d, i, j, si, sj)) W3(q, i, j) = F3(q, si, sj);
+  });
+}
+
+}  // namespace fv3b

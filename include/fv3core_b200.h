@@ -84,6 +84,39 @@ int fv3b_c_sw(fv3b_ctx* ctx, double* delp, double* pt, const double* u, const do
               double* uc, double* vc, double* ua, double* va, double* ut, double* vt, double* divgd,
               double* omga, double dt2, int nord, double* delpc, double* ptc, void* stream);
 
+/*
+ * D-grid shallow-water namelist (DGridShallowWaterLagrangianDynamicsConfig,
+ * fv3core/_config.py:137-160).  Flags are 0/1.
+ */
+typedef struct fv3b_dsw_config {
+  double dddmp, d2_bg, d2_bg_k1, d2_bg_k2, d4_bg, ke_bg, d_con, vtdm4, d_ext;
+  int32_t nord, n_sponge, grid_type;
+  int32_t hord_dp, hord_tm, hord_mt, hord_vt;
+  int32_t do_vort_damp, hydrostatic, do_f3d, do_skeb, inline_q, convert_ke;
+} fv3b_dsw_config;
+
+/*
+ * DGridShallowWaterLagrangianDynamics.__init__ (fv3core/stencils/d_sw.py:611-841):
+ * derives the per-level damping columns (get_column_namelist, d_sw.py:512-563)
+ * and damping coefficients and stores them in the context.  Rejects the
+ * options the reference rejects (grid_type >= 3, inline_q, d_ext > 0,
+ * damping columns <= 1e-5) with FV3B_ERR_UNSUPPORTED.
+ */
+int fv3b_d_sw_setup(fv3b_ctx* ctx, const fv3b_dsw_config* config);
+
+/*
+ * DGridShallowWaterLagrangianDynamics.__call__ (fv3core/stencils/d_sw.py:843-1131):
+ * FiniteVolumeFluxPrep, five FiniteVolumeTransport calls with del-n damping,
+ * kinetic-energy and vorticity terms, DivergenceDamping (with a2b_ord4) and
+ * the heat source.  Argument meaning as in the reference; all arrays are
+ * 3-D device fields.
+ */
+int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc, double* pt, double* u, double* v,
+              double* w, double* uc, double* vc, const double* ua, const double* va, double* divgd,
+              double* mfx, double* mfy, double* cx, double* cy, double* crx, double* cry, double* xfx,
+              double* yfx, double* q_con, const double* zh, double* heat_source, double* diss_est,
+              double dt, void* stream);
+
 /* Description of the last error raised on the calling host thread. */
 const char* fv3b_last_error(void);
 

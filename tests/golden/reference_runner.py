@@ -239,11 +239,12 @@ class ThreadComm:
                 sx = 0 if "x_interface" in q.dims else 1
                 sy = 0 if "y_interface" in q.dims else 1
                 nh = spec.n_points
+                nk = spec.extent[-1]
                 table = hm.scalar_table(n, h, sx, sy, nh)
                 rows = table[table[:, 0] == t]
                 for r in rows:
                     src = posts[r[3]][0][qi]
-                    q.data[r[1], r[2], :] = src[r[4], r[5], :]
+                    q.data[r[1], r[2], :nk] = src[r[4], r[5], :nk]
         else:
             qx_list, qy_list = quantity_lists
             for qi in range(len(qx_list)):
@@ -251,12 +252,13 @@ class ThreadComm:
                 stx = (0 if "x_interface" in qx.dims else 1, 0 if "y_interface" in qx.dims else 1)
                 sty = (0 if "x_interface" in qy.dims else 1, 0 if "y_interface" in qy.dims else 1)
                 nh = specs[0][qi].n_points
+                nk = specs[0][qi].extent[-1]
                 tables = hm.vector_tables(n, h, stx, sty, nh)
                 for dst, table in zip((qx, qy), tables):
                     rows = table[table[:, 0] == t]
                     for r in rows:
                         src = posts[r[3]][r[6]][qi]
-                        dst.data[r[1], r[2], :] = r[7] * src[r[4], r[5], :]
+                        dst.data[r[1], r[2], :nk] = r[7] * src[r[4], r[5], :nk]
 
     def synchronize_vector_interfaces(self, u_q, v_q):
         from fv3core_b200 import halo_map as hm
@@ -266,7 +268,8 @@ class ThreadComm:
         self.exchange.post(key, self.tile, [np.array(u_q.data, copy=True), np.array(v_q.data, copy=True)])
         posts = self.exchange.collect(key)
         table = hm.interface_sync_tables(self.n, self.h)
+        nk = u_q.extent[-1]
         for r in table[table[:, 0] == self.tile]:
             dst = (u_q, v_q)[r[1]]
             src = posts[r[4]][r[5]]
-            dst.data[r[2], r[3], :] = r[8] * src[r[6], r[7], :]
+            dst.data[r[2], r[3], :nk] = r[8] * src[r[6], r[7], :nk]

@@ -32,3 +32,22 @@ def run_c_sw(case, n, nz, nord=3):
     out["delpc"] = to_host(delpc)
     out["ptc"] = to_host(ptc)
     return out
+
+
+DSW_ARGS = ["delpc", "delp", "ptc", "pt", "u", "v", "w", "uc", "vc", "ua", "va", "divgd", "mfx", "mfy",
+            "cx", "cy", "crx", "cry", "xfx", "yfx", "q_con", "zh", "heat_source", "diss_est"]
+
+
+def run_d_sw(case, n, nz):
+    import torch
+
+    from fv3core_b200.config import baroclinic_dsw_config
+    from fv3core_b200.stencils.d_sw import DGridShallowWaterLagrangianDynamics
+    from fv3core_b200.storage import to_device, to_host
+
+    gd, sf = device_grid(n, nz)
+    dsw = DGridShallowWaterLagrangianDynamics(sf, gd, gd, None, False, False, baroclinic_dsw_config())
+    dev = {k: to_device(case[k]) for k in DSW_ARGS}
+    dsw(*[dev[k] for k in DSW_ARGS], case["dt"])
+    torch.cuda.synchronize()
+    return {k: to_host(dev[k]) for k in DSW_ARGS}
