@@ -284,9 +284,9 @@ class AcousticDynamics:
         dt = st["mdt"] / n_split
         dt2 = 0.5 * dt
         T = self.tmp
-        H.scalar(st["q_con"], st["cappa"])
-        H.scalar(st["delp"], st["pt"])
-        H.vector_d(st["u"], st["v"])
+        H.scalar(st["q_con"], st["cappa"], nk=nz)
+        H.scalar(st["delp"], st["pt"], nk=nz)
+        H.vector_d(st["u"], st["v"], nk=nz)
         # zero_data (dyn_core.py:47-63)
         full = t.m - 1
         for name in ("mfxd", "mfyd", "cxd", "cyd"):
@@ -295,14 +295,14 @@ class AcousticDynamics:
             st["diss_estd"][:, t.isc : t.iec + 1, t.jsc : t.jec + 1, :nz] = 0.0
         for it in range(n_split):
             remap_step = bool(cfg.get("breed_vortex_inline", False)) or it == n_split - 1
-            H.scalar(st["w"])
+            H.scalar(st["w"], nk=nz)
             if it == 0:
                 # set_gz (dyn_core.py:80-85) on the compute domain
                 I, J = slice(t.isc, t.iec + 1), slice(t.jsc, t.jec + 1)
                 T["gz"][:, I, J, nz] = self.zs[:, I, J]
                 for k in range(nz - 1, -1, -1):
                     T["gz"][:, I, J, k] = T["gz"][:, I, J, k + 1] - st["delz"][:, I, J, k]
-                H.scalar(T["gz"])
+                H.scalar(T["gz"], nk=nz + 1)
             delpc = np.zeros_like(st["delp"])
             ptc = np.zeros_like(st["delp"])
             for tt in range(6):
@@ -312,7 +312,7 @@ class AcousticDynamics:
                     T["divgd"][tt], st["omga"][tt], dt2, dcfg["nord"],
                 )
             if dcfg["nord"] > 0:
-                H.scalar_corner(T["divgd"])
+                H.scalar_corner(T["divgd"], nk=nz)
             full_b = (slice(None), slice(0, full), slice(0, full), slice(0, t.nk))
             if it == 0:
                 T["zh"][full_b] = T["gz"][full_b]
@@ -325,14 +325,14 @@ class AcousticDynamics:
                               st["q_con"][tt], delpc[tt], T["gz"][tt], T["pkc"][tt], st["omga"][tt], cfg["p_fac"],
                               t.n, nz)
                 p_grad_c(t, self.g[tt], st["uc"][tt], st["vc"][tt], delpc[tt], T["pkc"][tt], T["gz"][tt], dt2)
-            H.vector_c(st["uc"], st["vc"])
+            H.vector_c(st["uc"], st["vc"], nk=nz)
             for tt in range(6):
                 d_sw(t, self.g[tt], self.grid.f0[tt], self.dsw_states[tt], dcfg, T["vt"][tt], st["delp"][tt],
                      ptc[tt], st["pt"][tt], st["u"][tt], st["v"][tt], st["w"][tt], st["uc"][tt], st["vc"][tt],
                      st["ua"][tt], st["va"][tt], T["divgd"][tt], st["mfxd"][tt], st["mfyd"][tt], st["cxd"][tt],
                      st["cyd"][tt], T["crx"][tt], T["cry"][tt], T["xfx"][tt], T["yfx"][tt], st["q_con"][tt],
                      T["zh"][tt], T["heat_source"][tt], st["diss_estd"][tt], dt)
-            H.scalar(st["delp"], st["pt"], st["q_con"])
+            H.scalar(st["delp"], st["pt"], st["q_con"], nk=nz)
             for tt in range(6):
                 update_dz_d(t, self.g[tt], self.dzd_states[tt], dcfg["hord_tm"], self.zs[tt], T["zh"][tt],
                             T["crx"][tt], T["cry"][tt], T["xfx"][tt], T["yfx"][tt], st["wsd"][tt], dt)
@@ -340,8 +340,8 @@ class AcousticDynamics:
                              st["delz"][tt], st["q_con"][tt], st["delp"][tt], st["pt"][tt], T["zh"][tt],
                              st["pe"][tt], T["pkc"][tt], T["pk3"][tt], st["pk"][tt], st["peln"][tt], st["w"][tt],
                              cfg["p_fac"], t.n, nz)
-            H.scalar(T["zh"])
-            H.scalar(T["pkc"], n_halo=2)
+            H.scalar(T["zh"], nk=nz + 1)
+            H.scalar(T["pkc"], n_halo=2, nk=nz + 1)
             for tt in range(6):
                 if remap_step:
                     edge_pe(t, st["pe"][tt], st["delp"][tt], st["ptop"])
@@ -356,11 +356,11 @@ class AcousticDynamics:
                     ray_fast(t, st["u"][tt], st["v"][tt], st["w"][tt], self.dp_ref, self.pfull, dt, st["ptop"],
                              cfg["rf_cutoff"], cfg["tau"])
             if it != n_split - 1:
-                H.vector_d(st["u"], st["v"])
+                H.vector_d(st["u"], st["v"], nk=nz)
             else:
-                H.sync_vector_interfaces(st["u"], st["v"])
+                H.sync_vector_interfaces(st["u"], st["v"], nk=nz)
         if self.do_del2cubed:
-            H.scalar(T["heat_source"])
+            H.scalar(T["heat_source"], nk=nz)
             cd = C.CNST_0P20 * self.g[0].da_min
             for tt in range(6):
                 del2cubed(t, self.g[tt], T["heat_source"][tt], cd, min(3, dcfg["nord"] + 1), self.del2_scr[tt])

@@ -153,3 +153,36 @@ def d_sw_case(n=12, nz=8, seed=31):
 
 
 CASES["d_sw"] = d_sw_case
+
+
+# Acoustic substep loop (AcousticDynamics) of the baroclinic configuration:
+# acoustic namelist of examples/wrapped/config/baroclinic.yml in the reference,
+# with n_split reduced so the six-tile reference run stays short.
+ACOUSTIC_CONFIG = dict(
+    tau=10.0, k_split=1, n_split=2, m_split=0, delt_max=0.002, rf_cutoff=3000.0, rf_fast=True,
+    breed_vortex_inline=False, use_old_omega=True,
+)
+RIEMANN_CONFIG = dict(p_fac=0.05, a_imp=1.0, use_logp=False, beta=0.0)
+
+ACOUSTIC_STATE = ["u", "v", "w", "delz", "delp", "pt", "pe", "pk", "phis", "wsd", "omga", "ua", "va", "uc",
+                  "vc", "mfxd", "mfyd", "cxd", "cyd", "pkz", "peln", "q_con", "diss_estd", "cappa"]
+
+
+def acoustics_case(n=12, nz=8, seed=41, n_split=2):
+    st = base_state(n, nz, seed)
+    rng = np.random.default_rng(seed + 1000)
+    shp = st["delp"].shape
+    case = {name: np.array(st[name], copy=True) for name in ACOUSTIC_STATE if name in st}
+    case["w"] = 0.1 * rng.standard_normal(shp)
+    case["wsd"] = 0.01 * rng.standard_normal(shp[:3])
+    for name in ("omga", "ua", "va", "uc", "vc", "mfxd", "mfyd", "cxd", "cyd", "diss_estd"):
+        case[name] = np.zeros(shp)
+    case.update(
+        ak=np.asarray(st["ak"], dtype=np.float64), bk=np.asarray(st["bk"], dtype=np.float64),
+        pfull=np.asarray(st["pfull"], dtype=np.float64), ptop=st["ptop"], ks=st["ks"],
+        mdt=37.5 * n_split, n_map=1, akap=C.KAPPA, n_split=n_split,
+    )
+    return case
+
+
+CASES["acoustics"] = acoustics_case

@@ -96,7 +96,75 @@ def run_d_sw(case, n, nz):
     return out, {"region": "full storage"}
 
 
+ACOUSTIC_DIMS = {
+    "u": ("x", "y_interface", "z"), "v": ("x_interface", "y", "z"), "uc": ("x_interface", "y", "z"),
+    "vc": ("x", "y_interface", "z"), "w": ("x", "y", "z"), "delp": ("x", "y", "z"), "pt": ("x", "y", "z"),
+    "q_con": ("x", "y", "z"), "cappa": ("x", "y", "z"),
+}
+
+
+def run_acoustics(case, n, nz):
+    """Six AcousticDynamics instances (one per tile) stepping in lock step on
+    threads, their halo updates going through ``ThreadComm``."""
+    import threading
+    import types
+
+    from fv3core._config import (AcousticDynamicsConfig, DGridShallowWaterLagrangianDynamicsConfig,
+                                 RiemannConfig)
+    from fv3core.stencils.dyn_core import AcousticDynamics
+    from fv3core.utils.grid import quantity_wrap
+
+    grid = cases.grid_for(n)
+    cfg = AcousticDynamicsConfig(
+        **{**cases.ACOUSTIC_CONFIG, "n_split": int(case["n_split"])},
+        riemann=RiemannConfig(**cases.RIEMANN_CONFIG),
+        d_grid_shallow_water=DGridShallowWaterLagrangianDynamicsConfig(**cases.DSW_CONFIG),
+    )
+    exchange = rr._Exchange()
+    S = rr.storage
+    runs = []
+    for t in range(6):
+        tr = rr.TileReference(grid, t, nz)
+        tr.activate()
+        comm = rr.ThreadComm(t, n, 3, exchange)
+        ak, bk, pfull = (S(case[k], origin=(0,)) for k in ("ak", "bk", "pfull"))
+        phis = S(case["phis"][t], origin=(0, 0))
+        ad = AcousticDynamics(comm, tr.stencil_factory, tr.grid_data, tr.damping_coefficients, 0, False, False,
+                              cfg, ak, bk, pfull, phis)
+        state = types.SimpleNamespace()
+        for name in cases.ACOUSTIC_STATE:
+            arr = case[name][t]
+            setattr(state, name, S(arr, origin=(3, 3) if arr.ndim == 2 else (3, 3, 0)))
+        for name, dims in ACOUSTIC_DIMS.items():
+            setattr(state, name + "_quantity", quantity_wrap(getattr(state, name), dims, tr.grid_indexing))
+        state.ak, state.bk, state.pfull = ak, bk, pfull
+        for name in ("mdt", "n_map", "akap", "ptop", "ks"):
+            setattr(state, name, case[name])
+        runs.append((ad, state))
+    errors = []
+
+    def work(ad, state):
+        try:
+            ad(state)
+        except BaseException as exc:  # surfaced after join
+            errors.append(exc)
+            raise
+
+    threads = [threading.Thread(target=work, args=r) for r in runs]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    if errors:
+        raise errors[0]
+    out = {name: np.stack([np.asarray(getattr(st, name)) for _, st in runs]) for name in cases.ACOUSTIC_STATE}
+    for name in ("zh", "gz", "pkc", "pk3", "heat_source", "delpc", "ptc", "divgd"):
+        out["tmp_" + name] = np.stack([np.asarray(getattr(st, name)) for _, st in runs])
+    return out, {"region": "full storage"}
+
+
 RUNNERS = {
+    "acoustics": (run_acoustics, dict(n=12, nz=8, seed=41)),
     "d_sw": (run_d_sw, dict(n=12, nz=8, seed=31)),
     "c_sw": (run_c_sw, dict(n=12, nz=6, seed=21)),
     "riem_solver_c": (run_riem_solver_c, dict(n=12, nz=16, seed=11)),

@@ -191,7 +191,7 @@ class _HaloUpdater:
 
     def start(self, *quantity_lists):
         comm = self.comm
-        key = (id(self.specs[0]), self.kind, self.gen, comm.uid_of(self))
+        key = (self.kind, comm.uid_of(self), self.gen)
         self.gen += 1
         snap = [[np.array(q.data, copy=True) for q in ql] for ql in quantity_lists]
         comm.exchange.post(key, comm.tile, snap)

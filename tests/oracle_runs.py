@@ -52,3 +52,22 @@ def run_d_sw(case, n, nz, states=None):
         with np.errstate(all="ignore"):
             d_sw(T, ns, g.f0[t], st, cases.DSW_CONFIG, *[arrs[k] for k in DSW_ARGS], case["dt"])
     return out
+
+
+def run_acoustics(case, n, nz):
+    """The oracle's AcousticDynamics over all six tiles; returns the state
+    and the driver's temporaries (prefixed ``tmp_``)."""
+    from oracle.dyn_core import AcousticDynamics
+
+    g = cases.grid_for(n)
+    cfg = {**cases.ACOUSTIC_CONFIG, **cases.RIEMANN_CONFIG, "n_split": int(case["n_split"]),
+           "dsw": cases.DSW_CONFIG}
+    metrics = [cases.metric_namespace(n, t) for t in range(6)]
+    ad = AcousticDynamics(g, metrics, cfg, case["ak"], case["bk"], case["pfull"], case["phis"], nz)
+    st = {k: (np.array(v, copy=True) if isinstance(v, np.ndarray) else v) for k, v in case.items()}
+    with np.errstate(all="ignore"):
+        ad(st)
+    out = {k: st[k] for k in cases.ACOUSTIC_STATE}
+    for name, arr in ad.tmp.items():
+        out["tmp_" + name] = arr
+    return out
