@@ -30,6 +30,7 @@ class GridDims(ctypes.Structure):
 # name -> argument types after the leading dims pointer
 SIGNATURES = {
     "fv3b_riem_solver_c": [D, D, D, P, P, P, P, P, P, P, P, P, P],
+    "fv3b_riem_solver3": [ctypes.c_int, D, D, D] + [P] * 14 + [P],
 }
 
 # entry points whose first argument is the context (fv3b_ctx*)
@@ -37,6 +38,26 @@ CTX_SIGNATURES = {
     "fv3b_c_sw": [P, P, P, P, P, P, P, P, P, P, P, P, P, D, ctypes.c_int, P, P, P],
     "fv3b_d_sw_setup": [P],
     "fv3b_d_sw": [P] * 24 + [D, P],
+    "fv3b_update_dz_c": [P] * 6 + [D, P],
+    "fv3b_update_dz_d_setup": [P, ctypes.c_int],
+    "fv3b_update_dz_d": [P] * 7 + [D, P],
+    "fv3b_p_grad_c": [P] * 5 + [D, P],
+    "fv3b_nh_p_grad": [P] * 6 + [D, D, D, P],
+    "fv3b_edge_pe": [P, P, D, P],
+    "fv3b_pk3_halo": [P, P, D, D, P],
+    "fv3b_ray_fast": [P] * 5 + [D, D, D, D, ctypes.c_int, P],
+    "fv3b_del2cubed": [P, D, ctypes.c_int, P],
+    "fv3b_pkz_tempadjust": [P] * 6 + [D, ctypes.c_int, P],
+    "fv3b_halo_update_scalar": [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P],
+    "fv3b_halo_update_vector": [P, P, ctypes.c_int, ctypes.c_int, P],
+    "fv3b_synchronize_vector_interfaces": [P, P, ctypes.c_int, P],
+    "fv3b_acoustics_setup": [P] * 6,
+    "fv3b_acoustics": [P, P],
+}
+
+# entry points that return a pointer rather than a status
+PTR_SIGNATURES = {
+    "fv3b_acoustics_temporary": [ctypes.c_void_p, ctypes.c_char_p],
 }
 
 
@@ -48,6 +69,21 @@ class DswConfig(ctypes.Structure):
             "do_vort_damp", "hydrostatic", "do_f3d", "do_skeb", "inline_q", "convert_ke",
         )
     ]
+
+
+class AcousticConfig(ctypes.Structure):
+    _fields_ = [(n, D) for n in ("tau", "delt_max", "rf_cutoff", "p_fac")] + [
+        (n, I32) for n in ("k_split", "n_split", "rf_fast", "breed_vortex_inline", "use_old_omega", "reserved")
+    ]
+
+
+DYCORE_FIELDS = ("u", "v", "w", "delz", "delp", "pt", "pe", "pk", "phis", "wsd", "omga", "ua", "va", "uc", "vc",
+                 "mfxd", "mfyd", "cxd", "cyd", "pkz", "peln", "q_con", "diss_estd", "cappa")
+
+
+class DycoreState(ctypes.Structure):
+    _fields_ = [(n, P) for n in DYCORE_FIELDS] + [("mdt", D), ("akap", D), ("ptop", D), ("n_map", I32),
+                                                  ("ks", I32)]
 
 
 def lib():
@@ -71,6 +107,10 @@ def lib():
             fn = getattr(L, name)
             fn.argtypes = [ctypes.c_void_p] + args
             fn.restype = ctypes.c_int
+        for name, args in PTR_SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_void_p
         _lib = L
     return _lib
 
@@ -92,4 +132,4 @@ def call_ctx(name, ctx, *args):
 def exported_symbols():
     return ["fv3b_last_error", "fv3b_version", "fv3b_ctx_create", "fv3b_ctx_destroy"] + [
         k for k, v in SIGNATURES.items() if v is not None
-    ] + list(CTX_SIGNATURES)
+    ] + list(CTX_SIGNATURES) + list(PTR_SIGNATURES)

@@ -71,4 +71,54 @@ __device__ __forceinline__ bool bgrid_corner_y(const Dims& d, int i, int j, int&
   return false;
 }
 
+// fill_corners_{2,3}cells_mult_{x,y} (fv3core/utils/corners.py:128-303):
+// returns true and the source offset/multiplier if (i, j) is a filled corner
+// point of the given kind.
+struct CornerRule {
+  int di, dj;
+  double mult;
+};
+
+__device__ __forceinline__ bool corner_x(const Dims& d, int i, int j, bool three, double sw, double se, double nw,
+                                         double ne, CornerRule& r) {
+  int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
+  if (j == js - 1) {
+    if (i == s - 1) { r = {0, 1, sw}; return true; }
+    if (i == s - 2) { r = {1, 2, sw}; return true; }
+    if (i == e + 1) { r = {0, 1, se}; return true; }
+    if (i == e + 2) { r = {-1, 2, se}; return true; }
+    if (three && i == s - 3) { r = {2, 3, sw}; return true; }
+    if (three && i == e + 3) { r = {-2, 3, se}; return true; }
+  } else if (j == je + 1) {
+    if (i == s - 1) { r = {0, -1, nw}; return true; }
+    if (i == s - 2) { r = {1, -2, nw}; return true; }
+    if (i == e + 1) { r = {0, -1, ne}; return true; }
+    if (i == e + 2) { r = {-1, -2, ne}; return true; }
+    if (three && i == s - 3) { r = {2, -3, nw}; return true; }
+    if (three && i == e + 3) { r = {-2, -3, ne}; return true; }
+  }
+  return false;
+}
+
+__device__ __forceinline__ bool corner_y(const Dims& d, int i, int j, bool three, double sw, double se, double nw,
+                                         double ne, CornerRule& r) {
+  int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
+  if (i == s - 1) {
+    if (j == js - 1) { r = {1, 0, sw}; return true; }
+    if (j == js - 2) { r = {2, 1, sw}; return true; }
+    if (j == je + 1) { r = {1, 0, nw}; return true; }
+    if (j == je + 2) { r = {2, -1, nw}; return true; }
+    if (three && j == js - 3) { r = {3, 2, sw}; return true; }
+    if (three && j == je + 3) { r = {3, -2, nw}; return true; }
+  } else if (i == e + 1) {
+    if (j == js - 1) { r = {-1, 0, se}; return true; }
+    if (j == js - 2) { r = {-2, 1, se}; return true; }
+    if (j == je + 1) { r = {-1, 0, ne}; return true; }
+    if (j == je + 2) { r = {-2, -1, ne}; return true; }
+    if (three && j == js - 3) { r = {-3, 2, se}; return true; }
+    if (three && j == je + 3) { r = {-3, -2, ne}; return true; }
+  }
+  return false;
+}
+
 }  // namespace fv3b

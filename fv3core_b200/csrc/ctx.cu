@@ -41,6 +41,7 @@ extern "C" int fv3b_ctx_create(const fv3b_grid_dims* dims, const fv3b_metrics* m
 
 extern "C" int fv3b_ctx_destroy(fv3b_ctx* ctx) {
   if (!ctx) return FV3B_OK;
+  fv3b_acoustics_release(ctx);
   cudaError_t e = cudaFree(ctx->ws_base);
   cudaError_t e2 = cudaFree(ctx->col);
   delete ctx;

@@ -4,13 +4,17 @@
 
 namespace fv3b {
 constexpr int NWS = 40;   // 3-D scratch fields in the workspace
-constexpr int NCOL = 16;  // per-level column arrays
+constexpr int NCOL = 32;  // per-level column arrays
 constexpr int MAXLEV = 128;
 
 // indices of the per-level columns in ctx->col
 enum ColumnId {
   COL_NORD = 0, COL_NORD_V, COL_NORD_W, COL_NORD_T, COL_DAMP_VT, COL_DAMP_W, COL_DAMP_T, COL_D2_DIVG,
-  COL_D_CON, COL_KE_BG, COL_DAMP4_VT_C, COL_DAMP4_W_C, COL_DAMP4_VT, COL_DAMP4_T, COL_SPARE0, COL_SPARE1
+  COL_D_CON, COL_KE_BG, COL_DAMP4_VT_C, COL_DAMP4_W_C, COL_DAMP4_VT, COL_DAMP4_T, COL_SPARE0, COL_SPARE1,
+  // acoustic driver columns (AcousticDynamics.__init__): reference layer
+  // thickness, cubic-spline constants of UpdateHeightOnDGrid, Rayleigh
+  // damping factors
+  COL_DP_REF = 16, COL_SPLINE_GK, COL_SPLINE_BETA, COL_SPLINE_GAMMA, COL_RF, COL_RF_DM, COL_DP_RAY
 };
 
 // workspace slots (3-D scratch fields); a stage owns them only while it runs,
@@ -27,6 +31,16 @@ struct DswSetup {
   int nmax_v = 0, nmax_w = 0, nmax_t = 0;
   double dd8 = 0.0;
 };
+
+// RayleighDamping per-level factors, recomputed when their inputs change
+struct RayState {
+  bool ready = false;
+  double dt = 0, ptop = 0, rf_cutoff = 0, tau = 0;
+  double dp[MAXLEV], pfull[MAXLEV];
+  int k_rf = 0, k_nudge = 0;
+};
+
+struct AcousticState;  // dyn_core.cu
 }  // namespace fv3b
 
 struct fv3b_ctx {
@@ -36,4 +50,16 @@ struct fv3b_ctx {
   double* ws[fv3b::NWS];
   double* col = nullptr;  // [NCOL][MAXLEV] device columns
   fv3b::DswSetup dsw;
+  bool dzd_ready = false;
+  int dzd_hord_tm = 0;
+  fv3b::RayState ray;
+  fv3b::AcousticState* acoustic = nullptr;
 };
+
+namespace fv3b {
+// device pointer of per-level column `id`
+inline double* colp(fv3b_ctx* c, int id) { return c->col + (size_t)id * MAXLEV; }
+}  // namespace fv3b
+
+// frees the acoustic driver's temporaries (dyn_core.cu)
+void fv3b_acoustics_release(fv3b_ctx* ctx);

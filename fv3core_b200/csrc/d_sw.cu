@@ -22,8 +22,6 @@ namespace {
 
 constexpr double DCON_THRESHOLD = 1e-5;
 
-double* colp(fv3b_ctx* c, int id) { return c->col + (size_t)id * MAXLEV; }
-
 // ---------------------------------------------------------------- fxadv
 // FiniteVolumeFluxPrep.__call__ (fxadv.py:488-585)
 cudaError_t fxadv(const Dims d, const fv3b_metrics g, const double* uc, const double* vc, double* crx, double* cry,
@@ -406,7 +404,8 @@ extern "C" int fv3b_d_sw_setup(fv3b_ctx* ctx, const fv3b_dsw_config* cfg) {
     }
   }
   sp.dd8 = pow(ctx->m.da_min_c * cfg->d4_bg, sp.nonzero_nord + 1);
-  FV3B_CHECK(cudaMemcpy(ctx->col, cols.data(), sizeof(double) * cols.size(), cudaMemcpyHostToDevice));
+  // the D-grid columns only; the driver's columns (from COL_DP_REF on) are its own
+  FV3B_CHECK(cudaMemcpy(ctx->col, cols.data(), sizeof(double) * COL_DP_REF * MAXLEV, cudaMemcpyHostToDevice));
   sp.ready = true;
   return FV3B_OK;
 }
@@ -425,7 +424,7 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
   const DswSetup sp = ctx->dsw;
   const fv3b_dsw_config cfg = sp.cfg;
   cudaStream_t st = (cudaStream_t)stream;
-  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = d.nz, nk = d.nk;
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = d.nz;
   const int full = d.ni - 1;
   double** W = ctx->ws;
   double *tmp_fx = W[0], *tmp_fy = W[1], *tmp_gx = W[2], *tmp_gy = W[3], *tmp_fx2 = W[4], *tmp_fy2 = W[5];

@@ -1,0 +1,206 @@
+// Damping stages of the acoustic substep:
+//   RayleighDamping (fv3core/stencils/ray_fast.py), the fast Rayleigh
+//     friction on the top layers;
+//   HyperdiffusionDamping (fv3core/stencils/del2cubed.py), the del-2
+//     filter of the dissipation heat source;
+//   compute_pkz_tempadjust (fv3core/stencils/temperature_adjust.py), the
+//     temperature change from that heat.
+#include <math.h>
+
+#include <vector>
+
+#include "corners.cuh"
+#include "ctx.cuh"
+#include "stencil.cuh"
+
+using namespace fv3b;
+
+namespace {
+constexpr double PI = 3.1415926535897931;
+constexpr double SDAY = 86400.0;
+constexpr double GRAV = 9.80665;
+constexpr double RDGAS = 287.05;
+constexpr double CP_AIR = 1004.6;
+constexpr double CV_AIR = CP_AIR - RDGAS;
+constexpr double RDG = -RDGAS / GRAV;
+}  // namespace
+
+// RayleighDamping.__call__ (ray_fast.py:169-192) with ray_fast_wind_compute
+// (48-128).  dp and pfull are host arrays of npz layer values.  The
+// per-level factors depend only on (dt, ptop, dp, pfull) and are uploaded
+// when those change.  In each column the friction removed from the levels
+// with pfull < rf_cutoff is summed top down and given back, divided by the
+// accumulated layer mass, to the levels with pfull < rf_cutoff +
+// min(100, 10 ptop); pfull increases with k, so both level sets are
+// prefixes [0, k_rf) and [0, k_nudge).
+extern "C" int fv3b_ray_fast(fv3b_ctx* ctx, double* u, double* v, double* w, const double* dp, const double* pfull,
+                             double dt, double ptop, double rf_cutoff, double tau, int hydrostatic, void* stream) {
+  FV3B_REQUIRE(ctx && u && v && w && dp && pfull, "fv3b_ray_fast: null argument");
+  const Dims d = ctx->d;
+  const int nz = d.nz;
+  cudaStream_t st = (cudaStream_t)stream;
+  RayState& rs = ctx->ray;
+  bool same = rs.ready && rs.dt == dt && rs.ptop == ptop && rs.rf_cutoff == rf_cutoff && rs.tau == tau;
+  for (int k = 0; same && k < nz; ++k) same = rs.dp[k] == dp[k] && rs.pfull[k] == pfull[k];
+  if (!same) {
+    for (int k = 1; k < nz; ++k)
+      FV3B_REQUIRE(pfull[k] >= pfull[k - 1], "fv3b_ray_fast: pfull must increase with k");
+    const double nudge = rf_cutoff + (100.0 < 10.0 * ptop ? 100.0 : 10.0 * ptop);
+    const double tau0 = tau * SDAY;
+    std::vector<double> c((size_t)2 * MAXLEV, 0.0);
+    double *rf = c.data(), *dm = c.data() + MAXLEV;
+    int k_rf = 0, k_nudge = 0;
+    while (k_rf < nz && pfull[k_rf] < rf_cutoff) ++k_rf;
+    while (k_nudge < nz && pfull[k_nudge] < nudge) ++k_nudge;
+    if (k_rf == 0) k_nudge = 0;  // nothing removed, nothing given back
+    for (int k = 0; k < k_rf; ++k) {
+      double sn = sin(0.5 * PI * log(rf_cutoff / pfull[k]) / log(rf_cutoff / ptop));
+      double rfv = dt / tau0 * (sn * sn);
+      rf[k] = 1.0 / (1.0 + rfv);
+    }
+    // layer mass accumulated down to the last nudged level, then copied up
+    if (k_nudge > 0) {
+      dm[0] = dp[0];
+      for (int k = 1; k < k_nudge; ++k) dm[k] = dm[k - 1] + dp[k];
+      for (int k = k_nudge - 2; k >= 0; --k) dm[k] = dm[k + 1];
+    }
+    FV3B_CHECK(cudaMemcpy(colp(ctx, COL_RF), c.data(), sizeof(double) * c.size(), cudaMemcpyHostToDevice));
+    FV3B_CHECK(cudaMemcpy(colp(ctx, COL_DP_RAY), dp, sizeof(double) * nz, cudaMemcpyHostToDevice));
+    rs.ready = true;
+    rs.dt = dt;
+    rs.ptop = ptop;
+    rs.rf_cutoff = rf_cutoff;
+    rs.tau = tau;
+    for (int k = 0; k < nz; ++k) {
+      rs.dp[k] = dp[k];
+      rs.pfull[k] = pfull[k];
+    }
+    rs.k_rf = k_rf;
+    rs.k_nudge = k_nudge;
+  }
+  const int k_rf = rs.k_rf, k_nudge = rs.k_nudge;
+  if (k_rf == 0) return FV3B_OK;
+  const double* rf = colp(ctx, COL_RF);
+  const double* dm = colp(ctx, COL_RF_DM);
+  const double* dpc = colp(ctx, COL_DP_RAY);
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
+  const bool do_w = hydrostatic == 0;
+  FV3B_CHECK(launch_columns(s, e + 2, js, je + 2, st, [=] __device__(int t, int i, int j) {
+    const long long o0 = idx3(d, t, i, j, 0);
+    auto damp = [&](double* q) {
+      double total = 0.0;
+      for (int k = 0; k < k_rf; ++k) {
+        long long o = o0 + k * d.sk;
+        double c = q[o];
+        double lost = (1.0 - rf[k]) * dpc[k] * c;
+        total = k == 0 ? lost : total + lost;
+        q[o] = c * rf[k];
+      }
+      for (int k = 0; k < k_nudge; ++k) {
+        long long o = o0 + k * d.sk;
+        q[o] = q[o] + total / dm[k];
+      }
+    };
+    if (i <= e) damp(u);
+    if (j <= je) damp(v);
+    if (do_w && i <= e && j <= je)
+      for (int k = 0; k < k_rf; ++k) w[o0 + k * d.sk] = w[o0 + k * d.sk] * rf[k];
+  }));
+  return FV3B_OK;
+}
+
+// HyperdiffusionDamping.__call__ (del2cubed.py:152-181): ntimes = min(3,
+// nmax) del-2 passes on qdel with coefficient cd; pass n works on the
+// compute domain plus nt = ntimes-1-n halo rows.  The reference's corner
+// copies of its scratch q (copy_corners_x before the x fluxes, _y before
+// the y fluxes and the copy back) are reads through the corner rules.
+extern "C" int fv3b_del2cubed(fv3b_ctx* ctx, double* qdel, double cd, int nmax, void* stream) {
+  FV3B_REQUIRE(ctx && qdel, "fv3b_del2cubed: null argument");
+  const Dims d = ctx->d;
+  const fv3b_metrics g = ctx->m;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = d.nz;
+  const int full = d.ni - 1;
+  double *q = ctx->ws[0], *fx = ctx->ws[1], *fy = ctx->ws[2];
+  const int ntimes = nmax < 3 ? nmax : 3;
+  for (int n = 0; n < ntimes; ++n) {
+    const int nt = ntimes - (n + 1);
+    // corner_fill (del2cubed.py:41-75) into q, full domain
+    FV3B_CHECK(launch_box(Box{0, full, 0, full, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+      PT_SETUP(d, t, k);
+      const double third = 1.0 / 3.0;
+      double out = F3(qdel, i, j);
+      auto Q = [&](int di, int dj) { return F3(qdel, i + di, j + dj); };
+      if (j == js) {
+        if (i == s) out = (Q(0, 0) + Q(-1, 0) + Q(0, -1)) * third;
+        else if (i == s - 1) out = (Q(1, 0) + Q(0, 0) + Q(1, -1)) * third;
+        else if (i == e) out = (Q(0, 0) + Q(1, 0) + Q(0, -1)) * third;
+        else if (i == e + 1) out = (Q(-1, 0) + Q(0, 0) + Q(-1, -1)) * third;
+      } else if (j == js - 1) {
+        if (i == s) out = (Q(0, 1) + Q(-1, 1) + Q(0, 0)) * third;
+        else if (i == e) out = (Q(0, 1) + Q(1, 1) + Q(0, 0)) * third;
+      } else if (j == je) {
+        if (i == e) out = (Q(0, 0) + Q(1, 0) + Q(0, 1)) * third;
+        else if (i == e + 1) out = (Q(-1, 0) + Q(0, 0) + Q(-1, 1)) * third;
+        else if (i == s) out = (Q(0, 0) + Q(-1, 0) + Q(0, 1)) * third;
+        else if (i == s - 1) out = (Q(1, 0) + Q(0, 0) + Q(1, 1)) * third;
+      } else if (j == je + 1) {
+        if (i == e) out = (Q(0, -1) + Q(1, -1) + Q(0, 0)) * third;
+        else if (i == s) out = (Q(0, -1) + Q(-1, -1) + Q(0, 0)) * third;
+      }
+      W3(q, i, j) = out;
+    }));
+    // compute_zonal_flux / compute_meridional_flux on the X / Y interfaces
+    FV3B_CHECK(launch_box(Box{s - nt, e + 2 + nt, js - nt, je + 2 + nt, 0, nz}, st,
+                          [=] __device__(int t, int i, int j, int k) {
+                            PT_SETUP(d, t, k);
+                            auto qx = [&](int ii, int jj) {
+                              int si, sj;
+                              if (nt > 0 && copy_corner_x(d, ii, jj, si, sj)) return F3(q, si, sj);
+                              return F3(q, ii, jj);
+                            };
+                            auto qy = [&](int ii, int jj) {
+                              int si, sj;
+                              if (nt > 0 && copy_corner_y(d, ii, jj, si, sj)) return F3(q, si, sj);
+                              return F3(q, ii, jj);
+                            };
+                            if (j < je + 1 + nt) W3(fx, i, j) = F2(g.del6_v, i, j) * (qx(i - 1, j) - qx(i, j));
+                            if (i < e + 1 + nt) W3(fy, i, j) = F2(g.del6_u, i, j) * (qy(i, j - 1) - qy(i, j));
+                          }));
+    // copy back (q after both corner copies) and update_q
+    FV3B_CHECK(launch_box(Box{0, full, 0, full, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+      PT_SETUP(d, t, k);
+      int si, sj;
+      double qv = (nt > 0 && copy_corner_y(d, i, j, si, sj)) ? F3(q, si, sj) : F3(q, i, j);
+      if (i >= s - nt && i < e + 1 + nt && j >= js - nt && j < je + 1 + nt)
+        qv = qv + cd * F2(g.rarea, i, j) * (F3(fx, i, j) - F3(fx, i + 1, j) + F3(fy, i, j) - F3(fy, i, j + 1));
+      W3(qdel, i, j) = qv;
+    }));
+  }
+  return FV3B_OK;
+}
+
+// compute_pkz_tempadjust (temperature_adjust.py:8-44) on the compute domain,
+// levels [0, nk_heat).
+extern "C" int fv3b_pkz_tempadjust(fv3b_ctx* ctx, const double* delp, const double* delz, const double* cappa,
+                                   const double* heat_source, double* pt, double* pkz, double delt_time_factor,
+                                   int nk_heat, void* stream) {
+  FV3B_REQUIRE(ctx && delp && delz && cappa && heat_source && pt && pkz, "fv3b_pkz_tempadjust: null argument");
+  const Dims d = ctx->d;
+  FV3B_REQUIRE(nk_heat >= 0 && nk_heat <= d.nz, "fv3b_pkz_tempadjust: nk_heat out of range");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
+  FV3B_CHECK(launch_box(Box{s, e + 1, js, je + 1, 0, nk_heat}, st, [=] __device__(int t, int i, int j, int k) {
+    PT_SETUP(d, t, k);
+    double cp = F3(cappa, i, j), dp = F3(delp, i, j);
+    double p = pow(RDG * dp / F3(delz, i, j) * F3(pt, i, j), cp / (1.0 - cp));
+    double dtmp = F3(heat_source, i, j) / (CV_AIR * dp);
+    double lim = k == 0 ? delt_time_factor * 0.1 : (k == 1 ? delt_time_factor * 0.5 : delt_time_factor);
+    double a = fabs(dtmp);
+    double m = lim < a ? lim : a;
+    double deltmin = dtmp > 0.0 ? fabs(m) : -fabs(m);
+    W3(pkz, i, j) = p;
+    W3(pt, i, j) = F3(pt, i, j) + deltmin / p;
+  }));
+  return FV3B_OK;
+}

@@ -1,0 +1,128 @@
+// Pressure-gradient stages of the acoustic substep:
+//   p_grad_c_stencil (fv3core/stencils/dyn_core.py:101-145), nonhydrostatic;
+//   NonHydrostaticPressureGradient (fv3core/stencils/nh_p_grad.py);
+//   edge_pe (fv3core/stencils/pe_halo.py) and PK3Halo
+//   (fv3core/stencils/pk3_halo.py), the hydrostatic pressure on the rings
+//   of halo cells around the compute domain.
+#include <math.h>
+
+#include "a2b.cuh"
+#include "ctx.cuh"
+#include "stencil.cuh"
+
+using namespace fv3b;
+
+// p_grad_c_stencil, nonhydrostatic (wk = delpc), on [is, ie+1] x [js, je+1].
+extern "C" int fv3b_p_grad_c(fv3b_ctx* ctx, double* uc, double* vc, const double* delpc, const double* pkc,
+                             const double* gz, double dt2, void* stream) {
+  FV3B_REQUIRE(ctx && uc && vc && delpc && pkc && gz, "fv3b_p_grad_c: null argument");
+  const Dims d = ctx->d;
+  const fv3b_metrics g = ctx->m;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
+  FV3B_CHECK(launch_box(Box{s, e + 2, js, je + 2, 0, d.nz}, st, [=] __device__(int t, int i, int j, int k) {
+    PT_SETUP(d, t, k);
+    double wk = F3(delpc, i, j);
+    W3(uc, i, j) = F3(uc, i, j) + dt2 * F2(g.rdxc, i, j) / (F3(delpc, i - 1, j) + wk) *
+                                      ((F3K(gz, i - 1, j, 1) - F3(gz, i, j)) * (F3K(pkc, i, j, 1) - F3(pkc, i - 1, j)) +
+                                       (F3(gz, i - 1, j) - F3K(gz, i, j, 1)) * (F3K(pkc, i - 1, j, 1) - F3(pkc, i, j)));
+    W3(vc, i, j) = F3(vc, i, j) + dt2 * F2(g.rdyc, i, j) / (F3(delpc, i, j - 1) + wk) *
+                                      ((F3K(gz, i, j - 1, 1) - F3(gz, i, j)) * (F3K(pkc, i, j, 1) - F3(pkc, i, j - 1)) +
+                                       (F3(gz, i, j - 1) - F3K(gz, i, j, 1)) * (F3K(pkc, i, j - 1, 1) - F3(pkc, i, j)));
+  }));
+  return FV3B_OK;
+}
+
+// NonHydrostaticPressureGradient.__call__ (nh_p_grad.py:147-206).  pp, pk3
+// and gz are replaced by their B-grid interpolations (levels 1.., 1.., 0..);
+// the B-grid delp goes to scratch.  set_k0_and_calc_wk is folded into the
+// wind update: level 0 of pp and pk3 is read as its new value (0, ptop^akap)
+// and written by the level-0 threads.
+extern "C" int fv3b_nh_p_grad(fv3b_ctx* ctx, double* u, double* v, double* pp, double* gz, double* pk3,
+                              double* delp, double dt, double ptop, double akap, void* stream) {
+  FV3B_REQUIRE(ctx && u && v && pp && gz && pk3 && delp, "fv3b_nh_p_grad: null argument");
+  const Dims d = ctx->d;
+  const fv3b_metrics g = ctx->m;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = d.nz, nk = d.nk;
+  double *wk1 = ctx->ws[0], *qx = ctx->ws[1], *qy = ctx->ws[2], *edges = ctx->ws[3];
+  const double ptk = pow(ptop, akap);
+  FV3B_CHECK(a2b_ord4(d, g, pp, wk1, qx, qy, edges, 1, nk, st, true));
+  FV3B_CHECK(a2b_ord4(d, g, pk3, wk1, qx, qy, edges, 1, nk, st, true));
+  FV3B_CHECK(a2b_ord4(d, g, gz, wk1, qx, qy, edges, 0, nk, st, true));
+  FV3B_CHECK(a2b_ord4(d, g, delp, wk1, qx, qy, edges, 0, nz, st, false));
+  // calc_u on [is, ie] x [js, je+1], calc_v on [is, ie+1] x [js, je]
+  FV3B_CHECK(launch_box(Box{s, e + 2, js, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+    PT_SETUP(d, t, k);
+    auto P = [&](int ii, int jj, int dk) { return k + dk == 0 ? 0.0 : F3K(pp, ii, jj, dk); };
+    auto K3 = [&](int ii, int jj, int dk) { return k + dk == 0 ? ptk : F3K(pk3, ii, jj, dk); };
+    auto wk = [&](int ii, int jj) { return K3(ii, jj, 1) - K3(ii, jj, 0); };
+    if (i <= e) {
+      double du = dt / (wk(i, j) + wk(i + 1, j)) *
+                  ((F3K(gz, i, j, 1) - F3(gz, i + 1, j)) * (K3(i + 1, j, 1) - K3(i, j, 0)) +
+                   (F3(gz, i, j) - F3K(gz, i + 1, j, 1)) * (K3(i, j, 1) - K3(i + 1, j, 0)));
+      W3(u, i, j) = (F3(u, i, j) + du +
+                     dt / (F3(wk1, i, j) + F3(wk1, i + 1, j)) *
+                         ((F3K(gz, i, j, 1) - F3(gz, i + 1, j)) * (P(i + 1, j, 1) - P(i, j, 0)) +
+                          (F3(gz, i, j) - F3K(gz, i + 1, j, 1)) * (P(i, j, 1) - P(i + 1, j, 0)))) *
+                    F2(g.rdx, i, j);
+    }
+    if (j <= je) {
+      double dv = dt / (wk(i, j) + wk(i, j + 1)) *
+                  ((F3K(gz, i, j, 1) - F3(gz, i, j + 1)) * (K3(i, j + 1, 1) - K3(i, j, 0)) +
+                   (F3(gz, i, j) - F3K(gz, i, j + 1, 1)) * (K3(i, j, 1) - K3(i, j + 1, 0)));
+      W3(v, i, j) = (F3(v, i, j) + dv +
+                     dt / (F3(wk1, i, j) + F3(wk1, i, j + 1)) *
+                         ((F3K(gz, i, j, 1) - F3(gz, i, j + 1)) * (P(i, j + 1, 1) - P(i, j, 0)) +
+                          (F3(gz, i, j) - F3K(gz, i, j + 1, 1)) * (P(i, j, 1) - P(i, j + 1, 0)))) *
+                    F2(g.rdy, i, j);
+    }
+    if (k == 0) {
+      W3(pp, i, j) = 0.0;
+      W3(pk3, i, j) = ptk;
+    }
+  }));
+  return FV3B_OK;
+}
+
+// edge_pe (pe_halo.py:6-33): interface pressure on the one-cell ring around
+// the compute domain, summed from ptop.
+extern "C" int fv3b_edge_pe(fv3b_ctx* ctx, double* pe, const double* delp, double ptop, void* stream) {
+  FV3B_REQUIRE(ctx && pe && delp, "fv3b_edge_pe: null argument");
+  const Dims d = ctx->d;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nk = d.nk;
+  FV3B_CHECK(launch_columns(s - 1, e + 2, js - 1, je + 2, st, [=] __device__(int t, int i, int j) {
+    if (i >= s && i <= e && j >= js && j <= je) return;
+    long long o = idx3(d, t, i, j, 0);
+    double p = ptop;
+    pe[o] = p;
+    for (int k = 1; k < nk; ++k) {
+      p = p + delp[o];
+      o += d.sk;
+      pe[o] = p;
+    }
+  }));
+  return FV3B_OK;
+}
+
+// PK3Halo.__call__ (pk3_halo.py:36-68): pk3 = pe^akap on the two-cell ring,
+// levels 1..npz.
+extern "C" int fv3b_pk3_halo(fv3b_ctx* ctx, double* pk3, const double* delp, double ptop, double akap,
+                             void* stream) {
+  FV3B_REQUIRE(ctx && pk3 && delp, "fv3b_pk3_halo: null argument");
+  const Dims d = ctx->d;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nk = d.nk;
+  FV3B_CHECK(launch_columns(s - 2, e + 3, js - 2, je + 3, st, [=] __device__(int t, int i, int j) {
+    if (i >= s && i <= e && j >= js && j <= je) return;
+    long long o = idx3(d, t, i, j, 0);
+    double p = ptop;
+    for (int k = 1; k < nk; ++k) {
+      p = p + delp[o];
+      o += d.sk;
+      pk3[o] = pow(p, akap);
+    }
+  }));
+  return FV3B_OK;
+}

@@ -14,6 +14,8 @@ namespace fv3b {
 
 constexpr double GRAV = 9.80665;
 constexpr double RDGAS = 287.05;
+constexpr double RGRAV = 1.0 / GRAV;
+constexpr double KAPPA = RDGAS / 1004.6;
 constexpr int MAXK = 128;
 
 // Sim1 solve on one column (reference fv3core/stencils/sim1_solver.py:11-101).
@@ -150,5 +152,82 @@ extern "C" int fv3b_riem_solver_c(const fv3b_grid_dims* dims, double dt2, double
     }
   };
   FV3B_CHECK(launch_columns(d.isc - 1, d.iec + 2, d.jsc - 1, d.jec + 2, s, body));
+  return FV3B_OK;
+}
+
+// RiemannSolver3.__call__ (riem_solver3.py:145-242): precompute (24-67),
+// Sim1 solve, finalize (70-103) on the compute-domain columns, interface
+// levels 0..npz.
+extern "C" int fv3b_riem_solver3(const fv3b_grid_dims* dims, int last_call, double dt, double ptop, double p_fac,
+                                 const double* cappa, const double* zs, const double* wsd, double* delz,
+                                 const double* q_con, const double* delp, const double* pt, double* zh, double* pe,
+                                 double* ppe, double* pk3, double* pk, double* peln, double* w, void* stream) {
+  FV3B_REQUIRE(dims && cappa && zs && wsd && delz && q_con && delp && pt && zh && pe && ppe && pk3 && pk && peln && w,
+               "fv3b_riem_solver3: null argument");
+  Dims d = make_dims(dims);
+  FV3B_REQUIRE(d.nk <= MAXK && d.nk >= 3, "fv3b_riem_solver3: npz out of range (2..127)");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int K = d.nk;
+  const double peln1 = log(ptop);
+  const double ptk = exp(KAPPA * peln1);
+  const double t1g = 2.0 * dt * dt;
+  const double rdt = 1.0 / dt;
+  const bool last = last_call != 0;
+  auto body = [=] __device__(int t, int i, int j) {
+    double dm[MAXK], wc[MAXK], w1[MAXK], dz[MAXK], pem[MAXK], pm[MAXK], pec[MAXK], pp[MAXK], gam[MAXK],
+        aa[MAXK], peln_run[MAXK];
+    const long long o0 = idx3(d, t, i, j, 0);
+    // precompute
+    double pem_k = ptop, peg_k = ptop, pelng_k = peln1;
+    pem[0] = ptop;
+    peln_run[0] = peln1;
+    pk3[o0] = ptk;
+    for (int k = 0; k < K; ++k) {
+      long long o = o0 + k * d.sk;
+      double dmk = delp[o];
+      if (k < K - 1) {
+        double pem_n = pem_k + dmk;
+        double peg_n = peg_k + dmk * (1.0 - q_con[o]);
+        double pelng_n = log(peg_n);
+        double peln_n = log(pem_n);
+        pem[k + 1] = pem_n;
+        peln_run[k + 1] = peln_n;
+        pk3[o + d.sk] = exp(KAPPA * peln_n);
+        pm[k] = (peg_n - peg_k) / (pelng_n - pelng_k);
+        dz[k] = zh[o + d.sk] - zh[o];
+        pem_k = pem_n;
+        peg_k = peg_n;
+        pelng_k = pelng_n;
+      }
+      dm[k] = dmk * RGRAV;
+      wc[k] = w[o];
+    }
+    auto gm = [&](int k) { return 1.0 / (1.0 - cappa[o0 + k * d.sk]); };
+    auto ptr = [&](int k) { return pt[o0 + k * d.sk]; };
+    auto cp3 = [&](int k) { return cappa[o0 + k * d.sk]; };
+    sim1_column(K, dm, wc, w1, dz, pem, pm, pec, pp, gam, aa, gm, ptr, cp3, wsd[idx2(d, t, i, j)], dt, t1g, rdt,
+                p_fac);
+    // finalize (beta = 0, use_logp = False)
+    for (int k = 0; k < K; ++k) {
+      long long o = o0 + k * d.sk;
+      ppe[o] = pec[k];
+      if (last) {
+        peln[o] = peln_run[k];
+        pk[o] = pk3[o];
+        pe[o] = pem[k];
+      }
+      if (k < K - 1) {
+        w[o] = wc[k];
+        delz[o] = dz[k];
+      }
+    }
+    double z = zs[idx2(d, t, i, j)];
+    zh[o0 + (K - 1) * d.sk] = z;
+    for (int k = K - 2; k >= 0; --k) {
+      z = z - dz[k];
+      zh[o0 + k * d.sk] = z;
+    }
+  };
+  FV3B_CHECK(launch_columns(d.isc, d.iec + 1, d.jsc, d.jec + 1, s, body));
   return FV3B_OK;
 }

@@ -171,9 +171,12 @@ __device__ __forceinline__ int nord_at(const double* nord, int k) { return (int)
 // into fx2/fy2 using d2 as scratch.  Corner copies of d2 are applied on read
 // (a point of a corner block reads its copy source), which gives the values
 // the reference reads after copying the corners in place.
+// nlev is the number of levels (npz by default; UpdateHeightOnDGrid runs it
+// on npz + 1 interface levels).
 inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const double* q, double* fx2, double* fy2,
-                                 DelnCol col, double* d2, bool mass_weighted, int nmax, cudaStream_t st) {
-  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = d.nz;
+                                 DelnCol col, double* d2, bool mass_weighted, int nmax, cudaStream_t st,
+                                 int nlev = -1) {
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = nlev < 0 ? d.nz : nlev;
   cudaError_t err;
   // d2_damp_interval / copy_stencil_interval
   err = launch_box(Box{s - 1 - nmax, e + 2 + nmax, js - 1 - nmax, je + 2 + nmax, 0, nz}, st,

@@ -37,8 +37,6 @@ class Metrics(ctypes.Structure):
 
 
 
-
-
 class GridData:
     """All metric terms of an n x n cube on the GPU, plus the stage context."""
 
@@ -74,6 +72,7 @@ class GridData:
         if rc != 0:
             raise RuntimeError(f"fv3b_ctx_create failed ({rc}): {L.fv3b_last_error().decode()}")
         self.ctx = ctx
+        self.grid_indexing.context = ctx
 
     def close(self):
         if getattr(self, "ctx", None) is not None and self.ctx.value:

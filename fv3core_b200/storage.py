@@ -24,6 +24,9 @@ class GridIndexing:
         if not (south_edge and north_edge and west_edge and east_edge):
             raise NotImplementedError("each device array holds whole tiles (layout 1x1)")
         self.origin = (self.n_halo, self.n_halo, 0)
+        # the device context (fv3b_ctx*) of the GridData built on this grid;
+        # every stage class reaches the metric terms and workspace through it
+        self.context = None
 
     @property
     def n(self):

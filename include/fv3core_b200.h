@@ -13,9 +13,10 @@
  * Index (i, j) in a field is the reference's storage index: the compute
  * domain of a tile is i, j in [h, h+n) (cell centres) or [h, h+n] (edges).
  *
- * All calls are asynchronous on the given CUDA stream (cudaStream_t passed
+ * Stage calls are asynchronous on the given CUDA stream (cudaStream_t passed
  * as void*), allocate nothing, and return 0 on success or an FV3B_ERR_*
  * code; fv3b_last_error() describes the last failure of the calling thread.
+ * Only fv3b_ctx_create and the *_setup calls allocate or synchronise.
  */
 #ifndef FV3CORE_B200_H
 #define FV3CORE_B200_H
@@ -134,6 +135,139 @@ int fv3b_riem_solver_c(const fv3b_grid_dims* dims, double dt2, double ptop, doub
                        const double* cappa, const double* hs, const double* ws,
                        const double* ptc, const double* q_con, const double* delpc,
                        double* gz, double* pef, const double* w3, void* stream);
+
+/*
+ * RiemannSolver3.__call__ (fv3core/stencils/riem_solver3.py:145-242) with
+ * a_imp > 0.999, beta = 0, use_logp = False: compute-domain columns,
+ * interface levels 0..npz.  In: cappa, zs (2-D), wsd (2-D), q_con, delp, pt.
+ * In/out: delz, zh, w, pk3 (levels 0..npz of the compute domain).  Out: ppe
+ * (nonhydrostatic pressure perturbation); when last_call != 0 also pe, pk
+ * and peln.
+ */
+int fv3b_riem_solver3(const fv3b_grid_dims* dims, int last_call, double dt, double ptop, double p_fac,
+                      const double* cappa, const double* zs, const double* wsd, double* delz,
+                      const double* q_con, const double* delp, const double* pt, double* zh, double* pe,
+                      double* ppe, double* pk3, double* pk, double* peln, double* w, void* stream);
+
+/*
+ * UpdateGeopotentialHeightOnCGrid.__call__ (fv3core/stencils/updatedzc.py:123-163).
+ * dp_ref: device [npz+1] reference layer thickness; zs, ws: 2-D.
+ * In: ut, vt.  In/out: gz (interface heights).  Out: ws.
+ */
+int fv3b_update_dz_c(fv3b_ctx* ctx, const double* dp_ref, const double* zs, const double* ut, const double* vt,
+                     double* gz, double* ws, double dt, void* stream);
+
+/*
+ * UpdateHeightOnDGrid.__init__ (fv3core/stencils/updatedzd.py:189-320):
+ * dp_ref_host is the host [npz+1] reference layer thickness (dp0), hord_tm
+ * the PPM order of the height transport.  Needs
+ * fv3b_d_sw_setup first (the damping column namelist).  Synchronous.
+ */
+int fv3b_update_dz_d_setup(fv3b_ctx* ctx, const double* dp_ref_host, int hord_tm);
+
+/*
+ * UpdateHeightOnDGrid.__call__ (fv3core/stencils/updatedzd.py:323-393).
+ * In: zs (2-D), crx, cry, xfx, yfx.  In/out: zh.  Out: wsd (2-D).
+ */
+int fv3b_update_dz_d(fv3b_ctx* ctx, const double* zs, double* zh, const double* crx, const double* cry,
+                     const double* xfx, const double* yfx, double* wsd, double dt, void* stream);
+
+/* p_grad_c_stencil (fv3core/stencils/dyn_core.py:101-145), nonhydrostatic. */
+int fv3b_p_grad_c(fv3b_ctx* ctx, double* uc, double* vc, const double* delpc, const double* pkc,
+                  const double* gz, double dt2, void* stream);
+
+/*
+ * NonHydrostaticPressureGradient.__call__ (fv3core/stencils/nh_p_grad.py:147-206).
+ * pp, pk3 and gz are replaced by their B-grid values, as in the reference.
+ */
+int fv3b_nh_p_grad(fv3b_ctx* ctx, double* u, double* v, double* pp, double* gz, double* pk3, double* delp,
+                   double dt, double ptop, double akap, void* stream);
+
+/* edge_pe (fv3core/stencils/pe_halo.py:6-33). */
+int fv3b_edge_pe(fv3b_ctx* ctx, double* pe, const double* delp, double ptop, void* stream);
+
+/* PK3Halo.__call__ (fv3core/stencils/pk3_halo.py:36-68). */
+int fv3b_pk3_halo(fv3b_ctx* ctx, double* pk3, const double* delp, double ptop, double akap, void* stream);
+
+/*
+ * RayleighDamping.__call__ (fv3core/stencils/ray_fast.py:169-192); the
+ * constructor arguments rf_cutoff, tau, hydrostatic are passed per call.
+ * dp and pfull are HOST arrays of npz values (the reference's K fields);
+ * factors are re-uploaded (synchronously) only when they change.
+ */
+int fv3b_ray_fast(fv3b_ctx* ctx, double* u, double* v, double* w, const double* dp, const double* pfull,
+                  double dt, double ptop, double rf_cutoff, double tau, int hydrostatic, void* stream);
+
+/* HyperdiffusionDamping.__call__ (fv3core/stencils/del2cubed.py:152-181). */
+int fv3b_del2cubed(fv3b_ctx* ctx, double* qdel, double cd, int nmax, void* stream);
+
+/* compute_pkz_tempadjust (fv3core/stencils/temperature_adjust.py:8-44) on
+ * levels [0, nk_heat). */
+int fv3b_pkz_tempadjust(fv3b_ctx* ctx, const double* delp, const double* delz, const double* cappa,
+                        const double* heat_source, double* pt, double* pkz, double delt_time_factor, int nk_heat,
+                        void* stream);
+
+/*
+ * Halo updates, replacing fv3gfs-util's HaloUpdater.update /
+ * CubedSphereCommunicator.synchronize_vector_interfaces as the reference's
+ * AcousticDynamics._HaloUpdaters use them (fv3core/stencils/dyn_core.py:216-286).
+ * All six tiles are in one allocation, so an update is an on-device gather.
+ * stagger: 1 = cell centres, 0 = cell corners.  grid: 0 = D-grid (u, v),
+ * 1 = C-grid (uc, vc).  nlev: levels to update (npz for Z_DIM fields,
+ * npz+1 for Z_INTERFACE_DIM fields).
+ */
+int fv3b_halo_update_scalar(fv3b_ctx* ctx, double* field, int stagger, int n_halo, int nlev, void* stream);
+int fv3b_halo_update_vector(fv3b_ctx* ctx, double* x, double* y, int grid, int nlev, void* stream);
+int fv3b_synchronize_vector_interfaces(fv3b_ctx* ctx, double* u, double* v, int nlev, void* stream);
+
+/*
+ * AcousticDynamicsConfig (fv3core/_config.py:164-212) without the nested
+ * RiemannConfig / D-grid config (p_fac comes from the Riemann config; the
+ * D-grid namelist is passed separately).  Flags are 0/1.
+ */
+typedef struct fv3b_acoustic_config {
+  double tau, delt_max, rf_cutoff, p_fac;
+  int32_t k_split, n_split, rf_fast, breed_vortex_inline, use_old_omega, reserved;
+} fv3b_acoustic_config;
+
+/*
+ * The dycore state fields AcousticDynamics.__call__ reads and writes
+ * (fv3core/stencils/dyn_core.py:479-761), as device pointers in the layout
+ * above; phis and wsd are 2-D.  mdt, n_map, akap, ptop, ks are the state's
+ * scalars.
+ */
+typedef struct fv3b_dycore_state {
+  double *u, *v, *w, *delz, *delp, *pt, *pe, *pk, *phis, *wsd, *omga, *ua, *va, *uc, *vc;
+  double *mfxd, *mfyd, *cxd, *cyd, *pkz, *peln, *q_con, *diss_estd, *cappa;
+  double mdt, akap, ptop;
+  int32_t n_map, ks;
+} fv3b_dycore_state;
+
+/*
+ * AcousticDynamics.__init__ (fv3core/stencils/dyn_core.py:288-477): D-grid
+ * setup, reference layer thickness dp_ref from ak/bk, zs = phis/g, spline
+ * constants, and the substep temporaries (gz, zh, pkc, pk3, ut, vt, divgd,
+ * heat_source, crx, cry, xfx, yfx, delpc, ptc, ws3), which persist between
+ * calls as the reference's instance storages do.  ak, bk, pfull: HOST
+ * arrays of npz+1, npz+1, npz values; phis: device 2-D field.  Allocates
+ * (cudaMalloc) and synchronises.  Rejects what the reference rejects
+ * (d_ext != 0, beta != 0, use_logp, hydrostatic).
+ */
+int fv3b_acoustics_setup(fv3b_ctx* ctx, const fv3b_acoustic_config* config, const fv3b_dsw_config* dsw,
+                         const double* ak, const double* bk, const double* pfull, const double* phis);
+
+/*
+ * AcousticDynamics.__call__ (fv3core/stencils/dyn_core.py:479-761): the
+ * n_split acoustic substeps (c_sw, updatedzc, riem_solver_c, p_grad_c,
+ * d_sw, updatedzd, riem_solver3, pe/pk3 halos, nh_p_grad, ray_fast, halo
+ * updates) and the closing del2cubed / temperature adjustment.
+ */
+int fv3b_acoustics(fv3b_ctx* ctx, const fv3b_dycore_state* state, void* stream);
+
+/* Device pointer of one of the substep temporaries by its reference name
+ * ("gz", "zh", "pkc", "pk3", "ut", "vt", "divgd", "heat_source", "crx",
+ * "cry", "xfx", "yfx", "delpc", "ptc", "ws3", "zs", "dp_ref"), or NULL. */
+double* fv3b_acoustics_temporary(fv3b_ctx* ctx, const char* name);
 
 #ifdef __cplusplus
 }

@@ -254,7 +254,8 @@ class AcousticDynamics:
         self.tmp["gz"][:] = HUGE_R
         self.tmp["pk3"][:] = HUGE_R
         self.dp_ref = dp_ref_compute(np.asarray(ak), np.asarray(bk), nz)
-        self.zs = phis / C.GRAV
+        # dp_ref_compute multiplies by the reciprocal (dyn_core.py:79)
+        self.zs = phis * (1.0 / C.GRAV)
         self.pfull = np.asarray(pfull)
         dcfg = cfg["dsw"]
         self.dsw_states = [DSWState(t, metrics[tt], dcfg) for tt in range(6)]

@@ -51,3 +51,42 @@ def run_d_sw(case, n, nz):
     dsw(*[dev[k] for k in DSW_ARGS], case["dt"])
     torch.cuda.synchronize()
     return {k: to_host(dev[k]) for k in DSW_ARGS}
+
+
+def run_acoustics(case, n, nz):
+    """The package's AcousticDynamics on a case of ``cases.acoustics_case``;
+    returns the state and the driver's temporaries (prefixed ``tmp_``)."""
+    import types
+
+    import torch
+
+    from fv3core_b200.config import (AcousticDynamicsConfig, DGridShallowWaterLagrangianDynamicsConfig,
+                                     RiemannConfig)
+    from fv3core_b200.grid_data import GridData
+    from fv3core_b200.halo import DeviceCubedSphereCommunicator
+    from fv3core_b200.stencil import StencilConfig, StencilFactory
+    from fv3core_b200.stencils.dyn_core import AcousticDynamics
+    from fv3core_b200.storage import to_device, to_host
+
+    gd = GridData(cases.grid_for(n), nz)
+    sf = StencilFactory(StencilConfig(), gd.grid_indexing)
+    cfg = AcousticDynamicsConfig(
+        **{**cases.ACOUSTIC_CONFIG, "n_split": int(case["n_split"])},
+        riemann=RiemannConfig(**cases.RIEMANN_CONFIG),
+        d_grid_shallow_water=DGridShallowWaterLagrangianDynamicsConfig(**cases.DSW_CONFIG),
+    )
+    phis = to_device(case["phis"])
+    ad = AcousticDynamics(DeviceCubedSphereCommunicator(gd.grid_indexing), sf, gd, gd, 0, False, False, cfg,
+                          case["ak"], case["bk"], case["pfull"], phis)
+    st = types.SimpleNamespace(**{k: to_device(case[k]) for k in cases.ACOUSTIC_STATE})
+    st.phis = phis
+    for k in ("mdt", "n_map", "akap", "ptop", "ks"):
+        setattr(st, k, case[k])
+    ad(st)
+    torch.cuda.synchronize()
+    out = {k: to_host(getattr(st, k)) for k in cases.ACOUSTIC_STATE}
+    for name in ("gz", "zh", "pkc", "pk3", "heat_source", "divgd"):
+        out["tmp_" + name] = to_host(ad.temporary(name).clone())
+    gd.close()
+    return out
+
