@@ -11,6 +11,7 @@
 
 #include "corners.cuh"
 #include "ctx.cuh"
+#include "fmath.h"
 #include "stencil.cuh"
 
 using namespace fv3b;
@@ -193,7 +194,7 @@ extern "C" int fv3b_pkz_tempadjust(fv3b_ctx* ctx, const double* delp, const doub
   FV3B_CHECK(launch_box(Box{s, e + 1, js, je + 1, 0, nk_heat}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
     double cp = F3(cappa, i, j), dp = F3(delp, i, j);
-    double p = pow(RDG * dp / F3(delz, i, j) * F3(pt, i, j), cp / (1.0 - cp));
+    double p = fm::fm_pow(RDG * dp / F3(delz, i, j) * F3(pt, i, j), cp / (1.0 - cp));
     double dtmp = F3(heat_source, i, j) / (CV_AIR * dp);
     double lim = k == 0 ? delt_time_factor * 0.1 : (k == 1 ? delt_time_factor * 0.5 : delt_time_factor);
     double a = fabs(dtmp);

@@ -8,6 +8,7 @@
 
 #include "a2b.cuh"
 #include "ctx.cuh"
+#include "fmath.h"
 #include "stencil.cuh"
 
 using namespace fv3b;
@@ -121,7 +122,7 @@ extern "C" int fv3b_pk3_halo(fv3b_ctx* ctx, double* pk3, const double* delp, dou
     for (int k = 1; k < nk; ++k) {
       p = p + delp[o];
       o += d.sk;
-      pk3[o] = pow(p, akap);
+      pk3[o] = fm::fm_pow(p, akap);
     }
   }));
   return FV3B_OK;

@@ -5,10 +5,12 @@
 // back; neighbouring threads own neighbouring i, so every level load/store
 // is a coalesced row access.  Column work arrays live in per-thread local
 // memory (thread-interleaved, so also coalesced); MAXK bounds the number of
-// interface levels.
+// interface levels.  exp and log are the library's own (fmath.h), whose
+// host build the oracle uses, so results can be compared to the last bit.
 #include <math.h>
 
 #include "common.cuh"
+#include "fmath.h"
 
 namespace fv3b {
 
@@ -31,7 +33,7 @@ __device__ __forceinline__ void sim1_column(int K, const double* dm, double* w, 
                                             double dt, double t1g, double rdt, double p_fac) {
   // pe = exp(gm*log(-dm/dz*Rd*ptr)) - pm   (sim1_solver.py:27-29)
   for (int k = 0; k < K - 1; ++k) {
-    pe[k] = exp(gm(k) * log(-dm[k] / dz[k] * RDGAS * ptr(k))) - pm[k];
+    pe[k] = fm::fm_exp(gm(k) * fm::fm_log(-dm[k] / dz[k] * RDGAS * ptr(k))) - pm[k];
     w1[k] = w[k];
   }
   // forward elimination of the pressure system (sim1_solver.py:30-59)
@@ -94,7 +96,7 @@ __device__ __forceinline__ void sim1_column(int K, const double* dm, double* w, 
     }
     p1n = p1;
     double maxp = (p_fac * dm[k] > p1 + pm[k]) ? p_fac * pm[k] : p1 + pm[k];
-    dz[k] = -dm[k] * RDGAS * ptr(k) * exp((cp3(k) - 1.0) * log(maxp));
+    dz[k] = -dm[k] * RDGAS * ptr(k) * fm::fm_exp((cp3(k) - 1.0) * fm::fm_log(maxp));
   }
 }
 
@@ -129,7 +131,7 @@ extern "C" int fv3b_riem_solver_c(const fv3b_grid_dims* dims, double dt2, double
         double gz_next = gz[o + d.sk];
         dz[k] = gz_next - gz_prev;
         gz_prev = gz_next;
-        pm[k] = (peg_next - peg_k) / log(peg_next / peg_k);
+        pm[k] = (peg_next - peg_k) / fm::fm_log(peg_next / peg_k);
       }
       pem_k = pem_k + dmk;
       peg_k = peg_next;
@@ -188,11 +190,11 @@ extern "C" int fv3b_riem_solver3(const fv3b_grid_dims* dims, int last_call, doub
       if (k < K - 1) {
         double pem_n = pem_k + dmk;
         double peg_n = peg_k + dmk * (1.0 - q_con[o]);
-        double pelng_n = log(peg_n);
-        double peln_n = log(pem_n);
+        double pelng_n = fm::fm_log(peg_n);
+        double peln_n = fm::fm_log(pem_n);
         pem[k + 1] = pem_n;
         peln_run[k + 1] = peln_n;
-        pk3[o + d.sk] = exp(KAPPA * peln_n);
+        pk3[o + d.sk] = fm::fm_exp(KAPPA * peln_n);
         pm[k] = (peg_n - peg_k) / (pelng_n - pelng_k);
         dz[k] = zh[o + d.sk] - zh[o];
         pem_k = pem_n;

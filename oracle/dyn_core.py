@@ -11,6 +11,7 @@ import numpy as np
 
 from fv3core_b200 import constants as C
 
+from . import _math
 from . import corners
 from ._util import Tile, at, c3, put, region, sh
 from .a2b_ord4 import A2BScratch, a2b_ord4
@@ -149,7 +150,7 @@ def pk3_halo(t: Tile, pk3, delp, ptop, akap, pe_tmp):
     pe_tmp[:] = np.where(m, ptop, pe_tmp)
     for k in range(1, t.nk):
         pe_tmp[:] = np.where(m, pe_tmp + delp[:, :, k - 1], pe_tmp)
-        pk3[:, :, k] = np.where(m, pe_tmp ** akap, pk3[:, :, k])
+        pk3[:, :, k] = np.where(m, _math.power(pe_tmp, akap), pk3[:, :, k])
 
 
 def del2cubed(t: Tile, g, qdel, cd, nmax, scr):
@@ -201,8 +202,8 @@ def pkz_tempadjust(t: Tile, delp, delz, cappa, heat_source, pt, pkz, dtf, nk_hea
     B = (slice(s, e + 1), slice(js, je + 1), slice(0, nk_heat))
     dp, dz, cp, hs = delp[B], delz[B], cappa[B], heat_source[B]
     p = pkz[B]
-    p[...] = np.exp(cp / (1.0 - cp) * np.log(C.RDG * dp / dz * pt[B]))
-    p[...] = (C.RDG * dp / dz * pt[B]) ** (cp / (1.0 - cp))
+    # the reference first writes exp(cp/(1-cp) log(...)) and then overwrites it
+    p[...] = _math.power(C.RDG * dp / dz * pt[B], cp / (1.0 - cp))
     dtmp = hs / (C.CV_AIR * dp)
     fac = np.array([0.1 if k == 0 else (0.5 if k == 1 else 1.0) for k in range(nk_heat)])[None, None, :]
     deltmin = sign(np.minimum(dtf * fac, np.abs(dtmp)), dtmp)

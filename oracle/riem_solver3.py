@@ -9,6 +9,7 @@ import numpy as np
 
 from fv3core_b200 import constants as C
 
+from . import _math
 from .sim1 import sim1_solver
 
 
@@ -37,10 +38,10 @@ def riem_solver3(last_call, dt, cappa, ptop, zs, wsd, delz, q_con, delp, pt, zh,
     pelng[:, :, 0] = peln1
     for k in range(1, K):
         pem[:, :, k] = pem[:, :, k - 1] + dm[:, :, k - 1]
-        peln_run[:, :, k] = np.log(pem[:, :, k])
+        peln_run[:, :, k] = _math.log(pem[:, :, k])
         peg[:, :, k] = peg[:, :, k - 1] + dm[:, :, k - 1] * (1.0 - qc[:, :, k - 1])
-        pelng[:, :, k] = np.log(peg[:, :, k])
-        pk3[I, J, k] = np.exp(C.KAPPA * peln_run[:, :, k])
+        pelng[:, :, k] = _math.log(peg[:, :, k])
+        pk3[I, J, k] = _math.exp(C.KAPPA * peln_run[:, :, k])
     gm = 1.0 / (1.0 - cappa[box])
     dm = dm * C.RGRAV
     pm = np.full(shp, np.nan)

@@ -10,6 +10,7 @@ import numpy as np
 
 from fv3core_b200 import constants as C
 
+from . import _math
 from .sim1 import sim1_solver
 
 
@@ -35,7 +36,7 @@ def riem_solver_c(dt2, cappa, ptop, hs, ws, ptc, q_con, delpc, gz, pef, w3, p_fa
     gm = 1.0 / (1.0 - cappa[box])
     dm = dm / C.GRAV
     pm = np.full_like(dm, np.nan)
-    pm[:, :, : K - 1] = (peg[:, :, 1:K] - peg[:, :, : K - 1]) / np.log(peg[:, :, 1:K] / peg[:, :, : K - 1])
+    pm[:, :, : K - 1] = (peg[:, :, 1:K] - peg[:, :, : K - 1]) / _math.log(peg[:, :, 1:K] / peg[:, :, : K - 1])
     # sim1 (riem_solver_c.py:152-164 -> sim1_solver.py)
     t1g = 2.0 * dt2 * dt2
     rdt = 1.0 / dt2

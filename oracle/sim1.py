@@ -9,13 +9,15 @@ import numpy as np
 
 from fv3core_b200 import constants as C
 
+from . import _math
+
 
 def sim1_solver(w, dm, gm, dz, ptr, pm, pe, pem, wsr, cp3, dt, t1g, rdt, p_fac, nk):
     """Arrays are views [ni, nj, >=nk]; level nk-1 is the bottom interface."""
     K = nk
     sl = slice(0, K - 1)
     # PARALLEL interval(0, -1): pe, w1 (sim1_solver.py:27-29)
-    pe[:, :, sl] = np.exp(gm[:, :, sl] * np.log(-dm[:, :, sl] / dz[:, :, sl] * C.RDGAS * ptr[:, :, sl])) - pm[:, :, sl]
+    pe[:, :, sl] = _math.exp(gm[:, :, sl] * _math.log(-dm[:, :, sl] / dz[:, :, sl] * C.RDGAS * ptr[:, :, sl])) - pm[:, :, sl]
     w1 = w.copy()
     shp = w.shape[:2] + (K,)
     g_rat = np.full(shp, np.nan)
@@ -80,4 +82,4 @@ def sim1_solver(w, dm, gm, dz, ptr, pm, pe, pem, wsr, cp3, dt, t1g, rdt, p_fac, 
     # PARALLEL interval(0, -1): dz (sim1_solver.py:103-105)
     s = slice(0, K - 1)
     maxp = np.where(p_fac * dm[:, :, s] > p1[:, :, s] + pm[:, :, s], p_fac * pm[:, :, s], p1[:, :, s] + pm[:, :, s])
-    dz[:, :, s] = -dm[:, :, s] * C.RDGAS * ptr[:, :, s] * np.exp((cp3[:, :, s] - 1.0) * np.log(maxp))
+    dz[:, :, s] = -dm[:, :, s] * C.RDGAS * ptr[:, :, s] * _math.exp((cp3[:, :, s] - 1.0) * _math.log(maxp))

@@ -1,13 +1,22 @@
 """The acoustic-loop stages beside c_sw / d_sw / RiemannSolverC, one at a
-time: CUDA through the package's classes vs the oracle on seeded inputs.
-(The oracle of each stage is pinned by the full-substep golden test.)"""
+time: CUDA through the package's classes vs the oracle on seeded inputs,
+the oracle running the kernels' own exp/log/pow.  (The oracle of each stage
+is pinned by the full-substep golden test.)"""
 import numpy as np
 import pytest
+
+from oracle import _math
 
 import cases
 from metrics import parity_err
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def _device_math():
+    with _math.device_math():
+        yield
 H = 3
 SIZES = [(12, 8, 3), (24, 16, 4)]
 
