@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Acoustic-substep throughput on B200: AcousticDynamics (fv3core's dyn_core)
+on a C384 L79 cubed sphere, all six tiles on one GPU, FP64.
+
+One step = one AcousticDynamics call = n_split (6) acoustic substeps over
+the whole cube, on a Jablonowski-Williamson baroclinic-wave state with seeded
+noise (synthetic data).  ``value`` is cell-levels advanced per second per
+substep (6 * 384^2 * 79 cell-levels x n_split per step), device-timed with
+CUDA events, inputs resident in HBM (every 3-D field is 0.59 GB, far larger
+than the 126 MB L2, so no flush is needed).  ``e2e`` times the same call
+through the package's public API with the state copied in from pinned host
+memory and the results copied back every step.
+
+Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+N > 1 runs under torch.distributed.run: every rank advances its own replica
+(the path has no data exchange between GPUs), value = all ranks' cell-levels
+/ max-over-ranks time.
+
+``--impl reference`` times the reference algorithm's CPU restatement (the
+oracle) on the host cores, one worker process per core, each step a bounded
+sample (one C24 L79 substep per worker).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_CELL_LEVEL = 272  # compulsory FP64 state traffic per cell-level per substep (34 x 8 B)
+METRIC = "C384 L79 acoustic-substep cell-levels/s"
+UNIT = "cell-levels/s"
+
+
+def _env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def _measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        smax = [num(r[2]) for r in rows if num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- workload
+def build_problem(n, npz, n_split, seed, device="cuda"):
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from fv3core_b200 import _lib
+    from fv3core_b200.config import baroclinic_acoustic_config
+    from fv3core_b200.grid import CubedSphereGrid
+    from fv3core_b200.grid_data import GridData
+    from fv3core_b200.halo import DeviceCubedSphereCommunicator
+    from fv3core_b200.initial_state import baroclinic_state
+    from fv3core_b200.stencil import StencilConfig, StencilFactory
+    from fv3core_b200.stencils.dyn_core import AcousticDynamics
+    from fv3core_b200.storage import to_device
+
+    grid = CubedSphereGrid(n, 3)
+    st = baroclinic_state(grid, npz, seed=seed)
+    gd = GridData(grid, npz, device=device)
+    sf = StencilFactory(StencilConfig(), gd.grid_indexing)
+    cfg = baroclinic_acoustic_config(n_split=n_split)
+    import types
+
+    state = types.SimpleNamespace()
+    for name in _lib.DYCORE_FIELDS:
+        a = st[name] if name in st else None
+        if a is None:
+            state_shape = st["delp"].shape if name not in ("wsd",) else st["phis"].shape
+            import numpy as np
+
+            a = np.zeros(state_shape)
+        setattr(state, name, to_device(a))
+        if name in st:
+            del st[name]
+    ad = AcousticDynamics(DeviceCubedSphereCommunicator(gd.grid_indexing), sf, gd, gd, 0, False, False, cfg,
+                          st["ak"], st["bk"], st["pfull"], state.phis)
+    state.mdt = 225.0
+    state.n_map = 1
+    state.akap = 287.05 / 1004.6
+    state.ptop = st["ptop"]
+    state.ks = st["ks"]
+    torch.cuda.synchronize()
+    return gd, ad, state
+
+
+# fields AcousticDynamics reads (copied in for the end-to-end timing) and writes (copied out)
+E2E_IN = ("u", "v", "w", "delz", "delp", "pt", "pe", "pk", "phis", "wsd", "omga", "ua", "va", "uc", "vc", "pkz",
+          "peln", "q_con", "diss_estd", "cappa")
+E2E_OUT = ("u", "v", "w", "delz", "delp", "pt", "pe", "pk", "wsd", "omga", "ua", "va", "uc", "vc", "mfxd", "mfyd",
+           "cxd", "cyd", "pkz", "peln", "q_con", "diss_estd")
+
+
+def run_cuda(args):
+    import torch
+
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from fv3core_b200 import _lib
+
+    n, npz, n_split = args.n, args.npz, args.n_split
+    gd, ad, state = build_problem(n, npz, n_split, seed=1234 + rank)
+    stream = torch.cuda.current_stream()
+    cells = 6 * n * n * npz
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        ad(state)
+    barrier()
+    launches0 = _lib.launch_count()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        start.record(stream)
+        for _ in range(args.steps):
+            ad(state)
+        stop.record(stream)
+        barrier()
+    launches = _lib.launch_count() - launches0
+    ms = start.elapsed_time(stop) / args.steps
+    clocks = clk.summary()
+    finite = bool(torch.isfinite(state.delp).all().item() and torch.isfinite(state.u).all().item())
+
+    # end to end through the public API: pinned host state in, results out, every step
+    host = {k: torch.empty(getattr(state, k).shape, dtype=torch.float64, pin_memory=True)
+            for k in set(E2E_IN) | set(E2E_OUT)}
+    for k, h in host.items():
+        h.copy_(getattr(state, k))
+    torch.cuda.synchronize()
+    h2d = sum(host[k].numel() * 8 for k in E2E_IN)
+    d2h = sum(host[k].numel() * 8 for k in E2E_OUT)
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    for _ in range(1):  # one untimed warm-up round trip
+        for k in E2E_IN:
+            getattr(state, k).copy_(host[k], non_blocking=True)
+        ad(state)
+        for k in E2E_OUT:
+            host[k].copy_(getattr(state, k), non_blocking=True)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        for k in E2E_IN:
+            getattr(state, k).copy_(host[k], non_blocking=True)
+        ad(state)
+        for k in E2E_OUT:
+            host[k].copy_(getattr(state, k), non_blocking=True)
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+
+    # max over ranks
+    if dist is not None:
+        t = torch.tensor([ms, e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    value = world * cells * n_split / (ms * 1e-3)
+    e2e_value = world * cells * n_split / (e2e_ms * 1e-3)
+    peak, peak_kind = _measured_peak()
+    achieved = BYTES_PER_CELL_LEVEL * cells * n_split / (ms * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded baroclinic-wave state)",
+        "config": {
+            "workload": f"AcousticDynamics C{n} L{npz}, n_split={n_split}, 6 tiles on one GPU, FP64, nonhydrostatic",
+            "n": n, "npz": npz, "n_split": n_split, "dt_atmos": 225.0, "cell_levels": cells,
+            "l2": "inputs larger than L2 (each 3-D field 0.59 GB at C384 L79); no flush",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        },
+        "clocks": clocks,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_ms, "steps": e2e_steps},
+        "gpu_launches": launches,
+        "roofline": {
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "peak_source": peak_kind,
+            "scope": "whole AcousticDynamics call: 272 B compulsory traffic per cell-level per substep",
+        },
+        "finite": finite,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample(1, args.cpu_n, args.cpu_npz)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    gd.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------- CPU oracle
+def _oracle_worker(n, npz, seed, q):
+    """One bounded sample: one acoustic substep of the oracle on a C{n} L{npz}
+    case; returns (cell-level-substeps, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import numpy as np
+
+    import cases
+    from oracle.dyn_core import AcousticDynamics
+
+    case = cases.acoustics_case(n, npz, seed, n_split=1)
+    g = cases.grid_for(n)
+    cfg = {**cases.ACOUSTIC_CONFIG, **cases.RIEMANN_CONFIG, "n_split": 1, "dsw": cases.DSW_CONFIG}
+    metrics = [cases.metric_namespace(n, t) for t in range(6)]
+    ad = AcousticDynamics(g, metrics, cfg, case["ak"], case["bk"], case["pfull"], case["phis"], npz)
+    st = {k: (np.array(v, copy=True) if isinstance(v, np.ndarray) else v) for k, v in case.items()}
+    t0 = time.perf_counter()
+    with np.errstate(all="ignore"):
+        ad(st)
+    q.put((6 * n * n * npz, time.perf_counter() - t0))
+
+
+def cpu_sample(workers, n, npz, repeats=1):
+    """Oracle throughput (cell-levels/s per substep) with `workers` processes."""
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    total_cells, total_time = 0, 0.0
+    for r in range(repeats):
+        q = ctx.Queue()
+        procs = [ctx.Process(target=_oracle_worker, args=(n, npz, 7 + w + 100 * r, q)) for w in range(workers)]
+        for p in procs:
+            p.start()
+        res = [q.get() for _ in procs]
+        for p in procs:
+            p.join()
+        total_cells += sum(c for c, _ in res)
+        total_time += max(s for _, s in res)
+    value = total_cells / total_time
+    return {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
+            "sample": f"{repeats} x {workers} worker(s), each one acoustic substep of C{n} L{npz} (numpy FP64 oracle)"}
+
+
+def run_reference(args):
+    rank, world, _ = _env_rank()
+    if rank != 0:
+        return
+    try:
+        import psutil
+
+        mem_workers = int(psutil.virtual_memory().available // (3 << 30))
+    except Exception:
+        mem_workers = os.cpu_count() or 1
+    workers = max(1, min(os.cpu_count() or 1, mem_workers, args.ref_max_workers))
+    for _ in range(args.warmup):
+        cpu_sample(workers, args.ref_n, args.npz)
+    t0 = time.perf_counter()
+    samples = [cpu_sample(workers, args.ref_n, args.npz) for _ in range(args.steps)]
+    wall = time.perf_counter() - t0
+    value = statistics.median(s["value"] for s in samples)
+    cells_step = 6 * args.ref_n * args.ref_n * args.npz * workers
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * cells_step / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded baroclinic-wave state)",
+        "impl": "reference",
+        "config": {"workload": f"AcousticDynamics C{args.n} L{args.npz} (sampled at C{args.ref_n} L{args.npz}, "
+                               f"one substep per worker per step)", "n": args.n, "npz": args.npz},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
+                         "sample": samples[0]["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": wall,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
+    ap.add_argument("--n", type=int, default=384)
+    ap.add_argument("--npz", type=int, default=79)
+    ap.add_argument("--n-split", type=int, default=6)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-n", type=int, default=48, help="resolution of the CPU baseline sample")
+    ap.add_argument("--cpu-npz", type=int, default=79)
+    ap.add_argument("--ref-n", type=int, default=24, help="resolution of the reference arm's per-worker sample")
+    ap.add_argument("--ref-max-workers", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be at least 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_cuda(args)
+
+
+if __name__ == "__main__":
+    main()

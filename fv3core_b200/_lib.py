@@ -97,6 +97,8 @@ def lib():
         L = ctypes.CDLL(LIB_PATH)
         L.fv3b_last_error.restype = ctypes.c_char_p
         L.fv3b_version.restype = ctypes.c_char_p
+        L.fv3b_launch_count.restype = ctypes.c_longlong
+        L.fv3b_launch_count.argtypes = []
         for name, args in SIGNATURES.items():
             if args is None:
                 continue
@@ -130,6 +132,11 @@ def call_ctx(name, ctx, *args):
 
 
 def exported_symbols():
-    return ["fv3b_last_error", "fv3b_version", "fv3b_ctx_create", "fv3b_ctx_destroy"] + [
+    return ["fv3b_last_error", "fv3b_version", "fv3b_launch_count", "fv3b_ctx_create", "fv3b_ctx_destroy"] + [
         k for k, v in SIGNATURES.items() if v is not None
     ] + list(CTX_SIGNATURES) + list(PTR_SIGNATURES)
+
+
+def launch_count():
+    """Kernel launches issued by the library so far."""
+    return int(lib().fv3b_launch_count())

@@ -34,6 +34,10 @@ __global__ void box_kernel(Box b, F f) {
   if (i < b.i1 && j < b.j1) f(t, i, j, k);
 }
 
+// Counts kernel launches of this library (host side, all threads); read
+// through fv3b_launch_count().
+void note_launch();
+
 template <typename F>
 cudaError_t launch_box(const Box& b, cudaStream_t s, F f) {
   int ni = b.i1 - b.i0, nj = b.j1 - b.j0, nk = b.k1 - b.k0;
@@ -41,6 +45,7 @@ cudaError_t launch_box(const Box& b, cudaStream_t s, F f) {
   dim3 block(32, 4, 1);
   dim3 grid((ni + 31) / 32, (nj + 3) / 4, 6 * nk);
   box_kernel<<<grid, block, 0, s>>>(b, f);
+  note_launch();
   return cudaGetLastError();
 }
 
@@ -63,6 +68,7 @@ cudaError_t launch_columns(int i0, int i1, int j0, int j1, cudaStream_t s, F f, 
   if (ncol <= 0) return cudaSuccess;
   dim3 grid((ncol + block - 1) / block, 6, 1);
   column_kernel<<<grid, block, 0, s>>>(i0, i1, j0, j1, f);
+  note_launch();
   return cudaGetLastError();
 }
 

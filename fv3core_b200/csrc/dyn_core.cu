@@ -45,6 +45,7 @@ __global__ void fill_kernel(double* p, long long n, double v) {
 cudaError_t fill(double* p, long long n, double v, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   fill_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, n, v);
+  note_launch();
   return cudaGetLastError();
 }
 

@@ -76,6 +76,7 @@ cudaError_t halo_scalars(const Dims& d, double* const* fields, int nfields, int 
     fs.n = nfields - f0 < 4 ? nfields - f0 : 4;
     for (int q = 0; q < fs.n; ++q) fs.f[q] = fields[f0 + q];
     halo_scalar_kernel<<<grid, HALO_BLOCK, 0, st>>>(d, fs, stagger, stagger, n_halo, nlev);
+    note_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
@@ -86,12 +87,14 @@ cudaError_t halo_vector(const Dims& d, double* x, double* y, bool cgrid, int nle
   const int nc = halo_candidates(d, d.h);
   dim3 grid((nc + HALO_BLOCK - 1) / HALO_BLOCK, 12);
   halo_vector_kernel<<<grid, HALO_BLOCK, 0, st>>>(d, x, y, cgrid ? 1 : 0, nlev);
+  note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t sync_vector_interfaces(const Dims& d, double* u, double* v, int nlev, cudaStream_t st) {
   dim3 grid((d.n + HALO_BLOCK - 1) / HALO_BLOCK, 12);
   interface_sync_kernel<<<grid, HALO_BLOCK, 0, st>>>(d, u, v, nlev);
+  note_launch();
   return cudaGetLastError();
 }
 

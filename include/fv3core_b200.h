@@ -124,6 +124,10 @@ const char* fv3b_last_error(void);
 /* Library version string. */
 const char* fv3b_version(void);
 
+/* Number of kernel launches this library has issued since it was loaded
+ * (diagnostic; all host threads). */
+long long fv3b_launch_count(void);
+
 /*
  * RiemannSolverC.__call__  (fv3core/stencils/riem_solver_c.py:106-165,
  * with Sim1Solver, fv3core/stencils/sim1_solver.py:11-175).

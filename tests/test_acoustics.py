@@ -106,7 +106,9 @@ def test_gpu_against_numpy_transcendentals():
 
 @pytest.mark.gpu
 def test_gpu_full_storage_matches_oracle():
-    """Every point of every field, halos included, on the golden case."""
+    """Every point of every field, halos included, on the golden case,
+    except where the oracle holds NaN: those are points the reference never
+    writes (its storages there keep whatever memory held)."""
     import gpu_runs
     from oracle import _math
 
@@ -117,7 +119,8 @@ def test_gpu_full_storage_matches_oracle():
     gpu = gpu_runs.run_acoustics(case, n, nz)
     bad = {}
     for k in gpu:
-        e = parity_err(gpu[k], ref[k])
+        defined = ~np.isnan(ref[k])
+        e = parity_err(gpu[k][defined], ref[k][defined])
         if not e <= 1e-12:
             bad[k] = e
     assert not bad, bad
