@@ -12,19 +12,9 @@ constexpr double C1 = 2.0 / 3.0, C2 = -1.0 / 6.0;
 constexpr double B1 = 7.0 / 12.0, B2 = -1.0 / 12.0;
 constexpr double A1 = 9.0 / 16.0, A2 = -1.0 / 16.0;
 
-// great_circle_dist / extrap_corner (a2b_ord4.py:38-57)
-__device__ __forceinline__ double gcd(double p1a, double p1b, double p2a, double p2b) {
-  double sb = sin((p1b - p2b) / 2.0);
-  double sa = sin((p1a - p2a) / 2.0);
-  double tb = sb * sb, ta = sa * sa;
-  return asin(sqrt(tb + cos(p1b) * cos(p2b) * ta)) * 2.0;
-}
-__device__ __forceinline__ double extrap(double p0a, double p0b, double p1a, double p1b, double p2a, double p2b,
-                                         double qa, double qb) {
-  double x1 = gcd(p1a, p1b, p0a, p0b);
-  double x2 = gcd(p2a, p2b, p0a, p0b);
-  return qa + x1 / (x2 - x1) * (qa - qb);
-}
+// extrap_corner (a2b_ord4.py:45-57) with the grid-only ratio x1 / (x2 - x1)
+// of its great-circle distances precomputed (fv3b_metrics.a2b_extrap)
+__device__ __forceinline__ double extrap(double ratio, double qa, double qb) { return qa + ratio * (qa - qb); }
 
 // ppm_volume_mean edge formulas (a2b_ord4.py:340-451) along one axis; L(o)
 // reads qin at offset o, G(o) the A-grid spacing.
@@ -99,12 +89,12 @@ inline cudaError_t a2b_ord4(const Dims d, const fv3b_metrics g, double* qin, dou
         int oo[3][4] = {{0, -1, 1, -2}, {-1, -1, -2, -2}, {0, 0, 1, 1}};
         memcpy(o, oo, sizeof(o));
       }
-      double b1 = F2(g.bgrid1, i, j), b2 = F2(g.bgrid2, i, j);
+      const int corner = (wcol && srow) ? 0 : (ecol && srow) ? 1 : (ecol && nrow) ? 2 : 3;
+      const double* ratio = g.a2b_extrap + (t * 4 + corner) * 3;
       double ec[3];
       for (int m = 0; m < 3; ++m) {
         int i1 = i + o[m][0], j1 = j + o[m][1], i2 = i + o[m][2], j2 = j + o[m][3];
-        ec[m] = extrap(b1, b2, F2(g.agrid1, i1, j1), F2(g.agrid2, i1, j1), F2(g.agrid1, i2, j2),
-                       F2(g.agrid2, i2, j2), F3(qin, i1, j1), F3(qin, i2, j2));
+        ec[m] = extrap(ratio[m], F3(qin, i1, j1), F3(qin, i2, j2));
       }
       v = (ec[0] + ec[1] + ec[2]) * (1.0 / 3.0);
     } else if (wcol || ecol) {

@@ -1,11 +1,13 @@
 // exp, log and pow for the FP64 kernels, written from the mathematics so
 // that the same source compiles for the device and for the host (the
-// oracle's C helper includes this header).  Built without a*b+c contraction
-// on both sides (nvcc --fmad=false, gcc -ffp-contract=off), the host and
-// device results are bit-identical, which lets the kernels be checked
-// against the oracle to the last bit even where the substep amplifies
-// last-place differences of these functions (the Riemann solvers subtract
-// the hydrostatic pressure from exp(...) of the full pressure).
+// oracle's C helper includes this header).  Built without implicit a*b+c
+// contraction on both sides (nvcc --fmad=false, gcc -ffp-contract=off) and
+// with every fused multiply-add written out as fma() (exactly rounded in
+// IEEE 754 on both the GPU and the host), the host and device results are
+// bit-identical.  That lets the kernels be checked against the oracle to
+// the last bit even where the substep amplifies last-place differences of
+// these functions (the Riemann solvers subtract the hydrostatic pressure
+// from exp(...) of the full pressure).
 //
 // Methods:
 //   exp: Cody-Waite reduction x = k ln2 + r (ln2 split into a 32-bit head
@@ -19,7 +21,7 @@
 //        (the identity f - 2s = s f gives this form); e ln2 + f - f^2/2
 //        summed in double-double.
 //   pow: exp(y log x) with log x and y log x in double-double.
-// Double-double steps use Knuth's TwoSum and Dekker's product (no FMA).
+// Double-double steps use Knuth's TwoSum and the fma-based exact product.
 // Accuracy (tested on the host against correctly rounded values): all
 // three within 1 ulp, correctly rounded in all but a small fraction of
 // cases on the ranges the substep uses.
@@ -70,24 +72,16 @@ __host__ __device__ __forceinline__ double round_half_even(double x) {
 #endif
 }
 
-// Error-free transformations (Knuth TwoSum, Dekker's splitting product):
-// a + b = s + e and a * b = p + e exactly, without fused multiply-add.
+// Error-free transformations: a + b = s + e (Knuth's TwoSum) and
+// a * b = p + e (the exact product from one fused multiply-add).
 __host__ __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
   s = a + b;
   double bb = s - a;
   e = (a - (s - bb)) + (b - bb);
 }
-__host__ __device__ __forceinline__ void split(double a, double& hi, double& lo) {
-  double c = 134217729.0 * a;  // 2^27 + 1
-  hi = c - (c - a);
-  lo = a - hi;
-}
 __host__ __device__ __forceinline__ void two_prod(double a, double b, double& p, double& e) {
   p = a * b;
-  double ah, al, bh, bl;
-  split(a, ah, al);
-  split(b, bh, bl);
-  e = ((ah * bh - p) + ah * bl + al * bh) + al * bl;
+  e = fma(a, b, -p);
 }
 
 // exp(rh + rl) for |rh| <= ln2/2 + tiny, |rl| << ulp(rh):
@@ -96,19 +90,19 @@ __host__ __device__ __forceinline__ void two_prod(double a, double b, double& p,
 // the only rounding of size ~ulp left is the last one.
 __host__ __device__ __forceinline__ double exp_reduced(double rh, double rl) {
   double q = 1.0 / 6227020800.0;
-  q = q * rh + 1.0 / 479001600.0;
-  q = q * rh + 1.0 / 39916800.0;
-  q = q * rh + 1.0 / 3628800.0;
-  q = q * rh + 1.0 / 362880.0;
-  q = q * rh + 1.0 / 40320.0;
-  q = q * rh + 1.0 / 5040.0;
-  q = q * rh + 1.0 / 720.0;
-  q = q * rh + 1.0 / 120.0;
-  q = q * rh + 1.0 / 24.0;
-  q = q * rh + 1.0 / 6.0;
+  q = fma(q, rh, 1.0 / 479001600.0);
+  q = fma(q, rh, 1.0 / 39916800.0);
+  q = fma(q, rh, 1.0 / 3628800.0);
+  q = fma(q, rh, 1.0 / 362880.0);
+  q = fma(q, rh, 1.0 / 40320.0);
+  q = fma(q, rh, 1.0 / 5040.0);
+  q = fma(q, rh, 1.0 / 720.0);
+  q = fma(q, rh, 1.0 / 120.0);
+  q = fma(q, rh, 1.0 / 24.0);
+  q = fma(q, rh, 1.0 / 6.0);
   double r2h, r2l;
   two_prod(rh, rh, r2h, r2l);
-  const double small = 0.5 * r2l + (r2h * rh) * q + rl * (1.0 + rh);  // + exp'(r) rl
+  const double small = fma(r2h * rh, q, fma(rl, 1.0 + rh, 0.5 * r2l));  // + exp'(r) rl
   double s1, e1, sh, sl;
   two_sum(rh, 0.5 * r2h, s1, e1);
   two_sum(s1, e1 + small, sh, sl);
@@ -131,7 +125,7 @@ __host__ __device__ __forceinline__ double exp_dd(double xh, double xl) {
   const double kd = round_half_even(xh * LOG2E);
   const int k = (int)kd;
   const double t = xh - kd * LN2_HI;  // exact: kd * LN2_HI has <= 43 bits and is close to xh
-  const double c = kd * LN2_LO - xl;
+  const double c = fma(kd, LN2_LO, -xl);
   double rh = t - c;
   double rl = (t - rh) - c;
   return scale2(exp_reduced(rh, rl), k);
@@ -159,16 +153,16 @@ __host__ __device__ __forceinline__ void log_dd(double x, double& hi, double& lo
   const double z = s * s;
   // R = sum_{k=1..11} 2 z^k / (2k + 1)
   double R = 2.0 / 23.0;
-  R = R * z + 2.0 / 21.0;
-  R = R * z + 2.0 / 19.0;
-  R = R * z + 2.0 / 17.0;
-  R = R * z + 2.0 / 15.0;
-  R = R * z + 2.0 / 13.0;
-  R = R * z + 2.0 / 11.0;
-  R = R * z + 2.0 / 9.0;
-  R = R * z + 2.0 / 7.0;
-  R = R * z + 2.0 / 5.0;
-  R = R * z + 2.0 / 3.0;
+  R = fma(R, z, 2.0 / 21.0);
+  R = fma(R, z, 2.0 / 19.0);
+  R = fma(R, z, 2.0 / 17.0);
+  R = fma(R, z, 2.0 / 15.0);
+  R = fma(R, z, 2.0 / 13.0);
+  R = fma(R, z, 2.0 / 11.0);
+  R = fma(R, z, 2.0 / 9.0);
+  R = fma(R, z, 2.0 / 7.0);
+  R = fma(R, z, 2.0 / 5.0);
+  R = fma(R, z, 2.0 / 3.0);
   R = R * z;
   // log x = e ln2 + f - f^2/2 + s (f^2/2 + R); e*LN2_HI, f and f^2/2 (from
   // the exact square) are carried without rounding, the small rest rounded
@@ -176,7 +170,7 @@ __host__ __device__ __forceinline__ void log_dd(double x, double& hi, double& lo
   two_prod(f, f, sqh, sql);
   const double hfh = 0.5 * sqh, hfl = 0.5 * sql;  // exact halving
   const double dk = (double)e;
-  const double small = s * (hfh + R) + dk * LN2_LO - hfl;
+  const double small = fma(s, hfh + R, fma(dk, LN2_LO, -hfl));
   double a, ae, b, be;
   two_sum(dk * LN2_HI, f, a, ae);
   two_sum(a, -hfh, b, be);
@@ -205,7 +199,7 @@ __host__ __device__ __forceinline__ double fm_pow(double x, double y) {
   log_dd(x, lh, ll);
   double ph, pl;
   two_prod(y, lh, ph, pl);
-  pl = pl + y * ll;
+  pl = fma(y, ll, pl);
   double zh, zl;
   two_sum(ph, pl, zh, zl);
   return exp_dd(zh, zl);

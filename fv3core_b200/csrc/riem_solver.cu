@@ -3,10 +3,13 @@
 //
 // One thread owns one (tile, i, j) column and walks it top to bottom and
 // back; neighbouring threads own neighbouring i, so every level load/store
-// is a coalesced row access.  Column work arrays live in per-thread local
-// memory (thread-interleaved, so also coalesced); MAXK bounds the number of
-// interface levels.  exp and log are the library's own (fmath.h), whose
-// host build the oracle uses, so results can be compared to the last bit.
+// is a coalesced row access.  Only five per-level work arrays stay in the
+// thread's local memory (pem, pm, pp/pe, gam, w); everything else is
+// re-read from the input fields or computed on the fly, and the outputs are
+// written in the same bottom-up pass that produces them.  The arrays are
+// sized by a compile-time level bucket >= npz+1, so an L79 column keeps 3 KB.
+// exp and log are the library's own (fmath.h), whose host build the oracle
+// uses, so results can be compared to the last bit.
 #include <math.h>
 
 #include "common.cuh"
@@ -20,84 +23,240 @@ constexpr double RGRAV = 1.0 / GRAV;
 constexpr double KAPPA = RDGAS / 1004.6;
 constexpr int MAXK = 128;
 
-// Sim1 solve on one column (reference fv3core/stencils/sim1_solver.py:11-101).
-// K = number of interface levels (npz + 1).  On entry: dm (delta p / g),
-// w (vertical velocity, kept as w1), dz (layer depth, negative), pem (edge
-// pressure), pm (layer mean pressure); gm, ptr, cp3 come from the lambdas
-// (per level).  On exit: w (levels 0..K-2), pe (0..K-1, pressure
-// perturbation), dz (0..K-2).
-template <typename GM, typename PTR, typename CP3>
-__device__ __forceinline__ void sim1_column(int K, const double* dm, double* w, double* w1, double* dz,
-                                            const double* pem, const double* pm, double* pe, double* pp,
-                                            double* gam, double* aa, GM gm, PTR ptr, CP3 cp3, double wsr,
-                                            double dt, double t1g, double rdt, double p_fac) {
-  // pe = exp(gm*log(-dm/dz*Rd*ptr)) - pm   (sim1_solver.py:27-29)
-  for (int k = 0; k < K - 1; ++k) {
-    pe[k] = fm::fm_exp(gm(k) * fm::fm_log(-dm[k] / dz[k] * RDGAS * ptr(k))) - pm[k];
-    w1[k] = w[k];
-  }
+// Per-column inputs of the Sim1 solve (fv3core/stencils/sim1_solver.py:11-101).
+// K = number of interface levels (npz + 1).  DM(k): delta p / g; W1(k): w
+// at the start; DZ(k): layer depth at the start (negative); GM, PTR, CP3:
+// 1/(1-cappa), pt, cappa per level; pem, pm: edge pressure and layer-mean
+// pressure.  Results: w[0..K-2] (new w), pe[0..K-1] (pressure perturbation,
+// delivered through PE_OUT(k, value) in increasing k) and the new layer
+// depths through DZ_OUT(k, value) for k = K-2 .. 0 (bottom up).
+template <int NK, typename DMF, typename W1F, typename DZF, typename GMF, typename PTRF, typename CP3F,
+          typename PEOUT, typename DZOUT>
+__device__ __forceinline__ void sim1_column(int K, DMF DM, W1F W1, DZF DZ, GMF GM, PTRF PTR, CP3F CP3,
+                                            const double* pem, const double* pm, double* pp, double* gam, double* w,
+                                            double wsr, double dt, double t1g, double rdt, double p_fac,
+                                            PEOUT PE_OUT, DZOUT DZ_OUT) {
+  // pe = exp(gm*log(-dm/dz*Rd*ptr)) - pm   (sim1_solver.py:27-29), on the fly
+  auto pe1 = [&](int k) { return fm::fm_exp(GM(k) * fm::fm_log(-DM(k) / DZ(k) * RDGAS * PTR(k))) - pm[k]; };
   // forward elimination of the pressure system (sim1_solver.py:30-59)
-  double bb0 = (K - 2 > 0) ? 2.0 * (1.0 + dm[0] / dm[1]) : 2.0;
+  double pe_k = pe1(0);
+  double pe_k1 = pe1(1);
+  double bb0 = (K - 2 > 0) ? 2.0 * (1.0 + DM(0) / DM(1)) : 2.0;
   pp[0] = 0.0;
-  pp[1] = (K > 2 ? 3.0 * (pe[0] + (dm[0] / dm[1]) * pe[1]) : 3.0 * pe[0]) / bb0;
+  pp[1] = (K > 2 ? 3.0 * (pe_k + (DM(0) / DM(1)) * pe_k1) : 3.0 * pe_k) / bb0;
   double bet = bb0;
   for (int k = 1; k <= K - 2; ++k) {
-    double grm = dm[k - 1] / dm[k];
+    pe_k = pe_k1;
+    double grm = DM(k - 1) / DM(k);
     double g = grm / bet;
     double bbk, ddk;
     if (k < K - 2) {
-      double grk = dm[k] / dm[k + 1];
+      pe_k1 = pe1(k + 1);
+      double grk = DM(k) / DM(k + 1);
       bbk = 2.0 * (1.0 + grk);
-      ddk = 3.0 * (pe[k] + grk * pe[k + 1]);
+      ddk = 3.0 * (pe_k + grk * pe_k1);
     } else {
       bbk = 2.0;
-      ddk = 3.0 * pe[k];
+      ddk = 3.0 * pe_k;
     }
     gam[k] = g;
     bet = bbk - g;
     pp[k + 1] = (ddk - pp[k]) / bet;
   }
-  // back substitution and w coefficients (sim1_solver.py:60-63)
-  for (int k = K - 2; k >= 1; --k) {
-    pp[k] = pp[k] - gam[k] * pp[k + 1];
-    aa[k] = t1g * 0.5 * (gm(k - 1) + gm(k)) / (dz[k - 1] + dz[k]) * (pem[k] + pp[k]);
-  }
+  // back substitution (sim1_solver.py:60-63)
+  for (int k = K - 2; k >= 1; --k) pp[k] = pp[k] - gam[k] * pp[k + 1];
+  auto AA = [&](int k) { return t1g * 0.5 * (GM(k - 1) + GM(k)) / (DZ(k - 1) + DZ(k)) * (pem[k] + pp[k]); };
   // w solve (sim1_solver.py:65-90)
-  bet = dm[0] - aa[1];
-  w[0] = (dm[0] * w1[0] + dt * pp[1]) / bet;
+  double aak = AA(1);
+  bet = DM(0) - aak;
+  w[0] = (DM(0) * W1(0) + dt * pp[1]) / bet;
   for (int k = 1; k <= K - 3; ++k) {
-    double g = aa[k] / bet;
+    double aak1 = AA(k + 1);
+    double g = aak / bet;
     gam[k] = g;
-    bet = dm[k] - (aa[k] + aa[k + 1] + aa[k] * g);
-    w[k] = (dm[k] * w1[k] + dt * (pp[k + 1] - pp[k]) - aa[k] * w[k - 1]) / bet;
+    bet = DM(k) - (aak + aak1 + aak * g);
+    w[k] = (DM(k) * W1(k) + dt * (pp[k + 1] - pp[k]) - aak * w[k - 1]) / bet;
+    aak = aak1;
   }
   {
     int k = K - 2;
-    double p1 = t1g * gm(k) / dz[k] * (pem[k + 1] + pp[k + 1]);
-    double g = aa[k] / bet;
+    double p1 = t1g * GM(k) / DZ(k) * (pem[k + 1] + pp[k + 1]);
+    double g = aak / bet;
     gam[k] = g;
-    bet = dm[k] - (aa[k] + p1 + aa[k] * g);
-    w[k] = (dm[k] * w1[k] + dt * (pp[k + 1] - pp[k]) - p1 * wsr - aa[k] * w[k - 1]) / bet;
+    bet = DM(k) - (aak + p1 + aak * g);
+    w[k] = (DM(k) * W1(k) + dt * (pp[k + 1] - pp[k]) - p1 * wsr - aak * w[k - 1]) / bet;
   }
   for (int k = K - 3; k >= 0; --k) w[k] = w[k] - gam[k + 1] * w[k + 1];
-  // pressure perturbation from the w change (sim1_solver.py:91-95)
+  // pressure perturbation from the w change (sim1_solver.py:91-95); pp's
+  // storage is reused for it
+  double* pe = pp;
   pe[0] = 0.0;
-  for (int k = 1; k < K; ++k) pe[k] = pe[k - 1] + dm[k - 1] * (w[k - 1] - w1[k - 1]) * rdt;
-  // layer-mean perturbation and new dz (sim1_solver.py:96-105)
+  PE_OUT(0, 0.0);
+  for (int k = 1; k < K; ++k) {
+    pe[k] = pe[k - 1] + DM(k - 1) * (w[k - 1] - W1(k - 1)) * rdt;
+    PE_OUT(k, pe[k]);
+  }
+  // layer-mean perturbation and new dz (sim1_solver.py:96-105), bottom up
   double p1n = 0.0;
   for (int k = K - 2; k >= 0; --k) {
     double p1;
     if (k == K - 2) {
       p1 = (pe[k] + 2.0 * pe[k + 1]) * 1.0 / 3.0;
     } else {
-      double gr = dm[k] / dm[k + 1];
+      double gr = DM(k) / DM(k + 1);
       double bbk = 2.0 * (1.0 + gr);
       p1 = (pe[k] + bbk * pe[k + 1] + gr * pe[k + 2]) * 1.0 / 3.0 - gr * p1n;
     }
     p1n = p1;
-    double maxp = (p_fac * dm[k] > p1 + pm[k]) ? p_fac * pm[k] : p1 + pm[k];
-    dz[k] = -dm[k] * RDGAS * ptr(k) * fm::fm_exp((cp3(k) - 1.0) * fm::fm_log(maxp));
+    double maxp = (p_fac * DM(k) > p1 + pm[k]) ? p_fac * pm[k] : p1 + pm[k];
+    DZ_OUT(k, -DM(k) * RDGAS * PTR(k) * fm::fm_exp((CP3(k) - 1.0) * fm::fm_log(maxp)));
   }
+}
+
+struct RiemCArgs {
+  double dt2, ptop, p_fac;
+  const double *cappa, *hs, *ws, *ptc, *q_con, *delpc;
+  double *gz, *pef;
+  const double* w3;
+};
+
+// RiemannSolverC.__call__ body for one column (riem_solver_c.py:13-64)
+template <int NK>
+struct RiemC {
+  static __device__ __forceinline__ void run(const Dims& d, int t, int i, int j, const RiemCArgs& a) {
+    const double dt2 = a.dt2, ptop = a.ptop, p_fac = a.p_fac;
+    const double *cappa = a.cappa, *hs = a.hs, *ws = a.ws, *ptc = a.ptc, *q_con = a.q_con, *delpc = a.delpc;
+    double *gz = a.gz, *pef = a.pef;
+    const double* w3 = a.w3;
+    double pem[NK], pm[NK], pp[NK], gam[NK], w[NK];
+    const int K = d.nk;
+    const long long o0 = idx3(d, t, i, j, 0);
+    const long long sk = d.sk;
+    const double t1g = 2.0 * dt2 * dt2;
+    const double rdt = 1.0 / dt2;
+    // precompute (riem_solver_c.py:13-44)
+    double pem_k = ptop, peg_k = ptop;
+    for (int k = 0; k < K; ++k) {
+      const double dmk = delpc[o0 + k * sk];
+      pem[k] = pem_k;
+      const double peg_next = peg_k + dmk * (1.0 - q_con[o0 + k * sk]);
+      if (k < K - 1) pm[k] = (peg_next - peg_k) / fm::fm_log(peg_next / peg_k);
+      pem_k = pem_k + dmk;
+      peg_k = peg_next;
+    }
+    auto DM = [&](int k) { return delpc[o0 + k * sk] / GRAV; };
+    auto W1 = [&](int k) { return w3[o0 + k * sk]; };
+    auto DZ = [&](int k) { return gz[o0 + (k + 1) * sk] - gz[o0 + k * sk]; };
+    auto GM = [&](int k) { return 1.0 / (1.0 - cappa[o0 + k * sk]); };
+    auto PTR = [&](int k) { return ptc[o0 + k * sk]; };
+    auto CP3 = [&](int k) { return cappa[o0 + k * sk]; };
+    // finalize (riem_solver_c.py:46-64) fused with the solve's outputs; gz
+    // is rewritten bottom up only after its last read as an input
+    auto PE_OUT = [&](int k, double pe) { pef[o0 + k * sk] = k == 0 ? ptop : pe + pem[k]; };
+    double g = hs[idx2(d, t, i, j)];
+    auto DZ_OUT = [&](int k, double dz) {
+      if (k == K - 2) gz[o0 + (K - 1) * sk] = g;
+      g = g - dz * GRAV;
+      gz[o0 + k * sk] = g;
+    };
+    sim1_column<NK>(K, DM, W1, DZ, GM, PTR, CP3, pem, pm, pp, gam, w, ws[idx2(d, t, i, j)], dt2, t1g, rdt, p_fac,
+                    PE_OUT, DZ_OUT);
+  }
+};
+
+struct Riem3Args {
+  bool last;
+  double dt, ptop, p_fac, peln1, ptk;
+  const double *cappa, *zs, *wsd;
+  double* delz;
+  const double *q_con, *delp, *pt;
+  double *zh, *pe, *ppe, *pk3, *pk, *peln, *w;
+};
+
+// RiemannSolver3.__call__ body for one column (riem_solver3.py:24-103)
+template <int NK>
+struct Riem3 {
+  static __device__ __forceinline__ void run(const Dims& d, int t, int i, int j, const Riem3Args& a) {
+    const bool last = a.last;
+    const double dt = a.dt, ptop = a.ptop, p_fac = a.p_fac, peln1 = a.peln1, ptk = a.ptk;
+    const double *cappa = a.cappa, *zs = a.zs, *wsd = a.wsd, *q_con = a.q_con, *delp = a.delp, *pt = a.pt;
+    double *delz = a.delz, *zh = a.zh, *pe = a.pe, *ppe = a.ppe, *pk3 = a.pk3, *pk = a.pk, *peln = a.peln;
+    double* w_io = a.w;
+    double pem[NK], pm[NK], pp[NK], gam[NK], w[NK];
+    const int K = d.nk;
+    const long long o0 = idx3(d, t, i, j, 0);
+    const long long sk = d.sk;
+    const double t1g = 2.0 * dt * dt;
+    const double rdt = 1.0 / dt;
+    // precompute (riem_solver3.py:24-67); on the last call peln, pk and pe
+    // take their final values here (finalize, riem_solver3.py:70-103)
+    double pem_k = ptop, peg_k = ptop, pelng_k = peln1;
+    pem[0] = ptop;
+    pk3[o0] = ptk;
+    if (last) {
+      peln[o0] = peln1;
+      pk[o0] = ptk;
+      pe[o0] = ptop;
+    }
+    for (int k = 0; k < K - 1; ++k) {
+      const long long o = o0 + k * sk;
+      const double dmk = delp[o];
+      const double pem_n = pem_k + dmk;
+      const double peg_n = peg_k + dmk * (1.0 - q_con[o]);
+      const double pelng_n = fm::fm_log(peg_n);
+      const double peln_n = fm::fm_log(pem_n);
+      const double pk3_n = fm::fm_exp(KAPPA * peln_n);
+      pem[k + 1] = pem_n;
+      pk3[o + sk] = pk3_n;
+      if (last) {
+        peln[o + sk] = peln_n;
+        pk[o + sk] = pk3_n;
+        pe[o + sk] = pem_n;
+      }
+      pm[k] = (peg_n - peg_k) / (pelng_n - pelng_k);
+      pem_k = pem_n;
+      peg_k = peg_n;
+      pelng_k = pelng_n;
+    }
+    auto DM = [&](int k) { return delp[o0 + k * sk] * RGRAV; };
+    auto W1 = [&](int k) { return w_io[o0 + k * sk]; };
+    auto DZ = [&](int k) { return zh[o0 + (k + 1) * sk] - zh[o0 + k * sk]; };
+    auto GM = [&](int k) { return 1.0 / (1.0 - cappa[o0 + k * sk]); };
+    auto PTR = [&](int k) { return pt[o0 + k * sk]; };
+    auto CP3 = [&](int k) { return cappa[o0 + k * sk]; };
+    auto PE_OUT = [&](int k, double v) { ppe[o0 + k * sk] = v; };
+    // finalize: zh rebuilt from the new layer depths bottom up, after its
+    // last read as an input
+    double z = zs[idx2(d, t, i, j)];
+    auto DZ_OUT = [&](int k, double dz) {
+      if (k == K - 2) zh[o0 + (K - 1) * sk] = z;
+      delz[o0 + k * sk] = dz;
+      z = z - dz;
+      zh[o0 + k * sk] = z;
+    };
+    sim1_column<NK>(K, DM, W1, DZ, GM, PTR, CP3, pem, pm, pp, gam, w, wsd[idx2(d, t, i, j)], dt, t1g, rdt, p_fac,
+                    PE_OUT, DZ_OUT);
+    for (int k = 0; k < K - 1; ++k) w_io[o0 + k * sk] = w[k];
+  }
+};
+
+// Runs Body<NK>::run over the columns with NK the smallest level bucket >= K.
+template <template <int> class Body, typename A>
+cudaError_t launch_riemann(const Dims& d, int i0, int i1, int j0, int j1, cudaStream_t s, A args) {
+  const int K = d.nk;
+  const Dims dd = d;
+#define FV3B_RIEM_BUCKET(NK)                                                                             \
+  if (K <= NK)                                                                                           \
+    return launch_columns(i0, i1, j0, j1, s,                                                            \
+                          [=] __device__(int t, int i, int j) { Body<NK>::run(dd, t, i, j, args); }, 128);
+  FV3B_RIEM_BUCKET(16)
+  FV3B_RIEM_BUCKET(32)
+  FV3B_RIEM_BUCKET(64)
+  FV3B_RIEM_BUCKET(80)
+  FV3B_RIEM_BUCKET(96)
+  FV3B_RIEM_BUCKET(MAXK)
+#undef FV3B_RIEM_BUCKET
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace fv3b
@@ -112,48 +271,8 @@ extern "C" int fv3b_riem_solver_c(const fv3b_grid_dims* dims, double dt2, double
                "fv3b_riem_solver_c: null argument");
   Dims d = make_dims(dims);
   FV3B_REQUIRE(d.nk <= MAXK && d.nk >= 3, "fv3b_riem_solver_c: npz out of range (2..127)");
-  cudaStream_t s = (cudaStream_t)stream;
-  const int K = d.nk;
-  const double t1g = 2.0 * dt2 * dt2;
-  const double rdt = 1.0 / dt2;
-  auto body = [=] __device__(int t, int i, int j) {
-    double dm[MAXK], w[MAXK], w1[MAXK], dz[MAXK], pem[MAXK], pm[MAXK], pe[MAXK], pp[MAXK], gam[MAXK],
-        aa[MAXK];
-    // precompute (riem_solver_c.py:13-44)
-    double pem_k = ptop, peg_k = ptop;
-    double gz_prev = gz[idx3(d, t, i, j, 0)];
-    for (int k = 0; k < K; ++k) {
-      long long o = idx3(d, t, i, j, k);
-      double dmk = delpc[o];
-      pem[k] = pem_k;
-      double peg_next = peg_k + dmk * (1.0 - q_con[o]);
-      if (k < K - 1) {
-        double gz_next = gz[o + d.sk];
-        dz[k] = gz_next - gz_prev;
-        gz_prev = gz_next;
-        pm[k] = (peg_next - peg_k) / fm::fm_log(peg_next / peg_k);
-      }
-      pem_k = pem_k + dmk;
-      peg_k = peg_next;
-      dm[k] = dmk / GRAV;
-      w[k] = w3[o];
-    }
-    auto gm = [&](int k) { return 1.0 / (1.0 - cappa[idx3(d, t, i, j, k)]); };
-    auto ptr = [&](int k) { return ptc[idx3(d, t, i, j, k)]; };
-    auto cp3 = [&](int k) { return cappa[idx3(d, t, i, j, k)]; };
-    sim1_column(K, dm, w, w1, dz, pem, pm, pe, pp, gam, aa, gm, ptr, cp3, ws[idx2(d, t, i, j)], dt2, t1g,
-                rdt, p_fac);
-    // finalize (riem_solver_c.py:46-64)
-    pef[idx3(d, t, i, j, 0)] = ptop;
-    for (int k = 1; k < K; ++k) pef[idx3(d, t, i, j, k)] = pe[k] + pem[k];
-    double g = hs[idx2(d, t, i, j)];
-    gz[idx3(d, t, i, j, K - 1)] = g;
-    for (int k = K - 2; k >= 0; --k) {
-      g = g - dz[k] * GRAV;
-      gz[idx3(d, t, i, j, k)] = g;
-    }
-  };
-  FV3B_CHECK(launch_columns(d.isc - 1, d.iec + 2, d.jsc - 1, d.jec + 2, s, body));
+  RiemCArgs a{dt2, ptop, p_fac, cappa, hs, ws, ptc, q_con, delpc, gz, pef, w3};
+  FV3B_CHECK(launch_riemann<RiemC>(d, d.isc - 1, d.iec + 2, d.jsc - 1, d.jec + 2, (cudaStream_t)stream, a));
   return FV3B_OK;
 }
 
@@ -168,68 +287,10 @@ extern "C" int fv3b_riem_solver3(const fv3b_grid_dims* dims, int last_call, doub
                "fv3b_riem_solver3: null argument");
   Dims d = make_dims(dims);
   FV3B_REQUIRE(d.nk <= MAXK && d.nk >= 3, "fv3b_riem_solver3: npz out of range (2..127)");
-  cudaStream_t s = (cudaStream_t)stream;
-  const int K = d.nk;
   const double peln1 = log(ptop);
   const double ptk = exp(KAPPA * peln1);
-  const double t1g = 2.0 * dt * dt;
-  const double rdt = 1.0 / dt;
-  const bool last = last_call != 0;
-  auto body = [=] __device__(int t, int i, int j) {
-    double dm[MAXK], wc[MAXK], w1[MAXK], dz[MAXK], pem[MAXK], pm[MAXK], pec[MAXK], pp[MAXK], gam[MAXK],
-        aa[MAXK], peln_run[MAXK];
-    const long long o0 = idx3(d, t, i, j, 0);
-    // precompute
-    double pem_k = ptop, peg_k = ptop, pelng_k = peln1;
-    pem[0] = ptop;
-    peln_run[0] = peln1;
-    pk3[o0] = ptk;
-    for (int k = 0; k < K; ++k) {
-      long long o = o0 + k * d.sk;
-      double dmk = delp[o];
-      if (k < K - 1) {
-        double pem_n = pem_k + dmk;
-        double peg_n = peg_k + dmk * (1.0 - q_con[o]);
-        double pelng_n = fm::fm_log(peg_n);
-        double peln_n = fm::fm_log(pem_n);
-        pem[k + 1] = pem_n;
-        peln_run[k + 1] = peln_n;
-        pk3[o + d.sk] = fm::fm_exp(KAPPA * peln_n);
-        pm[k] = (peg_n - peg_k) / (pelng_n - pelng_k);
-        dz[k] = zh[o + d.sk] - zh[o];
-        pem_k = pem_n;
-        peg_k = peg_n;
-        pelng_k = pelng_n;
-      }
-      dm[k] = dmk * RGRAV;
-      wc[k] = w[o];
-    }
-    auto gm = [&](int k) { return 1.0 / (1.0 - cappa[o0 + k * d.sk]); };
-    auto ptr = [&](int k) { return pt[o0 + k * d.sk]; };
-    auto cp3 = [&](int k) { return cappa[o0 + k * d.sk]; };
-    sim1_column(K, dm, wc, w1, dz, pem, pm, pec, pp, gam, aa, gm, ptr, cp3, wsd[idx2(d, t, i, j)], dt, t1g, rdt,
-                p_fac);
-    // finalize (beta = 0, use_logp = False)
-    for (int k = 0; k < K; ++k) {
-      long long o = o0 + k * d.sk;
-      ppe[o] = pec[k];
-      if (last) {
-        peln[o] = peln_run[k];
-        pk[o] = pk3[o];
-        pe[o] = pem[k];
-      }
-      if (k < K - 1) {
-        w[o] = wc[k];
-        delz[o] = dz[k];
-      }
-    }
-    double z = zs[idx2(d, t, i, j)];
-    zh[o0 + (K - 1) * d.sk] = z;
-    for (int k = K - 2; k >= 0; --k) {
-      z = z - dz[k];
-      zh[o0 + k * d.sk] = z;
-    }
-  };
-  FV3B_CHECK(launch_columns(d.isc, d.iec + 1, d.jsc, d.jec + 1, s, body));
+  Riem3Args a{last_call != 0, dt, ptop, p_fac, peln1, ptk, cappa, zs, wsd, delz, q_con, delp, pt, zh, pe, ppe, pk3,
+              pk, peln, w};
+  FV3B_CHECK(launch_riemann<Riem3>(d, d.isc, d.iec + 1, d.jsc, d.jec + 1, (cudaStream_t)stream, a));
   return FV3B_OK;
 }

@@ -265,11 +265,47 @@ class CubedSphereGrid:
         self.bgrid1, self.bgrid2 = self.lon_b, self.lat_b
         # A->B edge interpolation factors (fv3core/grid/geometry.py:604-714)
         self.edge_w, self.edge_e, self.edge_s, self.edge_n = self._edge_factors(C)
+        self.a2b_extrap = self._a2b_extrap_ratios()
         # minimum areas over the six compute domains
         self.da_min = float(area[:, hs:he, hs:he].min())
         self.da_max = float(area[:, hs:he, hs:he].max())
         self.da_min_c = float(area_c[:, hs : he + 1, hs : he + 1].min())
         self.da_max_c = float(area_c[:, hs : he + 1, hs : he + 1].max())
+
+    # (near, far) A-grid offsets of the three extrapolations at each tile
+    # corner of a2b_ord4 (a2b_ord4.py:60-235); the corners are, in order, the
+    # B-grid points (is, js), (ie+1, js), (ie+1, je+1), (is, je+1), whose
+    # reference stencils are _sw, _nw, _ne, _se
+    A2B_CORNER_OFFSETS = (
+        (((0, 0), (1, 1)), ((-1, 0), (-2, 1)), ((0, -1), (1, -2))),
+        (((-1, 0), (-2, 1)), ((-1, -1), (-2, -2)), ((0, 0), (1, 1))),
+        (((-1, -1), (-2, -2)), ((0, -1), (1, -2)), ((-1, 0), (-2, 1))),
+        (((0, -1), (1, -2)), ((-1, -1), (-2, -2)), ((0, 0), (1, 1))),
+    )
+
+    def _a2b_extrap_ratios(self):
+        """x1 / (x2 - x1) of each cube-corner extrapolation of a2b_ord4
+        (extrap_corner, a2b_ord4.py:45-57): x1, x2 are the great-circle
+        distances (a2b_ord4.py:38-41) from the B-grid corner to the near and
+        far A-grid points.  They depend on the grid only, so they are computed
+        once here.  Returns [6, 4, 3] in the order of A2B_CORNER_OFFSETS."""
+        h, n = self.halo, self.n
+        s, e = h, h + n - 1
+        corners = ((s, s), (e + 1, s), (e + 1, e + 1), (s, e + 1))
+
+        def gcd(p1a, p1b, p2a, p2b):
+            tb = np.sin((p1b - p2b) / 2.0) ** 2.0
+            ta = np.sin((p1a - p2a) / 2.0) ** 2.0
+            return np.arcsin(np.sqrt(tb + np.cos(p1b) * np.cos(p2b) * ta)) * 2.0
+
+        out = np.zeros((6, 4, 3))
+        for c, (i, j) in enumerate(corners):
+            b1, b2 = self.bgrid1[:, i, j], self.bgrid2[:, i, j]
+            for m, ((di1, dj1), (di2, dj2)) in enumerate(self.A2B_CORNER_OFFSETS[c]):
+                x1 = gcd(self.agrid1[:, i + di1, j + dj1], self.agrid2[:, i + di1, j + dj1], b1, b2)
+                x2 = gcd(self.agrid1[:, i + di2, j + dj2], self.agrid2[:, i + di2, j + dj2], b1, b2)
+                out[:, c, m] = x1 / (x2 - x1)
+        return out
 
     def _corner_fix(self, cos_sg, sin_sg):
         """Angles in the 3x3 cube-corner halo blocks, which have no cell of

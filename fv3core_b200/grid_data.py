@@ -26,6 +26,7 @@ METRIC_FIELDS = [
     "fC", "f0",
     "agrid1", "agrid2", "bgrid1", "bgrid2",
     "edge_w", "edge_e", "edge_s", "edge_n",
+    "a2b_extrap",
 ]
 
 
@@ -47,9 +48,9 @@ class GridData:
         self.tensors = {}
         for name in METRIC_FIELDS:
             a = np.asarray(getattr(grid, name), dtype=np.float64)
-            if a.ndim == 3:  # [6, i, j] -> [6, j, i]
+            if a.ndim == 3 and name != "a2b_extrap":  # [6, i, j] -> [6, j, i]
                 t = torch.from_numpy(np.ascontiguousarray(a.transpose(0, 2, 1))).to(device)
-            else:  # edge factors [6, n+1]
+            else:  # edge factors [6, n+1], corner ratios [6, 4, 3]
                 t = torch.from_numpy(np.ascontiguousarray(a)).to(device)
             self.tensors[name] = t
             setattr(self, name, t)

@@ -45,7 +45,7 @@ typedef struct fv3b_grid_dims {
 /*
  * Grid metric terms (device pointers, owned by the caller, read only).
  * 2-D fields are [6][n+2h+1][n+2h+1]; the four edge factors are
- * [6][n+1] (index = position along the tile edge).  Replaces the reference's
+ * [6][n+1] (index = position along the tile edge); a2b_extrap is [6][4][3].  Replaces the reference's
  * GridData / DampingCoefficients containers (fv3core/utils/grid.py:475-799)
  * plus the legacy spec.grid fields the hot path reads (fC, f0, agrid, bgrid,
  * edge_*, divg_*).
@@ -62,6 +62,10 @@ typedef struct fv3b_metrics {
   const double *fC, *f0;
   const double *agrid1, *agrid2, *bgrid1, *bgrid2;
   const double *edge_w, *edge_e, *edge_s, *edge_n;
+  /* [6][4][3]: x1 / (x2 - x1) of a2b_ord4's cube-corner extrapolations
+   * (a2b_ord4.py:38-57), corners (is, js), (ie+1, js), (ie+1, je+1),
+   * (is, je+1), three extrapolations each in the reference's order */
+  const double* a2b_extrap;
   double da_min, da_min_c;
 } fv3b_metrics;
 

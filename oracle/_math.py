@@ -10,6 +10,8 @@ functions (cancellation in the Riemann solvers and the pressure gradient),
 and numpy's exp and power are not correctly rounded, so no other
 implementation can reproduce them exactly.  The functions themselves are
 checked against correctly rounded values in ``tests/test_fmath.py``.
+``host_sin``/``host_log`` serve per-level constants that the library
+computes on the host with the C library.
 """
 import contextlib
 import ctypes
@@ -28,7 +30,8 @@ _device = False
 
 
 def build():
-    """Compile the host helper (g++, no FMA contraction) if stale."""
+    """Compile the host helper (g++, no implicit FMA contraction; the header's
+    explicit fma() calls are exactly rounded in libm) if stale."""
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
     newest = max(os.path.getmtime(SRC), os.path.getmtime(HEADER))
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
@@ -73,6 +76,24 @@ def power(x, p):
     out = np.empty_like(xa)
     _load().pm_pow(xa.ctypes.data, pa.ctypes.data, out.ctypes.data, xa.size)
     return out if out.ndim else float(out.reshape(-1)[0])
+
+
+def host_sin(x):
+    """Per-level constants: numpy's sin, or in device-math mode the C
+    library's (what the library's host setup code calls)."""
+    if not _device:
+        return np.sin(x)
+    import math
+
+    return np.array([math.sin(v) for v in np.ravel(x)]).reshape(np.shape(x))
+
+
+def host_log(x):
+    if not _device:
+        return np.log(x)
+    import math
+
+    return np.array([math.log(v) for v in np.ravel(x)]).reshape(np.shape(x))
 
 
 @contextlib.contextmanager

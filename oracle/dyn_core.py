@@ -81,7 +81,8 @@ def ray_fast(t: Tile, u, v, w, dp, pfull, dt, ptop, rf_cutoff, tau, hydrostatic=
     dpk = np.asarray(dp)[:nz]
     tau0 = tau * C.SDAY
     with np.errstate(all="ignore"):
-        rfv = dt / tau0 * np.sin(0.5 * C.PI * np.log(rf_cutoff / pf) / np.log(rf_cutoff / ptop)) ** 2
+        rfv = dt / tau0 * _math.host_sin(0.5 * C.PI * _math.host_log(rf_cutoff / pf) / _math.host_log(
+            rf_cutoff / ptop)) ** 2
         rf = np.where(pf < rf_cutoff, 1.0 / (1.0 + rfv), np.nan)
     dm = np.full(nz, np.nan)
     if pf[0] < nudge:

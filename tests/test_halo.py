@@ -192,3 +192,23 @@ def test_sync_vector_interfaces_geometry():
     u, v = ue.copy(), ve.copy()
     HaloExchange(N, H).sync_vector_interfaces(u, v)
     assert np.abs(u - ue).max() < 1e-10 and np.abs(v - ve).max() < 1e-10
+
+
+def test_a2b_corner_ratios_match_the_oracle_formula():
+    """The grid's precomputed a2b_ord4 corner-extrapolation ratios equal the
+    oracle's on-the-fly great-circle formula bit for bit."""
+    from oracle.a2b_ord4 import great_circle_dist
+
+    from fv3core_b200.grid import CubedSphereGrid
+
+    n, h = 12, 3
+    g = CubedSphereGrid(n, h)
+    s, e = h, h + n - 1
+    corners = ((s, s), (e + 1, s), (e + 1, e + 1), (s, e + 1))
+    for t in range(6):
+        for c, (i, j) in enumerate(corners):
+            b1, b2 = g.bgrid1[t, i, j], g.bgrid2[t, i, j]
+            for m, ((di1, dj1), (di2, dj2)) in enumerate(g.A2B_CORNER_OFFSETS[c]):
+                x1 = great_circle_dist(g.agrid1[t, i + di1, j + dj1], g.agrid2[t, i + di1, j + dj1], b1, b2)
+                x2 = great_circle_dist(g.agrid1[t, i + di2, j + dj2], g.agrid2[t, i + di2, j + dj2], b1, b2)
+                assert x1 / (x2 - x1) == g.a2b_extrap[t, c, m]
