@@ -1,0 +1,133 @@
+// fv3b_del2cubed_noalloc: the heat-source filter of HyperdiffusionDamping
+// (fv3core/stencils/del2cubed.py:152-181) for callers that cannot let the
+// library allocate device memory.
+//
+// fv3b_del2cubed takes a context, and fv3b_ctx_create allocates the whole
+// stage workspace (40 full 3-D fields, tens of GB at C384) with cudaMalloc.
+// Some hosts cannot allow that: a model that hands all device memory to its
+// own pool (cudaMalloc from a library would fail, or fragment the pool),
+// or a coupler that wants only this filter and has budgeted no memory for
+// a context.  This entry point needs no context and allocates nothing.  Its
+// three scratch fields live in one file-scope device array of fixed size,
+// so the memory is reserved when the library's module is loaded, not when
+// the call runs.
+//
+// Sharing: there is one scratch array per device for the whole process.
+// Two calls that overlap in time on the same device (different streams, or
+// different host threads without ordering) race on it and give wrong
+// results.  Callers must order their calls, for example by issuing them all
+// on one stream.
+//
+// The arithmetic is the same as fv3b_del2cubed's, launch for launch.
+#include <mutex>
+
+#include "corners.cuh"
+#include "stencil.cuh"
+
+using namespace fv3b;
+
+namespace {
+
+// Scratch: three fields of at most FV3B_NOALLOC_FIELD_DOUBLES doubles each
+// (6 * (npz+1) * (n+7)^2 <= 1,500,000 covers C48 L79), 36 MB in total.
+constexpr long long FV3B_NOALLOC_FIELD_DOUBLES = 1500000;
+static __device__ __align__(256) double g_noalloc_scratch[3 * FV3B_NOALLOC_FIELD_DOUBLES];
+
+constexpr int MAX_DEVICES = 64;
+std::mutex g_scratch_mutex;
+double* g_scratch_addr[MAX_DEVICES] = {nullptr};
+
+// Device address of the scratch array on the current device, looked up once
+// per device.
+cudaError_t scratch_address(double** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (g_scratch_addr[dev] == nullptr) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_scratch_addr[dev] = static_cast<double*>(p);
+  }
+  *out = g_scratch_addr[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" int fv3b_del2cubed_noalloc(const fv3b_grid_dims* dims, const fv3b_metrics* metrics, double* qdel,
+                                      double cd, int nmax, void* stream) {
+  FV3B_REQUIRE(dims && metrics && qdel, "fv3b_del2cubed_noalloc: null argument");
+  FV3B_REQUIRE(dims->npx >= 4 && dims->n_halo == 3 && dims->npz >= 1,
+               "fv3b_del2cubed_noalloc: need npx >= 4, n_halo == 3, npz >= 1");
+  const Dims d = make_dims(dims);
+  FV3B_REQUIRE(d.st * 6 <= FV3B_NOALLOC_FIELD_DOUBLES,
+               "fv3b_del2cubed_noalloc: grid too large for the static scratch "
+               "(6*(npz+1)*(npx+7)^2 must be <= 1500000 doubles)");
+  const fv3b_metrics g = *metrics;
+  double* base = nullptr;
+  FV3B_CHECK(scratch_address(&base));
+  double *q = base, *fx = base + FV3B_NOALLOC_FIELD_DOUBLES, *fy = base + 2 * FV3B_NOALLOC_FIELD_DOUBLES;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = d.nz;
+  const int full = d.ni - 1;
+  const int ntimes = nmax < 3 ? nmax : 3;
+  for (int n = 0; n < ntimes; ++n) {
+    const int nt = ntimes - (n + 1);
+    // corner_fill (del2cubed.py:41-75) into q, full domain
+    FV3B_CHECK(launch_box(Box{0, full, 0, full, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+      PT_SETUP(d, t, k);
+      const double third = 1.0 / 3.0;
+      double out = F3(qdel, i, j);
+      auto Q = [&](int di, int dj) { return F3(qdel, i + di, j + dj); };
+      if (j == js) {
+        if (i == s) out = (Q(0, 0) + Q(-1, 0) + Q(0, -1)) * third;
+        else if (i == s - 1) out = (Q(1, 0) + Q(0, 0) + Q(1, -1)) * third;
+        else if (i == e) out = (Q(0, 0) + Q(1, 0) + Q(0, -1)) * third;
+        else if (i == e + 1) out = (Q(-1, 0) + Q(0, 0) + Q(-1, -1)) * third;
+      } else if (j == js - 1) {
+        if (i == s) out = (Q(0, 1) + Q(-1, 1) + Q(0, 0)) * third;
+        else if (i == e) out = (Q(0, 1) + Q(1, 1) + Q(0, 0)) * third;
+      } else if (j == je) {
+        if (i == e) out = (Q(0, 0) + Q(1, 0) + Q(0, 1)) * third;
+        else if (i == e + 1) out = (Q(-1, 0) + Q(0, 0) + Q(-1, 1)) * third;
+        else if (i == s) out = (Q(0, 0) + Q(-1, 0) + Q(0, 1)) * third;
+        else if (i == s - 1) out = (Q(1, 0) + Q(0, 0) + Q(1, 1)) * third;
+      } else if (j == je + 1) {
+        if (i == e) out = (Q(0, -1) + Q(1, -1) + Q(0, 0)) * third;
+        else if (i == s) out = (Q(0, -1) + Q(-1, -1) + Q(0, 0)) * third;
+      }
+      W3(q, i, j) = out;
+    }));
+    // compute_zonal_flux / compute_meridional_flux with the corner copies of
+    // q applied on read
+    FV3B_CHECK(launch_box(Box{s - nt, e + 2 + nt, js - nt, je + 2 + nt, 0, nz}, st,
+                          [=] __device__(int t, int i, int j, int k) {
+                            PT_SETUP(d, t, k);
+                            auto qx = [&](int ii, int jj) {
+                              int si, sj;
+                              if (nt > 0 && copy_corner_x(d, ii, jj, si, sj)) return F3(q, si, sj);
+                              return F3(q, ii, jj);
+                            };
+                            auto qy = [&](int ii, int jj) {
+                              int si, sj;
+                              if (nt > 0 && copy_corner_y(d, ii, jj, si, sj)) return F3(q, si, sj);
+                              return F3(q, ii, jj);
+                            };
+                            if (j < je + 1 + nt) W3(fx, i, j) = F2(g.del6_v, i, j) * (qx(i - 1, j) - qx(i, j));
+                            if (i < e + 1 + nt) W3(fy, i, j) = F2(g.del6_u, i, j) * (qy(i, j - 1) - qy(i, j));
+                          }));
+    // copy back and update_q
+    FV3B_CHECK(launch_box(Box{0, full, 0, full, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+      PT_SETUP(d, t, k);
+      int si, sj;
+      double qv = (nt > 0 && copy_corner_y(d, i, j, si, sj)) ? F3(q, si, sj) : F3(q, i, j);
+      if (i >= s - nt && i < e + 1 + nt && j >= js - nt && j < je + 1 + nt)
+        qv = qv + cd * F2(g.rarea, i, j) * (F3(fx, i, j) - F3(fx, i + 1, j) + F3(fy, i, j) - F3(fy, i, j + 1));
+      W3(qdel, i, j) = qv;
+    }));
+  }
+  return FV3B_OK;
+}

@@ -277,6 +277,21 @@ int fv3b_acoustics(fv3b_ctx* ctx, const fv3b_dycore_state* state, void* stream);
  * "cry", "xfx", "yfx", "delpc", "ptc", "ws3", "zs", "dp_ref"), or NULL. */
 double* fv3b_acoustics_temporary(fv3b_ctx* ctx, const char* name);
 
+/*
+ * fv3b_del2cubed_noalloc: no reference counterpart.  The same filter as
+ * fv3b_del2cubed (HyperdiffusionDamping, fv3core/stencils/del2cubed.py:152-181)
+ * for callers that cannot let the library allocate device memory: it takes
+ * no context (fv3b_ctx_create allocates the full stage workspace) and
+ * allocates nothing; its scratch is a fixed file-scope device array reserved
+ * when the library is loaded.  Grids with 6*(npz+1)*(npx+2*n_halo+1)^2 above
+ * 1,500,000 (larger than C48 L79) are rejected with FV3B_ERR_ARGUMENT.  The
+ * scratch is shared by every caller on a device: calls must not overlap in
+ * time (issue them on one stream, or order them).  metrics: as for
+ * fv3b_ctx_create (del6_u, del6_v and rarea are read).
+ */
+int fv3b_del2cubed_noalloc(const fv3b_grid_dims* dims, const fv3b_metrics* metrics, double* qdel, double cd, int nmax,
+                           void* stream);
+
 #ifdef __cplusplus
 }
 #endif
