@@ -1,0 +1,81 @@
+"""The C ABI: the library loads without a GPU, exports every function that
+include/fv3core_b200.h declares, and the ctypes mirrors of its structs have
+the C layout (checked against a host-compiled probe of the header)."""
+import ctypes
+import os
+import re
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "fv3core_b200.h")
+
+
+def _declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fv3b_\w+)\s*\(", text)))
+
+
+def test_header_declares_the_entry_points():
+    names = _declared_functions()
+    assert "fv3b_acoustics" in names and "fv3b_c_sw" in names and len(names) >= 25
+
+
+def test_library_exports_every_declared_function():
+    from fv3core_b200 import _lib
+
+    L = _lib.lib()
+    missing = [n for n in _declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_every_declared_function():
+    from fv3core_b200 import _lib
+
+    bound = set(_lib.exported_symbols())
+    assert set(_declared_functions()) <= bound, set(_declared_functions()) - bound
+
+
+def test_version_and_error_reporting_without_gpu():
+    from fv3core_b200 import _lib
+
+    L = _lib.lib()
+    assert L.fv3b_version().startswith(b"fv3core_b200")
+    # a null context is rejected on the host, before any CUDA call
+    rc = L.fv3b_edge_pe(None, None, None, 0.0, None)
+    assert rc == 1 and b"null argument" in L.fv3b_last_error()
+
+
+@pytest.fixture(scope="module")
+def c_layout(tmp_path_factory):
+    if shutil.which("gcc") is None:
+        pytest.skip("no host compiler")
+    src = tmp_path_factory.mktemp("abi") / "probe.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "fv3core_b200.h"\n'
+        "int main(void) {\n"
+        '  printf("fv3b_grid_dims %zu\\n", sizeof(fv3b_grid_dims));\n'
+        '  printf("fv3b_metrics %zu %zu\\n", sizeof(fv3b_metrics), offsetof(fv3b_metrics, da_min));\n'
+        '  printf("fv3b_dsw_config %zu\\n", sizeof(fv3b_dsw_config));\n'
+        '  printf("fv3b_acoustic_config %zu\\n", sizeof(fv3b_acoustic_config));\n'
+        '  printf("fv3b_dycore_state %zu %zu\\n", sizeof(fv3b_dycore_state), offsetof(fv3b_dycore_state, n_map));\n'
+        "  return 0;\n}\n"
+    )
+    exe = str(src.with_suffix(""))
+    subprocess.check_call(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), "-o", exe, str(src)])
+    out = subprocess.check_output([exe], text=True)
+    return {line.split()[0]: [int(x) for x in line.split()[1:]] for line in out.splitlines()}
+
+
+def test_struct_layouts_match_ctypes(c_layout):
+    from fv3core_b200 import _lib
+    from fv3core_b200.grid_data import Metrics
+
+    assert c_layout["fv3b_grid_dims"] == [ctypes.sizeof(_lib.GridDims)]
+    assert c_layout["fv3b_metrics"] == [ctypes.sizeof(Metrics), Metrics.da_min.offset]
+    assert c_layout["fv3b_dsw_config"] == [ctypes.sizeof(_lib.DswConfig)]
+    assert c_layout["fv3b_acoustic_config"] == [ctypes.sizeof(_lib.AcousticConfig)]
+    assert c_layout["fv3b_dycore_state"] == [ctypes.sizeof(_lib.DycoreState), _lib.DycoreState.n_map.offset]
