@@ -157,6 +157,168 @@ inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a
   });
 }
 
+// ---------------------------------------------------------------------------
+// Fused FiniteVolumeTransport: the three passes of fvtp2d() in one kernel.
+//
+// A 32 x 8 thread block owns a 32 x 8 tile of output points of one level.
+// It stages the q, q_y, Courant-number and area-flux tiles it needs (tile
+// plus a 3-point halo) in shared memory, computes the inner PPM means, the
+// q_i / q_j advected values and the outer PPM fluxes there, and writes only
+// fx and fy.  Every value it computes lies inside the reference's own
+// compute domain of that value, with the same operations, so results equal
+// fvtp2d()'s bit for bit.  q must already hold its x-corner copies (see
+// copy_corners_x_inplace); q_y is read through the y-corner rules.
+constexpr int FT_TX = 32, FT_TY = 8;
+
+// Line accessor into a shared-memory tile (row-major, row length `pitch`).
+struct SLine {
+  const double* p;
+  int step;
+  __device__ __forceinline__ double operator()(int o) const { return p[o * step]; }
+};
+
+struct FvTp2dFused {
+  const double* q;
+  const double *crx, *cry, *xfx, *yfx, *x_unit, *y_unit;
+  double *fx, *fy;
+  int mord_in, mord_out;
+};
+
+static __global__ void __launch_bounds__(FT_TX * FT_TY) fvtp2d_fused_kernel(const Dims d, const fv3b_metrics g,
+                                                                     const FvTp2dFused a) {
+  // tile regions (absolute storage indices)
+  constexpr int QX = FT_TX + 6, QY = FT_TY + 5;    // q:   [I0-3, I0+TX+3) x [J0-3, J0+TY+2)
+  constexpr int YX = FT_TX + 5, YY = FT_TY + 6;    // q_y: [I0-3, I0+TX+2) x [J0-3, J0+TY+3)
+  constexpr int CXX = FT_TX + 1, CXY = FT_TY + 5;  // crx, xfx, fx_mean: [I0, I0+TX+1) x [J0-3, J0+TY+2)
+  constexpr int CYX = FT_TX + 5, CYY = FT_TY + 1;  // cry, yfx, fy_mean: [I0-3, I0+TX+2) x [J0, J0+TY+1)
+  constexpr int AXX = FT_TX, AXY = FT_TY + 5;      // q_adv_x: [I0, I0+TX) x [J0-3, J0+TY+2)
+  constexpr int AYX = FT_TX + 5, AYY = FT_TY;      // q_adv_y: [I0-3, I0+TX+2) x [J0, J0+TY)
+  __shared__ double sq[QY][QX], sqy[YY][YX];
+  __shared__ double scrx[CXY][CXX], sxfx[CXY][CXX], sfxm[CXY][CXX];
+  __shared__ double scry[CYY][CYX], syfx[CYY][CYX], sfym[CYY][CYX];
+  __shared__ double sqax[AXY][AXX], sqay[AYY][AYX];
+
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
+  const int nbi = (e + 2 - s + FT_TX - 1) / FT_TX;
+  const int I0 = s + (blockIdx.x % nbi) * FT_TX;
+  const int J0 = js + (blockIdx.x / nbi) * FT_TY;
+  const int t = blockIdx.z, k = blockIdx.y;
+  const int tid = threadIdx.y * FT_TX + threadIdx.x;
+  constexpr int NT = FT_TX * FT_TY;
+  const long long b3 = (long long)t * d.st + (long long)k * d.sk;
+  auto inside = [&](int i, int j) { return i >= 0 && i < d.ni && j >= 0 && j < d.nj; };
+  auto ld = [&](const double* p, int i, int j) { return inside(i, j) ? p[b3 + (long long)j * d.sj + i] : 0.0; };
+
+  // stage the inputs
+  for (int x = tid; x < QX * QY; x += NT) {
+    int i = I0 - 3 + x % QX, j = J0 - 3 + x / QX;
+    sq[x / QX][x % QX] = ld(a.q, i, j);
+  }
+  for (int x = tid; x < YX * YY; x += NT) {
+    int i = I0 - 3 + x % YX, j = J0 - 3 + x / YX;
+    int si, sj;
+    sqy[x / YX][x % YX] = (inside(i, j) && copy_corner_y(d, i, j, si, sj)) ? ld(a.q, si, sj) : ld(a.q, i, j);
+  }
+  for (int x = tid; x < CXX * CXY; x += NT) {
+    int i = I0 + x % CXX, j = J0 - 3 + x / CXX;
+    scrx[x / CXX][x % CXX] = ld(a.crx, i, j);
+    sxfx[x / CXX][x % CXX] = ld(a.xfx, i, j);
+  }
+  for (int x = tid; x < CYX * CYY; x += NT) {
+    int i = I0 - 3 + x % CYX, j = J0 + x / CYX;
+    scry[x / CYX][x % CYX] = ld(a.cry, i, j);
+    syfx[x / CYX][x % CYX] = ld(a.yfx, i, j);
+  }
+  __syncthreads();
+  // inner PPM: fx_mean (x sweep of q), fy_mean (y sweep of q_y)
+  for (int x = tid; x < CXX * CXY; x += NT) {
+    int ci = x % CXX, cj = x / CXX;
+    int i = I0 + ci, j = J0 - 3 + cj;
+    if (!inside(i, j) || i + 2 >= d.ni) continue;
+    SLine q{&sq[cj][ci + 3], 1};
+    auto dxa = line2<0>(d, g.dxa, t, i, j);
+    sfxm[cj][ci] = ppm_flux(q, dxa, scrx[cj][ci], i, s, e, a.mord_in);
+  }
+  for (int x = tid; x < CYX * CYY; x += NT) {
+    int ci = x % CYX, cj = x / CYX;
+    int i = I0 - 3 + ci, j = J0 + cj;
+    if (!inside(i, j) || j + 2 >= d.nj) continue;
+    SLine q{&sqy[cj + 3][ci], YX};
+    auto dya = line2<1>(d, g.dya, t, i, j);
+    sfym[cj][ci] = ppm_flux(q, dya, scry[cj][ci], j, js, je, a.mord_in);
+  }
+  __syncthreads();
+  // q_i (fvtp2d.py:33-47) at x-sweep points, q_j (50-60) at y-sweep points
+  for (int x = tid; x < AYX * AYY; x += NT) {
+    int ci = x % AYX, cj = x / AYX;
+    int i = I0 - 3 + ci, j = J0 + cj;
+    if (!inside(i, j)) continue;
+    double area = g.area[idx2(d, t, i, j)];
+    double fyy0 = syfx[cj][ci] * sfym[cj][ci];
+    double fyy1 = syfx[cj + 1][ci] * sfym[cj + 1][ci];
+    sqay[cj][ci] = (sqy[cj + 3][ci] * area + fyy0 - fyy1) / (area + syfx[cj][ci] - syfx[cj + 1][ci]);
+  }
+  for (int x = tid; x < AXX * AXY; x += NT) {
+    int ci = x % AXX, cj = x / AXX;
+    int i = I0 + ci, j = J0 - 3 + cj;
+    if (!inside(i, j)) continue;
+    double area = g.area[idx2(d, t, i, j)];
+    double fx10 = sxfx[cj][ci] * sfxm[cj][ci];
+    double fx11 = sxfx[cj][ci + 1] * sfxm[cj][ci + 1];
+    double awx = area + sxfx[cj][ci] - sxfx[cj][ci + 1];
+    sqax[cj][ci] = (sq[cj][ci + 3] * area + fx10 - fx11) / awx;
+  }
+  __syncthreads();
+  // outer PPM and final fluxes (fvtp2d.py:63-93) for this thread's point
+  const int ti = threadIdx.x, tj = threadIdx.y;
+  const int i = I0 + ti, j = J0 + tj;
+  const long long o = b3 + (long long)j * d.sj + i;
+  if (i <= e + 1 && j <= je) {
+    SLine q{&sqay[tj][ti + 3], 1};
+    auto dxa = line2<0>(d, g.dxa, t, i, j);
+    double xo = ppm_flux(q, dxa, scrx[tj + 3][ti], i, s, e, a.mord_out);
+    a.fx[o] = 0.5 * (xo + sfxm[tj + 3][ti]) * a.x_unit[o];
+  }
+  if (i <= e && j <= je + 1) {
+    SLine q{&sqax[tj + 3][ti], AXX};
+    auto dya = line2<1>(d, g.dya, t, i, j);
+    double yo = ppm_flux(q, dya, scry[tj][ti + 3], j, js, je, a.mord_out);
+    a.fy[o] = 0.5 * (yo + sfym[tj][ti + 3]) * a.y_unit[o];
+  }
+}
+
+void note_launch();
+
+// FiniteVolumeTransport.__call__ (fvtp2d.py:249-362) without the damping
+// step, fused (see fvtp2d_fused_kernel); all npz+1 levels.
+inline cudaError_t fvtp2d_fused(const Dims d, const fv3b_metrics g, const double* q, const double* crx,
+                                const double* cry, const double* xfx, const double* yfx, const double* x_unit,
+                                const double* y_unit, double* fx, double* fy, int hord, cudaStream_t st) {
+  const int ord_in = hord == 10 ? 8 : hord;
+  FvTp2dFused a{q, crx, cry, xfx, yfx, x_unit, y_unit, fx, fy, ord_in < 0 ? -ord_in : ord_in, hord < 0 ? -hord : hord};
+  const int nbi = (d.iec + 2 - d.isc + FT_TX - 1) / FT_TX;
+  const int nbj = (d.jec + 2 - d.jsc + FT_TY - 1) / FT_TY;
+  dim3 grid(nbi * nbj, d.nk, 6), block(FT_TX, FT_TY);
+  fvtp2d_fused_kernel<<<grid, block, 0, st>>>(d, g, a);
+  note_launch();
+  return cudaGetLastError();
+}
+
+// The x half of CopyCornersXY in place (corners.py:64-117): only the 3 x 3
+// cube-corner blocks of q change; all npz+1 levels.
+inline cudaError_t copy_corners_x_inplace(const Dims d, double* q, cudaStream_t st) {
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
+  // 4 corner blocks of 3 x 3 points
+  return launch_box(Box{0, 12, 0, 3, 0, d.nk}, st, [=] __device__(int t, int x, int y, int k) {
+    PT_SETUP(d, t, k);
+    const int c = x / 3, a = x % 3;
+    const int i = (c == 0 || c == 2) ? s - 3 + a : e + 1 + a;
+    const int j = (c < 2) ? js - 3 + y : je + 1 + y;
+    int si, sj;
+    if (copy_corner_x(d, i, j, si, sj)) W3(q, i, j) = F3(q, si, sj);
+  });
+}
+
 // Per-level damping column on the device: nord band value and damp.
 struct DelnCol {
   const double* nord;  // [nk] per-level nord (band value, see nord_at)
