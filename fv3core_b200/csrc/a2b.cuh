@@ -67,10 +67,15 @@ inline cudaError_t a2b_ord4(const Dims d, const fv3b_metrics g, double* qin, dou
   cudaError_t err;
   if (k1 <= k0) return cudaSuccess;
   // corners (a2b_ord4.py:60-235, 616-654) and edges (313-336, 678-695)
-  err = launch_box(Box{s, e + 2, js, je + 2, k0, k1}, st, [=] __device__(int t, int i, int j, int k) {
+  // one thread per boundary point of [is, ie+1] x [js, je+1]: the south and
+  // north rows (corners included), then the west and east columns
+  err = launch_box(Box{0, 4 * (n + 1), 0, 1, k0, k1}, st, [=] __device__(int t, int p, int, int k) {
     PT_SETUP(d, t, k);
+    const int side = p / (n + 1), a = p % (n + 1);
+    if (side >= 2 && (a == 0 || a == n)) return;  // corners belong to the rows
+    const int i = side < 2 ? s + a : (side == 2 ? s : e + 1);
+    const int j = side == 0 ? js : (side == 1 ? je + 1 : js + a);
     bool wcol = i == s, ecol = i == e + 1, srow = j == js, nrow = j == je + 1;
-    if (!(wcol || ecol || srow || nrow)) return;
     double v;
     if ((wcol || ecol) && (srow || nrow)) {
       // offsets (near, far) of the three extrapolations; the reference's

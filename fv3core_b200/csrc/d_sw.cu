@@ -430,6 +430,7 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
   double *tmp_fx = W[0], *tmp_fy = W[1], *tmp_gx = W[2], *tmp_gy = W[3], *tmp_fx2 = W[4], *tmp_fy2 = W[5];
   double *tmp_dw = W[6], *tmp_wk = W[7], *tmp_vort = W[8], *tmp_ke = W[9], *tmp_heat_s = W[10];
   double *tmp_ut = W[11], *tmp_vt = W[12], *vort_x_delta = W[13], *vort_y_delta = W[14];
+  double *fx_mean = W[16], *fy_mean = W[17], *q_adv_x = W[18], *q_adv_y = W[19];
   double *dl_fx2 = W[20], *dl_fy2 = W[21], *dl_d2 = W[22];
   double *a2b_qx = W[23], *a2b_qy = W[24], *a2b_edges = W[25];
   double *ucc = W[WS_UC_CONTRA], *vcc = W[WS_VC_CONTRA];
@@ -450,7 +451,9 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
                        const double* mass, const DelnCol* dl, int nmax) -> cudaError_t {
     cudaError_t err = copy_corners_x_inplace(d, q, st);
     if (err != cudaSuccess) return err;
-    err = fvtp2d_fused(d, g, q, crx, cry, xfx, yfx, xmf ? xmf : xfx, ymf ? ymf : yfx, fx, fy, hord, st);
+    FvTp2dArgs a{q, crx, cry, xfx, yfx, xmf ? xmf : xfx, ymf ? ymf : yfx, fx, fy, hord,
+                 fx_mean, fy_mean, q_adv_x, q_adv_y};
+    err = fvtp2d(d, g, a, st);
     if (err != cudaSuccess) return err;
     if (dl) err = delnflux(d, g, q, fx, fy, *dl, mass, dl_fx2, dl_fy2, dl_d2, nmax, st);
     return err;

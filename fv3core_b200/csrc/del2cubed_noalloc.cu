@@ -12,7 +12,13 @@
 // so the memory is reserved when the library's module is loaded, not when
 // the call runs.
 //
-// Sharing: there is one scratch array per device for the whole process.
+// Set-up: the first call on a device looks up the device address of the
+// scratch array (cudaGetSymbolAddress, with that device current) and keeps
+// it for later calls; make that first call before any stream capture.
+//
+// Sharing: there is one scratch array per device for the whole process, and
+// it keeps the contents of the last call.  Nothing in it has to start at
+// zero: every scratch value a call reads was written earlier in that call.
 // Two calls that overlap in time on the same device (different streams, or
 // different host threads without ordering) race on it and give wrong
 // results.  Callers must order their calls, for example by issuing them all

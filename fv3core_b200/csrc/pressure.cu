@@ -37,8 +37,7 @@ extern "C" int fv3b_p_grad_c(fv3b_ctx* ctx, double* uc, double* vc, const double
 // NonHydrostaticPressureGradient.__call__ (nh_p_grad.py:147-206).  pp, pk3
 // and gz are replaced by their B-grid interpolations (levels 1.., 1.., 0..);
 // the B-grid delp goes to scratch.  set_k0_and_calc_wk is folded into the
-// wind update: level 0 of pp and pk3 is read as its new value (0, ptop^akap)
-// and written by the level-0 threads.
+// wind update: level 0 of pp and pk3 is read as its new value (0, ptop^akap).
 extern "C" int fv3b_nh_p_grad(fv3b_ctx* ctx, double* u, double* v, double* pp, double* gz, double* pk3,
                               double* delp, double dt, double ptop, double akap, void* stream) {
   FV3B_REQUIRE(ctx && u && v && pp && gz && pk3 && delp, "fv3b_nh_p_grad: null argument");
@@ -46,42 +45,48 @@ extern "C" int fv3b_nh_p_grad(fv3b_ctx* ctx, double* u, double* v, double* pp, d
   const fv3b_metrics g = ctx->m;
   cudaStream_t st = (cudaStream_t)stream;
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = d.nz, nk = d.nk;
+  // The B-grid values of pp, pk3 and gz go to scratch (the reference
+  // interpolates them in place); the wind update reads only the scratch
+  // copies and writes them back into pp, pk3, gz, which replaces the
+  // reference's copy passes.
   double *wk1 = ctx->ws[0], *qx = ctx->ws[1], *qy = ctx->ws[2], *edges = ctx->ws[3];
+  double *pp_b = ctx->ws[4], *pk3_b = ctx->ws[5], *gz_b = ctx->ws[6];
   const double ptk = pow(ptop, akap);
-  FV3B_CHECK(a2b_ord4(d, g, pp, wk1, qx, qy, edges, 1, nk, st, true));
-  FV3B_CHECK(a2b_ord4(d, g, pk3, wk1, qx, qy, edges, 1, nk, st, true));
-  FV3B_CHECK(a2b_ord4(d, g, gz, wk1, qx, qy, edges, 0, nk, st, true));
+  FV3B_CHECK(a2b_ord4(d, g, pp, pp_b, qx, qy, edges, 1, nk, st, false));
+  FV3B_CHECK(a2b_ord4(d, g, pk3, pk3_b, qx, qy, edges, 1, nk, st, false));
+  FV3B_CHECK(a2b_ord4(d, g, gz, gz_b, qx, qy, edges, 0, nk, st, false));
   FV3B_CHECK(a2b_ord4(d, g, delp, wk1, qx, qy, edges, 0, nz, st, false));
-  // calc_u on [is, ie] x [js, je+1], calc_v on [is, ie+1] x [js, je]
-  FV3B_CHECK(launch_box(Box{s, e + 2, js, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+  // calc_u on [is, ie] x [js, je+1], calc_v on [is, ie+1] x [js, je] (levels
+  // [0, npz)); every interface of [is, ie+1] x [js, je+1] takes its B-grid
+  // pp, pk3, gz, with pp = 0 and pk3 = ptop^akap on top (set_k0_and_calc_wk)
+  FV3B_CHECK(launch_box(Box{s, e + 2, js, je + 2, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    auto P = [&](int ii, int jj, int dk) { return k + dk == 0 ? 0.0 : F3K(pp, ii, jj, dk); };
-    auto K3 = [&](int ii, int jj, int dk) { return k + dk == 0 ? ptk : F3K(pk3, ii, jj, dk); };
+    auto P = [&](int ii, int jj, int dk) { return k + dk == 0 ? 0.0 : F3K(pp_b, ii, jj, dk); };
+    auto K3 = [&](int ii, int jj, int dk) { return k + dk == 0 ? ptk : F3K(pk3_b, ii, jj, dk); };
     auto wk = [&](int ii, int jj) { return K3(ii, jj, 1) - K3(ii, jj, 0); };
-    if (i <= e) {
+    if (k < nz && i <= e) {
       double du = dt / (wk(i, j) + wk(i + 1, j)) *
-                  ((F3K(gz, i, j, 1) - F3(gz, i + 1, j)) * (K3(i + 1, j, 1) - K3(i, j, 0)) +
-                   (F3(gz, i, j) - F3K(gz, i + 1, j, 1)) * (K3(i, j, 1) - K3(i + 1, j, 0)));
+                  ((F3K(gz_b, i, j, 1) - F3(gz_b, i + 1, j)) * (K3(i + 1, j, 1) - K3(i, j, 0)) +
+                   (F3(gz_b, i, j) - F3K(gz_b, i + 1, j, 1)) * (K3(i, j, 1) - K3(i + 1, j, 0)));
       W3(u, i, j) = (F3(u, i, j) + du +
                      dt / (F3(wk1, i, j) + F3(wk1, i + 1, j)) *
-                         ((F3K(gz, i, j, 1) - F3(gz, i + 1, j)) * (P(i + 1, j, 1) - P(i, j, 0)) +
-                          (F3(gz, i, j) - F3K(gz, i + 1, j, 1)) * (P(i, j, 1) - P(i + 1, j, 0)))) *
+                         ((F3K(gz_b, i, j, 1) - F3(gz_b, i + 1, j)) * (P(i + 1, j, 1) - P(i, j, 0)) +
+                          (F3(gz_b, i, j) - F3K(gz_b, i + 1, j, 1)) * (P(i, j, 1) - P(i + 1, j, 0)))) *
                     F2(g.rdx, i, j);
     }
-    if (j <= je) {
+    if (k < nz && j <= je) {
       double dv = dt / (wk(i, j) + wk(i, j + 1)) *
-                  ((F3K(gz, i, j, 1) - F3(gz, i, j + 1)) * (K3(i, j + 1, 1) - K3(i, j, 0)) +
-                   (F3(gz, i, j) - F3K(gz, i, j + 1, 1)) * (K3(i, j, 1) - K3(i, j + 1, 0)));
+                  ((F3K(gz_b, i, j, 1) - F3(gz_b, i, j + 1)) * (K3(i, j + 1, 1) - K3(i, j, 0)) +
+                   (F3(gz_b, i, j) - F3K(gz_b, i, j + 1, 1)) * (K3(i, j, 1) - K3(i, j + 1, 0)));
       W3(v, i, j) = (F3(v, i, j) + dv +
                      dt / (F3(wk1, i, j) + F3(wk1, i, j + 1)) *
-                         ((F3K(gz, i, j, 1) - F3(gz, i, j + 1)) * (P(i, j + 1, 1) - P(i, j, 0)) +
-                          (F3(gz, i, j) - F3K(gz, i, j + 1, 1)) * (P(i, j, 1) - P(i, j + 1, 0)))) *
+                         ((F3K(gz_b, i, j, 1) - F3(gz_b, i, j + 1)) * (P(i, j + 1, 1) - P(i, j, 0)) +
+                          (F3(gz_b, i, j) - F3K(gz_b, i, j + 1, 1)) * (P(i, j, 1) - P(i, j + 1, 0)))) *
                     F2(g.rdy, i, j);
     }
-    if (k == 0) {
-      W3(pp, i, j) = 0.0;
-      W3(pk3, i, j) = ptk;
-    }
+    W3(pp, i, j) = P(i, j, 0);
+    W3(pk3, i, j) = K3(i, j, 0);
+    W3(gz, i, j) = F3(gz_b, i, j);
   }));
   return FV3B_OK;
 }

@@ -45,6 +45,22 @@ __device__ __forceinline__ Line2<AXIS> line2(const Dims& d, const double* p, int
   return Line2<AXIS>{p, idx2(d, t, i, j), AXIS == 0 ? 1LL : (long long)d.ni};
 }
 
+// The reference's y-corner-copied copy of q (CopyCornersXY, corners.py:64-117)
+// read on the fly from q: a point of a cube-corner block takes its copy
+// source.  Sources never lie in a corner block, so this equals the copy
+// whether or not q's own corners already hold their x copies.
+__device__ __forceinline__ double qy_at(const Dims& d, const double* q, int t, int i, int j, int k) {
+  int si, sj;
+  if (copy_corner_y(d, i, j, si, sj)) return q[idx3(d, t, si, sj, k)];
+  return q[idx3(d, t, i, j, k)];
+}
+struct LineQY {
+  const Dims* d;
+  const double* q;
+  int t, i, j, k;
+  __device__ __forceinline__ double operator()(int o) const { return qy_at(*d, q, t, i, j + o, k); }
+};
+
 // compute_al (xppm.py:148-181) for the cell at offset o of the line; pos is
 // the absolute index (along AXIS) of offset 0, s/e the compute bounds.
 template <typename Q, typename A>
@@ -81,8 +97,7 @@ __device__ __forceinline__ double ppm_flux(const Q& q, const A& dxa, double c, i
 
 // Scratch and options of one FiniteVolumeTransport call.
 struct FvTp2dArgs {
-  const double* q_base;   // field (x-corner-copied in place)
-  const double* q_y;      // y-corner-copied copy
+  const double* q_base;   // field, its cube-corner blocks holding their x copies
   const double* crx;
   const double* cry;
   const double* xfx;
@@ -110,7 +125,7 @@ inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a
   // inner PPM: fy_mean on [is-3, ie+4] x [js, je+1], fx_mean on [is, ie+1] x [js-3, je+4]
   err = launch_box(Box{s - 3, e + 5, js - 3, je + 5, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
     if (i >= s - 3 && i < e + 5 && j >= js && j < je + 2) {
-      auto q = line3<1>(d, a.q_y, t, i, j, k);
+      LineQY q{&d, a.q_base, t, i, j, k};
       auto dya = line2<1>(d, g.dya, t, i, j);
       a.fy_mean[idx3(d, t, i, j, k)] = ppm_flux(q, dya, a.cry[idx3(d, t, i, j, k)], j, js, je, mord_in);
     }
@@ -129,7 +144,7 @@ inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a
       double fyy0 = F3(a.yfx, i, j) * F3(a.fy_mean, i, j);
       double fyy1 = F3(a.yfx, i, j + 1) * F3(a.fy_mean, i, j + 1);
       W3(a.q_adv_y, i, j) =
-          (F3(a.q_y, i, j) * area + fyy0 - fyy1) / (area + F3(a.yfx, i, j) - F3(a.yfx, i, j + 1));
+          (qy_at(d, a.q_base, t, i, j, k) * area + fyy0 - fyy1) / (area + F3(a.yfx, i, j) - F3(a.yfx, i, j + 1));
     }
     if (i >= s && i < e + 4) {
       double fx10 = F3(a.xfx, i, j) * F3(a.fx_mean, i, j);
@@ -155,153 +170,6 @@ inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a
       a.fy[o] = 0.5 * (yo + a.fy_mean[o]) * a.y_unit[o];
     }
   });
-}
-
-// ---------------------------------------------------------------------------
-// Fused FiniteVolumeTransport: the three passes of fvtp2d() in one kernel.
-//
-// A 32 x 8 thread block owns a 32 x 8 tile of output points of one level.
-// It stages the q, q_y, Courant-number and area-flux tiles it needs (tile
-// plus a 3-point halo) in shared memory, computes the inner PPM means, the
-// q_i / q_j advected values and the outer PPM fluxes there, and writes only
-// fx and fy.  Every value it computes lies inside the reference's own
-// compute domain of that value, with the same operations, so results equal
-// fvtp2d()'s bit for bit.  q must already hold its x-corner copies (see
-// copy_corners_x_inplace); q_y is read through the y-corner rules.
-constexpr int FT_TX = 32, FT_TY = 8;
-
-// Line accessor into a shared-memory tile (row-major, row length `pitch`).
-struct SLine {
-  const double* p;
-  int step;
-  __device__ __forceinline__ double operator()(int o) const { return p[o * step]; }
-};
-
-struct FvTp2dFused {
-  const double* q;
-  const double *crx, *cry, *xfx, *yfx, *x_unit, *y_unit;
-  double *fx, *fy;
-  int mord_in, mord_out;
-};
-
-static __global__ void __launch_bounds__(FT_TX * FT_TY) fvtp2d_fused_kernel(const Dims d, const fv3b_metrics g,
-                                                                     const FvTp2dFused a) {
-  // tile regions (absolute storage indices)
-  constexpr int QX = FT_TX + 6, QY = FT_TY + 5;    // q:   [I0-3, I0+TX+3) x [J0-3, J0+TY+2)
-  constexpr int YX = FT_TX + 5, YY = FT_TY + 6;    // q_y: [I0-3, I0+TX+2) x [J0-3, J0+TY+3)
-  constexpr int CXX = FT_TX + 1, CXY = FT_TY + 5;  // crx, xfx, fx_mean: [I0, I0+TX+1) x [J0-3, J0+TY+2)
-  constexpr int CYX = FT_TX + 5, CYY = FT_TY + 1;  // cry, yfx, fy_mean: [I0-3, I0+TX+2) x [J0, J0+TY+1)
-  constexpr int AXX = FT_TX, AXY = FT_TY + 5;      // q_adv_x: [I0, I0+TX) x [J0-3, J0+TY+2)
-  constexpr int AYX = FT_TX + 5, AYY = FT_TY;      // q_adv_y: [I0-3, I0+TX+2) x [J0, J0+TY)
-  __shared__ double sq[QY][QX], sqy[YY][YX];
-  __shared__ double scrx[CXY][CXX], sxfx[CXY][CXX], sfxm[CXY][CXX];
-  __shared__ double scry[CYY][CYX], syfx[CYY][CYX], sfym[CYY][CYX];
-  __shared__ double sqax[AXY][AXX], sqay[AYY][AYX];
-
-  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
-  const int nbi = (e + 2 - s + FT_TX - 1) / FT_TX;
-  const int I0 = s + (blockIdx.x % nbi) * FT_TX;
-  const int J0 = js + (blockIdx.x / nbi) * FT_TY;
-  const int t = blockIdx.z, k = blockIdx.y;
-  const int tid = threadIdx.y * FT_TX + threadIdx.x;
-  constexpr int NT = FT_TX * FT_TY;
-  const long long b3 = (long long)t * d.st + (long long)k * d.sk;
-  auto inside = [&](int i, int j) { return i >= 0 && i < d.ni && j >= 0 && j < d.nj; };
-  auto ld = [&](const double* p, int i, int j) { return inside(i, j) ? p[b3 + (long long)j * d.sj + i] : 0.0; };
-
-  // stage the inputs
-  for (int x = tid; x < QX * QY; x += NT) {
-    int i = I0 - 3 + x % QX, j = J0 - 3 + x / QX;
-    sq[x / QX][x % QX] = ld(a.q, i, j);
-  }
-  for (int x = tid; x < YX * YY; x += NT) {
-    int i = I0 - 3 + x % YX, j = J0 - 3 + x / YX;
-    int si, sj;
-    sqy[x / YX][x % YX] = (inside(i, j) && copy_corner_y(d, i, j, si, sj)) ? ld(a.q, si, sj) : ld(a.q, i, j);
-  }
-  for (int x = tid; x < CXX * CXY; x += NT) {
-    int i = I0 + x % CXX, j = J0 - 3 + x / CXX;
-    scrx[x / CXX][x % CXX] = ld(a.crx, i, j);
-    sxfx[x / CXX][x % CXX] = ld(a.xfx, i, j);
-  }
-  for (int x = tid; x < CYX * CYY; x += NT) {
-    int i = I0 - 3 + x % CYX, j = J0 + x / CYX;
-    scry[x / CYX][x % CYX] = ld(a.cry, i, j);
-    syfx[x / CYX][x % CYX] = ld(a.yfx, i, j);
-  }
-  __syncthreads();
-  // inner PPM: fx_mean (x sweep of q), fy_mean (y sweep of q_y)
-  for (int x = tid; x < CXX * CXY; x += NT) {
-    int ci = x % CXX, cj = x / CXX;
-    int i = I0 + ci, j = J0 - 3 + cj;
-    if (!inside(i, j) || i + 2 >= d.ni) continue;
-    SLine q{&sq[cj][ci + 3], 1};
-    auto dxa = line2<0>(d, g.dxa, t, i, j);
-    sfxm[cj][ci] = ppm_flux(q, dxa, scrx[cj][ci], i, s, e, a.mord_in);
-  }
-  for (int x = tid; x < CYX * CYY; x += NT) {
-    int ci = x % CYX, cj = x / CYX;
-    int i = I0 - 3 + ci, j = J0 + cj;
-    if (!inside(i, j) || j + 2 >= d.nj) continue;
-    SLine q{&sqy[cj + 3][ci], YX};
-    auto dya = line2<1>(d, g.dya, t, i, j);
-    sfym[cj][ci] = ppm_flux(q, dya, scry[cj][ci], j, js, je, a.mord_in);
-  }
-  __syncthreads();
-  // q_i (fvtp2d.py:33-47) at x-sweep points, q_j (50-60) at y-sweep points
-  for (int x = tid; x < AYX * AYY; x += NT) {
-    int ci = x % AYX, cj = x / AYX;
-    int i = I0 - 3 + ci, j = J0 + cj;
-    if (!inside(i, j)) continue;
-    double area = g.area[idx2(d, t, i, j)];
-    double fyy0 = syfx[cj][ci] * sfym[cj][ci];
-    double fyy1 = syfx[cj + 1][ci] * sfym[cj + 1][ci];
-    sqay[cj][ci] = (sqy[cj + 3][ci] * area + fyy0 - fyy1) / (area + syfx[cj][ci] - syfx[cj + 1][ci]);
-  }
-  for (int x = tid; x < AXX * AXY; x += NT) {
-    int ci = x % AXX, cj = x / AXX;
-    int i = I0 + ci, j = J0 - 3 + cj;
-    if (!inside(i, j)) continue;
-    double area = g.area[idx2(d, t, i, j)];
-    double fx10 = sxfx[cj][ci] * sfxm[cj][ci];
-    double fx11 = sxfx[cj][ci + 1] * sfxm[cj][ci + 1];
-    double awx = area + sxfx[cj][ci] - sxfx[cj][ci + 1];
-    sqax[cj][ci] = (sq[cj][ci + 3] * area + fx10 - fx11) / awx;
-  }
-  __syncthreads();
-  // outer PPM and final fluxes (fvtp2d.py:63-93) for this thread's point
-  const int ti = threadIdx.x, tj = threadIdx.y;
-  const int i = I0 + ti, j = J0 + tj;
-  const long long o = b3 + (long long)j * d.sj + i;
-  if (i <= e + 1 && j <= je) {
-    SLine q{&sqay[tj][ti + 3], 1};
-    auto dxa = line2<0>(d, g.dxa, t, i, j);
-    double xo = ppm_flux(q, dxa, scrx[tj + 3][ti], i, s, e, a.mord_out);
-    a.fx[o] = 0.5 * (xo + sfxm[tj + 3][ti]) * a.x_unit[o];
-  }
-  if (i <= e && j <= je + 1) {
-    SLine q{&sqax[tj + 3][ti], AXX};
-    auto dya = line2<1>(d, g.dya, t, i, j);
-    double yo = ppm_flux(q, dya, scry[tj][ti + 3], j, js, je, a.mord_out);
-    a.fy[o] = 0.5 * (yo + sfym[tj][ti + 3]) * a.y_unit[o];
-  }
-}
-
-void note_launch();
-
-// FiniteVolumeTransport.__call__ (fvtp2d.py:249-362) without the damping
-// step, fused (see fvtp2d_fused_kernel); all npz+1 levels.
-inline cudaError_t fvtp2d_fused(const Dims d, const fv3b_metrics g, const double* q, const double* crx,
-                                const double* cry, const double* xfx, const double* yfx, const double* x_unit,
-                                const double* y_unit, double* fx, double* fy, int hord, cudaStream_t st) {
-  const int ord_in = hord == 10 ? 8 : hord;
-  FvTp2dFused a{q, crx, cry, xfx, yfx, x_unit, y_unit, fx, fy, ord_in < 0 ? -ord_in : ord_in, hord < 0 ? -hord : hord};
-  const int nbi = (d.iec + 2 - d.isc + FT_TX - 1) / FT_TX;
-  const int nbj = (d.jec + 2 - d.jsc + FT_TY - 1) / FT_TY;
-  dim3 grid(nbi * nbj, d.nk, 6), block(FT_TX, FT_TY);
-  fvtp2d_fused_kernel<<<grid, block, 0, st>>>(d, g, a);
-  note_launch();
-  return cudaGetLastError();
 }
 
 // The x half of CopyCornersXY in place (corners.py:64-117): only the 3 x 3
@@ -426,16 +294,5 @@ inline cudaError_t delnflux(const Dims d, const fv3b_metrics g, const double* q,
   });
 }
 
-// CopyCornersXY on dims (X, Y, Z_INTERFACE) (corners.py:64-117): q gets its
-// x-differenceable corners in place, qy becomes the y-differenceable copy.
-inline cudaError_t copy_corners_xy(const Dims d, double* q, double* qy, cudaStream_t st) {
-  const int full = d.ni - 1;
-  return launch_box(Box{0, full, 0, full, 0, d.nk}, st, [=] __device__(int t, int i, int j, int k) {
-    PT_SETUP(d, t, k);
-    int si, sj;
-    W3(qy, i, j) = copy_corner_y(d, i, j, si, sj) ? F3(q, si, sj) : F3(q, i, j);
-    if (copy_corner_x(d, i, j, si, sj)) W3(q, i, j) = F3(q, si, sj);
-  });
-}
 
 }  // namespace fv3b

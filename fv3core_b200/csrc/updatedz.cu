@@ -136,6 +136,7 @@ extern "C" int fv3b_update_dz_d(fv3b_ctx* ctx, const double* zs, double* zh, con
   const int full = d.ni - 1;
   double** W = ctx->ws;
   double *crx_i = W[0], *cry_i = W[1], *xfx_i = W[2], *yfx_i = W[3], *fx = W[4], *fy = W[5];
+  double *fx_mean = W[7], *fy_mean = W[8], *q_adv_x = W[9], *q_adv_y = W[10];
   double *gzx_diff = W[11], *gzy_diff = W[12], *d2 = W[13];
   const double* gk = colp(ctx, COL_SPLINE_GK);
   const double* beta = colp(ctx, COL_SPLINE_BETA);
@@ -170,7 +171,9 @@ extern "C" int fv3b_update_dz_d(fv3b_ctx* ctx, const double* zs, double* zh, con
     }
   }));
   FV3B_CHECK(copy_corners_x_inplace(d, zh, st));
-  FV3B_CHECK(fvtp2d_fused(d, g, zh, crx_i, cry_i, xfx_i, yfx_i, xfx_i, yfx_i, fx, fy, ctx->dzd_hord_tm, st));
+  FvTp2dArgs a{zh, crx_i, cry_i, xfx_i, yfx_i, xfx_i, yfx_i, fx, fy, ctx->dzd_hord_tm,
+               fx_mean, fy_mean, q_adv_x, q_adv_y};
+  FV3B_CHECK(fvtp2d(d, g, a, st));
   // DelnFluxNoSG on npz + 1 levels with the raw damp_vt column
   DelnCol dl{colp(ctx, COL_NORD_V), colp(ctx, COL_DAMP_VT)};
   FV3B_CHECK(delnflux_nosg(d, g, zh, gzx_diff, gzy_diff, dl, d2, false, ctx->dsw.nmax_v, st, nk));

@@ -285,8 +285,11 @@ double* fv3b_acoustics_temporary(fv3b_ctx* ctx, const char* name);
  * allocates nothing; its scratch is a fixed file-scope device array reserved
  * when the library is loaded.  Grids with 6*(npz+1)*(npx+2*n_halo+1)^2 above
  * 1,500,000 (larger than C48 L79) are rejected with FV3B_ERR_ARGUMENT.  The
- * scratch is shared by every caller on a device: calls must not overlap in
- * time (issue them on one stream, or order them).  metrics: as for
+ * first call on a device looks up the scratch's device address (make it
+ * before any stream capture).  The scratch is shared by every caller on a
+ * device and keeps the last call's contents (nothing in it needs to start at
+ * zero): calls must not overlap in time (issue them on one stream, or order
+ * them).  metrics: as for
  * fv3b_ctx_create (del6_u, del6_v and rarea are read).
  */
 int fv3b_del2cubed_noalloc(const fv3b_grid_dims* dims, const fv3b_metrics* metrics, double* qdel, double cd, int nmax,
