@@ -1,6 +1,8 @@
 #!/usr/bin/env python
 """Acoustic-substep throughput on B200: AcousticDynamics (fv3core's dyn_core)
-on a C384 L79 cubed sphere, all six tiles on one GPU, FP64.
+on a C384 L79 cubed sphere, all six tiles on one GPU, in the mixed-precision
+build (FP32 fields and arithmetic, FP64 column solves) with the plain FP64
+build measured beside it, and the mixed build's error against FP64.
 
 One step = one AcousticDynamics call = n_split (6) acoustic substeps over
 the whole cube, on a Jablonowski-Williamson baroclinic-wave state with seeded
@@ -32,7 +34,6 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-BYTES_PER_CELL_LEVEL = 272  # compulsory FP64 state traffic per cell-level per substep (34 x 8 B)
 METRIC = "C384 L79 acoustic-substep cell-levels/s"
 UNIT = "cell-levels/s"
 
@@ -117,10 +118,15 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- workload
-def build_problem(n, npz, n_split, seed, device="cuda"):
+def build_problem(n, npz, n_split, seed, device="cuda", precision="f64", grid=None, state0=None):
+    """GridData, AcousticDynamics and a device state for one build.  grid and
+    state0 (a host baroclinic state) may be passed in to share them between
+    the two builds."""
+    import types
+
+    import numpy as np
     import torch
 
-    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
     from fv3core_b200 import _lib
     from fv3core_b200.config import baroclinic_acoustic_config
     from fv3core_b200.grid import CubedSphereGrid
@@ -131,24 +137,19 @@ def build_problem(n, npz, n_split, seed, device="cuda"):
     from fv3core_b200.stencils.dyn_core import AcousticDynamics
     from fv3core_b200.storage import to_device
 
-    grid = CubedSphereGrid(n, 3)
-    st = baroclinic_state(grid, npz, seed=seed)
-    gd = GridData(grid, npz, device=device)
+    grid = CubedSphereGrid(n, 3) if grid is None else grid
+    st = baroclinic_state(grid, npz, seed=seed) if state0 is None else state0
+    gd = GridData(grid, npz, device=device, precision=precision)
+    dtype = gd.grid_indexing.dtype
     sf = StencilFactory(StencilConfig(), gd.grid_indexing)
     cfg = baroclinic_acoustic_config(n_split=n_split)
-    import types
-
     state = types.SimpleNamespace()
     for name in _lib.DYCORE_FIELDS:
-        a = st[name] if name in st else None
-        if a is None:
-            state_shape = st["delp"].shape if name not in ("wsd",) else st["phis"].shape
-            import numpy as np
-
-            a = np.zeros(state_shape)
-        setattr(state, name, to_device(a))
         if name in st:
-            del st[name]
+            a = st[name]
+        else:
+            a = np.zeros(st["phis"].shape if name == "wsd" else st["delp"].shape)
+        setattr(state, name, to_device(a, dtype=dtype))
     ad = AcousticDynamics(DeviceCubedSphereCommunicator(gd.grid_indexing), sf, gd, gd, 0, False, False, cfg,
                           st["ak"], st["bk"], st["pfull"], state.phis)
     state.mdt = 225.0
@@ -167,6 +168,18 @@ E2E_OUT = ("u", "v", "w", "delz", "delp", "pt", "pe", "pk", "wsd", "omga", "ua",
            "cxd", "cyd", "pkz", "peln", "q_con", "diss_estd")
 
 
+def _compute(t, n, npz):
+    h = 3
+    return t[:, :npz, h:h + n, h:h + n]
+
+
+def _max_rel(a, b, n, npz):
+    import torch
+
+    a, b = _compute(a, n, npz).double(), _compute(b, n, npz).double()
+    return float((torch.abs(a - b) / torch.clamp(torch.abs(b), min=1e-30)).max())
+
+
 def run_cuda(args):
     import torch
 
@@ -180,101 +193,142 @@ def run_cuda(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from fv3core_b200 import _lib
+    from fv3core_b200.grid import CubedSphereGrid
+    from fv3core_b200.initial_state import baroclinic_state
 
     n, npz, n_split = args.n, args.npz, args.n_split
-    gd, ad, state = build_problem(n, npz, n_split, seed=1234 + rank)
     stream = torch.cuda.current_stream()
     cells = 6 * n * n * npz
+    grid = CubedSphereGrid(n, 3)
+    state0 = baroclinic_state(grid, npz, seed=1234 + rank)
+    precisions = {"both": ["f32", "f64"], "mixed": ["f32"], "f64": ["f64"]}[args.precision]
+    problems = {p: build_problem(n, npz, n_split, 1234 + rank, precision=p, grid=grid, state0=state0)
+                for p in precisions}
+    del state0
 
     def barrier():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
 
-    for _ in range(args.warmup):
-        ad(state)
-    barrier()
-    launches0 = _lib.launch_count()
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    # error of the mixed build against FP64 after one call (one dynamics
+    # step's acoustic part) from the same initial state
+    mixed_error = None
+    if len(precisions) == 2:
+        problems["f32"][1](problems["f32"][2])
+        problems["f64"][1](problems["f64"][2])
         barrier()
-        torch.cuda.nvtx.range_push("timed")
-        start.record(stream)
-        for _ in range(args.steps):
-            ad(state)
-        stop.record(stream)
-        torch.cuda.nvtx.range_pop()
-        barrier()
-    launches = _lib.launch_count() - launches0
-    ms = start.elapsed_time(stop) / args.steps
-    clocks = clk.summary()
-    h = 3
-    finite = all(bool(torch.isfinite(getattr(state, k)[:, :npz, h:h + n, h:h + n]).all().item())
-                 for k in ("u", "v", "w", "delp", "pt", "delz"))
+        mixed_error = {k: _max_rel(getattr(problems["f32"][2], k), getattr(problems["f64"][2], k), n, npz)
+                       for k in ("delp", "pt", "delz", "q_con")}
+        mixed_error["after"] = "one AcousticDynamics call (n_split acoustic substeps) from the same state"
 
-    # end to end through the public API: pinned host state in, results out, every step
-    host = {k: torch.empty(getattr(state, k).shape, dtype=torch.float64, pin_memory=True)
+    results = {}
+    for prec in precisions:
+        gd, ad, state = problems[prec]
+        for _ in range(args.warmup):
+            ad(state)
+        barrier()
+        launches0 = _lib.launch_count(prec)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            barrier()
+            torch.cuda.nvtx.range_push("timed" if prec == precisions[0] else "timed_" + prec)
+            start.record(stream)
+            for _ in range(args.steps):
+                ad(state)
+            stop.record(stream)
+            torch.cuda.nvtx.range_pop()
+            barrier()
+        launches = _lib.launch_count(prec) - launches0
+        ms = start.elapsed_time(stop) / args.steps
+        finite = all(bool(torch.isfinite(_compute(getattr(state, k), n, npz)).all().item())
+                     for k in ("u", "v", "w", "delp", "pt", "delz"))
+        results[prec] = {"ms": ms, "launches": launches, "clocks": clk.summary(), "finite": finite}
+
+    # end to end through the public API for the headline build: the state
+    # copied in from pinned host memory and the results copied back, every step
+    head = precisions[0]
+    gd, ad, state = problems[head]
+    host = {k: torch.empty(getattr(state, k).shape, dtype=getattr(state, k).dtype, pin_memory=True)
             for k in set(E2E_IN) | set(E2E_OUT)}
-    for k, h in host.items():
-        h.copy_(getattr(state, k))
+    for k, hb in host.items():
+        hb.copy_(getattr(state, k))
     torch.cuda.synchronize()
-    h2d = sum(host[k].numel() * 8 for k in E2E_IN)
-    d2h = sum(host[k].numel() * 8 for k in E2E_OUT)
+    h2d = sum(host[k].numel() * host[k].element_size() for k in E2E_IN)
+    d2h = sum(host[k].numel() * host[k].element_size() for k in E2E_OUT)
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
-    for _ in range(1):  # one untimed warm-up round trip
+
+    def e2e_step():
         for k in E2E_IN:
             getattr(state, k).copy_(host[k], non_blocking=True)
         ad(state)
         for k in E2E_OUT:
             host[k].copy_(getattr(state, k), non_blocking=True)
+
+    e2e_step()  # untimed warm-up round trip
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(e2e_steps):
-        for k in E2E_IN:
-            getattr(state, k).copy_(host[k], non_blocking=True)
-        ad(state)
-        for k in E2E_OUT:
-            host[k].copy_(getattr(state, k), non_blocking=True)
+        e2e_step()
     e1.record(stream)
     barrier()
     e2e_ms = e0.elapsed_time(e1) / e2e_steps
 
     # max over ranks
     if dist is not None:
-        t = torch.tensor([ms, e2e_ms], device="cuda", dtype=torch.float64)
+        vals = [results[p]["ms"] for p in precisions] + [e2e_ms]
+        t = torch.tensor(vals, device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
-    value = world * cells * n_split / (ms * 1e-3)
-    e2e_value = world * cells * n_split / (e2e_ms * 1e-3)
+        for q, p in enumerate(precisions):
+            results[p]["ms"] = float(t[q])
+        e2e_ms = float(t[-1])
     peak, peak_kind = _measured_peak()
-    achieved = BYTES_PER_CELL_LEVEL * cells * n_split / (ms * 1e-3) / 1e9
+
+    def roof(prec):
+        width = 4 if prec == "f32" else 8
+        achieved = 34 * width * cells * n_split / (results[prec]["ms"] * 1e-3) / 1e9
+        return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "peak_source": peak_kind,
+                "scope": f"whole AcousticDynamics call: {34 * width} B compulsory traffic per cell-level per "
+                         "substep (34 field transfers at the stored width)"}
+
+    ms = results[head]["ms"]
+    value = world * cells * n_split / (ms * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded baroclinic-wave state)",
+        "vs_baseline": None,
+        "dtype": "mixed: f32 fields and arithmetic, f64 column solves" if head == "f32" else "f64",
+        "data": "synthetic (seeded baroclinic-wave state)",
         "config": {
-            "workload": f"AcousticDynamics C{n} L{npz}, n_split={n_split}, 6 tiles on one GPU, FP64, nonhydrostatic",
+            "workload": f"AcousticDynamics C{n} L{npz}, n_split={n_split}, 6 tiles on one GPU, nonhydrostatic, "
+                        + ("mixed precision" if head == "f32" else "FP64"),
             "n": n, "npz": npz, "n_split": n_split, "dt_atmos": 225.0, "cell_levels": cells,
-            "l2": "inputs larger than L2 (each 3-D field 0.59 GB at C384 L79); no flush",
+            "l2": "inputs larger than L2 (each 3-D field 0.29-0.59 GB at C384 L79); no flush",
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
         },
-        "clocks": clocks,
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "ms_per_step": e2e_ms, "steps": e2e_steps},
-        "gpu_launches": launches,
-        "roofline": {
-            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "peak_source": peak_kind,
-            "scope": "whole AcousticDynamics call: 272 B compulsory traffic per cell-level per substep",
-        },
-        "finite": finite,
+        "clocks": results[head]["clocks"],
+        "e2e": {"value": world * cells * n_split / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "steps": e2e_steps},
+        "gpu_launches": results[head]["launches"],
+        "roofline": roof(head),
+        "finite": results[head]["finite"],
     }
+    if "f64" in results and head != "f64":
+        r = results["f64"]
+        line["fp64"] = {"value": world * cells * n_split / (r["ms"] * 1e-3), "ms_per_step": r["ms"],
+                        "roofline": roof("f64"), "gpu_launches": r["launches"], "clocks": r["clocks"],
+                        "finite": r["finite"]}
+        line["mixed_speedup_vs_fp64"] = r["ms"] / ms
+    if mixed_error is not None:
+        line["mixed_error_vs_fp64"] = mixed_error
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(1, args.cpu_n, args.cpu_npz)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    gd.close()
+    for gd, _, _ in problems.values():
+        gd.close()
     if dist is not None:
         dist.destroy_process_group()
 
@@ -365,6 +419,8 @@ def main():
     ap.add_argument("--n", type=int, default=384)
     ap.add_argument("--npz", type=int, default=79)
     ap.add_argument("--n-split", type=int, default=6)
+    ap.add_argument("--precision", choices=["both", "mixed", "f64"], default="both",
+                    help="both: the mixed-precision build is the headline, FP64 is measured beside it")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-n", type=int, default=48, help="resolution of the CPU baseline sample")
     ap.add_argument("--cpu-npz", type=int, default=79)

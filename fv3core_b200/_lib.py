@@ -8,8 +8,12 @@ import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfv3core_b200.so")
+# the FP64 build and the mixed-precision build (FP32 fields, FP64 column solves)
+LIB_PATHS = {"f64": LIB_PATH, "f32": os.path.join(_HERE, "libfv3core_b200_f32.so")}
 
-_lib = None
+_libs = {}
+# precision of each context, by its address (a context belongs to one build)
+_ctx_precision = {}
 
 P = ctypes.c_void_p
 D = ctypes.c_double
@@ -87,15 +91,17 @@ class DycoreState(ctypes.Structure):
                                                   ("ks", I32)]
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
+def lib(precision="f64"):
+    if precision not in LIB_PATHS:
+        raise ValueError(f"precision must be one of {sorted(LIB_PATHS)}, got {precision!r}")
+    if precision not in _libs:
+        path = LIB_PATHS[precision]
+        if not os.path.exists(path):
             raise ImportError(
-                f"{LIB_PATH} is missing: build it with `python -m fv3core_b200.build` "
+                f"{path} is missing: build it with `python -m fv3core_b200.build` "
                 "(there is no CPU fallback)"
             )
-        L = ctypes.CDLL(LIB_PATH)
+        L = ctypes.CDLL(path)
         L.fv3b_last_error.restype = ctypes.c_char_p
         L.fv3b_version.restype = ctypes.c_char_p
         L.fv3b_launch_count.restype = ctypes.c_longlong
@@ -114,21 +120,32 @@ def lib():
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = ctypes.c_void_p
-        _lib = L
-    return _lib
+        _libs[precision] = L
+    return _libs[precision]
 
 
-def call(name, dims, *args):
-    rc = getattr(lib(), name)(ctypes.byref(dims), *args)
+def register_context(ctx, precision):
+    _ctx_precision[ctx.value] = precision
+
+
+def context_precision(ctx):
+    value = ctx.value if isinstance(ctx, ctypes.c_void_p) else ctx
+    return _ctx_precision.get(value, "f64")
+
+
+def call(name, dims, *args, precision="f64"):
+    L = lib(precision)
+    rc = getattr(L, name)(ctypes.byref(dims), *args)
     if rc != 0:
-        msg = lib().fv3b_last_error().decode()
+        msg = L.fv3b_last_error().decode()
         raise ERRORS.get(rc, RuntimeError)(f"{name} failed ({rc}): {msg}")
 
 
 def call_ctx(name, ctx, *args):
-    rc = getattr(lib(), name)(ctx, *args)
+    L = lib(context_precision(ctx))
+    rc = getattr(L, name)(ctx, *args)
     if rc != 0:
-        msg = lib().fv3b_last_error().decode()
+        msg = L.fv3b_last_error().decode()
         raise ERRORS.get(rc, RuntimeError)(f"{name} failed ({rc}): {msg}")
 
 
@@ -138,6 +155,6 @@ def exported_symbols():
     ] + list(CTX_SIGNATURES) + list(PTR_SIGNATURES)
 
 
-def launch_count():
+def launch_count(precision="f64"):
     """Kernel launches issued by the library so far."""
-    return int(lib().fv3b_launch_count())
+    return int(lib(precision).fv3b_launch_count())

@@ -8,42 +8,42 @@
 namespace fv3b {
 
 namespace a2b {
-constexpr double C1 = 2.0 / 3.0, C2 = -1.0 / 6.0;
-constexpr double B1 = 7.0 / 12.0, B2 = -1.0 / 12.0;
-constexpr double A1 = 9.0 / 16.0, A2 = -1.0 / 16.0;
+constexpr real C1 = RC(2.0) / RC(3.0), C2 = -RC(1.0) / RC(6.0);
+constexpr real B1 = RC(7.0) / RC(12.0), B2 = -RC(1.0) / RC(12.0);
+constexpr real A1 = RC(9.0) / RC(16.0), A2 = -RC(1.0) / RC(16.0);
 
 // extrap_corner (a2b_ord4.py:45-57) with the grid-only ratio x1 / (x2 - x1)
 // of its great-circle distances precomputed (fv3b_metrics.a2b_extrap)
-__device__ __forceinline__ double extrap(double ratio, double qa, double qb) { return qa + ratio * (qa - qb); }
+__device__ __forceinline__ real extrap(real ratio, real qa, real qb) { return qa + ratio * (qa - qb); }
 
 // ppm_volume_mean edge formulas (a2b_ord4.py:340-451) along one axis; L(o)
 // reads qin at offset o, G(o) the A-grid spacing.
 template <typename L, typename Gs>
-__device__ __forceinline__ double vm_edge1(const L& q, const Gs& g) {
-  double g_in = g(1) / g(0), g_ou = g(-2) / g(-1);
-  return 0.5 * (((2.0 + g_in) * q(0) - q(1)) / (1.0 + g_in) + ((2.0 + g_ou) * q(-1) - q(-2)) / (1.0 + g_ou));
+__device__ __forceinline__ real vm_edge1(const L& q, const Gs& g) {
+  real g_in = g(1) / g(0), g_ou = g(-2) / g(-1);
+  return RC(0.5) * (((RC(2.0) + g_in) * q(0) - q(1)) / (RC(1.0) + g_in) + ((RC(2.0) + g_ou) * q(-1) - q(-2)) / (RC(1.0) + g_ou));
 }
 template <typename L, typename Gs>
-__device__ __forceinline__ double vm_edge2(const L& q, const Gs& g) {
-  double g_in = g(0) / g(-1), g_ou = g(-3) / g(-2);
-  double left = 0.5 * (((2.0 + g_in) * q(-1) - q(0)) / (1.0 + g_in) + ((2.0 + g_ou) * q(-2) - q(-3)) / (1.0 + g_ou));
-  double right = B2 * (q(-1) + q(2)) + B1 * (q(0) + q(1));
-  return (3.0 * (g_in * q(-1) + q(0)) - (g_in * left + right)) / (2.0 + 2.0 * g_in);
+__device__ __forceinline__ real vm_edge2(const L& q, const Gs& g) {
+  real g_in = g(0) / g(-1), g_ou = g(-3) / g(-2);
+  real left = RC(0.5) * (((RC(2.0) + g_in) * q(-1) - q(0)) / (RC(1.0) + g_in) + ((RC(2.0) + g_ou) * q(-2) - q(-3)) / (RC(1.0) + g_ou));
+  real right = B2 * (q(-1) + q(2)) + B1 * (q(0) + q(1));
+  return (RC(3.0) * (g_in * q(-1) + q(0)) - (g_in * left + right)) / (RC(2.0) + RC(2.0) * g_in);
 }
 template <typename L, typename Gs>
-__device__ __forceinline__ double vm_edge3(const L& q, const Gs& g) {
-  double g_in = g(-2) / g(-1), g_ou = g(1) / g(0);
-  return 0.5 * (((2.0 + g_in) * q(-1) - q(-2)) / (1.0 + g_in) + ((2.0 + g_ou) * q(0) - q(1)) / (1.0 + g_ou));
+__device__ __forceinline__ real vm_edge3(const L& q, const Gs& g) {
+  real g_in = g(-2) / g(-1), g_ou = g(1) / g(0);
+  return RC(0.5) * (((RC(2.0) + g_in) * q(-1) - q(-2)) / (RC(1.0) + g_in) + ((RC(2.0) + g_ou) * q(0) - q(1)) / (RC(1.0) + g_ou));
 }
 template <typename L, typename Gs>
-__device__ __forceinline__ double vm_edge4(const L& q, const Gs& g) {
-  double g_in = g(-1) / g(0), g_ou = g(2) / g(1);
-  double right = 0.5 * (((2.0 + g_in) * q(0) - q(-1)) / (1.0 + g_in) + ((2.0 + g_ou) * q(1) - q(2)) / (1.0 + g_ou));
-  double left = B2 * (q(-3) + q(0)) + B1 * (q(-2) + q(-1));
-  return (3.0 * (q(-1) + g_in * q(0)) - (g_in * right + left)) / (2.0 + 2.0 * g_in);
+__device__ __forceinline__ real vm_edge4(const L& q, const Gs& g) {
+  real g_in = g(-1) / g(0), g_ou = g(2) / g(1);
+  real right = RC(0.5) * (((RC(2.0) + g_in) * q(0) - q(-1)) / (RC(1.0) + g_in) + ((RC(2.0) + g_ou) * q(1) - q(2)) / (RC(1.0) + g_ou));
+  real left = B2 * (q(-3) + q(0)) + B1 * (q(-2) + q(-1));
+  return (RC(3.0) * (q(-1) + g_in * q(0)) - (g_in * right + left)) / (RC(2.0) + RC(2.0) * g_in);
 }
 template <typename L, typename Gs>
-__device__ __forceinline__ double volume_mean(const L& q, const Gs& g, int pos, int s, int e) {
+__device__ __forceinline__ real volume_mean(const L& q, const Gs& g, int pos, int s, int e) {
   // statement order of ppm_volume_mean_x: general, s, s+1, e+1, e
   if (pos == e) return vm_edge4(q, g);
   if (pos == e + 1) return vm_edge3(q, g);
@@ -55,13 +55,13 @@ __device__ __forceinline__ double volume_mean(const L& q, const Gs& g, int pos, 
 
 template <int AXIS>
 struct A2BLine {
-  const double* p;
+  const real* p;
   long long base, step;
-  __device__ __forceinline__ double operator()(int o) const { return p[base + o * step]; }
+  __device__ __forceinline__ real operator()(int o) const { return p[base + o * step]; }
 };
 
-inline cudaError_t a2b_ord4(const Dims d, const fv3b_metrics g, double* qin, double* qout, double* qx, double* qy,
-                            double* edges, int k0, int k1, cudaStream_t st, bool replace = false) {
+inline cudaError_t a2b_ord4(const Dims d, const fv3b_metrics g, real* qin, real* qout, real* qx, real* qy,
+                            real* edges, int k0, int k1, cudaStream_t st, bool replace = false) {
   using namespace a2b;
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, h = d.h, n = d.n;
   cudaError_t err;
@@ -76,7 +76,7 @@ inline cudaError_t a2b_ord4(const Dims d, const fv3b_metrics g, double* qin, dou
     const int i = side < 2 ? s + a : (side == 2 ? s : e + 1);
     const int j = side == 0 ? js : (side == 1 ? je + 1 : js + a);
     bool wcol = i == s, ecol = i == e + 1, srow = j == js, nrow = j == je + 1;
-    double v;
+    real v;
     if ((wcol || ecol) && (srow || nrow)) {
       // offsets (near, far) of the three extrapolations; the reference's
       // _nw/_se stencils run at the (ie+1, js) / (is, je+1) corners
@@ -95,29 +95,29 @@ inline cudaError_t a2b_ord4(const Dims d, const fv3b_metrics g, double* qin, dou
         memcpy(o, oo, sizeof(o));
       }
       const int corner = (wcol && srow) ? 0 : (ecol && srow) ? 1 : (ecol && nrow) ? 2 : 3;
-      const double* ratio = g.a2b_extrap + (t * 4 + corner) * 3;
-      double ec[3];
+      const real* ratio = g.a2b_extrap + (t * 4 + corner) * 3;
+      real ec[3];
       for (int m = 0; m < 3; ++m) {
         int i1 = i + o[m][0], j1 = j + o[m][1], i2 = i + o[m][2], j2 = j + o[m][3];
         ec[m] = extrap(ratio[m], F3(qin, i1, j1), F3(qin, i2, j2));
       }
-      v = (ec[0] + ec[1] + ec[2]) * (1.0 / 3.0);
+      v = (ec[0] + ec[1] + ec[2]) * (RC(1.0) / RC(3.0));
     } else if (wcol || ecol) {
-      const double* ef = wcol ? g.edge_w : g.edge_e;
-      double wgt = ef[t * (n + 1) + (j - h)];
+      const real* ef = wcol ? g.edge_w : g.edge_e;
+      real wgt = ef[t * (n + 1) + (j - h)];
       auto q2 = [&](int jj) {
         return (F3(qin, i - 1, jj) * F2(g.dxa, i, jj) + F3(qin, i, jj) * F2(g.dxa, i - 1, jj)) /
                (F2(g.dxa, i - 1, jj) + F2(g.dxa, i, jj));
       };
-      v = wgt * q2(j - 1) + (1.0 - wgt) * q2(j);
+      v = wgt * q2(j - 1) + (RC(1.0) - wgt) * q2(j);
     } else {
-      const double* ef = srow ? g.edge_s : g.edge_n;
-      double wgt = ef[t * (n + 1) + (i - h)];
+      const real* ef = srow ? g.edge_s : g.edge_n;
+      real wgt = ef[t * (n + 1) + (i - h)];
       auto q1 = [&](int ii) {
         return (F3(qin, ii, j - 1) * F2(g.dya, ii, j) + F3(qin, ii, j) * F2(g.dya, ii, j - 1)) /
                (F2(g.dya, ii, j - 1) + F2(g.dya, ii, j));
       };
-      v = wgt * q1(i - 1) + (1.0 - wgt) * q1(i);
+      v = wgt * q1(i - 1) + (RC(1.0) - wgt) * q1(i);
     }
     W3(qout, i, j) = v;
     W3(edges, i, j) = v;
@@ -143,25 +143,25 @@ inline cudaError_t a2b_ord4(const Dims d, const fv3b_metrics g, double* qin, dou
   // a2b_interpolation (a2b_ord4.py:286-310) on interior cell corners
   err = launch_box(Box{s + 1, e + 1, js + 1, je + 1, k0, k1}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    double qxx = A2 * (F3(qx, i, j - 2) + F3(qx, i, j + 1)) + A1 * (F3(qx, i, j - 1) + F3(qx, i, j));
-    double qyy = A2 * (F3(qy, i - 2, j) + F3(qy, i + 1, j)) + A1 * (F3(qy, i - 1, j) + F3(qy, i, j));
+    real qxx = A2 * (F3(qx, i, j - 2) + F3(qx, i, j + 1)) + A1 * (F3(qx, i, j - 1) + F3(qx, i, j));
+    real qyy = A2 * (F3(qy, i - 2, j) + F3(qy, i + 1, j)) + A1 * (F3(qy, i - 1, j) + F3(qy, i, j));
     if (j == js + 1) {
-      double up = A2 * (F3(qx, i, j - 1) + F3(qx, i, j + 2)) + A1 * (F3(qx, i, j) + F3(qx, i, j + 1));
+      real up = A2 * (F3(qx, i, j - 1) + F3(qx, i, j + 2)) + A1 * (F3(qx, i, j) + F3(qx, i, j + 1));
       qxx = C1 * (F3(qx, i, j - 1) + F3(qx, i, j)) + C2 * (F3(edges, i, j - 1) + up);
     }
     if (j == je) {
-      double lo = A2 * (F3(qx, i, j - 3) + F3(qx, i, j)) + A1 * (F3(qx, i, j - 2) + F3(qx, i, j - 1));
+      real lo = A2 * (F3(qx, i, j - 3) + F3(qx, i, j)) + A1 * (F3(qx, i, j - 2) + F3(qx, i, j - 1));
       qxx = C1 * (F3(qx, i, j - 1) + F3(qx, i, j)) + C2 * (F3(edges, i, j + 1) + lo);
     }
     if (i == s + 1) {
-      double right = A2 * (F3(qy, i - 1, j) + F3(qy, i + 2, j)) + A1 * (F3(qy, i, j) + F3(qy, i + 1, j));
+      real right = A2 * (F3(qy, i - 1, j) + F3(qy, i + 2, j)) + A1 * (F3(qy, i, j) + F3(qy, i + 1, j));
       qyy = C1 * (F3(qy, i - 1, j) + F3(qy, i, j)) + C2 * (F3(edges, i - 1, j) + right);
     }
     if (i == e) {
-      double left = A2 * (F3(qy, i - 3, j) + F3(qy, i, j)) + A1 * (F3(qy, i - 2, j) + F3(qy, i - 1, j));
+      real left = A2 * (F3(qy, i - 3, j) + F3(qy, i, j)) + A1 * (F3(qy, i - 2, j) + F3(qy, i - 1, j));
       qyy = C1 * (F3(qy, i - 1, j) + F3(qy, i, j)) + C2 * (F3(edges, i + 1, j) + left);
     }
-    W3(qout, i, j) = 0.5 * (qxx + qyy);
+    W3(qout, i, j) = RC(0.5) * (qxx + qyy);
   });
   if (err != cudaSuccess || !replace) return err;
   return launch_box(Box{s, e + 2, js, je + 2, k0, k1}, st, [=] __device__(int t, int i, int j, int k) {

@@ -14,27 +14,27 @@ using namespace fv3b;
 
 namespace {
 
-constexpr double C1 = -2.0 / 14.0, C2 = 11.0 / 14.0, C3 = 5.0 / 14.0;
-constexpr double A1 = 9.0 / 16.0, A2 = -1.0 / 16.0;
-constexpr double BIG = 1e30;
+constexpr real C1 = -RC(2.0) / RC(14.0), C2 = RC(11.0) / RC(14.0), C3 = RC(5.0) / RC(14.0);
+constexpr real A1 = RC(9.0) / RC(16.0), A2 = -RC(1.0) / RC(16.0);
+constexpr real BIG = RC(1e30);
 
 }  // namespace
 
-extern "C" int fv3b_c_sw(fv3b_ctx* ctx, double* delp, double* pt, const double* u, const double* v, double* w,
-                         double* uc, double* vc, double* ua, double* va, double* ut, double* vt, double* divgd,
-                         double* omga, double dt2, int nord, double* delpc, double* ptc, void* stream) {
+extern "C" int fv3b_c_sw(fv3b_ctx* ctx, real* delp, real* pt, const real* u, const real* v, real* w,
+                         real* uc, real* vc, real* ua, real* va, real* ut, real* vt, real* divgd,
+                         real* omga, double dt2, int nord, real* delpc, real* ptc, void* stream) {
   FV3B_REQUIRE(ctx && delp && pt && u && v && w && uc && vc && ua && va && ut && vt && divgd && omga && delpc && ptc,
                "fv3b_c_sw: null argument");
   const Dims d = ctx->d;
   const fv3b_metrics g = ctx->m;
   cudaStream_t st = (cudaStream_t)stream;
-  double* utmp = ctx->ws[0];
-  double* vtmp = ctx->ws[1];
-  double* tfx = ctx->ws[2];
-  double* tfx1 = ctx->ws[3];
-  double* tfx2 = ctx->ws[4];
-  double* tke = ctx->ws[5];
-  double* tvort = ctx->ws[6];
+  real* utmp = ctx->ws[0];
+  real* vtmp = ctx->ws[1];
+  real* tfx = ctx->ws[2];
+  real* tfx1 = ctx->ws[3];
+  real* tfx2 = ctx->ws[4];
+  real* tke = ctx->ws[5];
+  real* tvort = ctx->ws[6];
   const int nz = d.nz;
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
   const int full = d.ni - 1;  // halo domain is [0, n+2h)
@@ -47,23 +47,23 @@ extern "C" int fv3b_c_sw(fv3b_ctx* ctx, double* delp, double* pt, const double* 
   // (d2a2c_vect.py:18-21, 141-182, 248-260)
   FV3B_CHECK(launch_box(Box{0, full, 0, full, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    double ut_ = BIG, vt_ = BIG;
+    real ut_ = BIG, vt_ = BIG;
     if (i >= lo && i <= hi && j >= lo && j <= hi) {
       ut_ = A2 * (F3(u, i, j - 1) + F3(u, i, j + 2)) + A1 * (F3(u, i, j) + F3(u, i, j + 1));
       vt_ = A2 * (F3(v, i - 1, j) + F3(v, i + 2, j)) + A1 * (F3(v, i, j) + F3(v, i + 1, j));
     }
     bool avg = (j < js + off) || (j >= je - off + 1) || (i < s + off) || (i >= e - off + 1);
     if (avg) {
-      ut_ = 0.5 * (F3(u, i, j) + F3(u, i, j + 1));
-      vt_ = 0.5 * (F3(v, i, j) + F3(v, i + 1, j));
+      ut_ = RC(0.5) * (F3(u, i, j) + F3(u, i, j + 1));
+      vt_ = RC(0.5) * (F3(v, i, j) + F3(v, i + 1, j));
     }
     W3(utmp, i, j) = ut_;
     W3(vtmp, i, j) = vt_;
     // initialize_delpc_ptc (c_sw.py:372-376)
-    W3(delpc, i, j) = 0.0;
-    W3(ptc, i, j) = 0.0;
+    W3(delpc, i, j) = RC(0.0);
+    W3(ptc, i, j) = RC(0.0);
     if (i >= s - 2 && i < e + 3 && j >= js - 2 && j < je + 3) {
-      double cs = F2(g.cosa_s, i, j), r2 = F2(g.rsin2, i, j);
+      real cs = F2(g.cosa_s, i, j), r2 = F2(g.rsin2, i, j);
       W3(ua, i, j) = (ut_ - vt_ * cs) * r2;
       W3(va, i, j) = (vt_ - ut_ * cs) * r2;
     }
@@ -72,31 +72,31 @@ extern "C" int fv3b_c_sw(fv3b_ctx* ctx, double* delp, double* pt, const double* 
   FV3B_CHECK(launch_box(Box{s - 3, e + 4, js - 1, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
     CornerRule r;
-    if (corner_x(d, i, j, true, -1.0, 1.0, 1.0, -1.0, r)) W3(utmp, i, j) = r.mult * F3(vtmp, i + r.di, j + r.dj);
-    if (corner_x(d, i, j, false, -1.0, 1.0, 1.0, -1.0, r)) W3(ua, i, j) = r.mult * F3(va, i + r.di, j + r.dj);
+    if (corner_x(d, i, j, true, -RC(1.0), RC(1.0), RC(1.0), -RC(1.0), r)) W3(utmp, i, j) = r.mult * F3(vtmp, i + r.di, j + r.dj);
+    if (corner_x(d, i, j, false, -RC(1.0), RC(1.0), RC(1.0), -RC(1.0), r)) W3(ua, i, j) = r.mult * F3(va, i + r.di, j + r.dj);
   }));
   // ut_main + east_west_edges (d2a2c_vect.py:45-93, 263-273)
   FV3B_CHECK(launch_box(Box{s - 3, e + 4, js - 1, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    double cu = F2(g.cosa_u, i, j), ru = F2(g.rsin_u, i, j);
+    real cu = F2(g.cosa_u, i, j), ru = F2(g.rsin_u, i, j);
     if (i >= s + 2 && i <= e - 1) {
-      double ucv = A2 * (F3(utmp, i - 2, j) + F3(utmp, i + 1, j)) + A1 * (F3(utmp, i - 1, j) + F3(utmp, i, j));
+      real ucv = A2 * (F3(utmp, i - 2, j) + F3(utmp, i + 1, j)) + A1 * (F3(utmp, i - 1, j) + F3(utmp, i, j));
       W3(uc, i, j) = ucv;
       W3(ut, i, j) = (ucv - F3(v, i, j) * cu) * ru;
     } else if (i == s - 1 || i == e) {
-      double ucv = C1 * F3(utmp, i - 2, j) + C2 * F3(utmp, i - 1, j) + C3 * F3(utmp, i, j);
+      real ucv = C1 * F3(utmp, i - 2, j) + C2 * F3(utmp, i - 1, j) + C3 * F3(utmp, i, j);
       W3(uc, i, j) = ucv;
       W3(ut, i, j) = (ucv - F3(v, i, j) * cu) * ru;
     } else if (i == s || i == e + 1) {
-      double t1 = F2(g.dxa, i - 2, j) + F2(g.dxa, i - 1, j);
-      double t2 = F2(g.dxa, i, j) + F2(g.dxa, i + 1, j);
-      double n1 = (t1 + F2(g.dxa, i - 1, j)) * F3(ua, i - 1, j) - F2(g.dxa, i - 1, j) * F3(ua, i - 2, j);
-      double n2 = (t1 + F2(g.dxa, i, j)) * F3(ua, i, j) - F2(g.dxa, i, j) * F3(ua, i + 1, j);
-      double utc = 0.5 * (n1 / t1 + n2 / t2);
+      real t1 = F2(g.dxa, i - 2, j) + F2(g.dxa, i - 1, j);
+      real t2 = F2(g.dxa, i, j) + F2(g.dxa, i + 1, j);
+      real n1 = (t1 + F2(g.dxa, i - 1, j)) * F3(ua, i - 1, j) - F2(g.dxa, i - 1, j) * F3(ua, i - 2, j);
+      real n2 = (t1 + F2(g.dxa, i, j)) * F3(ua, i, j) - F2(g.dxa, i, j) * F3(ua, i + 1, j);
+      real utc = RC(0.5) * (n1 / t1 + n2 / t2);
       W3(ut, i, j) = utc;
       W3(uc, i, j) = utc > 0 ? utc * F2(g.sin_sg3, i - 1, j) : utc * F2(g.sin_sg1, i, j);
     } else if (i == s + 1 || i == e + 2) {
-      double ucv = C1 * F3(utmp, i + 1, j) + C2 * F3(utmp, i, j) + C3 * F3(utmp, i - 1, j);
+      real ucv = C1 * F3(utmp, i + 1, j) + C2 * F3(utmp, i, j) + C3 * F3(utmp, i - 1, j);
       W3(uc, i, j) = ucv;
       W3(ut, i, j) = (ucv - F3(v, i, j) * cu) * ru;
     }
@@ -105,22 +105,22 @@ extern "C" int fv3b_c_sw(fv3b_ctx* ctx, double* delp, double* pt, const double* 
   FV3B_CHECK(launch_box(Box{s - 1, e + 2, js - 3, je + 4, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
     CornerRule r;
-    if (corner_y(d, i, j, true, -1.0, 1.0, 1.0, -1.0, r)) W3(vtmp, i, j) = r.mult * F3(utmp, i + r.di, j + r.dj);
-    if (corner_y(d, i, j, false, -1.0, 1.0, 1.0, -1.0, r)) W3(va, i, j) = r.mult * F3(ua, i + r.di, j + r.dj);
+    if (corner_y(d, i, j, true, -RC(1.0), RC(1.0), RC(1.0), -RC(1.0), r)) W3(vtmp, i, j) = r.mult * F3(utmp, i + r.di, j + r.dj);
+    if (corner_y(d, i, j, false, -RC(1.0), RC(1.0), RC(1.0), -RC(1.0), r)) W3(va, i, j) = r.mult * F3(ua, i + r.di, j + r.dj);
   }));
   // north_south_edges + vt_main (d2a2c_vect.py:96-138, 276-286)
   FV3B_CHECK(launch_box(Box{s - 1, e + 2, js - 1, je + 3, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    double cv = F2(g.cosa_v, i, j), rv = F2(g.rsin_v, i, j);
-    double vcv;
+    real cv = F2(g.cosa_v, i, j), rv = F2(g.rsin_v, i, j);
+    real vcv;
     if (j == js - 1 || j == je) {
       vcv = C1 * F3(vtmp, i, j - 2) + C2 * F3(vtmp, i, j - 1) + C3 * F3(vtmp, i, j);
     } else if (j == js || j == je + 1) {
-      double t1 = F2(g.dya, i, j - 2) + F2(g.dya, i, j - 1);
-      double t2 = F2(g.dya, i, j) + F2(g.dya, i, j + 1);
-      double n1 = (t1 + F2(g.dya, i, j - 1)) * F3(va, i, j - 1) - F2(g.dya, i, j - 1) * F3(va, i, j - 2);
-      double n2 = (t1 + F2(g.dya, i, j)) * F3(va, i, j) - F2(g.dya, i, j) * F3(va, i, j + 1);
-      double vtc = 0.5 * (n1 / t1 + n2 / t2);
+      real t1 = F2(g.dya, i, j - 2) + F2(g.dya, i, j - 1);
+      real t2 = F2(g.dya, i, j) + F2(g.dya, i, j + 1);
+      real n1 = (t1 + F2(g.dya, i, j - 1)) * F3(va, i, j - 1) - F2(g.dya, i, j - 1) * F3(va, i, j - 2);
+      real n2 = (t1 + F2(g.dya, i, j)) * F3(va, i, j) - F2(g.dya, i, j) * F3(va, i, j + 1);
+      real vtc = RC(0.5) * (n1 / t1 + n2 / t2);
       W3(vt, i, j) = vtc;
       W3(vc, i, j) = vtc > 0 ? vtc * F2(g.sin_sg4, i, j - 1) : vtc * F2(g.sin_sg2, i, j);
       return;
@@ -138,37 +138,37 @@ extern "C" int fv3b_c_sw(fv3b_ctx* ctx, double* delp, double* pt, const double* 
     FV3B_CHECK(launch_box(Box{s, e + 2, js, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
       PT_SETUP(d, t, k);
       auto ufv = [&](int ii, int jj) {
-        return (F3(u, ii, jj) - 0.25 * (F3(va, ii, jj - 1) + F3(va, ii, jj)) *
+        return (F3(u, ii, jj) - RC(0.25) * (F3(va, ii, jj - 1) + F3(va, ii, jj)) *
                                     (F2(g.cos_sg4, ii, jj - 1) + F2(g.cos_sg2, ii, jj))) *
-               F2(g.dyc, ii, jj) * 0.5 * (F2(g.sin_sg4, ii, jj - 1) + F2(g.sin_sg2, ii, jj));
+               F2(g.dyc, ii, jj) * RC(0.5) * (F2(g.sin_sg4, ii, jj - 1) + F2(g.sin_sg2, ii, jj));
       };
       auto vfv = [&](int ii, int jj) {
-        return (F3(v, ii, jj) - 0.25 * (F3(ua, ii - 1, jj) + F3(ua, ii, jj)) *
+        return (F3(v, ii, jj) - RC(0.25) * (F3(ua, ii - 1, jj) + F3(ua, ii, jj)) *
                                     (F2(g.cos_sg3, ii - 1, jj) + F2(g.cos_sg1, ii, jj))) *
-               F2(g.dxc, ii, jj) * 0.5 * (F2(g.sin_sg3, ii - 1, jj) + F2(g.sin_sg1, ii, jj));
+               F2(g.dxc, ii, jj) * RC(0.5) * (F2(g.sin_sg3, ii - 1, jj) + F2(g.sin_sg1, ii, jj));
       };
-      double rac = F2(g.rarea_c, i, j);
-      double uf = ufv(i, j), vf = vfv(i, j);
-      double dd;
+      real rac = F2(g.rarea_c, i, j);
+      real uf = ufv(i, j), vf = vfv(i, j);
+      real dd;
       bool ew = (i == s || i == e + 1), ns = (j == js || j == je + 1);
-      double vf0 = F3(v, i, j) * F2(g.dxc, i, j) * 0.5 * (F2(g.sin_sg3, i - 1, j) + F2(g.sin_sg1, i, j));
-      double vf1 = F3(v, i, j - 1) * F2(g.dxc, i, j - 1) * 0.5 * (F2(g.sin_sg3, i - 1, j - 1) + F2(g.sin_sg1, i, j - 1));
-      double uf0 = F3(u, i, j) * F2(g.dyc, i, j) * 0.5 * (F2(g.sin_sg4, i, j - 1) + F2(g.sin_sg2, i, j));
-      double uf1b = F3(u, i - 1, j) * F2(g.dyc, i - 1, j) * 0.5 * (F2(g.sin_sg4, i - 1, j - 1) + F2(g.sin_sg2, i - 1, j));
+      real vf0 = F3(v, i, j) * F2(g.dxc, i, j) * RC(0.5) * (F2(g.sin_sg3, i - 1, j) + F2(g.sin_sg1, i, j));
+      real vf1 = F3(v, i, j - 1) * F2(g.dxc, i, j - 1) * RC(0.5) * (F2(g.sin_sg3, i - 1, j - 1) + F2(g.sin_sg1, i, j - 1));
+      real uf0 = F3(u, i, j) * F2(g.dyc, i, j) * RC(0.5) * (F2(g.sin_sg4, i, j - 1) + F2(g.sin_sg2, i, j));
+      real uf1b = F3(u, i - 1, j) * F2(g.dyc, i - 1, j) * RC(0.5) * (F2(g.sin_sg4, i - 1, j - 1) + F2(g.sin_sg2, i - 1, j));
       if (ns && ew) {
         if (j == js)
           dd = (-vf0 + uf1b - uf0) * rac;
         else
           dd = (vf1 + uf1b - uf0) * rac;
       } else if (ns) {
-        double vf1b = (F3(v, i, j - 1) - 0.25 * (F3(ua, i - 1, j - 1) + F3(ua, i, j - 1)) *
+        real vf1b = (F3(v, i, j - 1) - RC(0.25) * (F3(ua, i - 1, j - 1) + F3(ua, i, j - 1)) *
                                              (F2(g.cos_sg3, i - 1, j - 1) + F2(g.cos_sg1, i, j - 1))) *
-                      F2(g.dxc, i, j - 1) * 0.5 * (F2(g.sin_sg3, i - 1, j - 1) + F2(g.sin_sg1, i, j - 1));
+                      F2(g.dxc, i, j - 1) * RC(0.5) * (F2(g.sin_sg3, i - 1, j - 1) + F2(g.sin_sg1, i, j - 1));
         dd = (vf1b - vf + uf1b - uf0) * rac;
       } else if (ew) {
-        double uf1 = (F3(u, i - 1, j) - 0.25 * (F3(va, i - 1, j - 1) + F3(va, i - 1, j)) *
+        real uf1 = (F3(u, i - 1, j) - RC(0.25) * (F3(va, i - 1, j - 1) + F3(va, i - 1, j)) *
                                             (F2(g.cos_sg4, i - 1, j - 1) + F2(g.cos_sg2, i - 1, j))) *
-                     F2(g.dyc, i - 1, j) * 0.5 * (F2(g.sin_sg4, i - 1, j - 1) + F2(g.sin_sg2, i - 1, j));
+                     F2(g.dyc, i - 1, j) * RC(0.5) * (F2(g.sin_sg4, i - 1, j - 1) + F2(g.sin_sg2, i - 1, j));
         dd = (vf1 - vf0 + uf1 - uf) * rac;
       } else {
         dd = (vfv(i, j - 1) - vf + ufv(i - 1, j) - uf) * rac;
@@ -180,19 +180,19 @@ extern "C" int fv3b_c_sw(fv3b_ctx* ctx, double* delp, double* pt, const double* 
   FV3B_CHECK(launch_box(Box{s - 1, e + 3, js - 1, je + 3, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
     if (j < je + 2) {
-      double x = F3(ut, i, j);
+      real x = F3(ut, i, j);
       W3(ut, i, j) = x > 0 ? dt2 * x * F2(g.dy, i, j) * F2(g.sin_sg3, i - 1, j) : dt2 * x * F2(g.dy, i, j) * F2(g.sin_sg1, i, j);
     }
     if (i < e + 2) {
-      double y = F3(vt, i, j);
+      real y = F3(vt, i, j);
       W3(vt, i, j) = y > 0 ? dt2 * y * F2(g.dx, i, j) * F2(g.sin_sg4, i, j - 1) : dt2 * y * F2(g.dx, i, j) * F2(g.sin_sg2, i, j);
     }
   }));
   FV3B_CHECK(launch_box(Box{s - 2, e + 3, js - 1, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
     CornerRule r;
-    if (corner_x(d, i, j, false, 1.0, 1.0, 1.0, 1.0, r)) {
-      double a = F3(delp, i + r.di, j + r.dj), b = F3(pt, i + r.di, j + r.dj), c = F3(w, i + r.di, j + r.dj);
+    if (corner_x(d, i, j, false, RC(1.0), RC(1.0), RC(1.0), RC(1.0), r)) {
+      real a = F3(delp, i + r.di, j + r.dj), b = F3(pt, i + r.di, j + r.dj), c = F3(w, i + r.di, j + r.dj);
       W3(delp, i, j) = a;
       W3(pt, i, j) = b;
       W3(w, i, j) = c;
@@ -201,10 +201,10 @@ extern "C" int fv3b_c_sw(fv3b_ctx* ctx, double* delp, double* pt, const double* 
   // compute_nonhydro_fluxes_x (c_sw.py:67-82)
   FV3B_CHECK(launch_box(Box{s - 1, e + 3, js - 1, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    double utc = F3(ut, i, j);
-    bool p = utc > 0.0;
+    real utc = F3(ut, i, j);
+    bool p = utc > RC(0.0);
     int ii = p ? i - 1 : i;
-    double fx1 = utc * F3(delp, ii, j);
+    real fx1 = utc * F3(delp, ii, j);
     W3(tfx1, i, j) = fx1;
     W3(tfx, i, j) = fx1 * F3(pt, ii, j);
     W3(tfx2, i, j) = fx1 * F3(w, ii, j);
@@ -213,8 +213,8 @@ extern "C" int fv3b_c_sw(fv3b_ctx* ctx, double* delp, double* pt, const double* 
   FV3B_CHECK(launch_box(Box{s - 1, e + 2, js - 2, je + 3, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
     CornerRule r;
-    if (corner_y(d, i, j, false, 1.0, 1.0, 1.0, 1.0, r)) {
-      double a = F3(delp, i + r.di, j + r.dj), b = F3(pt, i + r.di, j + r.dj), c = F3(w, i + r.di, j + r.dj);
+    if (corner_y(d, i, j, false, RC(1.0), RC(1.0), RC(1.0), RC(1.0), r)) {
+      real a = F3(delp, i + r.di, j + r.dj), b = F3(pt, i + r.di, j + r.dj), c = F3(w, i + r.di, j + r.dj);
       W3(delp, i, j) = a;
       W3(pt, i, j) = b;
       W3(w, i, j) = c;
@@ -223,40 +223,40 @@ extern "C" int fv3b_c_sw(fv3b_ctx* ctx, double* delp, double* pt, const double* 
   // transportdelp_update_vorticity_and_kineticenergy (c_sw.py:85-169)
   FV3B_CHECK(launch_box(Box{s - 1, e + 2, js - 1, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    auto fy = [&](int jj, double& f1, double& f, double& f2) {
-      double vtc = F3(vt, i, jj);
-      int j2 = vtc > 0.0 ? jj - 1 : jj;
+    auto fy = [&](int jj, real& f1, real& f, real& f2) {
+      real vtc = F3(vt, i, jj);
+      int j2 = vtc > RC(0.0) ? jj - 1 : jj;
       f1 = vtc * F3(delp, i, j2);
       f = f1 * F3(pt, i, j2);
       f2 = f1 * F3(w, i, j2);
     };
-    double fy1a, fya, fy2a, fy1b, fyb, fy2b;
+    real fy1a, fya, fy2a, fy1b, fyb, fy2b;
     fy(j, fy1a, fya, fy2a);
     fy(j + 1, fy1b, fyb, fy2b);
-    double ra = F2(g.rarea, i, j);
-    double dp = F3(delp, i, j);
-    double dpc = dp + (F3(tfx1, i, j) - F3(tfx1, i + 1, j) + fy1a - fy1b) * ra;
+    real ra = F2(g.rarea, i, j);
+    real dp = F3(delp, i, j);
+    real dpc = dp + (F3(tfx1, i, j) - F3(tfx1, i + 1, j) + fy1a - fy1b) * ra;
     W3(delpc, i, j) = dpc;
     W3(ptc, i, j) = (F3(pt, i, j) * dp + (F3(tfx, i, j) - F3(tfx, i + 1, j) + fya - fyb) * ra) / dpc;
     W3(omga, i, j) = (F3(w, i, j) * dp + (F3(tfx2, i, j) - F3(tfx2, i + 1, j) + fy2a - fy2b) * ra) / dpc;
-    double uav = F3(ua, i, j), vav = F3(va, i, j);
-    double ke = uav > 0.0 ? F3(uc, i, j) : F3(uc, i + 1, j);
-    double vort = vav > 0.0 ? F3(vc, i, j) : F3(vc, i, j + 1);
-    if ((j == js - 1 || j == je) && vav <= 0.0) vort = vort * F2(g.sin_sg4, i, j) + F3(u, i, j + 1) * F2(g.cos_sg4, i, j);
-    if ((j == js || j == je + 1) && vav > 0.0) vort = vort * F2(g.sin_sg2, i, j) + F3(u, i, j) * F2(g.cos_sg2, i, j);
-    if ((i == e || i == s - 1) && uav <= 0.0) ke = ke * F2(g.sin_sg3, i, j) + F3(v, i + 1, j) * F2(g.cos_sg3, i, j);
-    if ((i == e + 1 || i == s) && uav > 0.0) ke = ke * F2(g.sin_sg1, i, j) + F3(v, i, j) * F2(g.cos_sg1, i, j);
-    W3(tke, i, j) = 0.5 * dt2 * (uav * ke + vav * vort);
+    real uav = F3(ua, i, j), vav = F3(va, i, j);
+    real ke = uav > RC(0.0) ? F3(uc, i, j) : F3(uc, i + 1, j);
+    real vort = vav > RC(0.0) ? F3(vc, i, j) : F3(vc, i, j + 1);
+    if ((j == js - 1 || j == je) && vav <= RC(0.0)) vort = vort * F2(g.sin_sg4, i, j) + F3(u, i, j + 1) * F2(g.cos_sg4, i, j);
+    if ((j == js || j == je + 1) && vav > RC(0.0)) vort = vort * F2(g.sin_sg2, i, j) + F3(u, i, j) * F2(g.cos_sg2, i, j);
+    if ((i == e || i == s - 1) && uav <= RC(0.0)) ke = ke * F2(g.sin_sg3, i, j) + F3(v, i + 1, j) * F2(g.cos_sg3, i, j);
+    if ((i == e + 1 || i == s) && uav > RC(0.0)) ke = ke * F2(g.sin_sg1, i, j) + F3(v, i, j) * F2(g.cos_sg1, i, j);
+    W3(tke, i, j) = RC(0.5) * dt2 * (uav * ke + vav * vort);
     W3(tvort, i, j) = vort;
   }));
   // circulation_cgrid + absolute_vorticity (c_sw.py:46-48, 292-322)
   FV3B_CHECK(launch_box(Box{s, e + 2, js, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    double fx = F2(g.dxc, i, j) * F3(uc, i, j);
-    double fy = F2(g.dyc, i, j) * F3(vc, i, j);
-    double fx1 = F2(g.dxc, i, j - 1) * F3(uc, i, j - 1);
-    double fy1 = F2(g.dyc, i - 1, j) * F3(vc, i - 1, j);
-    double vcv;
+    real fx = F2(g.dxc, i, j) * F3(uc, i, j);
+    real fy = F2(g.dyc, i, j) * F3(vc, i, j);
+    real fx1 = F2(g.dxc, i, j - 1) * F3(uc, i, j - 1);
+    real fy1 = F2(g.dyc, i - 1, j) * F3(vc, i - 1, j);
+    real vcv;
     bool cj = (j == js || j == je + 1);
     if (i == s && cj)
       vcv = fx1 - fx + fy;
@@ -270,17 +270,17 @@ extern "C" int fv3b_c_sw(fv3b_ctx* ctx, double* delp, double* pt, const double* 
   FV3B_CHECK(launch_box(Box{s, e + 2, js, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
     if (i <= e) {
-      double vcv = F3(vc, i, j);
-      double tf = (j == js || j == je + 1) ? dt2 * F3(u, i, j)
+      real vcv = F3(vc, i, j);
+      real tf = (j == js || j == je + 1) ? dt2 * F3(u, i, j)
                                            : dt2 * (F3(u, i, j) - vcv * F2(g.cosa_v, i, j)) / F2(g.sina_v, i, j);
-      double flux = tf > 0.0 ? F3(tvort, i, j) : F3(tvort, i + 1, j);
+      real flux = tf > RC(0.0) ? F3(tvort, i, j) : F3(tvort, i + 1, j);
       W3(vc, i, j) = vcv - tf * flux + F2(g.rdyc, i, j) * (F3(tke, i, j - 1) - F3(tke, i, j));
     }
     if (j <= je) {
-      double ucv = F3(uc, i, j);
-      double tf = (i == s || i == e + 1) ? dt2 * F3(v, i, j)
+      real ucv = F3(uc, i, j);
+      real tf = (i == s || i == e + 1) ? dt2 * F3(v, i, j)
                                          : dt2 * (F3(v, i, j) - ucv * F2(g.cosa_u, i, j)) / F2(g.sina_u, i, j);
-      double flux = tf > 0.0 ? F3(tvort, i, j) : F3(tvort, i, j + 1);
+      real flux = tf > RC(0.0) ? F3(tvort, i, j) : F3(tvort, i, j + 1);
       W3(uc, i, j) = ucv + tf * flux + F2(g.rdxc, i, j) * (F3(tke, i - 1, j) - F3(tke, i, j));
     }
   }));

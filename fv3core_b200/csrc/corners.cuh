@@ -76,11 +76,11 @@ __device__ __forceinline__ bool bgrid_corner_y(const Dims& d, int i, int j, int&
 // point of the given kind.
 struct CornerRule {
   int di, dj;
-  double mult;
+  real mult;
 };
 
-__device__ __forceinline__ bool corner_x(const Dims& d, int i, int j, bool three, double sw, double se, double nw,
-                                         double ne, CornerRule& r) {
+__device__ __forceinline__ bool corner_x(const Dims& d, int i, int j, bool three, real sw, real se, real nw,
+                                         real ne, CornerRule& r) {
   int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
   if (j == js - 1) {
     if (i == s - 1) { r = {0, 1, sw}; return true; }
@@ -100,8 +100,8 @@ __device__ __forceinline__ bool corner_x(const Dims& d, int i, int j, bool three
   return false;
 }
 
-__device__ __forceinline__ bool corner_y(const Dims& d, int i, int j, bool three, double sw, double se, double nw,
-                                         double ne, CornerRule& r) {
+__device__ __forceinline__ bool corner_y(const Dims& d, int i, int j, bool three, real sw, real se, real nw,
+                                         real ne, CornerRule& r) {
   int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
   if (i == s - 1) {
     if (j == js - 1) { r = {1, 0, sw}; return true; }

@@ -14,21 +14,21 @@ extern "C" int fv3b_ctx_create(const fv3b_grid_dims* dims, const fv3b_metrics* m
   c->d = make_dims(dims);
   c->m = *metrics;
   size_t n3 = (size_t)c->d.st * 6;
-  cudaError_t e = cudaMalloc((void**)&c->ws_base, n3 * sizeof(double) * NWS);
+  cudaError_t e = cudaMalloc((void**)&c->ws_base, n3 * sizeof(real) * NWS);
   if (e != cudaSuccess) {
     delete c;
     set_last_error("fv3b_ctx_create", e);
     return FV3B_ERR_CUDA;
   }
   for (int i = 0; i < NWS; ++i) c->ws[i] = c->ws_base + n3 * i;
-  e = cudaMalloc((void**)&c->col, sizeof(double) * NCOL * MAXLEV);
+  e = cudaMalloc((void**)&c->col, sizeof(real) * NCOL * MAXLEV);
   if (e != cudaSuccess) {
     cudaFree(c->ws_base);
     delete c;
     set_last_error("fv3b_ctx_create", e);
     return FV3B_ERR_CUDA;
   }
-  e = cudaMemset(c->ws_base, 0, n3 * sizeof(double) * NWS);
+  e = cudaMemset(c->ws_base, 0, n3 * sizeof(real) * NWS);
   if (e != cudaSuccess) {
     cudaFree(c->ws_base);
     delete c;

@@ -46,9 +46,9 @@ struct AcousticState;  // dyn_core.cu
 struct fv3b_ctx {
   fv3b::Dims d;
   fv3b_metrics m;
-  double* ws_base = nullptr;
-  double* ws[fv3b::NWS];
-  double* col = nullptr;  // [NCOL][MAXLEV] device columns
+  fv3b::real* ws_base = nullptr;
+  fv3b::real* ws[fv3b::NWS];
+  fv3b::real* col = nullptr;  // [NCOL][MAXLEV] device columns
   fv3b::DswSetup dsw;
   bool dzd_ready = false;
   int dzd_hord_tm = 0;
@@ -58,7 +58,7 @@ struct fv3b_ctx {
 
 namespace fv3b {
 // device pointer of per-level column `id`
-inline double* colp(fv3b_ctx* c, int id) { return c->col + (size_t)id * MAXLEV; }
+inline real* colp(fv3b_ctx* c, int id) { return c->col + (size_t)id * MAXLEV; }
 }  // namespace fv3b
 
 // frees the acoustic driver's temporaries (dyn_core.cu)

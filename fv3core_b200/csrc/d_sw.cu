@@ -24,29 +24,29 @@ constexpr double DCON_THRESHOLD = 1e-5;
 
 // ---------------------------------------------------------------- fxadv
 // FiniteVolumeFluxPrep.__call__ (fxadv.py:488-585)
-cudaError_t fxadv(const Dims d, const fv3b_metrics g, const double* uc, const double* vc, double* crx, double* cry,
-                  double* xfx, double* yfx, double* ucc, double* vcc, double dt, cudaStream_t st) {
+cudaError_t fxadv(const Dims d, const fv3b_metrics g, const real* uc, const real* vc, real* crx, real* cry,
+                  real* xfx, real* yfx, real* ucc, real* vcc, real dt, cudaStream_t st) {
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = d.nz;
   const int full = d.ni - 1;
   cudaError_t err;
   // main_uc_contra + uc_contra_y_edge (fxadv.py:11-39, 61-71); main_vc_contra (42-58)
   err = launch_box(Box{0, full, 0, full, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    double u_old = F3(ucc, i, j), v_old = F3(vcc, i, j);
-    double un = u_old;
+    real u_old = F3(ucc, i, j), v_old = F3(vcc, i, j);
+    real un = u_old;
     if (i >= s - 1 && i < e + 3) {
-      double vv = 0.25 * (F3(vc, i - 1, j) + F3(vc, i, j) + F3(vc, i - 1, j + 1) + F3(vc, i, j + 1));
+      real vv = RC(0.25) * (F3(vc, i - 1, j) + F3(vc, i, j) + F3(vc, i - 1, j + 1) + F3(vc, i, j + 1));
       un = (F3(uc, i, j) - vv * F2(g.cosa_u, i, j)) * F2(g.rsin_u, i, j);
     }
     if ((j >= js - 1 && j < js + 1) || (j >= je && j < je + 2)) un = u_old;
     if (i == s || i == e + 1) {
-      double x = F3(uc, i, j);
+      real x = F3(uc, i, j);
       un = x > 0 ? x / F2(g.sin_sg3, i - 1, j) : x / F2(g.sin_sg1, i, j);
     }
     W3(ucc, i, j) = un;
-    double vn = v_old;
+    real vn = v_old;
     if (j >= js - 1 && j < je + 3) {
-      double uu = 0.25 * (F3(uc, i, j - 1) + F3(uc, i + 1, j - 1) + F3(uc, i, j) + F3(uc, i + 1, j));
+      real uu = RC(0.25) * (F3(uc, i, j - 1) + F3(uc, i + 1, j - 1) + F3(uc, i, j) + F3(uc, i + 1, j));
       vn = (F3(vc, i, j) - uu * F2(g.cosa_v, i, j)) * F2(g.rsin_v, i, j);
     }
     if (j == js || j == je + 1) vn = v_old;
@@ -56,17 +56,17 @@ cudaError_t fxadv(const Dims d, const fv3b_metrics g, const double* uc, const do
   // vc_contra_y_edge + vc_contra_x_edge (fxadv.py:97-150)
   err = launch_box(Box{0, full, 0, full, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    double vn = F3(vcc, i, j);
+    real vn = F3(vcc, i, j);
     bool ycol = (i >= s - 1 && i < s + 1) || (i >= e && i < e + 2);
     if (ycol && j >= js && j < je + 2) {
       bool keep = (j >= js && j < js + 2) || (j >= je && j < je + 2);
       if (!keep) {
-        double uu = 0.25 * (F3(ucc, i, j - 1) + F3(ucc, i + 1, j - 1) + F3(ucc, i, j) + F3(ucc, i + 1, j));
-        vn = (F3(vc, i, j) - uu * F2(g.cosa_v, i, j)) * 1.0;
+        real uu = RC(0.25) * (F3(ucc, i, j - 1) + F3(ucc, i + 1, j - 1) + F3(ucc, i, j) + F3(ucc, i + 1, j));
+        vn = (F3(vc, i, j) - uu * F2(g.cosa_v, i, j)) * RC(1.0);
       }
     }
     if (j == js || j == je + 1) {
-      double y = F3(vc, i, j);
+      real y = F3(vc, i, j);
       vn = y > 0 ? y / F2(g.sin_sg4, i, j - 1) : y / F2(g.sin_sg2, i, j);
     }
     W3(vcc, i, j) = vn;
@@ -79,8 +79,8 @@ cudaError_t fxadv(const Dims d, const fv3b_metrics g, const double* uc, const do
     if (!rows) return;
     bool keep = (i >= s && i < s + 2) || (i >= e && i < e + 2);
     if (keep) return;
-    double vv = 0.25 * (F3(vcc, i - 1, j) + F3(vcc, i, j) + F3(vcc, i - 1, j + 1) + F3(vcc, i, j + 1));
-    W3(ucc, i, j) = (F3(uc, i, j) - vv * F2(g.cosa_u, i, j)) * 1.0;
+    real vv = RC(0.25) * (F3(vcc, i - 1, j) + F3(vcc, i, j) + F3(vcc, i - 1, j + 1) + F3(vcc, i, j + 1));
+    W3(ucc, i, j) = (F3(uc, i, j) - vv * F2(g.cosa_u, i, j)) * RC(1.0);
   });
   if (err != cudaSuccess) return err;
   // uc_contra_corners (fxadv.py:156-260): 8 points, none reads another's target
@@ -97,34 +97,34 @@ cudaError_t fxadv(const Dims d, const fv3b_metrics g, const double* uc, const do
       case 6: i = e; j = js; kind = 3; break;
       default: i = e; j = je + 1; kind = 3; break;
     }
-    double cu = F2(g.cosa_u, i, j), val;
+    real cu = F2(g.cosa_u, i, j), val;
     if (kind == 0) {
-      double cv = F2(g.cosa_v, i - 1, j);
-      double damp = 1.0 / (1.0 - 0.0625 * cu * cv);
-      val = (F3(uc, i, j) - 0.25 * cu *
+      real cv = F2(g.cosa_v, i - 1, j);
+      real damp = RC(1.0) / (RC(1.0) - RC(0.0625) * cu * cv);
+      val = (F3(uc, i, j) - RC(0.25) * cu *
                                 (F3(vcc, i - 1, j + 1) + F3(vcc, i, j + 1) + F3(vcc, i, j) + F3(vc, i - 1, j) -
-                                 0.25 * cv * (F3(ucc, i - 1, j) + F3(ucc, i - 1, j - 1) + F3(ucc, i, j - 1)))) *
+                                 RC(0.25) * cv * (F3(ucc, i - 1, j) + F3(ucc, i - 1, j - 1) + F3(ucc, i, j - 1)))) *
             damp;
     } else if (kind == 1) {
-      double cv = F2(g.cosa_v, i - 1, j + 1);
-      double damp = 1.0 / (1.0 - 0.0625 * cu * cv);
-      val = (F3(uc, i, j) - 0.25 * cu *
+      real cv = F2(g.cosa_v, i - 1, j + 1);
+      real damp = RC(1.0) / (RC(1.0) - RC(0.0625) * cu * cv);
+      val = (F3(uc, i, j) - RC(0.25) * cu *
                                 (F3(vcc, i - 1, j) + F3(vcc, i, j) + F3(vcc, i, j + 1) + F3(vc, i - 1, j + 1) -
-                                 0.25 * cv * (F3(ucc, i - 1, j) + F3(ucc, i - 1, j + 1) + F3(ucc, i, j + 1)))) *
+                                 RC(0.25) * cv * (F3(ucc, i - 1, j) + F3(ucc, i - 1, j + 1) + F3(ucc, i, j + 1)))) *
             damp;
     } else if (kind == 2) {
-      double cv = F2(g.cosa_v, i, j);
-      double damp = 1.0 / (1.0 - 0.0625 * cu * cv);
-      val = (F3(uc, i, j) - 0.25 * cu *
+      real cv = F2(g.cosa_v, i, j);
+      real damp = RC(1.0) / (RC(1.0) - RC(0.0625) * cu * cv);
+      val = (F3(uc, i, j) - RC(0.25) * cu *
                                 (F3(vcc, i, j + 1) + F3(vcc, i - 1, j + 1) + F3(vcc, i - 1, j) + F3(vc, i, j) -
-                                 0.25 * cv * (F3(ucc, i + 1, j) + F3(ucc, i + 1, j - 1) + F3(ucc, i, j - 1)))) *
+                                 RC(0.25) * cv * (F3(ucc, i + 1, j) + F3(ucc, i + 1, j - 1) + F3(ucc, i, j - 1)))) *
             damp;
     } else {
-      double cv = F2(g.cosa_v, i, j + 1);
-      double damp = 1.0 / (1.0 - 0.0625 * cu * cv);
-      val = (F3(uc, i, j) - 0.25 * cu *
+      real cv = F2(g.cosa_v, i, j + 1);
+      real damp = RC(1.0) / (RC(1.0) - RC(0.0625) * cu * cv);
+      val = (F3(uc, i, j) - RC(0.25) * cu *
                                 (F3(vcc, i, j) + F3(vcc, i - 1, j) + F3(vcc, i - 1, j + 1) + F3(vc, i, j + 1) -
-                                 0.25 * cv * (F3(ucc, i + 1, j) + F3(ucc, i + 1, j + 1) + F3(ucc, i, j + 1)))) *
+                                 RC(0.25) * cv * (F3(ucc, i + 1, j) + F3(ucc, i + 1, j + 1) + F3(ucc, i, j + 1)))) *
             damp;
     }
     W3(ucc, i, j) = val;
@@ -144,35 +144,35 @@ cudaError_t fxadv(const Dims d, const fv3b_metrics g, const double* uc, const do
       case 6: i = e; j = je; kind = 3; break;
       default: i = s - 1; j = je; kind = 3; break;
     }
-    double cv = F2(g.cosa_v, i, j), val;
-    const double* ut = ucc;
+    real cv = F2(g.cosa_v, i, j), val;
+    const real* ut = ucc;
     if (kind == 0) {
-      double cu = F2(g.cosa_u, i, j - 1);
-      double damp = 1.0 / (1.0 - 0.0625 * cu * cv);
-      val = (F3(vc, i, j) - 0.25 * cv *
+      real cu = F2(g.cosa_u, i, j - 1);
+      real damp = RC(1.0) / (RC(1.0) - RC(0.0625) * cu * cv);
+      val = (F3(vc, i, j) - RC(0.25) * cv *
                                 (F3(ut, i + 1, j - 1) + F3(ut, i + 1, j) + F3(ut, i, j) + F3(uc, i, j - 1) -
-                                 0.25 * cu * (F3(vcc, i, j - 1) + F3(vcc, i - 1, j - 1) + F3(vcc, i - 1, j)))) *
+                                 RC(0.25) * cu * (F3(vcc, i, j - 1) + F3(vcc, i - 1, j - 1) + F3(vcc, i - 1, j)))) *
             damp;
     } else if (kind == 1) {
-      double cu = F2(g.cosa_u, i + 1, j - 1);
-      double damp = 1.0 / (1.0 - 0.0625 * cu * cv);
-      val = (F3(vc, i, j) - 0.25 * cv *
+      real cu = F2(g.cosa_u, i + 1, j - 1);
+      real damp = RC(1.0) / (RC(1.0) - RC(0.0625) * cu * cv);
+      val = (F3(vc, i, j) - RC(0.25) * cv *
                                 (F3(ut, i, j - 1) + F3(ut, i, j) + F3(ut, i + 1, j) + F3(uc, i + 1, j - 1) -
-                                 0.25 * cu * (F3(vcc, i, j - 1) + F3(vcc, i + 1, j - 1) + F3(vcc, i + 1, j)))) *
+                                 RC(0.25) * cu * (F3(vcc, i, j - 1) + F3(vcc, i + 1, j - 1) + F3(vcc, i + 1, j)))) *
             damp;
     } else if (kind == 2) {
-      double cu = F2(g.cosa_u, i + 1, j);
-      double damp = 1.0 / (1.0 - 0.0625 * cu * cv);
-      val = (F3(vc, i, j) - 0.25 * cv *
+      real cu = F2(g.cosa_u, i + 1, j);
+      real damp = RC(1.0) / (RC(1.0) - RC(0.0625) * cu * cv);
+      val = (F3(vc, i, j) - RC(0.25) * cv *
                                 (F3(ut, i, j) + F3(ut, i, j - 1) + F3(ut, i + 1, j - 1) + F3(uc, i + 1, j) -
-                                 0.25 * cu * (F3(vcc, i, j + 1) + F3(vcc, i + 1, j + 1) + F3(vcc, i + 1, j)))) *
+                                 RC(0.25) * cu * (F3(vcc, i, j + 1) + F3(vcc, i + 1, j + 1) + F3(vcc, i + 1, j)))) *
             damp;
     } else {
-      double cu = F2(g.cosa_u, i, j);
-      double damp = 1.0 / (1.0 - 0.0625 * cu * cv);
-      val = (F3(vc, i, j) - 0.25 * cv *
+      real cu = F2(g.cosa_u, i, j);
+      real damp = RC(1.0) / (RC(1.0) - RC(0.0625) * cu * cv);
+      val = (F3(vc, i, j) - RC(0.25) * cv *
                                 (F3(ut, i + 1, j) + F3(ut, i + 1, j - 1) + F3(ut, i, j - 1) + F3(uc, i, j) -
-                                 0.25 * cu * (F3(vcc, i, j + 1) + F3(vcc, i - 1, j + 1) + F3(vcc, i - 1, j)))) *
+                                 RC(0.25) * cu * (F3(vcc, i, j + 1) + F3(vcc, i - 1, j + 1) + F3(vcc, i - 1, j)))) *
             damp;
     }
     W3(vcc, i, j) = val;
@@ -182,7 +182,7 @@ cudaError_t fxadv(const Dims d, const fv3b_metrics g, const double* uc, const do
   return launch_box(Box{0, full, 0, full, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
     if (i >= s && i < e + 2) {
-      double prod = dt * F3(ucc, i, j);
+      real prod = dt * F3(ucc, i, j);
       if (prod > 0) {
         W3(crx, i, j) = prod * F2(g.rdxa, i - 1, j);
         W3(xfx, i, j) = F2(g.dy, i, j) * prod * F2(g.sin_sg3, i - 1, j);
@@ -192,7 +192,7 @@ cudaError_t fxadv(const Dims d, const fv3b_metrics g, const double* uc, const do
       }
     }
     if (j >= js && j < je + 2) {
-      double prod = dt * F3(vcc, i, j);
+      real prod = dt * F3(vcc, i, j);
       if (prod > 0) {
         W3(cry, i, j) = prod * F2(g.rdya, i, j - 1);
         W3(yfx, i, j) = F2(g.dx, i, j) * prod * F2(g.sin_sg4, i, j - 1);
@@ -206,7 +206,7 @@ cudaError_t fxadv(const Dims d, const fv3b_metrics g, const double* uc, const do
 
 // ---------------------------------------------------------------- corner fills, sequential per level
 // fill_corners_bgrid_{x,y} (corners.py:598-722) on levels [k0, k1)
-cudaError_t fill_bgrid(const Dims d, double* q, bool xdir, int k0, int k1, cudaStream_t st) {
+cudaError_t fill_bgrid(const Dims d, real* q, bool xdir, int k0, int k1, cudaStream_t st) {
   return launch_box(Box{0, d.ni, 0, d.nj, k0, k1}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
     int si, sj;
@@ -218,13 +218,13 @@ cudaError_t fill_bgrid(const Dims d, double* q, bool xdir, int k0, int k1, cudaS
 // fill_corners_dgrid_defn (corners.py:993-1150) with x_in == x_out and
 // y_in == y_out: the rules run in the reference's order, one thread per
 // (tile, level), so reads see earlier rules' writes exactly as there.
-cudaError_t fill_dgrid(const Dims d, double* x, double* y, double mysign, int k0, int k1, cudaStream_t st) {
+cudaError_t fill_dgrid(const Dims d, real* x, real* y, real mysign, int k0, int k1, cudaStream_t st) {
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
   return launch_box(Box{0, 1, 0, 1, k0, k1}, st, [=] __device__(int t, int, int, int k) {
     PT_SETUP(d, t, k);
-    auto X = [&](int i, int j) -> double& { return x[_b3 + (long long)j * _sj + i]; };
-    auto Y = [&](int i, int j) -> double& { return y[_b3 + (long long)j * _sj + i]; };
-    const double m = mysign;
+    auto X = [&](int i, int j) -> real& { return x[_b3 + (long long)j * _sj + i]; };
+    auto Y = [&](int i, int j) -> real& { return y[_b3 + (long long)j * _sj + i]; };
+    const real m = mysign;
     // sw corner
     X(s - 1, js - 1) = m * Y(s - 1, js);
     Y(s - 1, js - 1) = m * X(s, js - 1);
@@ -405,15 +405,16 @@ extern "C" int fv3b_d_sw_setup(fv3b_ctx* ctx, const fv3b_dsw_config* cfg) {
   }
   sp.dd8 = pow(ctx->m.da_min_c * cfg->d4_bg, sp.nonzero_nord + 1);
   // the D-grid columns only; the driver's columns (from COL_DP_REF on) are its own
-  FV3B_CHECK(cudaMemcpy(ctx->col, cols.data(), sizeof(double) * COL_DP_REF * MAXLEV, cudaMemcpyHostToDevice));
+  const std::vector<real> cols_r(cols.begin(), cols.begin() + (size_t)COL_DP_REF * MAXLEV);
+  FV3B_CHECK(cudaMemcpy(ctx->col, cols_r.data(), sizeof(real) * cols_r.size(), cudaMemcpyHostToDevice));
   sp.ready = true;
   return FV3B_OK;
 }
 
-extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc, double* pt, double* u, double* v,
-                         double* w, double* uc, double* vc, const double* ua, const double* va, double* divgd,
-                         double* mfx, double* mfy, double* cx, double* cy, double* crx, double* cry, double* xfx,
-                         double* yfx, double* q_con, const double* zh, double* heat_source, double* diss_est,
+extern "C" int fv3b_d_sw(fv3b_ctx* ctx, real* delpc, real* delp, real* ptc, real* pt, real* u, real* v,
+                         real* w, real* uc, real* vc, const real* ua, const real* va, real* divgd,
+                         real* mfx, real* mfy, real* cx, real* cy, real* crx, real* cry, real* xfx,
+                         real* yfx, real* q_con, const real* zh, real* heat_source, real* diss_est,
                          double dt, void* stream) {
   FV3B_REQUIRE(ctx && delpc && delp && ptc && pt && u && v && w && uc && vc && ua && va && divgd && mfx && mfy &&
                    cx && cy && crx && cry && xfx && yfx && q_con && zh && heat_source && diss_est,
@@ -426,20 +427,20 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
   cudaStream_t st = (cudaStream_t)stream;
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = d.nz;
   const int full = d.ni - 1;
-  double** W = ctx->ws;
-  double *tmp_fx = W[0], *tmp_fy = W[1], *tmp_gx = W[2], *tmp_gy = W[3], *tmp_fx2 = W[4], *tmp_fy2 = W[5];
-  double *tmp_dw = W[6], *tmp_wk = W[7], *tmp_vort = W[8], *tmp_ke = W[9], *tmp_heat_s = W[10];
-  double *tmp_ut = W[11], *tmp_vt = W[12], *vort_x_delta = W[13], *vort_y_delta = W[14];
-  double *fx_mean = W[16], *fy_mean = W[17], *q_adv_x = W[18], *q_adv_y = W[19];
-  double *dl_fx2 = W[20], *dl_fy2 = W[21], *dl_d2 = W[22];
-  double *a2b_qx = W[23], *a2b_qy = W[24], *a2b_edges = W[25];
-  double *ucc = W[WS_UC_CONTRA], *vcc = W[WS_VC_CONTRA];
-  const double* col_nord = colp(ctx, COL_NORD);
-  const double* col_d2_divg = colp(ctx, COL_D2_DIVG);
-  const double* col_d_con = colp(ctx, COL_D_CON);
-  const double* col_ke_bg = colp(ctx, COL_KE_BG);
-  const double* col_damp_w = colp(ctx, COL_DAMP_W);
-  const double* col_damp_vt = colp(ctx, COL_DAMP_VT);
+  real** W = ctx->ws;
+  real *tmp_fx = W[0], *tmp_fy = W[1], *tmp_gx = W[2], *tmp_gy = W[3], *tmp_fx2 = W[4], *tmp_fy2 = W[5];
+  real *tmp_dw = W[6], *tmp_wk = W[7], *tmp_vort = W[8], *tmp_ke = W[9], *tmp_heat_s = W[10];
+  real *tmp_ut = W[11], *tmp_vt = W[12], *vort_x_delta = W[13], *vort_y_delta = W[14];
+  real *fx_mean = W[16], *fy_mean = W[17], *q_adv_x = W[18], *q_adv_y = W[19];
+  real *dl_fx2 = W[20], *dl_fy2 = W[21], *dl_d2 = W[22];
+  real *a2b_qx = W[23], *a2b_qy = W[24], *a2b_edges = W[25];
+  real *ucc = W[WS_UC_CONTRA], *vcc = W[WS_VC_CONTRA];
+  const real* col_nord = colp(ctx, COL_NORD);
+  const real* col_d2_divg = colp(ctx, COL_D2_DIVG);
+  const real* col_d_con = colp(ctx, COL_D_CON);
+  const real* col_ke_bg = colp(ctx, COL_KE_BG);
+  const real* col_damp_w = colp(ctx, COL_DAMP_W);
+  const real* col_damp_vt = colp(ctx, COL_DAMP_VT);
   DelnCol dl_v{colp(ctx, COL_NORD_V), colp(ctx, COL_DAMP4_VT)};
   DelnCol dl_t{colp(ctx, COL_NORD_T), colp(ctx, COL_DAMP4_T)};
   DelnCol nosg_w{colp(ctx, COL_NORD_W), colp(ctx, COL_DAMP4_W_C)};
@@ -447,8 +448,8 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
 
   FV3B_CHECK(fxadv(d, g, uc, vc, crx, cry, xfx, yfx, ucc, vcc, dt, st));
 
-  auto transport = [&](double* q, double* fx, double* fy, int hord, const double* xmf, const double* ymf,
-                       const double* mass, const DelnCol* dl, int nmax) -> cudaError_t {
+  auto transport = [&](real* q, real* fx, real* fy, int hord, const real* xmf, const real* ymf,
+                       const real* mass, const DelnCol* dl, int nmax) -> cudaError_t {
     cudaError_t err = copy_corners_x_inplace(d, q, st);
     if (err != cudaSuccess) return err;
     FvTp2dArgs a{q, crx, cry, xfx, yfx, xmf ? xmf : xfx, ymf ? ymf : yfx, fx, fy, hord,
@@ -470,16 +471,16 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
   if (!cfg.hydrostatic) {
     FV3B_CHECK(delnflux_nosg(d, g, w, tmp_fx2, tmp_fy2, nosg_w, tmp_wk, false, sp.nmax_w, st));
     // heat_diss (d_sw.py:347-365)
-    const double adt = fabs(dt);
+    const real adt = fabs(dt);
     FV3B_CHECK(launch_box(Box{s, e + 1, js, je + 1, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
       PT_SETUP(d, t, k);
-      double diss_e = F3(diss_est, i, j);
-      if (col_damp_w[k] > 1e-5) {
-        double dd8 = col_ke_bg[k] * adt;
-        double dw = (F3(tmp_fx2, i, j) - F3(tmp_fx2, i + 1, j) + F3(tmp_fy2, i, j) - F3(tmp_fy2, i, j + 1)) *
+      real diss_e = F3(diss_est, i, j);
+      if (col_damp_w[k] > RC(1e-5)) {
+        real dd8 = col_ke_bg[k] * adt;
+        real dw = (F3(tmp_fx2, i, j) - F3(tmp_fx2, i + 1, j) + F3(tmp_fy2, i, j) - F3(tmp_fy2, i, j + 1)) *
                     F2(g.rarea, i, j);
         W3(tmp_dw, i, j) = dw;
-        double hs = dd8 - dw * (F3(w, i, j) + 0.5 * dw);
+        real hs = dd8 - dw * (F3(w, i, j) + RC(0.5) * dw);
         W3(tmp_heat_s, i, j) = hs;
         W3(diss_est, i, j) = diss_e + hs;
       }
@@ -505,10 +506,10 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
   FV3B_CHECK(transport(pt, tmp_gx, tmp_gy, cfg.hord_tm, tmp_fx, tmp_fy, delp, &dl_v, sp.nmax_v));
   FV3B_CHECK(launch_box(Box{s, e + 1, js, je + 1, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    double ra = F2(g.rarea, i, j);
-    double dp = F3(delp, i, j);
-    double ptn = F3(pt, i, j) * dp + (F3(tmp_gx, i, j) - F3(tmp_gx, i + 1, j) + F3(tmp_gy, i, j) - F3(tmp_gy, i, j + 1)) * ra;
-    double dpn = dp + (F3(tmp_fx, i, j) - F3(tmp_fx, i + 1, j) + F3(tmp_fy, i, j) - F3(tmp_fy, i, j + 1)) * ra;
+    real ra = F2(g.rarea, i, j);
+    real dp = F3(delp, i, j);
+    real ptn = F3(pt, i, j) * dp + (F3(tmp_gx, i, j) - F3(tmp_gx, i + 1, j) + F3(tmp_gy, i, j) - F3(tmp_gy, i, j + 1)) * ra;
+    real dpn = dp + (F3(tmp_fx, i, j) - F3(tmp_fx, i + 1, j) + F3(tmp_fy, i, j) - F3(tmp_fy, i, j + 1)) * ra;
     W3(pt, i, j) = ptn / dpn;
     W3(delp, i, j) = dpn;
   }));
@@ -517,33 +518,33 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
     const int mord = cfg.hord_mt < 0 ? -cfg.hord_mt : cfg.hord_mt;
     FV3B_CHECK(launch_box(Box{s, e + 2, js, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
       PT_SETUP(d, t, k);
-      double ub_cov = 0.5 * (F3(uc, i, j - 1) + F3(uc, i, j));
-      double vb_cov = 0.5 * (F3(vc, i - 1, j) + F3(vc, i, j));
-      double ca = F2(g.cosa, i, j), rs = F2(g.rsina, i, j);
-      double ubc = (ub_cov - vb_cov * ca) * rs;
-      double vbc = (vb_cov - ub_cov * ca) * rs;
+      real ub_cov = RC(0.5) * (F3(uc, i, j - 1) + F3(uc, i, j));
+      real vb_cov = RC(0.5) * (F3(vc, i - 1, j) + F3(vc, i, j));
+      real ca = F2(g.cosa, i, j), rs = F2(g.rsina, i, j);
+      real ubc = (ub_cov - vb_cov * ca) * rs;
+      real vbc = (vb_cov - ub_cov * ca) * rs;
       bool ns = (j == js || j == je + 1), ew = (i == s || i == e + 1);
-      if (ns) ubc = 0.25 * (-F3(ucc, i, j - 2) + 3.0 * (F3(ucc, i, j - 1) + F3(ucc, i, j)) - F3(ucc, i, j + 1));
-      if (ew) ubc = 0.5 * (F3(ucc, i, j - 1) + F3(ucc, i, j));
-      if (ew) vbc = 0.25 * (-F3(vcc, i - 2, j) + 3.0 * (F3(vcc, i - 1, j) + F3(vcc, i, j)) - F3(vcc, i + 1, j));
-      if (ns) vbc = 0.5 * (F3(vcc, i - 1, j) + F3(vcc, i, j));
+      if (ns) ubc = RC(0.25) * (-F3(ucc, i, j - 2) + RC(3.0) * (F3(ucc, i, j - 1) + F3(ucc, i, j)) - F3(ucc, i, j + 1));
+      if (ew) ubc = RC(0.5) * (F3(ucc, i, j - 1) + F3(ucc, i, j));
+      if (ew) vbc = RC(0.25) * (-F3(vcc, i - 2, j) + RC(3.0) * (F3(vcc, i - 1, j) + F3(vcc, i, j)) - F3(vcc, i + 1, j));
+      if (ns) vbc = RC(0.5) * (F3(vcc, i - 1, j) + F3(vcc, i, j));
       // advect_v_along_y and advect_u_along_x: PPM of the D-grid wind with
       // cell-edge spacing dx/dy, corner-zeroed edge perturbations
-      auto advect = [&](auto qline, auto dxline, double rdx_m, double rdx_0, double ub, int pos, int sA, int eA,
+      auto advect = [&](auto qline, auto dxline, real rdx_m, real rdx_0, real ub, int pos, int sA, int eA,
                         bool zero_m, bool zero_0) {
-        double alm = ppm_al(qline, dxline, -1, pos, sA, eA);
-        double al0 = ppm_al(qline, dxline, 0, pos, sA, eA);
-        double alp = ppm_al(qline, dxline, 1, pos, sA, eA);
-        double qm = qline(-1), q0 = qline(0);
-        double blm = alm - qm, brm = al0 - qm;
-        double bl0 = al0 - q0, br0 = alp - q0;
-        if (zero_m) { blm = 0.0; brm = 0.0; }
-        if (zero_0) { bl0 = 0.0; br0 = 0.0; }
-        double b0m = blm + brm, b00 = bl0 + br0;
-        double cfl = ub > 0 ? ub * dt * rdx_m : ub * dt * rdx_0;
-        double fx0 = cfl > 0.0 ? (1.0 - cfl) * (brm - cfl * b0m) : (1.0 + cfl) * (bl0 + cfl * b00);
-        double mask = (ppm_smooth(blm, b0m, brm, mord) || ppm_smooth(bl0, b00, br0, mord)) ? 1.0 : 0.0;
-        return ub > 0.0 ? qm + fx0 * mask : q0 + fx0 * mask;
+        real alm = ppm_al(qline, dxline, -1, pos, sA, eA);
+        real al0 = ppm_al(qline, dxline, 0, pos, sA, eA);
+        real alp = ppm_al(qline, dxline, 1, pos, sA, eA);
+        real qm = qline(-1), q0 = qline(0);
+        real blm = alm - qm, brm = al0 - qm;
+        real bl0 = al0 - q0, br0 = alp - q0;
+        if (zero_m) { blm = RC(0.0); brm = RC(0.0); }
+        if (zero_0) { bl0 = RC(0.0); br0 = RC(0.0); }
+        real b0m = blm + brm, b00 = bl0 + br0;
+        real cfl = ub > 0 ? ub * dt * rdx_m : ub * dt * rdx_0;
+        real fx0 = cfl > RC(0.0) ? (RC(1.0) - cfl) * (brm - cfl * b0m) : (RC(1.0) + cfl) * (bl0 + cfl * b00);
+        real mask = (ppm_smooth(blm, b0m, brm, mord) || ppm_smooth(bl0, b00, br0, mord)) ? RC(1.0) : RC(0.0);
+        return ub > RC(0.0) ? qm + fx0 * mask : q0 + fx0 * mask;
       };
       // zero-corner regions of get_bl_br (xtp_u.py:40-46 / ytp_v.py)
       auto zc_x = [&](int ii, int jj) {
@@ -552,17 +553,17 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
       auto zc_y = [&](int ii, int jj) {
         return (ii == s || ii == e + 1) && ((jj >= js - 1 && jj < js + 1) || (jj >= je && jj < je + 2));
       };
-      double adv_v = advect(line3<1>(d, v, t, i, j, k), line2<1>(d, g.dy, t, i, j), F2(g.rdy, i, j - 1),
+      real adv_v = advect(line3<1>(d, v, t, i, j, k), line2<1>(d, g.dy, t, i, j), F2(g.rdy, i, j - 1),
                             F2(g.rdy, i, j), vbc, j, js, je, zc_y(i, j - 1), zc_y(i, j));
-      double adv_u = advect(line3<0>(d, u, t, i, j, k), line2<0>(d, g.dx, t, i, j), F2(g.rdx, i - 1, j),
+      real adv_u = advect(line3<0>(d, u, t, i, j, k), line2<0>(d, g.dx, t, i, j), F2(g.rdx, i - 1, j),
                             F2(g.rdx, i, j), ubc, i, s, e, zc_x(i - 1, j), zc_x(i, j));
-      double ke = 0.5 * dt * (ubc * adv_u + vbc * adv_v);
+      real ke = RC(0.5) * dt * (ubc * adv_u + vbc * adv_v);
       // all_corners_ke (d_sw.py:121-160)
       auto corner_ke = [&](int io1, int jo1, int io2, int vsign) {
-        double dt6 = dt / 6.0;
-        double ut0 = F3(ucc, i, j), utm = F3(ucc, i, j - 1);
-        double vt0 = F3(vcc, i, j), vtm = F3(vcc, i - 1, j);
-        double u0 = F3(u, i, j), um = F3(u, i - 1, j), v0 = F3(v, i, j), vm = F3(v, i, j - 1);
+        real dt6 = dt / RC(6.0);
+        real ut0 = F3(ucc, i, j), utm = F3(ucc, i, j - 1);
+        real vt0 = F3(vcc, i, j), vtm = F3(vcc, i - 1, j);
+        real u0 = F3(u, i, j), um = F3(u, i - 1, j), v0 = F3(v, i, j), vm = F3(v, i, j - 1);
         return dt6 * ((ut0 + utm) * ((io1 + 1) * u0 - (io1 * um)) + (vt0 + vtm) * ((jo1 + 1) * v0 - (jo1 * vm)) +
                       (((jo1 + 1) * ut0 - (jo1 * utm)) + vsign * ((io1 + 1) * vt0 - (io1 * vtm))) *
                           ((io2 + 1) * u0 - (io2 * um)));
@@ -577,18 +578,18 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
   // compute_vorticity (d_sw.py:468-490), full halo domain
   FV3B_CHECK(launch_box(Box{0, full, 0, full, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    double ra = F2(g.rarea, i, j);
-    double dxv = F2(g.dx, i, j), dyv = F2(g.dy, i, j);
-    double rdy_tmp = ra * dxv, rdx_tmp = ra * dyv;
+    real ra = F2(g.rarea, i, j);
+    real dxv = F2(g.dx, i, j), dyv = F2(g.dy, i, j);
+    real rdy_tmp = ra * dxv, rdx_tmp = ra * dyv;
     W3(tmp_wk, i, j) = (F3(u, i, j) - F3(u, i, j + 1) * F2(g.dx, i, j + 1) / dxv) * rdy_tmp +
                        (F3(v, i + 1, j) * F2(g.dy, i + 1, j) / dyv - F3(v, i, j)) * rdx_tmp;
   }));
   // adjust_w_and_qcon (d_sw.py:324-335)
   FV3B_CHECK(launch_box(Box{s, e + 1, js, je + 1, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    double dp = F3(delp, i, j);
-    double wn = F3(w, i, j) / dp;
-    if (col_damp_w[k] > 1e-5) wn = wn + F3(tmp_dw, i, j);
+    real dp = F3(delp, i, j);
+    real wn = F3(w, i, j) / dp;
+    if (col_damp_w[k] > RC(1e-5)) wn = wn + F3(tmp_dw, i, j);
     W3(w, i, j) = wn;
     W3(q_con, i, j) = F3(q_con, i, j) / dp;
   }));
@@ -596,27 +597,27 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
   {
     const int kz = sp.nonzero_nord_k;
     const int nn = sp.nonzero_nord;
-    const double dddmp = cfg.dddmp, da_min_c = g.da_min_c, dd8 = sp.dd8;
-    double* u_contra_dyc = ptc;
-    double* v_contra_dxc = tmp_vort;
+    const real dddmp = cfg.dddmp, da_min_c = g.da_min_c, dd8 = sp.dd8;
+    real* u_contra_dyc = ptc;
+    real* v_contra_dxc = tmp_vort;
     if (kz > 0) {
       // get_delpc, first computation, on the extent its second one reads
       FV3B_CHECK(launch_box(Box{s - 1, e + 2, js - 1, je + 2, 0, kz}, st, [=] __device__(int t, int i, int j, int k) {
         PT_SETUP(d, t, k);
         if (j >= js) {
-          double vfv = 0.5 * (F3(va, i, j - 1) + F3(va, i, j));
-          double uct = (F3(u, i, j) - vfv * F2(g.cosa_v, i, j)) * F2(g.sina_v, i, j);
+          real vfv = RC(0.5) * (F3(va, i, j - 1) + F3(va, i, j));
+          real uct = (F3(u, i, j) - vfv * F2(g.cosa_v, i, j)) * F2(g.sina_v, i, j);
           if (j == js || j == je + 1)
             uct = F3(vc, i, j) > 0 ? F3(u, i, j) * F2(g.sin_sg4, i, j - 1) : F3(u, i, j) * F2(g.sin_sg2, i, j);
           W3(u_contra_dyc, i, j) = uct * F2(g.dyc, i, j);
         }
         if (i >= s) {
-          double ufu = 0.5 * (F3(ua, i - 1, j) + F3(ua, i, j));
-          double vct = (F3(v, i, j) - ufu * F2(g.cosa_u, i, j)) * F2(g.sina_u, i, j);
+          real ufu = RC(0.5) * (F3(ua, i - 1, j) + F3(ua, i, j));
+          real vct = (F3(v, i, j) - ufu * F2(g.cosa_u, i, j)) * F2(g.sina_u, i, j);
           if (i == s || i == e + 1)
             vct = F3(uc, i, j) > 0 ? F3(v, i, j) * F2(g.sin_sg3, i - 1, j) : F3(v, i, j) * F2(g.sin_sg1, i, j);
-          double vcd = vct * F2(g.dxc, i, j);
-          if ((i == s || i == e + 1) && (j == je + 1 || j == js - 1)) vcd = 0.0;
+          real vcd = vct * F2(g.dxc, i, j);
+          if ((i == s || i == e + 1) && (j == je + 1 || j == js - 1)) vcd = RC(0.0);
           W3(v_contra_dxc, i, j) = vcd;
         }
       }));
@@ -625,14 +626,14 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
     FV3B_CHECK(launch_box(Box{s, e + 2, js, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
       PT_SETUP(d, t, k);
       if (k < kz) {
-        double dpc = F3(v_contra_dxc, i, j - 1) - F3(v_contra_dxc, i, j) + F3(u_contra_dyc, i - 1, j) -
+        real dpc = F3(v_contra_dxc, i, j - 1) - F3(v_contra_dxc, i, j) + F3(u_contra_dyc, i - 1, j) -
                      F3(u_contra_dyc, i, j);
         dpc = F2(g.rarea_c, i, j) * dpc;
         W3(delpc, i, j) = dpc;
-        double delpcdt = dpc * dt;
-        double mintmp = fmin(0.2, dddmp * fabs(delpcdt));
-        double damp = da_min_c * fmax(col_d2_divg[k], mintmp);
-        double vort = damp * dpc;
+        real delpcdt = dpc * dt;
+        real mintmp = fmin(RC(0.2), dddmp * fabs(delpcdt));
+        real damp = da_min_c * fmax(col_d2_divg[k], mintmp);
+        real vort = damp * dpc;
         W3(v_contra_dxc, i, j) = vort;
         W3(tmp_ke, i, j) = F3(tmp_ke, i, j) + vort;
       } else {
@@ -655,12 +656,12 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
                               PT_SETUP(d, t, k);
                               W3(uc, i, j) = (F3(divgd, i, j + 1) - F3(divgd, i, j)) * F2(g.divg_v, i, j);
                             }));
-      if (fillc) FV3B_CHECK(fill_dgrid(d, vc, uc, -1.0, kz, nz, st));
+      if (fillc) FV3B_CHECK(fill_dgrid(d, vc, uc, -RC(1.0), kz, nz, st));
       // redo_divg_d (divergence_damping.py:136-151)
       FV3B_CHECK(launch_box(Box{s - nt, e + nt + 2, js - nt, je + nt + 2, kz, nz}, st,
                             [=] __device__(int t, int i, int j, int k) {
                               PT_SETUP(d, t, k);
-                              double dd = F3(uc, i, j - 1) - F3(uc, i, j) + F3(vc, i - 1, j) - F3(vc, i, j);
+                              real dd = F3(uc, i, j - 1) - F3(uc, i, j) + F3(vc, i - 1, j) - F3(vc, i, j);
                               bool ci = (i == s || i == e + 1);
                               if (ci && j == js) dd = F3(vc, i - 1, j) - F3(vc, i, j) - F3(uc, i, j);
                               if (ci && j == je + 1) dd = F3(uc, i, j - 1) + F3(vc, i - 1, j) - F3(vc, i, j);
@@ -668,24 +669,24 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
                             }));
     }
     // _vorticity_calc: a2b_ord4(wk -> vort) then smagorinsky, on k >= kz
-    if (dddmp < 1e-5) {
+    if (dddmp < RC(1e-5)) {
       FV3B_CHECK(launch_box(Box{s - 3, e + 5, js - 3, je + 5, kz, nz}, st, [=] __device__(int t, int i, int j, int k) {
         PT_SETUP(d, t, k);
-        W3(v_contra_dxc, i, j) = 0.0;
+        W3(v_contra_dxc, i, j) = RC(0.0);
       }));
     } else {
       FV3B_CHECK(a2b_ord4(d, g, tmp_wk, v_contra_dxc, a2b_qx, a2b_qy, a2b_edges, kz, nz, st));
     }
     // smagorinsky_diffusion_approx + damping_nord_highorder (110-123, 154-156)
-    const double adt = fabs(dt);
-    const bool smag = !(dddmp < 1e-5);
+    const real adt = fabs(dt);
+    const bool smag = !(dddmp < RC(1e-5));
     FV3B_CHECK(launch_box(Box{s, e + 2, js, je + 2, kz, nz}, st, [=] __device__(int t, int i, int j, int k) {
       PT_SETUP(d, t, k);
-      double dpc = F3(delpc, i, j);
-      double vort = F3(v_contra_dxc, i, j);
+      real dpc = F3(delpc, i, j);
+      real vort = F3(v_contra_dxc, i, j);
       if (smag) vort = adt * sqrt(dpc * dpc + vort * vort);
-      double mintmp = fmin(0.2, dddmp * fabs(vort));
-      double damp = da_min_c * fmax(col_d2_divg[k], mintmp);
+      real mintmp = fmin(RC(0.2), dddmp * fabs(vort));
+      real damp = da_min_c * fmax(col_d2_divg[k], mintmp);
       vort = damp * dpc + dd8 * F3(divgd, i, j);
       W3(v_contra_dxc, i, j) = vort;
       W3(tmp_ke, i, j) = F3(tmp_ke, i, j) + vort;
@@ -720,20 +721,20 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
     const bool add_total = cfg.d_con > DCON_THRESHOLD || cfg.do_skeb;
     FV3B_CHECK(launch_box(Box{s, e + 2, js, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
       PT_SETUP(d, t, k);
-      double kf = col_d_con[k];
+      real kf = col_d_con[k];
       if (kf > DCON_THRESHOLD) {
         auto ubt = [&](int ii, int jj) { return (F3(vort_x_delta, ii, jj) + F3(tmp_vt, ii, jj)) * F2(g.rdx, ii, jj); };
         auto vbt = [&](int ii, int jj) { return (F3(vort_y_delta, ii, jj) - F3(tmp_ut, ii, jj)) * F2(g.rdy, ii, jj); };
         auto fyf = [&](int ii, int jj) { return F3(u, ii, jj) * F2(g.rdx, ii, jj); };
         auto fxf = [&](int ii, int jj) { return F3(v, ii, jj) * F2(g.rdy, ii, jj); };
-        double ub0 = ubt(i, j), ub1 = ubt(i, j + 1), vb0 = vbt(i, j), vb1 = vbt(i + 1, j);
-        double fy0 = fyf(i, j), fy1 = fyf(i, j + 1), fx0 = fxf(i, j), fx1 = fxf(i + 1, j);
-        double gy0 = fy0 * ub0, gy1 = fy1 * ub1, gx0 = fx0 * vb0, gx1 = fx1 * vb1;
-        double u2 = fy0 + fy1, du2 = ub0 + ub1, v2 = fx0 + fx1, dv2 = vb0 + vb1;
-        double dampterm = F2(g.rsin2, i, j) * ((ub0 * ub0 + ub1 * ub1 + vb0 * vb0 + vb1 * vb1) +
-                                               2.0 * (gy0 + gy1 + gx0 + gx1) -
+        real ub0 = ubt(i, j), ub1 = ubt(i, j + 1), vb0 = vbt(i, j), vb1 = vbt(i + 1, j);
+        real fy0 = fyf(i, j), fy1 = fyf(i, j + 1), fx0 = fxf(i, j), fx1 = fxf(i + 1, j);
+        real gy0 = fy0 * ub0, gy1 = fy1 * ub1, gx0 = fx0 * vb0, gx1 = fx1 * vb1;
+        real u2 = fy0 + fy1, du2 = ub0 + ub1, v2 = fx0 + fx1, dv2 = vb0 + vb1;
+        real dampterm = F2(g.rsin2, i, j) * ((ub0 * ub0 + ub1 * ub1 + vb0 * vb0 + vb1 * vb1) +
+                                               RC(2.0) * (gy0 + gy1 + gx0 + gx1) -
                                                F2(g.cosa_s, i, j) * (u2 * dv2 + v2 * du2 + du2 * dv2));
-        double hs = F3(delp, i, j) * (F3(tmp_heat_s, i, j) - 0.25 * kf * dampterm);
+        real hs = F3(delp, i, j) * (F3(tmp_heat_s, i, j) - RC(0.25) * kf * dampterm);
         W3(tmp_heat_s, i, j) = hs;
         if (add_total && i <= e && j <= je) W3(heat_source, i, j) = F3(heat_source, i, j) + hs;
       } else if (add_total && i <= e && j <= je) {
@@ -744,7 +745,7 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc
   // update_u_and_v (d_sw.py:441-465)
   FV3B_CHECK(launch_box(Box{s, e + 2, js, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    if (!(col_damp_vt[k] > 1e-5)) return;
+    if (!(col_damp_vt[k] > RC(1e-5))) return;
     if (i <= e) W3(u, i, j) = F3(u, i, j) + F3(tmp_vt, i, j);
     if (j <= je) W3(v, i, j) = F3(v, i, j) - F3(tmp_ut, i, j);
   }));

@@ -19,11 +19,11 @@ using namespace fv3b;
 namespace {
 constexpr double PI = 3.1415926535897931;
 constexpr double SDAY = 86400.0;
-constexpr double GRAV = 9.80665;
-constexpr double RDGAS = 287.05;
-constexpr double CP_AIR = 1004.6;
-constexpr double CV_AIR = CP_AIR - RDGAS;
-constexpr double RDG = -RDGAS / GRAV;
+constexpr real GRAV = RC(9.80665);
+constexpr real RDGAS = RC(287.05);
+constexpr real CP_AIR = RC(1004.6);
+constexpr real CV_AIR = CP_AIR - RDGAS;
+constexpr real RDG = -RDGAS / GRAV;
 }  // namespace
 
 // RayleighDamping.__call__ (ray_fast.py:169-192) with ray_fast_wind_compute
@@ -34,7 +34,7 @@ constexpr double RDG = -RDGAS / GRAV;
 // accumulated layer mass, to the levels with pfull < rf_cutoff +
 // min(100, 10 ptop); pfull increases with k, so both level sets are
 // prefixes [0, k_rf) and [0, k_nudge).
-extern "C" int fv3b_ray_fast(fv3b_ctx* ctx, double* u, double* v, double* w, const double* dp, const double* pfull,
+extern "C" int fv3b_ray_fast(fv3b_ctx* ctx, real* u, real* v, real* w, const double* dp, const double* pfull,
                              double dt, double ptop, double rf_cutoff, double tau, int hydrostatic, void* stream) {
   FV3B_REQUIRE(ctx && u && v && w && dp && pfull, "fv3b_ray_fast: null argument");
   const Dims d = ctx->d;
@@ -65,8 +65,10 @@ extern "C" int fv3b_ray_fast(fv3b_ctx* ctx, double* u, double* v, double* w, con
       for (int k = 1; k < k_nudge; ++k) dm[k] = dm[k - 1] + dp[k];
       for (int k = k_nudge - 2; k >= 0; --k) dm[k] = dm[k + 1];
     }
-    FV3B_CHECK(cudaMemcpy(colp(ctx, COL_RF), c.data(), sizeof(double) * c.size(), cudaMemcpyHostToDevice));
-    FV3B_CHECK(cudaMemcpy(colp(ctx, COL_DP_RAY), dp, sizeof(double) * nz, cudaMemcpyHostToDevice));
+    std::vector<real> c_r(c.begin(), c.end());
+    FV3B_CHECK(cudaMemcpy(colp(ctx, COL_RF), c_r.data(), sizeof(real) * c_r.size(), cudaMemcpyHostToDevice));
+    std::vector<real> dp_r(dp, dp + nz);
+    FV3B_CHECK(cudaMemcpy(colp(ctx, COL_DP_RAY), dp_r.data(), sizeof(real) * nz, cudaMemcpyHostToDevice));
     rs.ready = true;
     rs.dt = dt;
     rs.ptop = ptop;
@@ -81,19 +83,19 @@ extern "C" int fv3b_ray_fast(fv3b_ctx* ctx, double* u, double* v, double* w, con
   }
   const int k_rf = rs.k_rf, k_nudge = rs.k_nudge;
   if (k_rf == 0) return FV3B_OK;
-  const double* rf = colp(ctx, COL_RF);
-  const double* dm = colp(ctx, COL_RF_DM);
-  const double* dpc = colp(ctx, COL_DP_RAY);
+  const real* rf = colp(ctx, COL_RF);
+  const real* dm = colp(ctx, COL_RF_DM);
+  const real* dpc = colp(ctx, COL_DP_RAY);
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
   const bool do_w = hydrostatic == 0;
   FV3B_CHECK(launch_columns(s, e + 2, js, je + 2, st, [=] __device__(int t, int i, int j) {
     const long long o0 = idx3(d, t, i, j, 0);
-    auto damp = [&](double* q) {
-      double total = 0.0;
+    auto damp = [&](real* q) {
+      real total = RC(0.0);
       for (int k = 0; k < k_rf; ++k) {
         long long o = o0 + k * d.sk;
-        double c = q[o];
-        double lost = (1.0 - rf[k]) * dpc[k] * c;
+        real c = q[o];
+        real lost = (RC(1.0) - rf[k]) * dpc[k] * c;
         total = k == 0 ? lost : total + lost;
         q[o] = c * rf[k];
       }
@@ -115,22 +117,22 @@ extern "C" int fv3b_ray_fast(fv3b_ctx* ctx, double* u, double* v, double* w, con
 // compute domain plus nt = ntimes-1-n halo rows.  The reference's corner
 // copies of its scratch q (copy_corners_x before the x fluxes, _y before
 // the y fluxes and the copy back) are reads through the corner rules.
-extern "C" int fv3b_del2cubed(fv3b_ctx* ctx, double* qdel, double cd, int nmax, void* stream) {
+extern "C" int fv3b_del2cubed(fv3b_ctx* ctx, real* qdel, double cd, int nmax, void* stream) {
   FV3B_REQUIRE(ctx && qdel, "fv3b_del2cubed: null argument");
   const Dims d = ctx->d;
   const fv3b_metrics g = ctx->m;
   cudaStream_t st = (cudaStream_t)stream;
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = d.nz;
   const int full = d.ni - 1;
-  double *q = ctx->ws[0], *fx = ctx->ws[1], *fy = ctx->ws[2];
+  real *q = ctx->ws[0], *fx = ctx->ws[1], *fy = ctx->ws[2];
   const int ntimes = nmax < 3 ? nmax : 3;
   for (int n = 0; n < ntimes; ++n) {
     const int nt = ntimes - (n + 1);
     // corner_fill (del2cubed.py:41-75) into q, full domain
     FV3B_CHECK(launch_box(Box{0, full, 0, full, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
       PT_SETUP(d, t, k);
-      const double third = 1.0 / 3.0;
-      double out = F3(qdel, i, j);
+      const real third = RC(1.0) / RC(3.0);
+      real out = F3(qdel, i, j);
       auto Q = [&](int di, int dj) { return F3(qdel, i + di, j + dj); };
       if (j == js) {
         if (i == s) out = (Q(0, 0) + Q(-1, 0) + Q(0, -1)) * third;
@@ -172,7 +174,7 @@ extern "C" int fv3b_del2cubed(fv3b_ctx* ctx, double* qdel, double cd, int nmax, 
     FV3B_CHECK(launch_box(Box{0, full, 0, full, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
       PT_SETUP(d, t, k);
       int si, sj;
-      double qv = (nt > 0 && copy_corner_y(d, i, j, si, sj)) ? F3(q, si, sj) : F3(q, i, j);
+      real qv = (nt > 0 && copy_corner_y(d, i, j, si, sj)) ? F3(q, si, sj) : F3(q, i, j);
       if (i >= s - nt && i < e + 1 + nt && j >= js - nt && j < je + 1 + nt)
         qv = qv + cd * F2(g.rarea, i, j) * (F3(fx, i, j) - F3(fx, i + 1, j) + F3(fy, i, j) - F3(fy, i, j + 1));
       W3(qdel, i, j) = qv;
@@ -183,8 +185,8 @@ extern "C" int fv3b_del2cubed(fv3b_ctx* ctx, double* qdel, double cd, int nmax, 
 
 // compute_pkz_tempadjust (temperature_adjust.py:8-44) on the compute domain,
 // levels [0, nk_heat).
-extern "C" int fv3b_pkz_tempadjust(fv3b_ctx* ctx, const double* delp, const double* delz, const double* cappa,
-                                   const double* heat_source, double* pt, double* pkz, double delt_time_factor,
+extern "C" int fv3b_pkz_tempadjust(fv3b_ctx* ctx, const real* delp, const real* delz, const real* cappa,
+                                   const real* heat_source, real* pt, real* pkz, double delt_time_factor,
                                    int nk_heat, void* stream) {
   FV3B_REQUIRE(ctx && delp && delz && cappa && heat_source && pt && pkz, "fv3b_pkz_tempadjust: null argument");
   const Dims d = ctx->d;
@@ -193,13 +195,13 @@ extern "C" int fv3b_pkz_tempadjust(fv3b_ctx* ctx, const double* delp, const doub
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
   FV3B_CHECK(launch_box(Box{s, e + 1, js, je + 1, 0, nk_heat}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    double cp = F3(cappa, i, j), dp = F3(delp, i, j);
-    double p = fm::fm_pow(RDG * dp / F3(delz, i, j) * F3(pt, i, j), cp / (1.0 - cp));
-    double dtmp = F3(heat_source, i, j) / (CV_AIR * dp);
-    double lim = k == 0 ? delt_time_factor * 0.1 : (k == 1 ? delt_time_factor * 0.5 : delt_time_factor);
-    double a = fabs(dtmp);
-    double m = lim < a ? lim : a;
-    double deltmin = dtmp > 0.0 ? fabs(m) : -fabs(m);
+    real cp = F3(cappa, i, j), dp = F3(delp, i, j);
+    real p = fm::fm_pow(RDG * dp / F3(delz, i, j) * F3(pt, i, j), cp / (RC(1.0) - cp));
+    real dtmp = F3(heat_source, i, j) / (CV_AIR * dp);
+    real lim = k == 0 ? delt_time_factor * RC(0.1) : (k == 1 ? delt_time_factor * RC(0.5) : delt_time_factor);
+    real a = fabs(dtmp);
+    real m = lim < a ? lim : a;
+    real deltmin = dtmp > RC(0.0) ? fabs(m) : -fabs(m);
     W3(pkz, i, j) = p;
     W3(pt, i, j) = F3(pt, i, j) + deltmin / p;
   }));

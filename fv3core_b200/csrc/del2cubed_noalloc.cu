@@ -37,15 +37,15 @@ namespace {
 // Scratch: three fields of at most FV3B_NOALLOC_FIELD_DOUBLES doubles each
 // (6 * (npz+1) * (n+7)^2 <= 1,500,000 covers C48 L79), 36 MB in total.
 constexpr long long FV3B_NOALLOC_FIELD_DOUBLES = 1500000;
-static __device__ __align__(256) double g_noalloc_scratch[3 * FV3B_NOALLOC_FIELD_DOUBLES];
+static __device__ __align__(256) real g_noalloc_scratch[3 * FV3B_NOALLOC_FIELD_DOUBLES];
 
 constexpr int MAX_DEVICES = 64;
 std::mutex g_scratch_mutex;
-double* g_scratch_addr[MAX_DEVICES] = {nullptr};
+real* g_scratch_addr[MAX_DEVICES] = {nullptr};
 
 // Device address of the scratch array on the current device, looked up once
 // per device.
-cudaError_t scratch_address(double** out) {
+cudaError_t scratch_address(real** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
@@ -55,7 +55,7 @@ cudaError_t scratch_address(double** out) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
-    g_scratch_addr[dev] = static_cast<double*>(p);
+    g_scratch_addr[dev] = static_cast<real*>(p);
   }
   *out = g_scratch_addr[dev];
   return cudaSuccess;
@@ -63,7 +63,7 @@ cudaError_t scratch_address(double** out) {
 
 }  // namespace
 
-extern "C" int fv3b_del2cubed_noalloc(const fv3b_grid_dims* dims, const fv3b_metrics* metrics, double* qdel,
+extern "C" int fv3b_del2cubed_noalloc(const fv3b_grid_dims* dims, const fv3b_metrics* metrics, real* qdel,
                                       double cd, int nmax, void* stream) {
   FV3B_REQUIRE(dims && metrics && qdel, "fv3b_del2cubed_noalloc: null argument");
   FV3B_REQUIRE(dims->npx >= 4 && dims->n_halo == 3 && dims->npz >= 1,
@@ -73,9 +73,9 @@ extern "C" int fv3b_del2cubed_noalloc(const fv3b_grid_dims* dims, const fv3b_met
                "fv3b_del2cubed_noalloc: grid too large for the static scratch "
                "(6*(npz+1)*(npx+7)^2 must be <= 1500000 doubles)");
   const fv3b_metrics g = *metrics;
-  double* base = nullptr;
+  real* base = nullptr;
   FV3B_CHECK(scratch_address(&base));
-  double *q = base, *fx = base + FV3B_NOALLOC_FIELD_DOUBLES, *fy = base + 2 * FV3B_NOALLOC_FIELD_DOUBLES;
+  real *q = base, *fx = base + FV3B_NOALLOC_FIELD_DOUBLES, *fy = base + 2 * FV3B_NOALLOC_FIELD_DOUBLES;
   cudaStream_t st = (cudaStream_t)stream;
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = d.nz;
   const int full = d.ni - 1;
@@ -85,8 +85,8 @@ extern "C" int fv3b_del2cubed_noalloc(const fv3b_grid_dims* dims, const fv3b_met
     // corner_fill (del2cubed.py:41-75) into q, full domain
     FV3B_CHECK(launch_box(Box{0, full, 0, full, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
       PT_SETUP(d, t, k);
-      const double third = 1.0 / 3.0;
-      double out = F3(qdel, i, j);
+      const real third = RC(1.0) / RC(3.0);
+      real out = F3(qdel, i, j);
       auto Q = [&](int di, int dj) { return F3(qdel, i + di, j + dj); };
       if (j == js) {
         if (i == s) out = (Q(0, 0) + Q(-1, 0) + Q(0, -1)) * third;
@@ -129,7 +129,7 @@ extern "C" int fv3b_del2cubed_noalloc(const fv3b_grid_dims* dims, const fv3b_met
     FV3B_CHECK(launch_box(Box{0, full, 0, full, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
       PT_SETUP(d, t, k);
       int si, sj;
-      double qv = (nt > 0 && copy_corner_y(d, i, j, si, sj)) ? F3(q, si, sj) : F3(q, i, j);
+      real qv = (nt > 0 && copy_corner_y(d, i, j, si, sj)) ? F3(q, si, sj) : F3(q, i, j);
       if (i >= s - nt && i < e + 1 + nt && j >= js - nt && j < je + 1 + nt)
         qv = qv + cd * F2(g.rarea, i, j) * (F3(fx, i, j) - F3(fx, i + 1, j) + F3(fy, i, j) - F3(fy, i, j + 1));
       W3(qdel, i, j) = qv;

@@ -28,6 +28,13 @@
 
 namespace fv3b {
 
+// Element type of the fields: double in the FP64 build, float in the
+// mixed-precision build (FV3B_REAL_T=float, see include/fv3core_b200.h).
+// RC(x) gives a floating constant that type, so constant-times-field
+// arithmetic stays in the build's precision.
+using real = fv3b_real;
+#define RC(x) (static_cast<::fv3b::real>(x))
+
 struct Dims {
   int n, h, nz;
   int ni, nj, nk;

@@ -15,8 +15,10 @@
 
 namespace fv3b {
 
-constexpr double HUGE_R = 1.0e40;
-constexpr double GRAV_ = 9.80665;
+// fill value of the gz and pk3 temporaries (dyn_core.py:333-336); FP32
+// holds 1e30 instead of 1e40
+constexpr double HUGE_R = sizeof(real) == sizeof(double) ? 1.0e40 : 1.0e30;
+constexpr real GRAV_ = RC(9.80665);
 constexpr double KAPPA_ = 287.05 / 1004.6;
 
 enum TmpId {
@@ -27,9 +29,9 @@ static const char* const TMP_NAMES[N_TMP3] = {"gz",  "zh",  "pkc", "pk3", "ut", 
 
 struct AcousticState {
   fv3b_acoustic_config cfg;
-  double* base = nullptr;
-  double* tmp[N_TMP3];
-  double *ws3 = nullptr, *zs = nullptr;
+  real* base = nullptr;
+  real* tmp[N_TMP3];
+  real *ws3 = nullptr, *zs = nullptr;
   std::vector<double> dp_ref, pfull;
   int nk_heat = 0;
   bool do_del2cubed = false;
@@ -37,12 +39,12 @@ struct AcousticState {
 };
 
 namespace {
-__global__ void fill_kernel(double* p, long long n, double v) {
+__global__ void fill_kernel(real* p, long long n, real v) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i < n) p[i] = v;
 }
 
-cudaError_t fill(double* p, long long n, double v, cudaStream_t st) {
+cudaError_t fill(real* p, long long n, real v, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   fill_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, n, v);
   note_launch();
@@ -62,7 +64,7 @@ int nk_heat_dissipation(const fv3b_dsw_config& c, int npz) {
 using namespace fv3b;
 
 extern "C" int fv3b_acoustics_setup(fv3b_ctx* ctx, const fv3b_acoustic_config* config, const fv3b_dsw_config* dsw,
-                                    const double* ak, const double* bk, const double* pfull, const double* phis) {
+                                    const double* ak, const double* bk, const double* pfull, const real* phis) {
   FV3B_REQUIRE(ctx && config && dsw && ak && bk && pfull && phis, "fv3b_acoustics_setup: null argument");
   FV3B_REQUIRE(dsw->d_ext == 0.0, "fv3b_acoustics_setup: d_ext != 0 is not implemented");
   FV3B_REQUIRE(!dsw->hydrostatic, "fv3b_acoustics_setup: only the nonhydrostatic dynamics are implemented");
@@ -77,7 +79,7 @@ extern "C" int fv3b_acoustics_setup(fv3b_ctx* ctx, const fv3b_acoustic_config* c
     a = new (std::nothrow) AcousticState();
     FV3B_REQUIRE(a != nullptr, "fv3b_acoustics_setup: out of host memory");
     const size_t n3 = (size_t)d.st * 6, n2 = (size_t)d.st2 * 6;
-    cudaError_t e = cudaMalloc((void**)&a->base, sizeof(double) * (n3 * N_TMP3 + 2 * n2));
+    cudaError_t e = cudaMalloc((void**)&a->base, sizeof(real) * (n3 * N_TMP3 + 2 * n2));
     if (e != cudaSuccess) {
       delete a;
       set_last_error("fv3b_acoustics_setup", e);
@@ -101,19 +103,19 @@ extern "C" int fv3b_acoustics_setup(fv3b_ctx* ctx, const fv3b_acoustic_config* c
   a->cd = 0.2 * ctx->m.da_min;
   // temporaries: zero, gz and pk3 at HUGE_R (dyn_core.py:333-336)
   const size_t n3 = (size_t)d.st * 6, n2 = (size_t)d.st2 * 6;
-  FV3B_CHECK(cudaMemset(a->base, 0, sizeof(double) * (n3 * N_TMP3 + 2 * n2)));
+  FV3B_CHECK(cudaMemset(a->base, 0, sizeof(real) * (n3 * N_TMP3 + 2 * n2)));
   FV3B_CHECK(fill(a->tmp[T_GZ], (long long)n3, HUGE_R, 0));
   FV3B_CHECK(fill(a->tmp[T_PK3], (long long)n3, HUGE_R, 0));
   // zs = phis * (1 / g) (dp_ref_compute, dyn_core.py:79)
-  double* zs = a->zs;
+  real* zs = a->zs;
   FV3B_CHECK(launch_columns(0, d.ni, 0, d.nj, 0, [=] __device__(int t, int i, int j) {
-    zs[idx2(d, t, i, j)] = phis[idx2(d, t, i, j)] * (1.0 / GRAV_);
+    zs[idx2(d, t, i, j)] = phis[idx2(d, t, i, j)] * (RC(1.0) / GRAV_);
   }));
   FV3B_CHECK(cudaDeviceSynchronize());
   return FV3B_OK;
 }
 
-extern "C" double* fv3b_acoustics_temporary(fv3b_ctx* ctx, const char* name) {
+extern "C" real* fv3b_acoustics_temporary(fv3b_ctx* ctx, const char* name) {
   if (!ctx || !ctx->acoustic || !name) return nullptr;
   AcousticState* a = ctx->acoustic;
   for (int q = 0; q < N_TMP3; ++q)
@@ -150,12 +152,12 @@ extern "C" int fv3b_acoustics(fv3b_ctx* ctx, const fv3b_dycore_state* S, void* s
   const int full = d.ni - 1;
   cudaStream_t st = (cudaStream_t)stream;
   fv3b_grid_dims gd{d.n, d.h, d.nz, 0};
-  double** T = a->tmp;
-  double *gz = T[T_GZ], *zh = T[T_ZH], *pkc = T[T_PKC], *pk3 = T[T_PK3], *ut = T[T_UT], *vt = T[T_VT];
-  double *divgd = T[T_DIVGD], *heat = T[T_HEAT], *crx = T[T_CRX], *cry = T[T_CRY], *xfx = T[T_XFX],
+  real** T = a->tmp;
+  real *gz = T[T_GZ], *zh = T[T_ZH], *pkc = T[T_PKC], *pk3 = T[T_PK3], *ut = T[T_UT], *vt = T[T_VT];
+  real *divgd = T[T_DIVGD], *heat = T[T_HEAT], *crx = T[T_CRX], *cry = T[T_CRY], *xfx = T[T_XFX],
          *yfx = T[T_YFX], *delpc = T[T_DELPC], *ptc = T[T_PTC];
-  double *ws3 = a->ws3, *zs = a->zs;
-  const double* dp_ref = colp(ctx, COL_DP_REF);
+  real *ws3 = a->ws3, *zs = a->zs;
+  const real* dp_ref = colp(ctx, COL_DP_REF);
   const int n_split = cfg.n_split;
   const double akap = KAPPA_;
   const double dt = S->mdt / n_split;
@@ -163,23 +165,23 @@ extern "C" int fv3b_acoustics(fv3b_ctx* ctx, const fv3b_dycore_state* S, void* s
   const double ptop = S->ptop;
 
   {
-    double* qc[2] = {S->q_con, S->cappa};
+    real* qc[2] = {S->q_con, S->cappa};
     FV3B_CHECK(halo_scalars(d, qc, 2, 1, d.h, nz, st));
-    double* dpt[2] = {S->delp, S->pt};
+    real* dpt[2] = {S->delp, S->pt};
     FV3B_CHECK(halo_scalars(d, dpt, 2, 1, d.h, nz, st));
     FV3B_CHECK(halo_vector(d, S->u, S->v, false, nz, st));
   }
   // zero_data (dyn_core.py:47-63)
   {
-    double *mfxd = S->mfxd, *mfyd = S->mfyd, *cxd = S->cxd, *cyd = S->cyd, *diss = S->diss_estd;
+    real *mfxd = S->mfxd, *mfyd = S->mfyd, *cxd = S->cxd, *cyd = S->cyd, *diss = S->diss_estd;
     const bool first = S->n_map == 1;
     FV3B_CHECK(launch_box(Box{0, full, 0, full, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
       PT_SETUP(d, t, k);
-      W3(mfxd, i, j) = 0.0;
-      W3(mfyd, i, j) = 0.0;
-      W3(cxd, i, j) = 0.0;
-      W3(cyd, i, j) = 0.0;
-      if (first && i >= s && i <= e && j >= js && j <= je) W3(diss, i, j) = 0.0;
+      W3(mfxd, i, j) = RC(0.0);
+      W3(mfyd, i, j) = RC(0.0);
+      W3(cxd, i, j) = RC(0.0);
+      W3(cyd, i, j) = RC(0.0);
+      if (first && i >= s && i <= e && j >= js && j <= je) W3(diss, i, j) = RC(0.0);
     }));
   }
   for (int it = 0; it < n_split; ++it) {
@@ -187,10 +189,10 @@ extern "C" int fv3b_acoustics(fv3b_ctx* ctx, const fv3b_dycore_state* S, void* s
     FV3B_CHECK(halo_scalars(d, &S->w, 1, 1, d.h, nz, st));
     if (it == 0) {
       // set_gz (dyn_core.py:80-85) on the compute domain
-      const double* delz = S->delz;
+      const real* delz = S->delz;
       FV3B_CHECK(launch_columns(s, e + 1, js, je + 1, st, [=] __device__(int t, int i, int j) {
         long long o = idx3(d, t, i, j, nz);
-        double g = zs[idx2(d, t, i, j)];
+        real g = zs[idx2(d, t, i, j)];
         gz[o] = g;
         for (int k = nz - 1; k >= 0; --k) {
           o -= d.sk;
@@ -205,8 +207,8 @@ extern "C" int fv3b_acoustics(fv3b_ctx* ctx, const fv3b_dycore_state* S, void* s
     if (dcfg.nord > 0) FV3B_CHECK(halo_scalars(d, &divgd, 1, 0, d.h, nz, st));
     // copy_stencil on the full domain, every interface
     {
-      const double* src = it == 0 ? gz : zh;
-      double* dst = it == 0 ? zh : gz;
+      const real* src = it == 0 ? gz : zh;
+      real* dst = it == 0 ? zh : gz;
       FV3B_CHECK(launch_box(Box{0, full, 0, full, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
         PT_SETUP(d, t, k);
         W3(dst, i, j) = F3(src, i, j);
@@ -220,7 +222,7 @@ extern "C" int fv3b_acoustics(fv3b_ctx* ctx, const fv3b_dycore_state* S, void* s
     FV3B_CALL(fv3b_d_sw(ctx, vt, S->delp, ptc, S->pt, S->u, S->v, S->w, S->uc, S->vc, S->ua, S->va, divgd, S->mfxd,
                         S->mfyd, S->cxd, S->cyd, crx, cry, xfx, yfx, S->q_con, zh, heat, S->diss_estd, dt, st));
     {
-      double* f3[3] = {S->delp, S->pt, S->q_con};
+      real* f3[3] = {S->delp, S->pt, S->q_con};
       FV3B_CHECK(halo_scalars(d, f3, 3, 1, d.h, nz, st));
     }
     FV3B_CALL(fv3b_update_dz_d(ctx, zs, zh, crx, cry, xfx, yfx, S->wsd, dt, st));

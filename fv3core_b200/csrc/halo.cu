@@ -12,7 +12,7 @@ namespace {
 constexpr int HALO_BLOCK = 128;
 
 struct FieldSet {
-  double* f[4];
+  real* f[4];
   int n;
 };
 
@@ -27,12 +27,12 @@ __global__ void halo_scalar_kernel(Dims d, FieldSet fs, int sx, int sy, int n_ha
   if (!halo_source(d, t, i, j, 0, sxo, syo, n_halo, src)) return;
   const long long dst = idx3(d, t, i, j, 0), from = idx3(d, src.t, src.i, src.j, 0);
   for (int q = 0; q < fs.n; ++q) {
-    double* f = fs.f[q];
+    real* f = fs.f[q];
     for (int k = 0; k < nlev; ++k) f[dst + k * d.sk] = f[from + k * d.sk];
   }
 }
 
-__global__ void halo_vector_kernel(Dims d, double* x, double* y, int cgrid, int nlev) {
+__global__ void halo_vector_kernel(Dims d, real* x, real* y, int cgrid, int nlev) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   const int t = blockIdx.y >> 1, comp = blockIdx.y & 1;
   const int n_halo = d.h;
@@ -45,29 +45,29 @@ __global__ void halo_vector_kernel(Dims d, double* x, double* y, int cgrid, int 
   if (!halo_point(d, p, sxo[comp], syo[comp], n_halo, i, j)) return;
   HaloSource src;
   if (!halo_source(d, t, i, j, comp, sxo, syo, n_halo, src)) return;
-  double* dstf = comp == 0 ? x : y;
-  const double* srcf = src.comp == 0 ? x : y;
-  const double sign = (double)src.sign;
+  real* dstf = comp == 0 ? x : y;
+  const real* srcf = src.comp == 0 ? x : y;
+  const real sign = (real)src.sign;
   const long long dst = idx3(d, t, i, j, 0), from = idx3(d, src.t, src.i, src.j, 0);
   for (int k = 0; k < nlev; ++k) dstf[dst + k * d.sk] = sign * srcf[from + k * d.sk];
 }
 
-__global__ void interface_sync_kernel(Dims d, double* u, double* v, int nlev) {
+__global__ void interface_sync_kernel(Dims d, real* u, real* v, int nlev) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
   const int t = blockIdx.y >> 1, comp = blockIdx.y & 1;
   if (a >= d.n) return;
   HaloSource dst;
   interface_sync_target(d, t, comp == 0 ? EDGE_S : EDGE_W, a, dst);
   const int si = comp == 0 ? d.h + a : d.h, sj = comp == 0 ? d.h : d.h + a;
-  const double* srcf = comp == 0 ? u : v;
-  double* dstf = dst.comp == 0 ? u : v;
-  const double sign = (double)dst.sign;
+  const real* srcf = comp == 0 ? u : v;
+  real* dstf = dst.comp == 0 ? u : v;
+  const real sign = (real)dst.sign;
   const long long from = idx3(d, t, si, sj, 0), to = idx3(d, dst.t, dst.i, dst.j, 0);
   for (int k = 0; k < nlev; ++k) dstf[to + k * d.sk] = sign * srcf[from + k * d.sk];
 }
 }  // namespace
 
-cudaError_t halo_scalars(const Dims& d, double* const* fields, int nfields, int stagger, int n_halo, int nlev,
+cudaError_t halo_scalars(const Dims& d, real* const* fields, int nfields, int stagger, int n_halo, int nlev,
                          cudaStream_t st) {
   const int nc = halo_candidates(d, n_halo);
   dim3 grid((nc + HALO_BLOCK - 1) / HALO_BLOCK, 6);
@@ -83,7 +83,7 @@ cudaError_t halo_scalars(const Dims& d, double* const* fields, int nfields, int 
   return cudaSuccess;
 }
 
-cudaError_t halo_vector(const Dims& d, double* x, double* y, bool cgrid, int nlev, cudaStream_t st) {
+cudaError_t halo_vector(const Dims& d, real* x, real* y, bool cgrid, int nlev, cudaStream_t st) {
   const int nc = halo_candidates(d, d.h);
   dim3 grid((nc + HALO_BLOCK - 1) / HALO_BLOCK, 12);
   halo_vector_kernel<<<grid, HALO_BLOCK, 0, st>>>(d, x, y, cgrid ? 1 : 0, nlev);
@@ -91,7 +91,7 @@ cudaError_t halo_vector(const Dims& d, double* x, double* y, bool cgrid, int nle
   return cudaGetLastError();
 }
 
-cudaError_t sync_vector_interfaces(const Dims& d, double* u, double* v, int nlev, cudaStream_t st) {
+cudaError_t sync_vector_interfaces(const Dims& d, real* u, real* v, int nlev, cudaStream_t st) {
   dim3 grid((d.n + HALO_BLOCK - 1) / HALO_BLOCK, 12);
   interface_sync_kernel<<<grid, HALO_BLOCK, 0, st>>>(d, u, v, nlev);
   note_launch();
@@ -105,7 +105,7 @@ using namespace fv3b;
 // HaloUpdater.update of one scalar field (fv3gfs-util, as the reference's
 // AcousticDynamics uses it): stagger 1 = cell centres (X, Y), 0 = cell
 // corners (X_INTERFACE, Y_INTERFACE); n_halo rows; nlev levels.
-extern "C" int fv3b_halo_update_scalar(fv3b_ctx* ctx, double* field, int stagger, int n_halo, int nlev,
+extern "C" int fv3b_halo_update_scalar(fv3b_ctx* ctx, real* field, int stagger, int n_halo, int nlev,
                                        void* stream) {
   FV3B_REQUIRE(ctx && field, "fv3b_halo_update_scalar: null argument");
   FV3B_REQUIRE(stagger == 0 || stagger == 1, "fv3b_halo_update_scalar: stagger must be 0 or 1");
@@ -117,7 +117,7 @@ extern "C" int fv3b_halo_update_scalar(fv3b_ctx* ctx, double* field, int stagger
 
 // Vector HaloUpdater.update: grid 0 = D-grid winds (u, v), 1 = C-grid winds
 // (uc, vc); full halo width.
-extern "C" int fv3b_halo_update_vector(fv3b_ctx* ctx, double* x, double* y, int grid, int nlev, void* stream) {
+extern "C" int fv3b_halo_update_vector(fv3b_ctx* ctx, real* x, real* y, int grid, int nlev, void* stream) {
   FV3B_REQUIRE(ctx && x && y, "fv3b_halo_update_vector: null argument");
   FV3B_REQUIRE(grid == 0 || grid == 1, "fv3b_halo_update_vector: grid must be 0 (D) or 1 (C)");
   FV3B_REQUIRE(nlev >= 1 && nlev <= ctx->d.nk, "fv3b_halo_update_vector: nlev out of range");
@@ -126,7 +126,7 @@ extern "C" int fv3b_halo_update_vector(fv3b_ctx* ctx, double* x, double* y, int 
 }
 
 // CubedSphereCommunicator.synchronize_vector_interfaces for D-grid winds.
-extern "C" int fv3b_synchronize_vector_interfaces(fv3b_ctx* ctx, double* u, double* v, int nlev, void* stream) {
+extern "C" int fv3b_synchronize_vector_interfaces(fv3b_ctx* ctx, real* u, real* v, int nlev, void* stream) {
   FV3B_REQUIRE(ctx && u && v, "fv3b_synchronize_vector_interfaces: null argument");
   FV3B_REQUIRE(nlev >= 1 && nlev <= ctx->d.nk, "fv3b_synchronize_vector_interfaces: nlev out of range");
   FV3B_CHECK(sync_vector_interfaces(ctx->d, u, v, nlev, (cudaStream_t)stream));

@@ -9,7 +9,9 @@
 // written in the same bottom-up pass that produces them.  The arrays are
 // sized by a compile-time level bucket >= npz+1, so an L79 column keeps 3 KB.
 // exp and log are the library's own (fmath.h), whose host build the oracle
-// uses, so results can be compared to the last bit.
+// uses, so results can be compared to the last bit.  The column arithmetic
+// is FP64 in both builds; in the mixed-precision build the fields it reads
+// and writes are FP32.
 #include <math.h>
 
 #include "common.cuh"
@@ -115,9 +117,9 @@ __device__ __forceinline__ void sim1_column(int K, DMF DM, W1F W1, DZF DZ, GMF G
 
 struct RiemCArgs {
   double dt2, ptop, p_fac;
-  const double *cappa, *hs, *ws, *ptc, *q_con, *delpc;
-  double *gz, *pef;
-  const double* w3;
+  const real *cappa, *hs, *ws, *ptc, *q_con, *delpc;
+  real *gz, *pef;
+  const real* w3;
 };
 
 // RiemannSolverC.__call__ body for one column (riem_solver_c.py:13-64)
@@ -125,9 +127,9 @@ template <int NK>
 struct RiemC {
   static __device__ __forceinline__ void run(const Dims& d, int t, int i, int j, const RiemCArgs& a) {
     const double dt2 = a.dt2, ptop = a.ptop, p_fac = a.p_fac;
-    const double *cappa = a.cappa, *hs = a.hs, *ws = a.ws, *ptc = a.ptc, *q_con = a.q_con, *delpc = a.delpc;
-    double *gz = a.gz, *pef = a.pef;
-    const double* w3 = a.w3;
+    const real *cappa = a.cappa, *hs = a.hs, *ws = a.ws, *ptc = a.ptc, *q_con = a.q_con, *delpc = a.delpc;
+    real *gz = a.gz, *pef = a.pef;
+    const real* w3 = a.w3;
     double pem[NK], pm[NK], pp[NK], gam[NK], w[NK];
     const int K = d.nk;
     const long long o0 = idx3(d, t, i, j, 0);
@@ -146,7 +148,7 @@ struct RiemC {
     }
     auto DM = [&](int k) { return delpc[o0 + k * sk] / GRAV; };
     auto W1 = [&](int k) { return w3[o0 + k * sk]; };
-    auto DZ = [&](int k) { return gz[o0 + (k + 1) * sk] - gz[o0 + k * sk]; };
+    auto DZ = [&](int k) { return (double)gz[o0 + (k + 1) * sk] - (double)gz[o0 + k * sk]; };
     auto GM = [&](int k) { return 1.0 / (1.0 - cappa[o0 + k * sk]); };
     auto PTR = [&](int k) { return ptc[o0 + k * sk]; };
     auto CP3 = [&](int k) { return cappa[o0 + k * sk]; };
@@ -167,10 +169,10 @@ struct RiemC {
 struct Riem3Args {
   bool last;
   double dt, ptop, p_fac, peln1, ptk;
-  const double *cappa, *zs, *wsd;
-  double* delz;
-  const double *q_con, *delp, *pt;
-  double *zh, *pe, *ppe, *pk3, *pk, *peln, *w;
+  const real *cappa, *zs, *wsd;
+  real* delz;
+  const real *q_con, *delp, *pt;
+  real *zh, *pe, *ppe, *pk3, *pk, *peln, *w;
 };
 
 // RiemannSolver3.__call__ body for one column (riem_solver3.py:24-103)
@@ -179,9 +181,9 @@ struct Riem3 {
   static __device__ __forceinline__ void run(const Dims& d, int t, int i, int j, const Riem3Args& a) {
     const bool last = a.last;
     const double dt = a.dt, ptop = a.ptop, p_fac = a.p_fac, peln1 = a.peln1, ptk = a.ptk;
-    const double *cappa = a.cappa, *zs = a.zs, *wsd = a.wsd, *q_con = a.q_con, *delp = a.delp, *pt = a.pt;
-    double *delz = a.delz, *zh = a.zh, *pe = a.pe, *ppe = a.ppe, *pk3 = a.pk3, *pk = a.pk, *peln = a.peln;
-    double* w_io = a.w;
+    const real *cappa = a.cappa, *zs = a.zs, *wsd = a.wsd, *q_con = a.q_con, *delp = a.delp, *pt = a.pt;
+    real *delz = a.delz, *zh = a.zh, *pe = a.pe, *ppe = a.ppe, *pk3 = a.pk3, *pk = a.pk, *peln = a.peln;
+    real* w_io = a.w;
     double pem[NK], pm[NK], pp[NK], gam[NK], w[NK];
     const int K = d.nk;
     const long long o0 = idx3(d, t, i, j, 0);
@@ -220,7 +222,7 @@ struct Riem3 {
     }
     auto DM = [&](int k) { return delp[o0 + k * sk] * RGRAV; };
     auto W1 = [&](int k) { return w_io[o0 + k * sk]; };
-    auto DZ = [&](int k) { return zh[o0 + (k + 1) * sk] - zh[o0 + k * sk]; };
+    auto DZ = [&](int k) { return (double)zh[o0 + (k + 1) * sk] - (double)zh[o0 + k * sk]; };
     auto GM = [&](int k) { return 1.0 / (1.0 - cappa[o0 + k * sk]); };
     auto PTR = [&](int k) { return pt[o0 + k * sk]; };
     auto CP3 = [&](int k) { return cappa[o0 + k * sk]; };
@@ -264,9 +266,9 @@ cudaError_t launch_riemann(const Dims& d, int i0, int i1, int j0, int j1, cudaSt
 using namespace fv3b;
 
 extern "C" int fv3b_riem_solver_c(const fv3b_grid_dims* dims, double dt2, double ptop, double p_fac,
-                                  const double* cappa, const double* hs, const double* ws,
-                                  const double* ptc, const double* q_con, const double* delpc,
-                                  double* gz, double* pef, const double* w3, void* stream) {
+                                  const real* cappa, const real* hs, const real* ws,
+                                  const real* ptc, const real* q_con, const real* delpc,
+                                  real* gz, real* pef, const real* w3, void* stream) {
   FV3B_REQUIRE(dims && cappa && hs && ws && ptc && q_con && delpc && gz && pef && w3,
                "fv3b_riem_solver_c: null argument");
   Dims d = make_dims(dims);
@@ -280,9 +282,9 @@ extern "C" int fv3b_riem_solver_c(const fv3b_grid_dims* dims, double dt2, double
 // Sim1 solve, finalize (70-103) on the compute-domain columns, interface
 // levels 0..npz.
 extern "C" int fv3b_riem_solver3(const fv3b_grid_dims* dims, int last_call, double dt, double ptop, double p_fac,
-                                 const double* cappa, const double* zs, const double* wsd, double* delz,
-                                 const double* q_con, const double* delp, const double* pt, double* zh, double* pe,
-                                 double* ppe, double* pk3, double* pk, double* peln, double* w, void* stream) {
+                                 const real* cappa, const real* zs, const real* wsd, real* delz,
+                                 const real* q_con, const real* delp, const real* pt, real* zh, real* pe,
+                                 real* ppe, real* pk3, real* pk, real* peln, real* w, void* stream) {
   FV3B_REQUIRE(dims && cappa && zs && wsd && delz && q_con && delp && pt && zh && pe && ppe && pk3 && pk && peln && w,
                "fv3b_riem_solver3: null argument");
   Dims d = make_dims(dims);

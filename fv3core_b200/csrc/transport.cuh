@@ -15,33 +15,33 @@
 namespace fv3b {
 
 // ppm.py:8-20
-constexpr double PPM_C1 = -2.0 / 14.0, PPM_C2 = 11.0 / 14.0, PPM_C3 = 5.0 / 14.0;
-constexpr double PPM_P1 = 7.0 / 12.0, PPM_P2 = -1.0 / 12.0;
+constexpr real PPM_C1 = -RC(2.0) / RC(14.0), PPM_C2 = RC(11.0) / RC(14.0), PPM_C3 = RC(5.0) / RC(14.0);
+constexpr real PPM_P1 = RC(7.0) / RC(12.0), PPM_P2 = -RC(1.0) / RC(12.0);
 
 // Accessor of a 3-D field along one axis through point (i, j) of level k:
 // at(o) = f[i + o, j] (AXIS 0) or f[i, j + o] (AXIS 1).
 template <int AXIS>
 struct Line3 {
-  const double* p;
+  const real* p;
   long long base;  // index of (i, j, k)
   long long step;  // 1 or sj
-  __device__ __forceinline__ double operator()(int o) const { return p[base + o * step]; }
+  __device__ __forceinline__ real operator()(int o) const { return p[base + o * step]; }
 };
 
 template <int AXIS>
 struct Line2 {
-  const double* p;
+  const real* p;
   long long base;
   long long step;
-  __device__ __forceinline__ double operator()(int o) const { return p[base + o * step]; }
+  __device__ __forceinline__ real operator()(int o) const { return p[base + o * step]; }
 };
 
 template <int AXIS>
-__device__ __forceinline__ Line3<AXIS> line3(const Dims& d, const double* p, int t, int i, int j, int k) {
+__device__ __forceinline__ Line3<AXIS> line3(const Dims& d, const real* p, int t, int i, int j, int k) {
   return Line3<AXIS>{p, idx3(d, t, i, j, k), AXIS == 0 ? 1LL : d.sj};
 }
 template <int AXIS>
-__device__ __forceinline__ Line2<AXIS> line2(const Dims& d, const double* p, int t, int i, int j) {
+__device__ __forceinline__ Line2<AXIS> line2(const Dims& d, const real* p, int t, int i, int j) {
   return Line2<AXIS>{p, idx2(d, t, i, j), AXIS == 0 ? 1LL : (long long)d.ni};
 }
 
@@ -49,68 +49,68 @@ __device__ __forceinline__ Line2<AXIS> line2(const Dims& d, const double* p, int
 // read on the fly from q: a point of a cube-corner block takes its copy
 // source.  Sources never lie in a corner block, so this equals the copy
 // whether or not q's own corners already hold their x copies.
-__device__ __forceinline__ double qy_at(const Dims& d, const double* q, int t, int i, int j, int k) {
+__device__ __forceinline__ real qy_at(const Dims& d, const real* q, int t, int i, int j, int k) {
   int si, sj;
   if (copy_corner_y(d, i, j, si, sj)) return q[idx3(d, t, si, sj, k)];
   return q[idx3(d, t, i, j, k)];
 }
 struct LineQY {
   const Dims* d;
-  const double* q;
+  const real* q;
   int t, i, j, k;
-  __device__ __forceinline__ double operator()(int o) const { return qy_at(*d, q, t, i, j + o, k); }
+  __device__ __forceinline__ real operator()(int o) const { return qy_at(*d, q, t, i, j + o, k); }
 };
 
 // compute_al (xppm.py:148-181) for the cell at offset o of the line; pos is
 // the absolute index (along AXIS) of offset 0, s/e the compute bounds.
 template <typename Q, typename A>
-__device__ __forceinline__ double ppm_al(const Q& q, const A& dxa, int o, int pos, int s, int e) {
+__device__ __forceinline__ real ppm_al(const Q& q, const A& dxa, int o, int pos, int s, int e) {
   int ii = pos + o;
   if (ii == s + 1 || ii == e + 2) return PPM_C3 * q(o - 1) + PPM_C2 * q(o) + PPM_C1 * q(o + 1);
   if (ii == s || ii == e + 1)
-    return 0.5 * (((2.0 * dxa(o - 1) + dxa(o - 2)) * q(o - 1) - dxa(o - 1) * q(o - 2)) / (dxa(o - 2) + dxa(o - 1)) +
-                  ((2.0 * dxa(o) + dxa(o + 1)) * q(o) - dxa(o) * q(o + 1)) / (dxa(o) + dxa(o + 1)));
+    return RC(0.5) * (((RC(2.0) * dxa(o - 1) + dxa(o - 2)) * q(o - 1) - dxa(o - 1) * q(o - 2)) / (dxa(o - 2) + dxa(o - 1)) +
+                  ((RC(2.0) * dxa(o) + dxa(o + 1)) * q(o) - dxa(o) * q(o + 1)) / (dxa(o) + dxa(o + 1)));
   if (ii == s - 1 || ii == e) return PPM_C1 * q(o - 2) + PPM_C2 * q(o - 1) + PPM_C3 * q(o);
   return PPM_P1 * (q(o - 1) + q(o)) + PPM_P2 * (q(o - 2) + q(o + 1));
 }
 
-__device__ __forceinline__ bool ppm_smooth(double bl, double b0, double br, int mord) {
+__device__ __forceinline__ bool ppm_smooth(real bl, real b0, real br, int mord) {
   if (mord == 5) return bl * br < 0;
-  return (3.0 * fabs(b0)) < fabs(bl - br);
+  return (RC(3.0) * fabs(b0)) < fabs(bl - br);
 }
 
 // Mean of q advected through the interface at offset 0 (between cells -1
 // and 0) for Courant number c: get_flux (xppm.py:65-72) with fx1_fn,
 // get_advection_mask and apply_flux (xppm.py:19-61).
 template <typename Q, typename A>
-__device__ __forceinline__ double ppm_flux(const Q& q, const A& dxa, double c, int pos, int s, int e, int mord) {
-  double alm = ppm_al(q, dxa, -1, pos, s, e);
-  double al0 = ppm_al(q, dxa, 0, pos, s, e);
-  double alp = ppm_al(q, dxa, 1, pos, s, e);
-  double qm = q(-1), q0 = q(0);
-  double blm = alm - qm, brm = al0 - qm, b0m = blm + brm;
-  double bl0 = al0 - q0, br0 = alp - q0, b00 = bl0 + br0;
-  double mask = (ppm_smooth(blm, b0m, brm, mord) || ppm_smooth(bl0, b00, br0, mord)) ? 1.0 : 0.0;
-  double fx1 = c > 0.0 ? (1.0 - c) * (brm - c * b0m) : (1.0 + c) * (bl0 + c * b00);
-  return c > 0.0 ? qm + fx1 * mask : q0 + fx1 * mask;
+__device__ __forceinline__ real ppm_flux(const Q& q, const A& dxa, real c, int pos, int s, int e, int mord) {
+  real alm = ppm_al(q, dxa, -1, pos, s, e);
+  real al0 = ppm_al(q, dxa, 0, pos, s, e);
+  real alp = ppm_al(q, dxa, 1, pos, s, e);
+  real qm = q(-1), q0 = q(0);
+  real blm = alm - qm, brm = al0 - qm, b0m = blm + brm;
+  real bl0 = al0 - q0, br0 = alp - q0, b00 = bl0 + br0;
+  real mask = (ppm_smooth(blm, b0m, brm, mord) || ppm_smooth(bl0, b00, br0, mord)) ? RC(1.0) : RC(0.0);
+  real fx1 = c > RC(0.0) ? (RC(1.0) - c) * (brm - c * b0m) : (RC(1.0) + c) * (bl0 + c * b00);
+  return c > RC(0.0) ? qm + fx1 * mask : q0 + fx1 * mask;
 }
 
 // Scratch and options of one FiniteVolumeTransport call.
 struct FvTp2dArgs {
-  const double* q_base;   // field, its cube-corner blocks holding their x copies
-  const double* crx;
-  const double* cry;
-  const double* xfx;
-  const double* yfx;
-  const double* x_unit;   // x_mass_flux or xfx
-  const double* y_unit;
-  double* fx;
-  double* fy;
+  const real* q_base;   // field, its cube-corner blocks holding their x copies
+  const real* crx;
+  const real* cry;
+  const real* xfx;
+  const real* yfx;
+  const real* x_unit;   // x_mass_flux or xfx
+  const real* y_unit;
+  real* fx;
+  real* fy;
   int hord;
-  double* fx_mean;
-  double* fy_mean;
-  double* q_adv_x;
-  double* q_adv_y;
+  real* fx_mean;
+  real* fy_mean;
+  real* q_adv_x;
+  real* q_adv_y;
 };
 
 // FiniteVolumeTransport.__call__ (fvtp2d.py:249-362) without the damping
@@ -125,9 +125,13 @@ inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a
   // inner PPM: fy_mean on [is-3, ie+4] x [js, je+1], fx_mean on [is, ie+1] x [js-3, je+4]
   err = launch_box(Box{s - 3, e + 5, js - 3, je + 5, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
     if (i >= s - 3 && i < e + 5 && j >= js && j < je + 2) {
-      LineQY q{&d, a.q_base, t, i, j, k};
       auto dya = line2<1>(d, g.dya, t, i, j);
-      a.fy_mean[idx3(d, t, i, j, k)] = ppm_flux(q, dya, a.cry[idx3(d, t, i, j, k)], j, js, je, mord_in);
+      const long long o = idx3(d, t, i, j, k);
+      if (i >= s && i <= e) {  // no cube-corner point on this line: plain reads
+        a.fy_mean[o] = ppm_flux(line3<1>(d, a.q_base, t, i, j, k), dya, a.cry[o], j, js, je, mord_in);
+      } else {
+        a.fy_mean[o] = ppm_flux(LineQY{&d, a.q_base, t, i, j, k}, dya, a.cry[o], j, js, je, mord_in);
+      }
     }
     if (i >= s && i < e + 2 && j >= js - 3 && j < je + 5) {
       auto q = line3<0>(d, a.q_base, t, i, j, k);
@@ -139,17 +143,18 @@ inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a
   // q_i (fvtp2d.py:33-47) on [0, n+6) x [js, je+4), q_j (50-60) on [is, ie+4) x [0, n+6)
   err = launch_box(Box{0, full, 0, full, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    double area = F2(g.area, i, j);
+    real area = F2(g.area, i, j);
     if (j >= js && j < je + 4) {
-      double fyy0 = F3(a.yfx, i, j) * F3(a.fy_mean, i, j);
-      double fyy1 = F3(a.yfx, i, j + 1) * F3(a.fy_mean, i, j + 1);
+      real fyy0 = F3(a.yfx, i, j) * F3(a.fy_mean, i, j);
+      real fyy1 = F3(a.yfx, i, j + 1) * F3(a.fy_mean, i, j + 1);
       W3(a.q_adv_y, i, j) =
-          (qy_at(d, a.q_base, t, i, j, k) * area + fyy0 - fyy1) / (area + F3(a.yfx, i, j) - F3(a.yfx, i, j + 1));
+          ((i >= s && i <= e ? F3(a.q_base, i, j) : qy_at(d, a.q_base, t, i, j, k)) * area + fyy0 - fyy1) /
+          (area + F3(a.yfx, i, j) - F3(a.yfx, i, j + 1));
     }
     if (i >= s && i < e + 4) {
-      double fx10 = F3(a.xfx, i, j) * F3(a.fx_mean, i, j);
-      double fx11 = F3(a.xfx, i + 1, j) * F3(a.fx_mean, i + 1, j);
-      double awx = area + F3(a.xfx, i, j) - F3(a.xfx, i + 1, j);
+      real fx10 = F3(a.xfx, i, j) * F3(a.fx_mean, i, j);
+      real fx11 = F3(a.xfx, i + 1, j) * F3(a.fx_mean, i + 1, j);
+      real awx = area + F3(a.xfx, i, j) - F3(a.xfx, i + 1, j);
       W3(a.q_adv_x, i, j) = (F3(a.q_base, i, j) * area + fx10 - fx11) / awx;
     }
   });
@@ -160,21 +165,21 @@ inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a
     if (j <= je) {
       auto q = line3<0>(d, a.q_adv_y, t, i, j, k);
       auto dxa = line2<0>(d, g.dxa, t, i, j);
-      double xo = ppm_flux(q, dxa, a.crx[o], i, s, e, mord_out);
-      a.fx[o] = 0.5 * (xo + a.fx_mean[o]) * a.x_unit[o];
+      real xo = ppm_flux(q, dxa, a.crx[o], i, s, e, mord_out);
+      a.fx[o] = RC(0.5) * (xo + a.fx_mean[o]) * a.x_unit[o];
     }
     if (i <= e) {
       auto q = line3<1>(d, a.q_adv_x, t, i, j, k);
       auto dya = line2<1>(d, g.dya, t, i, j);
-      double yo = ppm_flux(q, dya, a.cry[o], j, js, je, mord_out);
-      a.fy[o] = 0.5 * (yo + a.fy_mean[o]) * a.y_unit[o];
+      real yo = ppm_flux(q, dya, a.cry[o], j, js, je, mord_out);
+      a.fy[o] = RC(0.5) * (yo + a.fy_mean[o]) * a.y_unit[o];
     }
   });
 }
 
 // The x half of CopyCornersXY in place (corners.py:64-117): only the 3 x 3
 // cube-corner blocks of q change; all npz+1 levels.
-inline cudaError_t copy_corners_x_inplace(const Dims d, double* q, cudaStream_t st) {
+inline cudaError_t copy_corners_x_inplace(const Dims d, real* q, cudaStream_t st) {
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
   // 4 corner blocks of 3 x 3 points
   return launch_box(Box{0, 12, 0, 3, 0, d.nk}, st, [=] __device__(int t, int x, int y, int k) {
@@ -189,13 +194,13 @@ inline cudaError_t copy_corners_x_inplace(const Dims d, double* q, cudaStream_t 
 
 // Per-level damping column on the device: nord band value and damp.
 struct DelnCol {
-  const double* nord;  // [nk] per-level nord (band value, see nord_at)
-  const double* damp;  // [nk]
+  const real* nord;  // [nk] per-level nord (band value, see nord_at)
+  const real* damp;  // [nk]
 };
 
 // nord of level k: the reference folds the column into bands k = 0, 1, 2, 3+
 // (delnflux.py intervals with externals nord0..nord3).
-__device__ __forceinline__ int nord_at(const double* nord, int k) { return (int)nord[k < 3 ? k : 3]; }
+__device__ __forceinline__ int nord_at(const real* nord, int k) { return (int)nord[k < 3 ? k : 3]; }
 
 // DelnFluxNoSG.__call__ (delnflux.py:1156-1207): del-n diffusive fluxes of q
 // into fx2/fy2 using d2 as scratch.  Corner copies of d2 are applied on read
@@ -203,8 +208,8 @@ __device__ __forceinline__ int nord_at(const double* nord, int k) { return (int)
 // the reference reads after copying the corners in place.
 // nlev is the number of levels (npz by default; UpdateHeightOnDGrid runs it
 // on npz + 1 interface levels).
-inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const double* q, double* fx2, double* fy2,
-                                 DelnCol col, double* d2, bool mass_weighted, int nmax, cudaStream_t st,
+inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const real* q, real* fx2, real* fy2,
+                                 DelnCol col, real* d2, bool mass_weighted, int nmax, cudaStream_t st,
                                  int nlev = -1) {
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = nlev < 0 ? d.nz : nlev;
   cudaError_t err;
@@ -246,11 +251,11 @@ inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const doubl
                           fy_in = i >= s && i < e + 1 && j >= js && j < je + 2;
                         }
                         if (fx_in) {
-                          double v = F2(g.del6_v, i, j) * (d2x(i - 1, j) - d2x(i, j));
+                          real v = F2(g.del6_v, i, j) * (d2x(i - 1, j) - d2x(i, j));
                           W3(fx2, i, j) = first ? v : -v;
                         }
                         if (fy_in) {
-                          double v = F2(g.del6_u, i, j) * (d2y(i, j - 1) - d2y(i, j));
+                          real v = F2(g.del6_u, i, j) * (d2y(i, j - 1) - d2y(i, j));
                           W3(fy2, i, j) = first ? v : -v;
                         }
                       });
@@ -276,8 +281,8 @@ inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const doubl
 
 // DelnFlux.__call__ (delnflux.py:963-998): damped fluxes added to fx, fy on
 // the cell corners of the compute domain.
-inline cudaError_t delnflux(const Dims d, const fv3b_metrics g, const double* q, double* fx, double* fy, DelnCol col,
-                           const double* mass, double* fx2, double* fy2, double* d2, int nmax, cudaStream_t st) {
+inline cudaError_t delnflux(const Dims d, const fv3b_metrics g, const real* q, real* fx, real* fy, DelnCol col,
+                           const real* mass, real* fx2, real* fy2, real* d2, int nmax, cudaStream_t st) {
   cudaError_t err = delnflux_nosg(d, g, q, fx2, fy2, col, d2, mass != nullptr, nmax, st);
   if (err != cudaSuccess) return err;
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
@@ -287,9 +292,9 @@ inline cudaError_t delnflux(const Dims d, const fv3b_metrics g, const double* q,
       W3(fx, i, j) = F3(fx, i, j) + F3(fx2, i, j);
       W3(fy, i, j) = F3(fy, i, j) + F3(fy2, i, j);
     } else {
-      double dk = col.damp[k];
-      W3(fx, i, j) = F3(fx, i, j) + 0.5 * dk * (F3(mass, i - 1, j) + F3(mass, i, j)) * F3(fx2, i, j);
-      W3(fy, i, j) = F3(fy, i, j) + 0.5 * dk * (F3(mass, i, j - 1) + F3(mass, i, j)) * F3(fy2, i, j);
+      real dk = col.damp[k];
+      W3(fx, i, j) = F3(fx, i, j) + RC(0.5) * dk * (F3(mass, i - 1, j) + F3(mass, i, j)) * F3(fx2, i, j);
+      W3(fy, i, j) = F3(fy, i, j) + RC(0.5) * dk * (F3(mass, i, j - 1) + F3(mass, i, j)) * F3(fy2, i, j);
     }
   });
 }

@@ -41,17 +41,19 @@ class Metrics(ctypes.Structure):
 class GridData:
     """All metric terms of an n x n cube on the GPU, plus the stage context."""
 
-    def __init__(self, grid: CubedSphereGrid, npz: int, device="cuda"):
+    def __init__(self, grid: CubedSphereGrid, npz: int, device="cuda", precision="f64"):
         self.grid = grid
-        self.grid_indexing = GridIndexing((grid.n, grid.n, npz), grid.halo)
+        self.precision = precision
+        self.grid_indexing = GridIndexing((grid.n, grid.n, npz), grid.halo, precision=precision)
+        tdtype = self.grid_indexing.dtype
         self.device = device
         self.tensors = {}
         for name in METRIC_FIELDS:
             a = np.asarray(getattr(grid, name), dtype=np.float64)
             if a.ndim == 3 and name != "a2b_extrap":  # [6, i, j] -> [6, j, i]
-                t = torch.from_numpy(np.ascontiguousarray(a.transpose(0, 2, 1))).to(device)
+                t = torch.from_numpy(np.ascontiguousarray(a.transpose(0, 2, 1))).to(device=device, dtype=tdtype)
             else:  # edge factors [6, n+1], corner ratios [6, 4, 3]
-                t = torch.from_numpy(np.ascontiguousarray(a)).to(device)
+                t = torch.from_numpy(np.ascontiguousarray(a)).to(device=device, dtype=tdtype)
             self.tensors[name] = t
             setattr(self, name, t)
         self.da_min = grid.da_min
@@ -63,7 +65,7 @@ class GridData:
         m.da_min_c = self.da_min_c
         self._metrics = m
         self._dims = self.grid_indexing.dims()
-        L = _lib.lib()
+        L = _lib.lib(precision)
         L.fv3b_ctx_create.argtypes = [ctypes.POINTER(_lib.GridDims), ctypes.POINTER(Metrics), ctypes.POINTER(ctypes.c_void_p)]
         L.fv3b_ctx_create.restype = ctypes.c_int
         L.fv3b_ctx_destroy.argtypes = [ctypes.c_void_p]
@@ -73,11 +75,12 @@ class GridData:
         if rc != 0:
             raise RuntimeError(f"fv3b_ctx_create failed ({rc}): {L.fv3b_last_error().decode()}")
         self.ctx = ctx
+        _lib.register_context(ctx, precision)
         self.grid_indexing.context = ctx
 
     def close(self):
         if getattr(self, "ctx", None) is not None and self.ctx.value:
-            _lib.lib().fv3b_ctx_destroy(self.ctx)
+            _lib.lib(self.precision).fv3b_ctx_destroy(self.ctx)
             self.ctx = None
 
     def __del__(self):

@@ -71,12 +71,13 @@ class AcousticDynamics:
 
         if name not in TEMPORARIES:
             raise KeyError(name)
-        ptr = _lib.lib().fv3b_acoustics_temporary(self._ctx, name.encode())
+        ptr = _lib.lib(self._gi.precision).fv3b_acoustics_temporary(self._ctx, name.encode())
         m, _, nk = self._gi.max_shape
         shape = {"ws3": (6, m, m), "zs": (6, m, m), "dp_ref": (nk,)}.get(name, (6, nk, m, m))
 
         class _View:
-            __cuda_array_interface__ = {"shape": shape, "typestr": "<f8", "data": (ptr, False), "version": 3,
+            __cuda_array_interface__ = {"shape": shape, "typestr": "<f4" if self._gi.precision == "f32" else "<f8",
+                                        "data": (ptr, False), "version": 3,
                                         "strides": None}
 
         return torch.as_tensor(_View(), device="cuda")

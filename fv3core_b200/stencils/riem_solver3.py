@@ -26,4 +26,5 @@ class RiemannSolver3:
             f3(cappa, "cappa"), check_field(zs, gi, "2d", "zs"), check_field(wsd, gi, "2d", "wsd"),
             f3(delz, "delz"), f3(q_con, "q_con"), f3(delp, "delp"), f3(pt, "pt"), f3(zh, "zh"), f3(pe, "pe"),
             f3(ppe, "ppe"), f3(pk3, "pk3"), f3(pk, "pk"), f3(peln, "peln"), f3(w, "w"), stream_ptr(),
+            precision=gi.precision,
         )

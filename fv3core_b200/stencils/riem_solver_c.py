@@ -31,4 +31,5 @@ class RiemannSolverC:
             check_field(pef, gi, "3d", "pef"),
             check_field(w3, gi, "3d", "w3"),
             stream_ptr(),
+            precision=gi.precision,
         )

@@ -16,7 +16,8 @@ class GridIndexing:
     """Index helper with the reference's names (fv3core/utils/stencil.py:280-642)
     for all six tiles of an n x n x npz cube."""
 
-    def __init__(self, domain, n_halo=3, south_edge=True, north_edge=True, west_edge=True, east_edge=True):
+    def __init__(self, domain, n_halo=3, south_edge=True, north_edge=True, west_edge=True, east_edge=True,
+                 precision="f64"):
         self.domain = tuple(int(x) for x in domain)
         self.n_halo = int(n_halo)
         if self.domain[0] != self.domain[1]:
@@ -27,6 +28,12 @@ class GridIndexing:
         # the device context (fv3b_ctx*) of the GridData built on this grid;
         # every stage class reaches the metric terms and workspace through it
         self.context = None
+        # "f64" (FP64 fields) or "f32" (the mixed-precision build's FP32 fields)
+        self.precision = precision
+
+    @property
+    def dtype(self):
+        return torch.float32 if self.precision == "f32" else torch.float64
 
     @property
     def n(self):
@@ -56,8 +63,9 @@ class GridIndexing:
         return GridDims(self.n, self.n_halo, self.npz, 0)
 
 
-def empty(gi: GridIndexing, kind="3d", device="cuda", dtype=torch.float64):
+def empty(gi: GridIndexing, kind="3d", device="cuda", dtype=None):
     m, _, nk = gi.max_shape
+    dtype = gi.dtype if dtype is None else dtype
     if kind == "3d":
         t = torch.empty((6, nk, m, m), device=device, dtype=dtype)
     elif kind == "2d":
@@ -69,7 +77,7 @@ def empty(gi: GridIndexing, kind="3d", device="cuda", dtype=torch.float64):
     return t
 
 
-def zeros(gi, kind="3d", device="cuda", dtype=torch.float64):
+def zeros(gi, kind="3d", device="cuda", dtype=None):
     return empty(gi, kind, device, dtype).zero_()
 
 
@@ -108,8 +116,8 @@ def check_field(t, gi, kind, name):
         raise TypeError(f"{name}: expected a torch tensor in device layout, got {type(t).__name__}")
     if tuple(t.shape) != want or not t.is_contiguous():
         raise ValueError(f"{name}: expected contiguous device layout {want}, got {tuple(t.shape)}")
-    if t.dtype != torch.float64:
-        raise TypeError(f"{name}: expected float64, got {t.dtype}")
+    if t.dtype != gi.dtype:
+        raise TypeError(f"{name}: expected {gi.dtype}, got {t.dtype}")
     if not t.is_cuda:
         raise ValueError(f"{name}: must be a CUDA tensor")
     return t.data_ptr()

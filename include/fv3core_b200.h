@@ -6,10 +6,10 @@
  * reference runs one cube tile per MPI rank; here all six tiles live in one
  * device allocation and every call advances all of them.
  *
- * Memory layout (device pointers, FP64 unless stated):
- *   3-D field   double[6][npz+1][n+2h+1][n+2h+1]   (i fastest)
- *   2-D field   double[6][n+2h+1][n+2h+1]
- *   1-D field   double[npz+1]
+ * Memory layout (device pointers of fv3b_real, defined below):
+ *   3-D field   fv3b_real[6][npz+1][n+2h+1][n+2h+1]   (i fastest)
+ *   2-D field   fv3b_real[6][n+2h+1][n+2h+1]
+ *   1-D field   fv3b_real[npz+1]
  * Index (i, j) in a field is the reference's storage index: the compute
  * domain of a tile is i, j in [h, h+n) (cell centres) or [h, h+n] (edges).
  *
@@ -22,6 +22,20 @@
 #define FV3CORE_B200_H
 
 #include <stdint.h>
+
+/*
+ * Field element type.  libfv3core_b200.so is the FP64 build (fv3b_real =
+ * double).  libfv3core_b200_f32.so is the mixed-precision build of the same
+ * sources (compile with FV3B_REAL_T=float to use it): fields and metric
+ * terms are FP32 in memory and the bulk arithmetic is FP32, while the
+ * Riemann solvers' column solves, the pe/peln/pk log-pressure integration
+ * and the delp column sums run in FP64.  Scalars, configuration structs and
+ * host arrays are double in both builds.
+ */
+#ifndef FV3B_REAL_T
+#define FV3B_REAL_T double
+#endif
+typedef FV3B_REAL_T fv3b_real;
 
 #ifdef __cplusplus
 extern "C" {
@@ -51,21 +65,21 @@ typedef struct fv3b_grid_dims {
  * edge_*, divg_*).
  */
 typedef struct fv3b_metrics {
-  const double *dx, *dy, *dxa, *dya, *dxc, *dyc;
-  const double *rdx, *rdy, *rdxa, *rdya, *rdxc, *rdyc;
-  const double *area, *rarea, *rarea_c;
-  const double *sin_sg1, *sin_sg2, *sin_sg3, *sin_sg4;
-  const double *cos_sg1, *cos_sg2, *cos_sg3, *cos_sg4;
-  const double *cosa, *cosa_u, *cosa_v, *cosa_s, *sina_u, *sina_v;
-  const double *rsina, *rsin_u, *rsin_v, *rsin2;
-  const double *del6_u, *del6_v, *divg_u, *divg_v;
-  const double *fC, *f0;
-  const double *agrid1, *agrid2, *bgrid1, *bgrid2;
-  const double *edge_w, *edge_e, *edge_s, *edge_n;
+  const fv3b_real *dx, *dy, *dxa, *dya, *dxc, *dyc;
+  const fv3b_real *rdx, *rdy, *rdxa, *rdya, *rdxc, *rdyc;
+  const fv3b_real *area, *rarea, *rarea_c;
+  const fv3b_real *sin_sg1, *sin_sg2, *sin_sg3, *sin_sg4;
+  const fv3b_real *cos_sg1, *cos_sg2, *cos_sg3, *cos_sg4;
+  const fv3b_real *cosa, *cosa_u, *cosa_v, *cosa_s, *sina_u, *sina_v;
+  const fv3b_real *rsina, *rsin_u, *rsin_v, *rsin2;
+  const fv3b_real *del6_u, *del6_v, *divg_u, *divg_v;
+  const fv3b_real *fC, *f0;
+  const fv3b_real *agrid1, *agrid2, *bgrid1, *bgrid2;
+  const fv3b_real *edge_w, *edge_e, *edge_s, *edge_n;
   /* [6][4][3]: x1 / (x2 - x1) of a2b_ord4's cube-corner extrapolations
    * (a2b_ord4.py:38-57), corners (is, js), (ie+1, js), (ie+1, je+1),
    * (is, je+1), three extrapolations each in the reference's order */
-  const double* a2b_extrap;
+  const fv3b_real* a2b_extrap;
   double da_min, da_min_c;
 } fv3b_metrics;
 
@@ -85,9 +99,9 @@ int fv3b_ctx_destroy(fv3b_ctx* ctx);
  * In: u, v.  In/out: delp, pt, w (cube-corner halos are filled, as in the
  * reference), uc, vc, ua, va, ut, vt, divgd, omga.  Out: delpc, ptc.
  */
-int fv3b_c_sw(fv3b_ctx* ctx, double* delp, double* pt, const double* u, const double* v, double* w,
-              double* uc, double* vc, double* ua, double* va, double* ut, double* vt, double* divgd,
-              double* omga, double dt2, int nord, double* delpc, double* ptc, void* stream);
+int fv3b_c_sw(fv3b_ctx* ctx, fv3b_real* delp, fv3b_real* pt, const fv3b_real* u, const fv3b_real* v, fv3b_real* w,
+              fv3b_real* uc, fv3b_real* vc, fv3b_real* ua, fv3b_real* va, fv3b_real* ut, fv3b_real* vt, fv3b_real* divgd,
+              fv3b_real* omga, double dt2, int nord, fv3b_real* delpc, fv3b_real* ptc, void* stream);
 
 /*
  * D-grid shallow-water namelist (DGridShallowWaterLagrangianDynamicsConfig,
@@ -116,10 +130,10 @@ int fv3b_d_sw_setup(fv3b_ctx* ctx, const fv3b_dsw_config* config);
  * the heat source.  Argument meaning as in the reference; all arrays are
  * 3-D device fields.
  */
-int fv3b_d_sw(fv3b_ctx* ctx, double* delpc, double* delp, double* ptc, double* pt, double* u, double* v,
-              double* w, double* uc, double* vc, const double* ua, const double* va, double* divgd,
-              double* mfx, double* mfy, double* cx, double* cy, double* crx, double* cry, double* xfx,
-              double* yfx, double* q_con, const double* zh, double* heat_source, double* diss_est,
+int fv3b_d_sw(fv3b_ctx* ctx, fv3b_real* delpc, fv3b_real* delp, fv3b_real* ptc, fv3b_real* pt, fv3b_real* u, fv3b_real* v,
+              fv3b_real* w, fv3b_real* uc, fv3b_real* vc, const fv3b_real* ua, const fv3b_real* va, fv3b_real* divgd,
+              fv3b_real* mfx, fv3b_real* mfy, fv3b_real* cx, fv3b_real* cy, fv3b_real* crx, fv3b_real* cry, fv3b_real* xfx,
+              fv3b_real* yfx, fv3b_real* q_con, const fv3b_real* zh, fv3b_real* heat_source, fv3b_real* diss_est,
               double dt, void* stream);
 
 /* Description of the last error raised on the calling host thread. */
@@ -140,9 +154,9 @@ long long fv3b_launch_count(void);
  * (heights in, geopotential out).  Out: pef.
  */
 int fv3b_riem_solver_c(const fv3b_grid_dims* dims, double dt2, double ptop, double p_fac,
-                       const double* cappa, const double* hs, const double* ws,
-                       const double* ptc, const double* q_con, const double* delpc,
-                       double* gz, double* pef, const double* w3, void* stream);
+                       const fv3b_real* cappa, const fv3b_real* hs, const fv3b_real* ws,
+                       const fv3b_real* ptc, const fv3b_real* q_con, const fv3b_real* delpc,
+                       fv3b_real* gz, fv3b_real* pef, const fv3b_real* w3, void* stream);
 
 /*
  * RiemannSolver3.__call__ (fv3core/stencils/riem_solver3.py:145-242) with
@@ -153,17 +167,17 @@ int fv3b_riem_solver_c(const fv3b_grid_dims* dims, double dt2, double ptop, doub
  * and peln.
  */
 int fv3b_riem_solver3(const fv3b_grid_dims* dims, int last_call, double dt, double ptop, double p_fac,
-                      const double* cappa, const double* zs, const double* wsd, double* delz,
-                      const double* q_con, const double* delp, const double* pt, double* zh, double* pe,
-                      double* ppe, double* pk3, double* pk, double* peln, double* w, void* stream);
+                      const fv3b_real* cappa, const fv3b_real* zs, const fv3b_real* wsd, fv3b_real* delz,
+                      const fv3b_real* q_con, const fv3b_real* delp, const fv3b_real* pt, fv3b_real* zh, fv3b_real* pe,
+                      fv3b_real* ppe, fv3b_real* pk3, fv3b_real* pk, fv3b_real* peln, fv3b_real* w, void* stream);
 
 /*
  * UpdateGeopotentialHeightOnCGrid.__call__ (fv3core/stencils/updatedzc.py:123-163).
  * dp_ref: device [npz+1] reference layer thickness; zs, ws: 2-D.
  * In: ut, vt.  In/out: gz (interface heights).  Out: ws.
  */
-int fv3b_update_dz_c(fv3b_ctx* ctx, const double* dp_ref, const double* zs, const double* ut, const double* vt,
-                     double* gz, double* ws, double dt, void* stream);
+int fv3b_update_dz_c(fv3b_ctx* ctx, const fv3b_real* dp_ref, const fv3b_real* zs, const fv3b_real* ut, const fv3b_real* vt,
+                     fv3b_real* gz, fv3b_real* ws, double dt, void* stream);
 
 /*
  * UpdateHeightOnDGrid.__init__ (fv3core/stencils/updatedzd.py:189-320):
@@ -177,25 +191,25 @@ int fv3b_update_dz_d_setup(fv3b_ctx* ctx, const double* dp_ref_host, int hord_tm
  * UpdateHeightOnDGrid.__call__ (fv3core/stencils/updatedzd.py:323-393).
  * In: zs (2-D), crx, cry, xfx, yfx.  In/out: zh.  Out: wsd (2-D).
  */
-int fv3b_update_dz_d(fv3b_ctx* ctx, const double* zs, double* zh, const double* crx, const double* cry,
-                     const double* xfx, const double* yfx, double* wsd, double dt, void* stream);
+int fv3b_update_dz_d(fv3b_ctx* ctx, const fv3b_real* zs, fv3b_real* zh, const fv3b_real* crx, const fv3b_real* cry,
+                     const fv3b_real* xfx, const fv3b_real* yfx, fv3b_real* wsd, double dt, void* stream);
 
 /* p_grad_c_stencil (fv3core/stencils/dyn_core.py:101-145), nonhydrostatic. */
-int fv3b_p_grad_c(fv3b_ctx* ctx, double* uc, double* vc, const double* delpc, const double* pkc,
-                  const double* gz, double dt2, void* stream);
+int fv3b_p_grad_c(fv3b_ctx* ctx, fv3b_real* uc, fv3b_real* vc, const fv3b_real* delpc, const fv3b_real* pkc,
+                  const fv3b_real* gz, double dt2, void* stream);
 
 /*
  * NonHydrostaticPressureGradient.__call__ (fv3core/stencils/nh_p_grad.py:147-206).
  * pp, pk3 and gz are replaced by their B-grid values, as in the reference.
  */
-int fv3b_nh_p_grad(fv3b_ctx* ctx, double* u, double* v, double* pp, double* gz, double* pk3, double* delp,
+int fv3b_nh_p_grad(fv3b_ctx* ctx, fv3b_real* u, fv3b_real* v, fv3b_real* pp, fv3b_real* gz, fv3b_real* pk3, fv3b_real* delp,
                    double dt, double ptop, double akap, void* stream);
 
 /* edge_pe (fv3core/stencils/pe_halo.py:6-33). */
-int fv3b_edge_pe(fv3b_ctx* ctx, double* pe, const double* delp, double ptop, void* stream);
+int fv3b_edge_pe(fv3b_ctx* ctx, fv3b_real* pe, const fv3b_real* delp, double ptop, void* stream);
 
 /* PK3Halo.__call__ (fv3core/stencils/pk3_halo.py:36-68). */
-int fv3b_pk3_halo(fv3b_ctx* ctx, double* pk3, const double* delp, double ptop, double akap, void* stream);
+int fv3b_pk3_halo(fv3b_ctx* ctx, fv3b_real* pk3, const fv3b_real* delp, double ptop, double akap, void* stream);
 
 /*
  * RayleighDamping.__call__ (fv3core/stencils/ray_fast.py:169-192); the
@@ -203,16 +217,16 @@ int fv3b_pk3_halo(fv3b_ctx* ctx, double* pk3, const double* delp, double ptop, d
  * dp and pfull are HOST arrays of npz values (the reference's K fields);
  * factors are re-uploaded (synchronously) only when they change.
  */
-int fv3b_ray_fast(fv3b_ctx* ctx, double* u, double* v, double* w, const double* dp, const double* pfull,
+int fv3b_ray_fast(fv3b_ctx* ctx, fv3b_real* u, fv3b_real* v, fv3b_real* w, const double* dp, const double* pfull,
                   double dt, double ptop, double rf_cutoff, double tau, int hydrostatic, void* stream);
 
 /* HyperdiffusionDamping.__call__ (fv3core/stencils/del2cubed.py:152-181). */
-int fv3b_del2cubed(fv3b_ctx* ctx, double* qdel, double cd, int nmax, void* stream);
+int fv3b_del2cubed(fv3b_ctx* ctx, fv3b_real* qdel, double cd, int nmax, void* stream);
 
 /* compute_pkz_tempadjust (fv3core/stencils/temperature_adjust.py:8-44) on
  * levels [0, nk_heat). */
-int fv3b_pkz_tempadjust(fv3b_ctx* ctx, const double* delp, const double* delz, const double* cappa,
-                        const double* heat_source, double* pt, double* pkz, double delt_time_factor, int nk_heat,
+int fv3b_pkz_tempadjust(fv3b_ctx* ctx, const fv3b_real* delp, const fv3b_real* delz, const fv3b_real* cappa,
+                        const fv3b_real* heat_source, fv3b_real* pt, fv3b_real* pkz, double delt_time_factor, int nk_heat,
                         void* stream);
 
 /*
@@ -224,9 +238,9 @@ int fv3b_pkz_tempadjust(fv3b_ctx* ctx, const double* delp, const double* delz, c
  * 1 = C-grid (uc, vc).  nlev: levels to update (npz for Z_DIM fields,
  * npz+1 for Z_INTERFACE_DIM fields).
  */
-int fv3b_halo_update_scalar(fv3b_ctx* ctx, double* field, int stagger, int n_halo, int nlev, void* stream);
-int fv3b_halo_update_vector(fv3b_ctx* ctx, double* x, double* y, int grid, int nlev, void* stream);
-int fv3b_synchronize_vector_interfaces(fv3b_ctx* ctx, double* u, double* v, int nlev, void* stream);
+int fv3b_halo_update_scalar(fv3b_ctx* ctx, fv3b_real* field, int stagger, int n_halo, int nlev, void* stream);
+int fv3b_halo_update_vector(fv3b_ctx* ctx, fv3b_real* x, fv3b_real* y, int grid, int nlev, void* stream);
+int fv3b_synchronize_vector_interfaces(fv3b_ctx* ctx, fv3b_real* u, fv3b_real* v, int nlev, void* stream);
 
 /*
  * AcousticDynamicsConfig (fv3core/_config.py:164-212) without the nested
@@ -245,8 +259,8 @@ typedef struct fv3b_acoustic_config {
  * scalars.
  */
 typedef struct fv3b_dycore_state {
-  double *u, *v, *w, *delz, *delp, *pt, *pe, *pk, *phis, *wsd, *omga, *ua, *va, *uc, *vc;
-  double *mfxd, *mfyd, *cxd, *cyd, *pkz, *peln, *q_con, *diss_estd, *cappa;
+  fv3b_real *u, *v, *w, *delz, *delp, *pt, *pe, *pk, *phis, *wsd, *omga, *ua, *va, *uc, *vc;
+  fv3b_real *mfxd, *mfyd, *cxd, *cyd, *pkz, *peln, *q_con, *diss_estd, *cappa;
   double mdt, akap, ptop;
   int32_t n_map, ks;
 } fv3b_dycore_state;
@@ -262,7 +276,7 @@ typedef struct fv3b_dycore_state {
  * (d_ext != 0, beta != 0, use_logp, hydrostatic).
  */
 int fv3b_acoustics_setup(fv3b_ctx* ctx, const fv3b_acoustic_config* config, const fv3b_dsw_config* dsw,
-                         const double* ak, const double* bk, const double* pfull, const double* phis);
+                         const double* ak, const double* bk, const double* pfull, const fv3b_real* phis);
 
 /*
  * AcousticDynamics.__call__ (fv3core/stencils/dyn_core.py:479-761): the
@@ -275,7 +289,7 @@ int fv3b_acoustics(fv3b_ctx* ctx, const fv3b_dycore_state* state, void* stream);
 /* Device pointer of one of the substep temporaries by its reference name
  * ("gz", "zh", "pkc", "pk3", "ut", "vt", "divgd", "heat_source", "crx",
  * "cry", "xfx", "yfx", "delpc", "ptc", "ws3", "zs", "dp_ref"), or NULL. */
-double* fv3b_acoustics_temporary(fv3b_ctx* ctx, const char* name);
+fv3b_real* fv3b_acoustics_temporary(fv3b_ctx* ctx, const char* name);
 
 /*
  * fv3b_del2cubed_noalloc: no reference counterpart.  The same filter as
@@ -292,7 +306,7 @@ double* fv3b_acoustics_temporary(fv3b_ctx* ctx, const char* name);
  * them).  metrics: as for
  * fv3b_ctx_create (del6_u, del6_v and rarea are read).
  */
-int fv3b_del2cubed_noalloc(const fv3b_grid_dims* dims, const fv3b_metrics* metrics, double* qdel, double cd, int nmax,
+int fv3b_del2cubed_noalloc(const fv3b_grid_dims* dims, const fv3b_metrics* metrics, fv3b_real* qdel, double cd, int nmax,
                            void* stream);
 
 #ifdef __cplusplus

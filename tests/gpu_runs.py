@@ -53,7 +53,7 @@ def run_d_sw(case, n, nz):
     return {k: to_host(dev[k]) for k in DSW_ARGS}
 
 
-def run_acoustics(case, n, nz):
+def run_acoustics(case, n, nz, precision="f64"):
     """The package's AcousticDynamics on a case of ``cases.acoustics_case``;
     returns the state and the driver's temporaries (prefixed ``tmp_``)."""
     import types
@@ -68,17 +68,18 @@ def run_acoustics(case, n, nz):
     from fv3core_b200.stencils.dyn_core import AcousticDynamics
     from fv3core_b200.storage import to_device, to_host
 
-    gd = GridData(cases.grid_for(n), nz)
+    gd = GridData(cases.grid_for(n), nz, precision=precision)
+    dtype = gd.grid_indexing.dtype
     sf = StencilFactory(StencilConfig(), gd.grid_indexing)
     cfg = AcousticDynamicsConfig(
         **{**cases.ACOUSTIC_CONFIG, "n_split": int(case["n_split"])},
         riemann=RiemannConfig(**cases.RIEMANN_CONFIG),
         d_grid_shallow_water=DGridShallowWaterLagrangianDynamicsConfig(**cases.DSW_CONFIG),
     )
-    phis = to_device(case["phis"])
+    phis = to_device(case["phis"], dtype=dtype)
     ad = AcousticDynamics(DeviceCubedSphereCommunicator(gd.grid_indexing), sf, gd, gd, 0, False, False, cfg,
                           case["ak"], case["bk"], case["pfull"], phis)
-    st = types.SimpleNamespace(**{k: to_device(case[k]) for k in cases.ACOUSTIC_STATE})
+    st = types.SimpleNamespace(**{k: to_device(case[k], dtype=dtype) for k in cases.ACOUSTIC_STATE})
     st.phis = phis
     for k in ("mdt", "n_map", "akap", "ptop", "ks"):
         setattr(st, k, case[k])
