@@ -106,6 +106,10 @@ def lib(precision="f64"):
         L.fv3b_version.restype = ctypes.c_char_p
         L.fv3b_launch_count.restype = ctypes.c_longlong
         L.fv3b_launch_count.argtypes = []
+        L.fv3b_set_launch_shape.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.fv3b_set_launch_shape.restype = ctypes.c_int
+        L.fv3b_get_launch_shape.argtypes = [ctypes.POINTER(ctypes.c_int)] * 3
+        L.fv3b_get_launch_shape.restype = None
         for name, args in SIGNATURES.items():
             if args is None:
                 continue
@@ -150,7 +154,8 @@ def call_ctx(name, ctx, *args):
 
 
 def exported_symbols():
-    return ["fv3b_last_error", "fv3b_version", "fv3b_launch_count", "fv3b_ctx_create", "fv3b_ctx_destroy"] + [
+    return ["fv3b_last_error", "fv3b_version", "fv3b_launch_count", "fv3b_set_launch_shape", "fv3b_get_launch_shape",
+            "fv3b_ctx_create", "fv3b_ctx_destroy"] + [
         k for k, v in SIGNATURES.items() if v is not None
     ] + list(CTX_SIGNATURES) + list(PTR_SIGNATURES)
 
@@ -158,3 +163,15 @@ def exported_symbols():
 def launch_count(precision="f64"):
     """Kernel launches issued by the library so far."""
     return int(lib(precision).fv3b_launch_count())
+
+
+def set_launch_shape(box_x, box_y, col, precision="f64"):
+    rc = lib(precision).fv3b_set_launch_shape(int(box_x), int(box_y), int(col))
+    if rc != 0:
+        raise ValueError(lib(precision).fv3b_last_error().decode())
+
+
+def get_launch_shape(precision="f64"):
+    v = [ctypes.c_int(), ctypes.c_int(), ctypes.c_int()]
+    lib(precision).fv3b_get_launch_shape(*[ctypes.byref(x) for x in v])
+    return tuple(x.value for x in v)

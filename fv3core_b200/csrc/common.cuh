@@ -38,12 +38,21 @@ __global__ void box_kernel(Box b, F f) {
 // through fv3b_launch_count().
 void note_launch();
 
+// Thread-block shapes of the box and column kernels: process-wide settings
+// (fv3b_set_launch_shape), chosen by the autotuner; the shape changes no
+// result, since every thread computes its own points.
+struct LaunchShape {
+  int box_x = 32, box_y = 4, col = 128;
+};
+const LaunchShape& launch_shape();
+
 template <typename F>
 cudaError_t launch_box(const Box& b, cudaStream_t s, F f) {
   int ni = b.i1 - b.i0, nj = b.j1 - b.j0, nk = b.k1 - b.k0;
   if (ni <= 0 || nj <= 0 || nk <= 0) return cudaSuccess;
-  dim3 block(32, 4, 1);
-  dim3 grid((ni + 31) / 32, (nj + 3) / 4, 6 * nk);
+  const LaunchShape& ls = launch_shape();
+  dim3 block(ls.box_x, ls.box_y, 1);
+  dim3 grid((ni + ls.box_x - 1) / ls.box_x, (nj + ls.box_y - 1) / ls.box_y, 6 * nk);
   box_kernel<<<grid, block, 0, s>>>(b, f);
   note_launch();
   return cudaGetLastError();
@@ -63,7 +72,8 @@ __global__ void column_kernel(int i0, int i1, int j0, int j1, F f) {
 }
 
 template <typename F>
-cudaError_t launch_columns(int i0, int i1, int j0, int j1, cudaStream_t s, F f, int block = 128) {
+cudaError_t launch_columns(int i0, int i1, int j0, int j1, cudaStream_t s, F f, int block = 0) {
+  if (block <= 0) block = launch_shape().col;
   int ncol = (i1 - i0) * (j1 - j0);
   if (ncol <= 0) return cudaSuccess;
   dim3 grid((ncol + block - 1) / block, 6, 1);

@@ -10,7 +10,7 @@ constexpr int MAXLEV = 128;
 // indices of the per-level columns in ctx->col
 enum ColumnId {
   COL_NORD = 0, COL_NORD_V, COL_NORD_W, COL_NORD_T, COL_DAMP_VT, COL_DAMP_W, COL_DAMP_T, COL_D2_DIVG,
-  COL_D_CON, COL_KE_BG, COL_DAMP4_VT_C, COL_DAMP4_W_C, COL_DAMP4_VT, COL_DAMP4_T, COL_SPARE0, COL_SPARE1,
+  COL_D_CON, COL_KE_BG, COL_DAMP4_VT_C, COL_DAMP4_W_C, COL_DAMP4_VT, COL_DAMP4_T, COL_DAMP_VT_DZ, COL_SPARE1,
   // acoustic driver columns (AcousticDynamics.__init__): reference layer
   // thickness, cubic-spline constants of UpdateHeightOnDGrid, Rayleigh
   // damping factors
@@ -30,6 +30,9 @@ struct DswSetup {
   int nonzero_nord_k = 0, nonzero_nord = 0;
   int nmax_v = 0, nmax_w = 0, nmax_t = 0;
   double dd8 = 0.0;
+  // power-of-two range scales of the del-n passes (1 in double builds) and
+  // dd8 divided by area_scale_c^nonzero_nord
+  double area_scale = 1.0, area_scale_c = 1.0, dd8_scaled = 0.0;
 };
 
 // RayleighDamping per-level factors, recomputed when their inputs change

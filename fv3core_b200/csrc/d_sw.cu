@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "a2b.cuh"
@@ -404,6 +405,32 @@ extern "C" int fv3b_d_sw_setup(fv3b_ctx* ctx, const fv3b_dsw_config* cfg) {
     }
   }
   sp.dd8 = pow(ctx->m.da_min_c * cfg->d4_bg, sp.nonzero_nord + 1);
+  // Range scaling of the del-n iterations.  Each pass of a del-n operator
+  // divides by a cell area (1e8..1e12 m^2) and the damping coefficient
+  // carries one area per pass, so at nord = 3 the coefficients
+  // (damp * da_min)^4 reach 1e40 and the iterated differences 1e-40: outside
+  // the single-precision range.  With fields in single precision every pass
+  // multiplies by S, a power of two near the smallest area, and the
+  // coefficient of a level that takes nmax passes is divided by S^nmax.  S is
+  // a power of two, so both scalings are exact and the fluxes are the same
+  // numbers the unscaled formula gives; double builds use S = 1.
+  const bool scale_range = sizeof(fv3b::real) < sizeof(double);
+  sp.area_scale = scale_range ? std::ldexp(1.0, std::ilogb(ctx->m.da_min)) : 1.0;
+  sp.area_scale_c = scale_range ? std::ldexp(1.0, std::ilogb(ctx->m.da_min_c)) : 1.0;
+  auto scale_levels = [&](int damp_id, int nord_id, int nmax, double scale) {
+    if (nmax == 0) return;
+    const double f = std::pow(scale, -nmax);
+    for (int k = 0; k < MAXLEV; ++k)
+      if (C(nord_id)[k < 3 ? k : 3] > 0) C(damp_id)[k] *= f;
+  };
+  // UpdateHeightOnDGrid damps with the raw damp_vt column over npz + 1 levels
+  for (int k = 0; k < MAXLEV; ++k) C(COL_DAMP_VT_DZ)[k] = C(COL_DAMP_VT)[k];
+  scale_levels(COL_DAMP_VT_DZ, COL_NORD_V, sp.nmax_v, sp.area_scale);
+  scale_levels(COL_DAMP4_VT, COL_NORD_V, sp.nmax_v, sp.area_scale);
+  scale_levels(COL_DAMP4_T, COL_NORD_T, sp.nmax_t, sp.area_scale);
+  scale_levels(COL_DAMP4_W_C, COL_NORD_W, sp.nmax_w, sp.area_scale);
+  scale_levels(COL_DAMP4_VT_C, COL_NORD_V, sp.nmax_v, sp.area_scale);
+  sp.dd8_scaled = sp.dd8 * std::pow(sp.area_scale_c, -sp.nonzero_nord);
   // the D-grid columns only; the driver's columns (from COL_DP_REF on) are its own
   const std::vector<real> cols_r(cols.begin(), cols.begin() + (size_t)COL_DP_REF * MAXLEV);
   FV3B_CHECK(cudaMemcpy(ctx->col, cols_r.data(), sizeof(real) * cols_r.size(), cudaMemcpyHostToDevice));
@@ -441,10 +468,11 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, real* delpc, real* delp, real* ptc, real
   const real* col_ke_bg = colp(ctx, COL_KE_BG);
   const real* col_damp_w = colp(ctx, COL_DAMP_W);
   const real* col_damp_vt = colp(ctx, COL_DAMP_VT);
-  DelnCol dl_v{colp(ctx, COL_NORD_V), colp(ctx, COL_DAMP4_VT)};
-  DelnCol dl_t{colp(ctx, COL_NORD_T), colp(ctx, COL_DAMP4_T)};
-  DelnCol nosg_w{colp(ctx, COL_NORD_W), colp(ctx, COL_DAMP4_W_C)};
-  DelnCol nosg_v{colp(ctx, COL_NORD_V), colp(ctx, COL_DAMP4_VT_C)};
+  const real area_scale = static_cast<real>(sp.area_scale);
+  DelnCol dl_v{colp(ctx, COL_NORD_V), colp(ctx, COL_DAMP4_VT), area_scale};
+  DelnCol dl_t{colp(ctx, COL_NORD_T), colp(ctx, COL_DAMP4_T), area_scale};
+  DelnCol nosg_w{colp(ctx, COL_NORD_W), colp(ctx, COL_DAMP4_W_C), area_scale};
+  DelnCol nosg_v{colp(ctx, COL_NORD_V), colp(ctx, COL_DAMP4_VT_C), area_scale};
 
   FV3B_CHECK(fxadv(d, g, uc, vc, crx, cry, xfx, yfx, ucc, vcc, dt, st));
 
@@ -597,7 +625,8 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, real* delpc, real* delp, real* ptc, real
   {
     const int kz = sp.nonzero_nord_k;
     const int nn = sp.nonzero_nord;
-    const real dddmp = cfg.dddmp, da_min_c = g.da_min_c, dd8 = sp.dd8;
+    const real dddmp = cfg.dddmp, da_min_c = g.da_min_c, dd8 = sp.dd8_scaled;
+    const real rscale_c = static_cast<real>(sp.area_scale_c);
     real* u_contra_dyc = ptc;
     real* v_contra_dxc = tmp_vort;
     if (kz > 0) {
@@ -665,7 +694,7 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, real* delpc, real* delp, real* ptc, real
                               bool ci = (i == s || i == e + 1);
                               if (ci && j == js) dd = F3(vc, i - 1, j) - F3(vc, i, j) - F3(uc, i, j);
                               if (ci && j == je + 1) dd = F3(uc, i, j - 1) + F3(vc, i - 1, j) - F3(vc, i, j);
-                              W3(divgd, i, j) = dd * F2(g.rarea_c, i, j);
+                              W3(divgd, i, j) = dd * F2(g.rarea_c, i, j) * rscale_c;
                             }));
     }
     // _vorticity_calc: a2b_ord4(wk -> vort) then smagorinsky, on k >= kz

@@ -250,7 +250,7 @@ cudaError_t launch_riemann(const Dims& d, int i0, int i1, int j0, int j1, cudaSt
 #define FV3B_RIEM_BUCKET(NK)                                                                             \
   if (K <= NK)                                                                                           \
     return launch_columns(i0, i1, j0, j1, s,                                                            \
-                          [=] __device__(int t, int i, int j) { Body<NK>::run(dd, t, i, j, args); }, 128);
+                          [=] __device__(int t, int i, int j) { Body<NK>::run(dd, t, i, j, args); });
   FV3B_RIEM_BUCKET(16)
   FV3B_RIEM_BUCKET(32)
   FV3B_RIEM_BUCKET(64)

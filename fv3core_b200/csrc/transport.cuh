@@ -195,7 +195,8 @@ inline cudaError_t copy_corners_x_inplace(const Dims d, real* q, cudaStream_t st
 // Per-level damping column on the device: nord band value and damp.
 struct DelnCol {
   const real* nord;  // [nk] per-level nord (band value, see nord_at)
-  const real* damp;  // [nk]
+  const real* damp;  // [nk], divided by rscale^nmax on levels that iterate
+  real rscale;       // factor of every del-n pass (power of two; 1 in double builds)
 };
 
 // nord of level k: the reference folds the column into bands k = 0, 1, 2, 3+
@@ -270,7 +271,7 @@ inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const real*
                        PT_SETUP(d, t, k);
                        if (nord_at(col.nord, k) == 0) return;
                        W3(d2, i, j) = (F3(fx2, i, j) - F3(fx2, i + 1, j) + F3(fy2, i, j) - F3(fy2, i, j + 1)) *
-                                      F2(g.rarea, i, j);
+                                      F2(g.rarea, i, j) * col.rscale;
                      });
     if (err != cudaSuccess) return err;
     err = flux_pass(nt, false);

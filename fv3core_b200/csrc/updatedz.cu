@@ -175,8 +175,9 @@ extern "C" int fv3b_update_dz_d(fv3b_ctx* ctx, const real* zs, real* zh, const r
   FvTp2dArgs a{zh, crx_i, cry_i, xfx_i, yfx_i, xfx_i, yfx_i, fx, fy, ctx->dzd_hord_tm,
                fx_mean, fy_mean, q_adv_x, q_adv_y};
   FV3B_CHECK(fvtp2d(d, g, a, st));
-  // DelnFluxNoSG on npz + 1 levels with the raw damp_vt column
-  DelnCol dl{colp(ctx, COL_NORD_V), colp(ctx, COL_DAMP_VT)};
+  // DelnFluxNoSG on npz + 1 levels with the raw damp_vt column (range-scaled
+  // copy, identical to damp_vt in double builds)
+  DelnCol dl{colp(ctx, COL_NORD_V), colp(ctx, COL_DAMP_VT_DZ), static_cast<real>(ctx->dsw.area_scale)};
   FV3B_CHECK(delnflux_nosg(d, g, zh, gzx_diff, gzy_diff, dl, d2, false, ctx->dsw.nmax_v, st, nk));
   // apply_height_fluxes (updatedzd.py:63-118) fused with the surface w and
   // DZ_MIN floor, bottom up per column of the compute domain

@@ -94,3 +94,16 @@ class AcousticDynamics:
         s.n_map = int(state.n_map)
         s.ks = int(getattr(state, "ks", 0))
         _lib.call_ctx("fv3b_acoustics", self._ctx, ctypes.addressof(s), stream_ptr())
+
+    def capture(self, state):
+        """Record one call on ``state`` in a CUDA graph and return it;
+        ``graph.replay()`` then advances the same tensors.  Make one eager
+        call first: it uploads the per-level Rayleigh factors, which a
+        capture cannot do."""
+        import torch
+
+        graph = torch.cuda.CUDAGraph()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(graph):
+            self(state)
+        return graph

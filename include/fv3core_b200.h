@@ -146,6 +146,13 @@ const char* fv3b_version(void);
  * (diagnostic; all host threads). */
 long long fv3b_launch_count(void);
 
+/* Thread-block shapes of the stencil kernels: box kernels get box_x * box_y
+ * threads (box_x a multiple of 32, at most 1024 threads), column kernels col
+ * threads (a multiple of 32).  Process-wide; results do not depend on it.
+ * fv3core_b200.autotune picks it by timing. */
+int fv3b_set_launch_shape(int box_x, int box_y, int col);
+void fv3b_get_launch_shape(int* box_x, int* box_y, int* col);
+
 /*
  * RiemannSolverC.__call__  (fv3core/stencils/riem_solver_c.py:106-165,
  * with Sim1Solver, fv3core/stencils/sim1_solver.py:11-175).

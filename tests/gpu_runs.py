@@ -53,12 +53,10 @@ def run_d_sw(case, n, nz):
     return {k: to_host(dev[k]) for k in DSW_ARGS}
 
 
-def run_acoustics(case, n, nz, precision="f64"):
-    """The package's AcousticDynamics on a case of ``cases.acoustics_case``;
-    returns the state and the driver's temporaries (prefixed ``tmp_``)."""
+def make_acoustics(case, n, nz, precision="f64"):
+    """(grid data, AcousticDynamics, device state) for a case of
+    ``cases.acoustics_case``."""
     import types
-
-    import torch
 
     from fv3core_b200.config import (AcousticDynamicsConfig, DGridShallowWaterLagrangianDynamicsConfig,
                                      RiemannConfig)
@@ -66,7 +64,7 @@ def run_acoustics(case, n, nz, precision="f64"):
     from fv3core_b200.halo import DeviceCubedSphereCommunicator
     from fv3core_b200.stencil import StencilConfig, StencilFactory
     from fv3core_b200.stencils.dyn_core import AcousticDynamics
-    from fv3core_b200.storage import to_device, to_host
+    from fv3core_b200.storage import to_device
 
     gd = GridData(cases.grid_for(n), nz, precision=precision)
     dtype = gd.grid_indexing.dtype
@@ -83,6 +81,17 @@ def run_acoustics(case, n, nz, precision="f64"):
     st.phis = phis
     for k in ("mdt", "n_map", "akap", "ptop", "ks"):
         setattr(st, k, case[k])
+    return gd, ad, st
+
+
+def run_acoustics(case, n, nz, precision="f64"):
+    """The package's AcousticDynamics on a case of ``cases.acoustics_case``;
+    returns the state and the driver's temporaries (prefixed ``tmp_``)."""
+    import torch
+
+    from fv3core_b200.storage import to_host
+
+    gd, ad, st = make_acoustics(case, n, nz, precision)
     ad(st)
     torch.cuda.synchronize()
     out = {k: to_host(getattr(st, k)) for k in cases.ACOUSTIC_STATE}

@@ -49,6 +49,21 @@ def test_version_and_error_reporting_without_gpu():
     assert rc == 1 and b"null argument" in L.fv3b_last_error()
 
 
+def test_launch_shape_setting_without_gpu():
+    from fv3core_b200 import _lib
+
+    for precision in ("f64", "f32"):
+        default = _lib.get_launch_shape(precision)
+        assert default == (32, 4, 128)
+        _lib.set_launch_shape(64, 2, 256, precision=precision)
+        assert _lib.get_launch_shape(precision) == (64, 2, 256)
+        for bad in [(48, 4, 128), (32, 64, 128), (32, 4, 100), (32, 0, 128)]:
+            with pytest.raises(ValueError):
+                _lib.set_launch_shape(*bad, precision=precision)
+        assert _lib.get_launch_shape(precision) == (64, 2, 256)
+        _lib.set_launch_shape(*default, precision=precision)
+
+
 @pytest.fixture(scope="module")
 def c_layout(tmp_path_factory):
     if shutil.which("gcc") is None:
