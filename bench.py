@@ -211,36 +211,69 @@ def run_cuda(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    # Every step starts from the initial state.  Repeated acoustic calls
+    # without the vertical remapping that follows each one in a full
+    # dynamics step let the Lagrangian layers deform, and at C384 the state
+    # leaves the physical range after a few calls; restarting keeps every
+    # timed call on the same, valid input.  The device-to-device reset runs
+    # before each call, outside that call's timing events.
+    initial = {p: {k: getattr(problems[p][2], k).clone() for k in _lib.DYCORE_FIELDS} for p in precisions}
+
+    def reset(prec):
+        state = problems[prec][2]
+        for k, t in initial[prec].items():
+            getattr(state, k).copy_(t)
+
     # error of the mixed build against FP64 after one call (one dynamics
     # step's acoustic part) from the same initial state
+    # from the same state; and, to separate the build's own arithmetic
+    # error from the state's sensitivity to its inputs, FP64 started from
+    # the initial state rounded to FP32 (the mixed build's input)
     mixed_error = None
     if len(precisions) == 2:
-        problems["f32"][1](problems["f32"][2])
-        problems["f64"][1](problems["f64"][2])
+        fields = ("delp", "pt", "delz", "q_con")
+        s32, s64 = problems["f32"][2], problems["f64"][2]
+        problems["f32"][1](s32)
+        problems["f64"][1](s64)
         barrier()
-        mixed_error = {k: _max_rel(getattr(problems["f32"][2], k), getattr(problems["f64"][2], k), n, npz)
-                       for k in ("delp", "pt", "delz", "q_con")}
-        mixed_error["after"] = "one AcousticDynamics call (n_split acoustic substeps) from the same state"
+        ref = {k: getattr(s64, k).clone() for k in fields}
+        mixed = {k: _max_rel(getattr(s32, k), ref[k], n, npz) for k in fields}
+        for k, t in initial["f64"].items():
+            getattr(s64, k).copy_(t.float())
+        problems["f64"][1](s64)
+        barrier()
+        floor = {k: _max_rel(getattr(s64, k), ref[k], n, npz) for k in fields}
+        arith = {k: _max_rel(getattr(s32, k), getattr(s64, k), n, npz) for k in fields}
+        del ref
+        mixed_error = {
+            "mixed_vs_fp64": mixed, "fp64_from_fp32_rounded_input_vs_fp64": floor,
+            "mixed_vs_fp64_from_same_input": arith,
+            "after": "one AcousticDynamics call (n_split acoustic substeps) from the same state; max relative "
+                     "error over the compute domain",
+        }
 
     results = {}
     for prec in precisions:
         gd, ad, state = problems[prec]
         for _ in range(args.warmup):
+            reset(prec)
             ad(state)
         barrier()
         launches0 = _lib.launch_count(prec)
-        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(args.steps)]
         with ClockSampler(local) as clk:
             barrier()
             torch.cuda.nvtx.range_push("timed" if prec == precisions[0] else "timed_" + prec)
-            start.record(stream)
-            for _ in range(args.steps):
+            for start, stop in events:
+                reset(prec)
+                start.record(stream)
                 ad(state)
-            stop.record(stream)
+                stop.record(stream)
             torch.cuda.nvtx.range_pop()
             barrier()
         launches = _lib.launch_count(prec) - launches0
-        ms = start.elapsed_time(stop) / args.steps
+        ms = sum(a.elapsed_time(b) for a, b in events) / args.steps
         finite = all(bool(torch.isfinite(_compute(getattr(state, k), n, npz)).all().item())
                      for k in ("u", "v", "w", "delp", "pt", "delz"))
         results[prec] = {"ms": ms, "launches": launches, "clocks": clk.summary(), "finite": finite}
@@ -252,7 +285,7 @@ def run_cuda(args):
     host = {k: torch.empty(getattr(state, k).shape, dtype=getattr(state, k).dtype, pin_memory=True)
             for k in set(E2E_IN) | set(E2E_OUT)}
     for k, hb in host.items():
-        hb.copy_(getattr(state, k))
+        hb.copy_(initial[head][k] if k in initial[head] else getattr(state, k))
     torch.cuda.synchronize()
     h2d = sum(host[k].numel() * host[k].element_size() for k in E2E_IN)
     d2h = sum(host[k].numel() * host[k].element_size() for k in E2E_OUT)
@@ -410,6 +443,100 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _parse_members(spec):
+    """'16x48x79,8x96x79' -> [(48, 79), ... repeated]."""
+    out = []
+    for part in spec.split(","):
+        count, n, npz = (int(x) for x in part.lower().split("x"))
+        out += [(n, npz)] * count
+    return out
+
+
+def run_ensemble(args):
+    """Ensemble of seed-perturbed members at mixed resolutions, one
+    AcousticDynamics call per member per step: eager launches against one
+    CUDA graph of the whole ensemble step, optionally after the launch-shape
+    autotuner.  Each step first returns every member to its initial state
+    (a device-to-device copy, inside both timings)."""
+    import torch
+
+    from fv3core_b200 import _lib, autotune
+    from fv3core_b200.ensemble import Ensemble
+
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    prec = "f64" if args.precision == "f64" else "f32"
+    spec = _parse_members(args.members)
+    ens = Ensemble([(n, npz, 1000 * rank + q) for q, (n, npz) in enumerate(spec)], precision=prec,
+                   n_split=args.n_split)
+    ens.step()  # the first call uploads per-level factors
+    ens.keep_initial()
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    shape = _lib.get_launch_shape(prec)
+    tuned = None
+    if args.autotune:
+        shape, timings = autotune.tune(lambda: ens.step(reset=True), precision=prec, repeats=1)
+        tuned = {"x".join(map(str, k)): round(v, 3) for k, v in timings.items()}
+
+    def timed(run):
+        for _ in range(args.warmup):
+            run()
+        barrier()
+        l0 = _lib.launch_count(prec)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            barrier()
+            a.record(stream)
+            for _ in range(args.steps):
+                run()
+            b.record(stream)
+            barrier()
+        return a.elapsed_time(b) / args.steps, _lib.launch_count(prec) - l0, clk.summary()
+
+    eager_ms, eager_launches, _ = timed(lambda: ens.step(reset=True))
+    graph = ens.capture(reset=True)
+    graph_ms, _, clocks = timed(graph.replay)
+    graph_launches = eager_launches  # the graph replays the same kernels
+    if dist is not None:
+        t = torch.tensor([eager_ms, graph_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        eager_ms, graph_ms = float(t[0]), float(t[1])
+    cells = ens.cell_levels * args.n_split * world
+    line = {
+        "metric": "ensemble acoustic-substep cell-levels/s", "value": cells / (graph_ms * 1e-3),
+        "unit": "cell-levels/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": graph_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "mixed: f32 fields and arithmetic, f64 column solves" if prec == "f32" else "f64",
+        "data": "synthetic (seeded baroclinic-wave states, one seed per member)",
+        "config": {"workload": f"ensemble {args.members} (count x n x npz), n_split={args.n_split}, one CUDA "
+                               "graph per ensemble step; each step resets the members to their initial state",
+                   "members": len(spec), "cell_levels": ens.cell_levels, "launch_shape": list(shape),
+                   "autotune_ms": tuned, "l2": "inputs larger than L2 in total; no flush"},
+        "clocks": clocks, "gpu_launches": graph_launches,
+        "eager": {"value": cells / (eager_ms * 1e-3), "ms_per_step": eager_ms},
+        "graph_speedup_vs_eager": eager_ms / graph_ms,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del graph
+    ens.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -427,11 +554,17 @@ def main():
     ap.add_argument("--ref-n", type=int, default=24, help="resolution of the reference arm's per-worker sample")
     ap.add_argument("--ref-max-workers", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["acoustics", "ensemble"], default="acoustics",
+                    help="ensemble: the mixed-resolution ensemble with CUDA-graph steps")
+    ap.add_argument("--members", default="16x48x79,8x96x79,4x192x63")
+    ap.add_argument("--autotune", action="store_true", help="ensemble: pick the launch shape by timing first")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be at least 3")
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "ensemble":
+        run_ensemble(args)
     else:
         run_cuda(args)
 

@@ -56,7 +56,7 @@ __device__ __forceinline__ real volume_mean(const L& q, const Gs& g, int pos, in
 template <int AXIS>
 struct A2BLine {
   const real* p;
-  long long base, step;
+  idx_t base, step;
   __device__ __forceinline__ real operator()(int o) const { return p[base + o * step]; }
 };
 
@@ -126,8 +126,8 @@ inline cudaError_t a2b_ord4(const Dims d, const fv3b_metrics g, real* qin, real*
   // ppm_volume_mean_x on [is, ie+1] x [js-2, je+2], _y on [is-2, ie+2] x [js, je+1]
   err = launch_box(Box{s - 2, e + 3, js - 2, je + 3, k0, k1}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
-    long long b = idx3(d, t, i, j, k);
-    long long b2 = idx2(d, t, i, j);
+    idx_t b = idx3(d, t, i, j, k);
+    idx_t b2 = idx2(d, t, i, j);
     if (i >= s && i < e + 2) {
       A2BLine<0> q{qin, b, 1};
       A2BLine<0> gx{g.dxa, b2, 1};
@@ -135,7 +135,7 @@ inline cudaError_t a2b_ord4(const Dims d, const fv3b_metrics g, real* qin, real*
     }
     if (j >= js && j < je + 2) {
       A2BLine<1> q{qin, b, d.sj};
-      A2BLine<1> gy{g.dya, b2, (long long)d.ni};
+      A2BLine<1> gy{g.dya, b2, (idx_t)d.ni};
       W3(qy, i, j) = volume_mean(q, gy, j, js, je);
     }
   });

@@ -9,6 +9,7 @@ extern "C" int fv3b_ctx_create(const fv3b_grid_dims* dims, const fv3b_metrics* m
   FV3B_REQUIRE(dims && metrics && out, "fv3b_ctx_create: null argument");
   FV3B_REQUIRE(dims->npx >= 4 && dims->n_halo == 3 && dims->npz >= 2 && dims->npz < 127,
                "fv3b_ctx_create: need npx >= 4, n_halo == 3, 2 <= npz < 127");
+  FV3B_REQUIRE(dims_fit(dims), "fv3b_ctx_create: a 3-D field of the six tiles must hold fewer than 2^31 elements");
   fv3b_ctx* c = new (std::nothrow) fv3b_ctx();
   FV3B_REQUIRE(c != nullptr, "fv3b_ctx_create: out of host memory");
   c->d = make_dims(dims);

@@ -4,6 +4,9 @@
 
 namespace fv3b {
 constexpr int NWS = 40;   // 3-D scratch fields in the workspace
+// the last workspace field is the second scratch of the del-n ping-pong
+// (delnflux_nosg); no stage uses it for anything else
+constexpr int WS_DELN_ALT = NWS - 1;
 constexpr int NCOL = 32;  // per-level column arrays
 constexpr int MAXLEV = 128;
 

@@ -223,8 +223,8 @@ cudaError_t fill_dgrid(const Dims d, real* x, real* y, real mysign, int k0, int 
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
   return launch_box(Box{0, 1, 0, 1, k0, k1}, st, [=] __device__(int t, int, int, int k) {
     PT_SETUP(d, t, k);
-    auto X = [&](int i, int j) -> real& { return x[_b3 + (long long)j * _sj + i]; };
-    auto Y = [&](int i, int j) -> real& { return y[_b3 + (long long)j * _sj + i]; };
+    auto X = [&](int i, int j) -> real& { return x[_b3 + j * _sj + i]; };
+    auto Y = [&](int i, int j) -> real& { return y[_b3 + j * _sj + i]; };
     const real m = mysign;
     // sw corner
     X(s - 1, js - 1) = m * Y(s - 1, js);
@@ -461,6 +461,7 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, real* delpc, real* delp, real* ptc, real
   real *fx_mean = W[16], *fy_mean = W[17], *q_adv_x = W[18], *q_adv_y = W[19];
   real *dl_fx2 = W[20], *dl_fy2 = W[21], *dl_d2 = W[22];
   real *a2b_qx = W[23], *a2b_qy = W[24], *a2b_edges = W[25];
+  real* deln_alt = W[WS_DELN_ALT];
   real *ucc = W[WS_UC_CONTRA], *vcc = W[WS_VC_CONTRA];
   const real* col_nord = colp(ctx, COL_NORD);
   const real* col_d2_divg = colp(ctx, COL_D2_DIVG);
@@ -484,7 +485,7 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, real* delpc, real* delp, real* ptc, real
                  fx_mean, fy_mean, q_adv_x, q_adv_y};
     err = fvtp2d(d, g, a, st);
     if (err != cudaSuccess) return err;
-    if (dl) err = delnflux(d, g, q, fx, fy, *dl, mass, dl_fx2, dl_fy2, dl_d2, nmax, st);
+    if (dl) err = delnflux(d, g, q, fx, fy, *dl, mass, dl_fx2, dl_fy2, dl_d2, deln_alt, nmax, st);
     return err;
   };
   // delp transport (d_sw.py:910-918) and flux_capacitor (90-117)
@@ -497,7 +498,7 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, real* delpc, real* delp, real* ptc, real
     W3(mfy, i, j) = F3(mfy, i, j) + F3(tmp_fy, i, j);
   }));
   if (!cfg.hydrostatic) {
-    FV3B_CHECK(delnflux_nosg(d, g, w, tmp_fx2, tmp_fy2, nosg_w, tmp_wk, false, sp.nmax_w, st));
+    FV3B_CHECK(delnflux_nosg(d, g, w, tmp_fx2, tmp_fy2, nosg_w, tmp_wk, deln_alt, false, sp.nmax_w, st));
     // heat_diss (d_sw.py:347-365)
     const real adt = fabs(dt);
     FV3B_CHECK(launch_box(Box{s, e + 1, js, je + 1, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
@@ -560,9 +561,8 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, real* delpc, real* delp, real* ptc, real
       // cell-edge spacing dx/dy, corner-zeroed edge perturbations
       auto advect = [&](auto qline, auto dxline, real rdx_m, real rdx_0, real ub, int pos, int sA, int eA,
                         bool zero_m, bool zero_0) {
-        real alm = ppm_al(qline, dxline, -1, pos, sA, eA);
-        real al0 = ppm_al(qline, dxline, 0, pos, sA, eA);
-        real alp = ppm_al(qline, dxline, 1, pos, sA, eA);
+        real alm, al0, alp;
+        ppm_al3(qline, dxline, pos, sA, eA, alm, al0, alp);
         real qm = qline(-1), q0 = qline(0);
         real blm = alm - qm, brm = al0 - qm;
         real bl0 = al0 - q0, br0 = alp - q0;
@@ -744,7 +744,7 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, real* delpc, real* delp, real* ptc, real
     if (i <= e) W3(u, i, j) = F3(u, i, j) * F2(g.dx, i, j) + F3(tmp_ke, i, j) - F3(tmp_ke, i + 1, j) + F3(tmp_fy, i, j);
     if (j <= je) W3(v, i, j) = F3(v, i, j) * F2(g.dy, i, j) + F3(tmp_ke, i, j) - F3(tmp_ke, i, j + 1) - F3(tmp_fx, i, j);
   }));
-  FV3B_CHECK(delnflux_nosg(d, g, tmp_wk, tmp_ut, tmp_vt, nosg_v, tmp_vort, false, sp.nmax_v, st));
+  FV3B_CHECK(delnflux_nosg(d, g, tmp_wk, tmp_ut, tmp_vt, nosg_v, tmp_vort, deln_alt, false, sp.nmax_v, st));
   // heat_source_from_vorticity_damping (d_sw.py:368-438)
   {
     const bool add_total = cfg.d_con > DCON_THRESHOLD || cfg.do_skeb;

@@ -89,19 +89,19 @@ extern "C" int fv3b_ray_fast(fv3b_ctx* ctx, real* u, real* v, real* w, const dou
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
   const bool do_w = hydrostatic == 0;
   FV3B_CHECK(launch_columns(s, e + 2, js, je + 2, st, [=] __device__(int t, int i, int j) {
-    const long long o0 = idx3(d, t, i, j, 0);
+    const idx_t o0 = idx3(d, t, i, j, 0);
     auto damp = [&](real* q) {
-      real total = RC(0.0);
+      double total = 0.0;  // column sum in double in every build
       for (int k = 0; k < k_rf; ++k) {
-        long long o = o0 + k * d.sk;
+        idx_t o = o0 + k * d.sk;
         real c = q[o];
         real lost = (RC(1.0) - rf[k]) * dpc[k] * c;
         total = k == 0 ? lost : total + lost;
         q[o] = c * rf[k];
       }
       for (int k = 0; k < k_nudge; ++k) {
-        long long o = o0 + k * d.sk;
-        q[o] = q[o] + total / dm[k];
+        idx_t o = o0 + k * d.sk;
+        q[o] = q[o] + static_cast<real>(total / dm[k]);
       }
     };
     if (i <= e) damp(u);

@@ -68,6 +68,8 @@ extern "C" int fv3b_del2cubed_noalloc(const fv3b_grid_dims* dims, const fv3b_met
   FV3B_REQUIRE(dims && metrics && qdel, "fv3b_del2cubed_noalloc: null argument");
   FV3B_REQUIRE(dims->npx >= 4 && dims->n_halo == 3 && dims->npz >= 1,
                "fv3b_del2cubed_noalloc: need npx >= 4, n_halo == 3, npz >= 1");
+  FV3B_REQUIRE(dims_fit(dims), "fv3b_del2cubed_noalloc: grid too large for the static scratch "
+                               "(6*(npz+1)*(npx+7)^2 must be <= 1500000 doubles)");
   const Dims d = make_dims(dims);
   FV3B_REQUIRE(d.st * 6 <= FV3B_NOALLOC_FIELD_DOUBLES,
                "fv3b_del2cubed_noalloc: grid too large for the static scratch "

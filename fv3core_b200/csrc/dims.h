@@ -35,13 +35,25 @@ namespace fv3b {
 using real = fv3b_real;
 #define RC(x) (static_cast<::fv3b::real>(x))
 
+// Offsets into a field are 32-bit integers, which keeps the index
+// arithmetic of the stencils to single 32-bit multiply-adds: a 3-D field of
+// all six tiles must hold fewer than 2^31 elements (C1536 L79 holds 1.1e9).
+// dims_fit checks it; every entry point that takes grid sizes calls it.
+using idx_t = int;
+
 struct Dims {
   int n, h, nz;
   int ni, nj, nk;
-  long long sj, sk, st;  // 3-D strides (i stride is 1)
-  long long st2;         // 2-D tile stride (j stride is ni)
+  idx_t sj, sk, st;  // 3-D strides (i stride is 1)
+  idx_t st2;         // 2-D tile stride (j stride is ni)
   int isc, iec, jsc, jec;  // compute domain (inclusive), storage indices
 };
+
+inline bool dims_fit(const fv3b_grid_dims* g) {
+  if (g->npx < 1 || g->npz < 1 || g->n_halo < 0) return false;
+  const long long ni = (long long)g->npx + 2LL * g->n_halo + 1;
+  return 6LL * ni * ni * (g->npz + 1LL) < (1LL << 31);
+}
 
 inline Dims make_dims(const fv3b_grid_dims* g) {
   Dims d;
@@ -52,9 +64,9 @@ inline Dims make_dims(const fv3b_grid_dims* g) {
   d.nj = d.ni;
   d.nk = d.nz + 1;
   d.sj = d.ni;
-  d.sk = (long long)d.ni * d.nj;
+  d.sk = d.ni * d.nj;
   d.st = d.sk * d.nk;
-  d.st2 = (long long)d.ni * d.nj;
+  d.st2 = d.ni * d.nj;
   d.isc = d.h;
   d.iec = d.h + d.n - 1;
   d.jsc = d.h;
@@ -62,11 +74,11 @@ inline Dims make_dims(const fv3b_grid_dims* g) {
   return d;
 }
 
-__host__ __device__ __forceinline__ long long idx3(const Dims& d, int t, int i, int j, int k) {
+__host__ __device__ __forceinline__ idx_t idx3(const Dims& d, int t, int i, int j, int k) {
   return t * d.st + k * d.sk + j * d.sj + i;
 }
-__host__ __device__ __forceinline__ long long idx2(const Dims& d, int t, int i, int j) {
-  return t * d.st2 + (long long)j * d.ni + i;
+__host__ __device__ __forceinline__ idx_t idx2(const Dims& d, int t, int i, int j) {
+  return t * d.st2 + j * d.ni + i;
 }
 
 }  // namespace fv3b

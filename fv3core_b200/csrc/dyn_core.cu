@@ -191,13 +191,13 @@ extern "C" int fv3b_acoustics(fv3b_ctx* ctx, const fv3b_dycore_state* S, void* s
       // set_gz (dyn_core.py:80-85) on the compute domain
       const real* delz = S->delz;
       FV3B_CHECK(launch_columns(s, e + 1, js, je + 1, st, [=] __device__(int t, int i, int j) {
-        long long o = idx3(d, t, i, j, nz);
-        real g = zs[idx2(d, t, i, j)];
-        gz[o] = g;
+        idx_t o = idx3(d, t, i, j, nz);
+        double g = zs[idx2(d, t, i, j)];  // column sum in double in every build
+        gz[o] = static_cast<real>(g);
         for (int k = nz - 1; k >= 0; --k) {
           o -= d.sk;
           g = g - delz[o];
-          gz[o] = g;
+          gz[o] = static_cast<real>(g);
         }
       }));
       FV3B_CHECK(halo_scalars(d, &gz, 1, 1, d.h, nk, st));

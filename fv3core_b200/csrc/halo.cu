@@ -25,7 +25,7 @@ __global__ void halo_scalar_kernel(Dims d, FieldSet fs, int sx, int sy, int n_ha
   const int sxo[2] = {sx, sx}, syo[2] = {sy, sy};
   HaloSource src;
   if (!halo_source(d, t, i, j, 0, sxo, syo, n_halo, src)) return;
-  const long long dst = idx3(d, t, i, j, 0), from = idx3(d, src.t, src.i, src.j, 0);
+  const idx_t dst = idx3(d, t, i, j, 0), from = idx3(d, src.t, src.i, src.j, 0);
   for (int q = 0; q < fs.n; ++q) {
     real* f = fs.f[q];
     for (int k = 0; k < nlev; ++k) f[dst + k * d.sk] = f[from + k * d.sk];
@@ -48,7 +48,7 @@ __global__ void halo_vector_kernel(Dims d, real* x, real* y, int cgrid, int nlev
   real* dstf = comp == 0 ? x : y;
   const real* srcf = src.comp == 0 ? x : y;
   const real sign = (real)src.sign;
-  const long long dst = idx3(d, t, i, j, 0), from = idx3(d, src.t, src.i, src.j, 0);
+  const idx_t dst = idx3(d, t, i, j, 0), from = idx3(d, src.t, src.i, src.j, 0);
   for (int k = 0; k < nlev; ++k) dstf[dst + k * d.sk] = sign * srcf[from + k * d.sk];
 }
 
@@ -62,7 +62,7 @@ __global__ void interface_sync_kernel(Dims d, real* u, real* v, int nlev) {
   const real* srcf = comp == 0 ? u : v;
   real* dstf = dst.comp == 0 ? u : v;
   const real sign = (real)dst.sign;
-  const long long from = idx3(d, t, si, sj, 0), to = idx3(d, dst.t, dst.i, dst.j, 0);
+  const idx_t from = idx3(d, t, si, sj, 0), to = idx3(d, dst.t, dst.i, dst.j, 0);
   for (int k = 0; k < nlev; ++k) dstf[to + k * d.sk] = sign * srcf[from + k * d.sk];
 }
 }  // namespace

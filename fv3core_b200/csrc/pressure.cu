@@ -100,13 +100,13 @@ extern "C" int fv3b_edge_pe(fv3b_ctx* ctx, real* pe, const real* delp, double pt
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nk = d.nk;
   FV3B_CHECK(launch_columns(s - 1, e + 2, js - 1, je + 2, st, [=] __device__(int t, int i, int j) {
     if (i >= s && i <= e && j >= js && j <= je) return;
-    long long o = idx3(d, t, i, j, 0);
-    real p = ptop;
-    pe[o] = p;
+    idx_t o = idx3(d, t, i, j, 0);
+    double p = ptop;  // column sums of delp in double in every build
+    pe[o] = static_cast<real>(p);
     for (int k = 1; k < nk; ++k) {
       p = p + delp[o];
       o += d.sk;
-      pe[o] = p;
+      pe[o] = static_cast<real>(p);
     }
   }));
   return FV3B_OK;
@@ -122,12 +122,12 @@ extern "C" int fv3b_pk3_halo(fv3b_ctx* ctx, real* pk3, const real* delp, double 
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nk = d.nk;
   FV3B_CHECK(launch_columns(s - 2, e + 3, js - 2, je + 3, st, [=] __device__(int t, int i, int j) {
     if (i >= s && i <= e && j >= js && j <= je) return;
-    long long o = idx3(d, t, i, j, 0);
-    real p = ptop;
+    idx_t o = idx3(d, t, i, j, 0);
+    double p = ptop;  // column sums of delp in double in every build
     for (int k = 1; k < nk; ++k) {
       p = p + delp[o];
       o += d.sk;
-      pk3[o] = fm::fm_pow(p, akap);
+      pk3[o] = static_cast<real>(fm::fm_pow(p, akap));
     }
   }));
   return FV3B_OK;

@@ -3,11 +3,12 @@
 //
 // One thread owns one (tile, i, j) column and walks it top to bottom and
 // back; neighbouring threads own neighbouring i, so every level load/store
-// is a coalesced row access.  Only five per-level work arrays stay in the
-// thread's local memory (pem, pm, pp/pe, gam, w); everything else is
-// re-read from the input fields or computed on the fly, and the outputs are
-// written in the same bottom-up pass that produces them.  The arrays are
-// sized by a compile-time level bucket >= npz+1, so an L79 column keeps 3 KB.
+// is a coalesced row access.  Only four per-level work arrays stay in the
+// thread's local memory (pm, pp/pe, gam, w); the edge pressures are running
+// sums rebuilt where they are used, everything else is re-read from the
+// input fields or computed on the fly, and the outputs are written in the
+// same bottom-up pass that produces them.  The arrays are sized by a
+// compile-time level bucket >= npz+1, so an L79 column keeps 2.5 KB.
 // exp and log are the library's own (fmath.h), whose host build the oracle
 // uses, so results can be compared to the last bit.  The column arithmetic
 // is FP64 in both builds; in the mixed-precision build the fields it reads
@@ -26,16 +27,16 @@ constexpr double KAPPA = RDGAS / 1004.6;
 constexpr int MAXK = 128;
 
 // Per-column inputs of the Sim1 solve (fv3core/stencils/sim1_solver.py:11-101).
-// K = number of interface levels (npz + 1).  DM(k): delta p / g; W1(k): w
+// K = number of interface levels (npz + 1).  DM(k): delta p / g; DP(k):
+// delta p, whose running sums from ptop are the edge pressures pem; W1(k): w
 // at the start; DZ(k): layer depth at the start (negative); GM, PTR, CP3:
-// 1/(1-cappa), pt, cappa per level; pem, pm: edge pressure and layer-mean
-// pressure.  Results: w[0..K-2] (new w), pe[0..K-1] (pressure perturbation,
+// 1/(1-cappa), pt, cappa per level; pm: layer-mean pressure.  Results: w[0..K-2] (new w), pe[0..K-1] (pressure perturbation,
 // delivered through PE_OUT(k, value) in increasing k) and the new layer
 // depths through DZ_OUT(k, value) for k = K-2 .. 0 (bottom up).
-template <int NK, typename DMF, typename W1F, typename DZF, typename GMF, typename PTRF, typename CP3F,
-          typename PEOUT, typename DZOUT>
-__device__ __forceinline__ void sim1_column(int K, DMF DM, W1F W1, DZF DZ, GMF GM, PTRF PTR, CP3F CP3,
-                                            const double* pem, const double* pm, double* pp, double* gam, double* w,
+template <int NK, typename DMF, typename DPF, typename W1F, typename DZF, typename GMF, typename PTRF,
+          typename CP3F, typename PEOUT, typename DZOUT>
+__device__ __forceinline__ void sim1_column(int K, DMF DM, DPF DP, double ptop, W1F W1, DZF DZ, GMF GM, PTRF PTR,
+                                            CP3F CP3, const double* pm, double* pp, double* gam, double* w,
                                             double wsr, double dt, double t1g, double rdt, double p_fac,
                                             PEOUT PE_OUT, DZOUT DZ_OUT) {
   // pe = exp(gm*log(-dm/dz*Rd*ptr)) - pm   (sim1_solver.py:27-29), on the fly
@@ -67,13 +68,19 @@ __device__ __forceinline__ void sim1_column(int K, DMF DM, W1F W1, DZF DZ, GMF G
   }
   // back substitution (sim1_solver.py:60-63)
   for (int k = K - 2; k >= 1; --k) pp[k] = pp[k] - gam[k] * pp[k + 1];
-  auto AA = [&](int k) { return t1g * 0.5 * (GM(k - 1) + GM(k)) / (DZ(k - 1) + DZ(k)) * (pem[k] + pp[k]); };
+  // edge pressures pem[k] = ptop + sum of dp above, rebuilt by the same
+  // running sum as the callers' precompute (no per-level array)
+  double pem_run = ptop + DP(0);  // pem[1]
+  auto AA = [&](int k, double pem_k) {
+    return t1g * 0.5 * (GM(k - 1) + GM(k)) / (DZ(k - 1) + DZ(k)) * (pem_k + pp[k]);
+  };
   // w solve (sim1_solver.py:65-90)
-  double aak = AA(1);
+  double aak = AA(1, pem_run);
   bet = DM(0) - aak;
   w[0] = (DM(0) * W1(0) + dt * pp[1]) / bet;
   for (int k = 1; k <= K - 3; ++k) {
-    double aak1 = AA(k + 1);
+    pem_run = pem_run + DP(k);  // pem[k + 1]
+    double aak1 = AA(k + 1, pem_run);
     double g = aak / bet;
     gam[k] = g;
     bet = DM(k) - (aak + aak1 + aak * g);
@@ -82,7 +89,8 @@ __device__ __forceinline__ void sim1_column(int K, DMF DM, W1F W1, DZF DZ, GMF G
   }
   {
     int k = K - 2;
-    double p1 = t1g * GM(k) / DZ(k) * (pem[k + 1] + pp[k + 1]);
+    pem_run = pem_run + DP(k);  // pem[K - 1]
+    double p1 = t1g * GM(k) / DZ(k) * (pem_run + pp[k + 1]);
     double g = aak / bet;
     gam[k] = g;
     bet = DM(k) - (aak + p1 + aak * g);
@@ -130,39 +138,43 @@ struct RiemC {
     const real *cappa = a.cappa, *hs = a.hs, *ws = a.ws, *ptc = a.ptc, *q_con = a.q_con, *delpc = a.delpc;
     real *gz = a.gz, *pef = a.pef;
     const real* w3 = a.w3;
-    double pem[NK], pm[NK], pp[NK], gam[NK], w[NK];
+    double pm[NK], pp[NK], gam[NK], w[NK];
     const int K = d.nk;
-    const long long o0 = idx3(d, t, i, j, 0);
-    const long long sk = d.sk;
+    const idx_t o0 = idx3(d, t, i, j, 0);
+    const idx_t sk = d.sk;
     const double t1g = 2.0 * dt2 * dt2;
     const double rdt = 1.0 / dt2;
-    // precompute (riem_solver_c.py:13-44)
-    double pem_k = ptop, peg_k = ptop;
-    for (int k = 0; k < K; ++k) {
-      const double dmk = delpc[o0 + k * sk];
-      pem[k] = pem_k;
-      const double peg_next = peg_k + dmk * (1.0 - q_con[o0 + k * sk]);
-      if (k < K - 1) pm[k] = (peg_next - peg_k) / fm::fm_log(peg_next / peg_k);
-      pem_k = pem_k + dmk;
+    // precompute (riem_solver_c.py:13-44); the edge pressures pem are
+    // running sums rebuilt where they are used
+    double peg_k = ptop;
+    for (int k = 0; k < K - 1; ++k) {
+      const double dmk = __ldg(&delpc[o0 + k * sk]);
+      const double peg_next = peg_k + dmk * (1.0 - __ldg(&q_con[o0 + k * sk]));
+      pm[k] = (peg_next - peg_k) / fm::fm_log(peg_next / peg_k);
       peg_k = peg_next;
     }
-    auto DM = [&](int k) { return delpc[o0 + k * sk] / GRAV; };
-    auto W1 = [&](int k) { return w3[o0 + k * sk]; };
+    auto DM = [&](int k) { return __ldg(&delpc[o0 + k * sk]) / GRAV; };
+    auto DP = [&](int k) { return (double)__ldg(&delpc[o0 + k * sk]); };
+    auto W1 = [&](int k) { return __ldg(&w3[o0 + k * sk]); };
     auto DZ = [&](int k) { return (double)gz[o0 + (k + 1) * sk] - (double)gz[o0 + k * sk]; };
-    auto GM = [&](int k) { return 1.0 / (1.0 - cappa[o0 + k * sk]); };
-    auto PTR = [&](int k) { return ptc[o0 + k * sk]; };
-    auto CP3 = [&](int k) { return cappa[o0 + k * sk]; };
+    auto GM = [&](int k) { return 1.0 / (1.0 - __ldg(&cappa[o0 + k * sk])); };
+    auto PTR = [&](int k) { return __ldg(&ptc[o0 + k * sk]); };
+    auto CP3 = [&](int k) { return (double)__ldg(&cappa[o0 + k * sk]); };
     // finalize (riem_solver_c.py:46-64) fused with the solve's outputs; gz
     // is rewritten bottom up only after its last read as an input
-    auto PE_OUT = [&](int k, double pe) { pef[o0 + k * sk] = k == 0 ? ptop : pe + pem[k]; };
+    double pem_pe = ptop;
+    auto PE_OUT = [&](int k, double pe) {
+      if (k > 0) pem_pe = pem_pe + DP(k - 1);
+      pef[o0 + k * sk] = k == 0 ? ptop : pe + pem_pe;
+    };
     double g = hs[idx2(d, t, i, j)];
     auto DZ_OUT = [&](int k, double dz) {
       if (k == K - 2) gz[o0 + (K - 1) * sk] = g;
       g = g - dz * GRAV;
       gz[o0 + k * sk] = g;
     };
-    sim1_column<NK>(K, DM, W1, DZ, GM, PTR, CP3, pem, pm, pp, gam, w, ws[idx2(d, t, i, j)], dt2, t1g, rdt, p_fac,
-                    PE_OUT, DZ_OUT);
+    sim1_column<NK>(K, DM, DP, ptop, W1, DZ, GM, PTR, CP3, pm, pp, gam, w, ws[idx2(d, t, i, j)], dt2, t1g, rdt,
+                    p_fac, PE_OUT, DZ_OUT);
   }
 };
 
@@ -184,16 +196,15 @@ struct Riem3 {
     const real *cappa = a.cappa, *zs = a.zs, *wsd = a.wsd, *q_con = a.q_con, *delp = a.delp, *pt = a.pt;
     real *delz = a.delz, *zh = a.zh, *pe = a.pe, *ppe = a.ppe, *pk3 = a.pk3, *pk = a.pk, *peln = a.peln;
     real* w_io = a.w;
-    double pem[NK], pm[NK], pp[NK], gam[NK], w[NK];
+    double pm[NK], pp[NK], gam[NK], w[NK];
     const int K = d.nk;
-    const long long o0 = idx3(d, t, i, j, 0);
-    const long long sk = d.sk;
+    const idx_t o0 = idx3(d, t, i, j, 0);
+    const idx_t sk = d.sk;
     const double t1g = 2.0 * dt * dt;
     const double rdt = 1.0 / dt;
     // precompute (riem_solver3.py:24-67); on the last call peln, pk and pe
     // take their final values here (finalize, riem_solver3.py:70-103)
     double pem_k = ptop, peg_k = ptop, pelng_k = peln1;
-    pem[0] = ptop;
     pk3[o0] = ptk;
     if (last) {
       peln[o0] = peln1;
@@ -201,14 +212,13 @@ struct Riem3 {
       pe[o0] = ptop;
     }
     for (int k = 0; k < K - 1; ++k) {
-      const long long o = o0 + k * sk;
+      const idx_t o = o0 + k * sk;
       const double dmk = delp[o];
       const double pem_n = pem_k + dmk;
       const double peg_n = peg_k + dmk * (1.0 - q_con[o]);
       const double pelng_n = fm::fm_log(peg_n);
       const double peln_n = fm::fm_log(pem_n);
       const double pk3_n = fm::fm_exp(KAPPA * peln_n);
-      pem[k + 1] = pem_n;
       pk3[o + sk] = pk3_n;
       if (last) {
         peln[o + sk] = peln_n;
@@ -220,12 +230,13 @@ struct Riem3 {
       peg_k = peg_n;
       pelng_k = pelng_n;
     }
-    auto DM = [&](int k) { return delp[o0 + k * sk] * RGRAV; };
+    auto DM = [&](int k) { return __ldg(&delp[o0 + k * sk]) * RGRAV; };
+    auto DP = [&](int k) { return (double)__ldg(&delp[o0 + k * sk]); };
     auto W1 = [&](int k) { return w_io[o0 + k * sk]; };
     auto DZ = [&](int k) { return (double)zh[o0 + (k + 1) * sk] - (double)zh[o0 + k * sk]; };
-    auto GM = [&](int k) { return 1.0 / (1.0 - cappa[o0 + k * sk]); };
-    auto PTR = [&](int k) { return pt[o0 + k * sk]; };
-    auto CP3 = [&](int k) { return cappa[o0 + k * sk]; };
+    auto GM = [&](int k) { return 1.0 / (1.0 - __ldg(&cappa[o0 + k * sk])); };
+    auto PTR = [&](int k) { return __ldg(&pt[o0 + k * sk]); };
+    auto CP3 = [&](int k) { return (double)__ldg(&cappa[o0 + k * sk]); };
     auto PE_OUT = [&](int k, double v) { ppe[o0 + k * sk] = v; };
     // finalize: zh rebuilt from the new layer depths bottom up, after its
     // last read as an input
@@ -236,8 +247,8 @@ struct Riem3 {
       z = z - dz;
       zh[o0 + k * sk] = z;
     };
-    sim1_column<NK>(K, DM, W1, DZ, GM, PTR, CP3, pem, pm, pp, gam, w, wsd[idx2(d, t, i, j)], dt, t1g, rdt, p_fac,
-                    PE_OUT, DZ_OUT);
+    sim1_column<NK>(K, DM, DP, ptop, W1, DZ, GM, PTR, CP3, pm, pp, gam, w, wsd[idx2(d, t, i, j)], dt, t1g, rdt,
+                    p_fac, PE_OUT, DZ_OUT);
     for (int k = 0; k < K - 1; ++k) w_io[o0 + k * sk] = w[k];
   }
 };
@@ -271,6 +282,7 @@ extern "C" int fv3b_riem_solver_c(const fv3b_grid_dims* dims, double dt2, double
                                   real* gz, real* pef, const real* w3, void* stream) {
   FV3B_REQUIRE(dims && cappa && hs && ws && ptc && q_con && delpc && gz && pef && w3,
                "fv3b_riem_solver_c: null argument");
+  FV3B_REQUIRE(dims_fit(dims), "fv3b_riem_solver_c: a 3-D field of the six tiles must hold fewer than 2^31 elements");
   Dims d = make_dims(dims);
   FV3B_REQUIRE(d.nk <= MAXK && d.nk >= 3, "fv3b_riem_solver_c: npz out of range (2..127)");
   RiemCArgs a{dt2, ptop, p_fac, cappa, hs, ws, ptc, q_con, delpc, gz, pef, w3};
@@ -287,6 +299,7 @@ extern "C" int fv3b_riem_solver3(const fv3b_grid_dims* dims, int last_call, doub
                                  real* ppe, real* pk3, real* pk, real* peln, real* w, void* stream) {
   FV3B_REQUIRE(dims && cappa && zs && wsd && delz && q_con && delp && pt && zh && pe && ppe && pk3 && pk && peln && w,
                "fv3b_riem_solver3: null argument");
+  FV3B_REQUIRE(dims_fit(dims), "fv3b_riem_solver3: a 3-D field of the six tiles must hold fewer than 2^31 elements");
   Dims d = make_dims(dims);
   FV3B_REQUIRE(d.nk <= MAXK && d.nk >= 3, "fv3b_riem_solver3: npz out of range (2..127)");
   const double peln1 = log(ptop);

@@ -6,14 +6,14 @@
 #include "common.cuh"
 
 #define PT_SETUP(d, t, k)                                  \
-  const long long _b3 = (long long)(t) * (d).st + (long long)(k) * (d).sk; \
-  const long long _b2 = (long long)(t) * (d).st2;          \
-  const long long _sj = (d).sj;                            \
+  const ::fv3b::idx_t _b3 = (t) * (d).st + (k) * (d).sk;   \
+  const ::fv3b::idx_t _b2 = (t) * (d).st2;                 \
+  const ::fv3b::idx_t _sj = (d).sj;                        \
   (void)_b3;                                               \
   (void)_b2;                                               \
   (void)_sj
 
-#define F3(p, i, j) ((p)[_b3 + (long long)(j) * _sj + (i)])
-#define W3(p, i, j) ((p)[_b3 + (long long)(j) * _sj + (i)])
-#define F3K(p, i, j, dk) ((p)[_b3 + (long long)(dk) * d.sk + (long long)(j) * _sj + (i)])
-#define F2(p, i, j) ((p)[_b2 + (long long)(j) * _sj + (i)])
+#define F3(p, i, j) ((p)[_b3 + (j) * _sj + (i)])
+#define W3(p, i, j) ((p)[_b3 + (j) * _sj + (i)])
+#define F3K(p, i, j, dk) ((p)[_b3 + (dk) * d.sk + (j) * _sj + (i)])
+#define F2(p, i, j) ((p)[_b2 + (j) * _sj + (i)])

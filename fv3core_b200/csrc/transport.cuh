@@ -23,26 +23,26 @@ constexpr real PPM_P1 = RC(7.0) / RC(12.0), PPM_P2 = -RC(1.0) / RC(12.0);
 template <int AXIS>
 struct Line3 {
   const real* p;
-  long long base;  // index of (i, j, k)
-  long long step;  // 1 or sj
+  idx_t base;  // index of (i, j, k)
+  idx_t step;  // 1 or sj
   __device__ __forceinline__ real operator()(int o) const { return p[base + o * step]; }
 };
 
 template <int AXIS>
 struct Line2 {
   const real* p;
-  long long base;
-  long long step;
+  idx_t base;
+  idx_t step;
   __device__ __forceinline__ real operator()(int o) const { return p[base + o * step]; }
 };
 
 template <int AXIS>
 __device__ __forceinline__ Line3<AXIS> line3(const Dims& d, const real* p, int t, int i, int j, int k) {
-  return Line3<AXIS>{p, idx3(d, t, i, j, k), AXIS == 0 ? 1LL : d.sj};
+  return Line3<AXIS>{p, idx3(d, t, i, j, k), AXIS == 0 ? idx_t(1) : d.sj};
 }
 template <int AXIS>
 __device__ __forceinline__ Line2<AXIS> line2(const Dims& d, const real* p, int t, int i, int j) {
-  return Line2<AXIS>{p, idx2(d, t, i, j), AXIS == 0 ? 1LL : (long long)d.ni};
+  return Line2<AXIS>{p, idx2(d, t, i, j), AXIS == 0 ? idx_t(1) : (idx_t)d.ni};
 }
 
 // The reference's y-corner-copied copy of q (CopyCornersXY, corners.py:64-117)
@@ -74,6 +74,25 @@ __device__ __forceinline__ real ppm_al(const Q& q, const A& dxa, int o, int pos,
   return PPM_P1 * (q(o - 1) + q(o)) + PPM_P2 * (q(o - 2) + q(o + 1));
 }
 
+// The three interface values around cell offset 0 (offsets -1, 0, 1) of a
+// line.  Away from the tile edges (no offset on an edge row) the six cells
+// are loaded once and the interior formula is used; otherwise each value
+// takes ppm_al's edge rules.  Same operations in the same order either way.
+template <typename Q, typename A>
+__device__ __forceinline__ void ppm_al3(const Q& q, const A& dxa, int pos, int s, int e, real& alm, real& al0,
+                                        real& alp) {
+  if (pos - 1 >= s + 2 && pos + 1 <= e - 1) {
+    const real q_3 = q(-3), q_2 = q(-2), q_1 = q(-1), q0 = q(0), q1 = q(1), q2 = q(2);
+    alm = PPM_P1 * (q_2 + q_1) + PPM_P2 * (q_3 + q0);
+    al0 = PPM_P1 * (q_1 + q0) + PPM_P2 * (q_2 + q1);
+    alp = PPM_P1 * (q0 + q1) + PPM_P2 * (q_1 + q2);
+    return;
+  }
+  alm = ppm_al(q, dxa, -1, pos, s, e);
+  al0 = ppm_al(q, dxa, 0, pos, s, e);
+  alp = ppm_al(q, dxa, 1, pos, s, e);
+}
+
 __device__ __forceinline__ bool ppm_smooth(real bl, real b0, real br, int mord) {
   if (mord == 5) return bl * br < 0;
   return (RC(3.0) * fabs(b0)) < fabs(bl - br);
@@ -84,9 +103,8 @@ __device__ __forceinline__ bool ppm_smooth(real bl, real b0, real br, int mord) 
 // get_advection_mask and apply_flux (xppm.py:19-61).
 template <typename Q, typename A>
 __device__ __forceinline__ real ppm_flux(const Q& q, const A& dxa, real c, int pos, int s, int e, int mord) {
-  real alm = ppm_al(q, dxa, -1, pos, s, e);
-  real al0 = ppm_al(q, dxa, 0, pos, s, e);
-  real alp = ppm_al(q, dxa, 1, pos, s, e);
+  real alm, al0, alp;
+  ppm_al3(q, dxa, pos, s, e, alm, al0, alp);
   real qm = q(-1), q0 = q(0);
   real blm = alm - qm, brm = al0 - qm, b0m = blm + brm;
   real bl0 = al0 - q0, br0 = alp - q0, b00 = bl0 + br0;
@@ -126,7 +144,7 @@ inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a
   err = launch_box(Box{s - 3, e + 5, js - 3, je + 5, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
     if (i >= s - 3 && i < e + 5 && j >= js && j < je + 2) {
       auto dya = line2<1>(d, g.dya, t, i, j);
-      const long long o = idx3(d, t, i, j, k);
+      const idx_t o = idx3(d, t, i, j, k);
       if (i >= s && i <= e) {  // no cube-corner point on this line: plain reads
         a.fy_mean[o] = ppm_flux(line3<1>(d, a.q_base, t, i, j, k), dya, a.cry[o], j, js, je, mord_in);
       } else {
@@ -161,7 +179,7 @@ inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a
   if (err != cudaSuccess) return err;
   // outer PPM and final_fluxes (fvtp2d.py:63-93) on [is, ie+1] x [js, je+1]
   return launch_box(Box{s, e + 2, js, je + 2, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
-    long long o = idx3(d, t, i, j, k);
+    idx_t o = idx3(d, t, i, j, k);
     if (j <= je) {
       auto q = line3<0>(d, a.q_adv_y, t, i, j, k);
       auto dxa = line2<0>(d, g.dxa, t, i, j);
@@ -203,78 +221,106 @@ struct DelnCol {
 // (delnflux.py intervals with externals nord0..nord3).
 __device__ __forceinline__ int nord_at(const real* nord, int k) { return (int)nord[k < 3 ? k : 3]; }
 
+// One point of a del-n flux pass: fx = del6_v * (d2(i-1, j) - d2(i, j)) and
+// fy = del6_u * (d2(i, j-1) - d2(i, j)) on the pass's region (lo halo rows;
+// levels with nord = 0 the compute-domain faces), corner points mapped to
+// their copy sources first (fx_calc_stencil_nord / fy_calc_stencil_nord,
+// delnflux.py:183-233).  D2(i, j) gives d2 at a point.
+template <typename D2F>
+__device__ __forceinline__ void deln_flux_point(const Dims& d, const fv3b_metrics& g, int t, int i, int j, int k,
+                                                int lo, int nk_, bool first, real* wx, real* wy, const D2F& D2) {
+  PT_SETUP(d, t, k);
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
+  const bool corners = nk_ > 0;
+  auto d2x = [&](int ii, int jj) {
+    int si, sj;
+    if (corners && copy_corner_x(d, ii, jj, si, sj)) return D2(si, sj);
+    return D2(ii, jj);
+  };
+  auto d2y = [&](int ii, int jj) {
+    int si, sj;
+    if (corners && copy_corner_y(d, ii, jj, si, sj)) return D2(si, sj);
+    return D2(ii, jj);
+  };
+  bool fx_in, fy_in;
+  if (nk_ > 0) {
+    fx_in = i >= s - lo && i < e + 2 + lo && j >= js - lo && j < je + 1 + lo;
+    fy_in = i >= s - lo && i < e + 1 + lo && j >= js - lo && j < je + 2 + lo;
+  } else {
+    fx_in = i >= s && i < e + 2 && j >= js && j < je + 1;
+    fy_in = i >= s && i < e + 1 && j >= js && j < je + 2;
+  }
+  if (fx_in) {
+    real v = F2(g.del6_v, i, j) * (d2x(i - 1, j) - d2x(i, j));
+    W3(wx, i, j) = first ? v : -v;
+  }
+  if (fy_in) {
+    real v = F2(g.del6_u, i, j) * (d2y(i, j - 1) - d2y(i, j));
+    W3(wy, i, j) = first ? v : -v;
+  }
+}
+
 // DelnFluxNoSG.__call__ (delnflux.py:1156-1207): del-n diffusive fluxes of q
-// into fx2/fy2 using d2 as scratch.  Corner copies of d2 are applied on read
-// (a point of a corner block reads its copy source), which gives the values
-// the reference reads after copying the corners in place.
+// into fx2/fy2.  Corner copies of d2 are applied on read (a point of a
+// corner block reads its copy source), which gives the values the reference
+// reads after copying the corners in place.
+//
+// The reference alternates a d2 stencil (d2 = damp * q, then the divergence
+// of the last fluxes times rarea) with a flux stencil that differences d2.
+// Here each flux pass computes the d2 values it needs on the fly from q or
+// from the previous pass's fluxes, with the reference's operation order, so
+// d2 is never stored: nmax + 1 passes instead of 2 * (nmax + 1).  Every d2
+// point a pass reads (corner sources included) lies inside the region where
+// the reference computes d2, so the values are the same.  Consecutive
+// passes ping-pong between (fx2, fy2) and the scratch pair (ax, ay), ending
+// in (fx2, fy2); levels with nord = 0 take the first pass only, written to
+// (fx2, fy2).
 // nlev is the number of levels (npz by default; UpdateHeightOnDGrid runs it
 // on npz + 1 interface levels).
 inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const real* q, real* fx2, real* fy2,
-                                 DelnCol col, real* d2, bool mass_weighted, int nmax, cudaStream_t st,
+                                 DelnCol col, real* ax, real* ay, bool mass_weighted, int nmax, cudaStream_t st,
                                  int nlev = -1) {
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = nlev < 0 ? d.nz : nlev;
-  cudaError_t err;
-  // d2_damp_interval / copy_stencil_interval
-  err = launch_box(Box{s - 1 - nmax, e + 2 + nmax, js - 1 - nmax, je + 2 + nmax, 0, nz}, st,
-                   [=] __device__(int t, int i, int j, int k) {
-                     PT_SETUP(d, t, k);
-                     int nk_ = nord_at(col.nord, k);
-                     bool in0 = i >= s - 1 && i < e + 2 && j >= js - 1 && j < je + 2;
-                     if (nk_ > 0 || in0) W3(d2, i, j) = mass_weighted ? F3(q, i, j) : col.damp[k] * F3(q, i, j);
-                   });
-  if (err != cudaSuccess) return err;
-  auto flux_pass = [&](int nt, bool first) {
-    // first pass: fx_calc_stencil_nord / fy_calc_stencil_nord (all levels);
-    // later passes: fx/fy_calc_stencil_column (levels with nord > 0)
-    int lo = first ? nmax : nt;
-    return launch_box(Box{s - lo, e + 2 + lo, js - lo, je + 2 + lo, 0, nz}, st,
-                      [=] __device__(int t, int i, int j, int k) {
-                        PT_SETUP(d, t, k);
-                        int nk_ = nord_at(col.nord, k);
-                        if (!first && nk_ == 0) return;
-                        bool corners = nk_ > 0;
-                        auto d2x = [&](int ii, int jj) {
-                          int si, sj;
-                          if (corners && copy_corner_x(d, ii, jj, si, sj)) return F3(d2, si, sj);
-                          return F3(d2, ii, jj);
-                        };
-                        auto d2y = [&](int ii, int jj) {
-                          int si, sj;
-                          if (corners && copy_corner_y(d, ii, jj, si, sj)) return F3(d2, si, sj);
-                          return F3(d2, ii, jj);
-                        };
-                        bool fx_in, fy_in;
-                        if (nk_ > 0) {
-                          fx_in = i >= s - lo && i < e + 2 + lo && j >= js - lo && j < je + 1 + lo;
-                          fy_in = i >= s - lo && i < e + 1 + lo && j >= js - lo && j < je + 2 + lo;
-                        } else {
-                          fx_in = i >= s && i < e + 2 && j >= js && j < je + 1;
-                          fy_in = i >= s && i < e + 1 && j >= js && j < je + 2;
-                        }
-                        if (fx_in) {
-                          real v = F2(g.del6_v, i, j) * (d2x(i - 1, j) - d2x(i, j));
-                          W3(fx2, i, j) = first ? v : -v;
-                        }
-                        if (fy_in) {
-                          real v = F2(g.del6_u, i, j) * (d2y(i, j - 1) - d2y(i, j));
-                          W3(fy2, i, j) = first ? v : -v;
-                        }
-                      });
-  };
-  err = flux_pass(nmax, true);
-  if (err != cudaSuccess) return err;
-  for (int n = 0; n < nmax; ++n) {
-    int nt = nmax - 1 - n;
-    // d2_highorder_stencil (delnflux.py:159-181)
-    err = launch_box(Box{s - nt - 1, e + nt + 2, js - nt - 1, je + nt + 2, 0, nz}, st,
-                     [=] __device__(int t, int i, int j, int k) {
-                       PT_SETUP(d, t, k);
-                       if (nord_at(col.nord, k) == 0) return;
-                       W3(d2, i, j) = (F3(fx2, i, j) - F3(fx2, i + 1, j) + F3(fy2, i, j) - F3(fy2, i, j + 1)) *
-                                      F2(g.rarea, i, j) * col.rscale;
-                     });
+  // pass p writes (fx2, fy2) when nmax - p is even, so the last pass does
+  auto out_x = [&](int p) { return ((nmax - p) % 2 == 0) ? fx2 : ax; };
+  auto out_y = [&](int p) { return ((nmax - p) % 2 == 0) ? fy2 : ay; };
+  // first pass: d2 = damp * q (d2_damp_interval) or q (copy_stencil_interval)
+  {
+    const int lo = nmax;
+    real *wx = out_x(0), *wy = out_y(0);
+    cudaError_t err = launch_box(Box{s - lo, e + 2 + lo, js - lo, je + 2 + lo, 0, nz}, st,
+                                 [=] __device__(int t, int i, int j, int k) {
+                                   const int nk_ = nord_at(col.nord, k);
+                                   const idx_t b3 = t * d.st + k * d.sk;
+                                   const real damp = col.damp[k];
+                                   auto D2 = [&](int ii, int jj) {
+                                     const real qv = q[b3 + jj * d.sj + ii];
+                                     return mass_weighted ? qv : damp * qv;
+                                   };
+                                   deln_flux_point(d, g, t, i, j, k, lo, nk_, true, nk_ > 0 ? wx : fx2,
+                                                   nk_ > 0 ? wy : fy2, D2);
+                                 });
     if (err != cudaSuccess) return err;
-    err = flux_pass(nt, false);
+  }
+  // later passes on levels with nord > 0: d2 from the previous fluxes
+  // (d2_highorder_stencil, delnflux.py:159-181), then the fluxes
+  // (fx/fy_calc_stencil_column)
+  for (int p = 1; p <= nmax; ++p) {
+    const int lo = nmax - p;
+    const real *px = out_x(p - 1), *py = out_y(p - 1);
+    real *wx = out_x(p), *wy = out_y(p);
+    cudaError_t err = launch_box(Box{s - lo, e + 2 + lo, js - lo, je + 2 + lo, 0, nz}, st,
+                                 [=] __device__(int t, int i, int j, int k) {
+                                   const int nk_ = nord_at(col.nord, k);
+                                   if (nk_ == 0) return;
+                                   const idx_t b3 = t * d.st + k * d.sk, b2 = t * d.st2;
+                                   auto D2 = [&](int ii, int jj) {
+                                     const idx_t o = b3 + jj * d.sj + ii;
+                                     return (px[o] - px[o + 1] + py[o] - py[o + d.sj]) *
+                                            g.rarea[b2 + jj * d.sj + ii] * col.rscale;
+                                   };
+                                   deln_flux_point(d, g, t, i, j, k, lo, nk_, false, wx, wy, D2);
+                                 });
     if (err != cudaSuccess) return err;
   }
   return cudaSuccess;
@@ -283,8 +329,8 @@ inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const real*
 // DelnFlux.__call__ (delnflux.py:963-998): damped fluxes added to fx, fy on
 // the cell corners of the compute domain.
 inline cudaError_t delnflux(const Dims d, const fv3b_metrics g, const real* q, real* fx, real* fy, DelnCol col,
-                           const real* mass, real* fx2, real* fy2, real* d2, int nmax, cudaStream_t st) {
-  cudaError_t err = delnflux_nosg(d, g, q, fx2, fy2, col, d2, mass != nullptr, nmax, st);
+                           const real* mass, real* fx2, real* fy2, real* ax, real* ay, int nmax, cudaStream_t st) {
+  cudaError_t err = delnflux_nosg(d, g, q, fx2, fy2, col, ax, ay, mass != nullptr, nmax, st);
   if (err != cudaSuccess) return err;
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
   return launch_box(Box{s, e + 2, js, je + 2, 0, d.nz}, st, [=] __device__(int t, int i, int j, int k) {

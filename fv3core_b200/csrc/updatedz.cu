@@ -85,7 +85,7 @@ extern "C" int fv3b_update_dz_c(fv3b_ctx* ctx, const real* dp_ref, const real* z
   // surface w and the DZ_MIN floor, bottom up (updatedzc.py:100-120)
   const real rdt = RC(1.0) / dt;
   FV3B_CHECK(launch_columns(s - 1, e + 2, js - 1, je + 2, st, [=] __device__(int t, int i, int j) {
-    long long o = idx3(d, t, i, j, nk - 1);
+    idx_t o = idx3(d, t, i, j, nk - 1);
     real below = gz_new[o];
     gz[o] = below;
     ws[idx2(d, t, i, j)] = (zs[idx2(d, t, i, j)] - below) * rdt;
@@ -147,8 +147,8 @@ extern "C" int fv3b_update_dz_d(fv3b_ctx* ctx, const real* zs, real* zh, const r
   FV3B_CHECK(launch_columns(0, full, 0, full, st, [=] __device__(int t, int i, int j) {
     const real* src[4] = {crx, xfx, cry, yfx};
     real* dst[4] = {crx_i, xfx_i, cry_i, yfx_i};
-    const long long o0 = idx3(d, t, i, j, 0);
-    const long long sk = d.sk;
+    const idx_t o0 = idx3(d, t, i, j, 0);
+    const idx_t sk = d.sk;
     for (int f = 0; f < 4; ++f) {
       const real* q = src[f] + o0;
       real* out = dst[f] + o0;
@@ -178,7 +178,7 @@ extern "C" int fv3b_update_dz_d(fv3b_ctx* ctx, const real* zs, real* zh, const r
   // DelnFluxNoSG on npz + 1 levels with the raw damp_vt column (range-scaled
   // copy, identical to damp_vt in double builds)
   DelnCol dl{colp(ctx, COL_NORD_V), colp(ctx, COL_DAMP_VT_DZ), static_cast<real>(ctx->dsw.area_scale)};
-  FV3B_CHECK(delnflux_nosg(d, g, zh, gzx_diff, gzy_diff, dl, d2, false, ctx->dsw.nmax_v, st, nk));
+  FV3B_CHECK(delnflux_nosg(d, g, zh, gzx_diff, gzy_diff, dl, d2, W[WS_DELN_ALT], false, ctx->dsw.nmax_v, st, nk));
   // apply_height_fluxes (updatedzd.py:63-118) fused with the surface w and
   // DZ_MIN floor, bottom up per column of the compute domain
   FV3B_CHECK(launch_columns(s, e + 1, js, je + 1, st, [=] __device__(int t, int i, int j) {
@@ -192,7 +192,7 @@ extern "C" int fv3b_update_dz_d(fv3b_ctx* ctx, const real* zs, real* zh, const r
           (F3(gzx_diff, i, j) - F3(gzx_diff, i + 1, j) + F3(gzy_diff, i, j) - F3(gzy_diff, i, j + 1)) / area;
       return adv + diff;
     };
-    long long o = idx3(d, t, i, j, nk - 1);
+    idx_t o = idx3(d, t, i, j, nk - 1);
     real below = new_height(nk - 1);
     zh[o] = below;
     wsd[idx2(d, t, i, j)] = (zs[idx2(d, t, i, j)] - below) / dt;

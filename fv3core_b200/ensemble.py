@@ -23,9 +23,9 @@ from .storage import to_device
 
 
 class Member:
-    def __init__(self, n, npz, seed, precision="f64", n_split=6, mdt=225.0, noise=1.0e-3):
+    def __init__(self, n, npz, seed, precision="f64", n_split=6, mdt=225.0, noise=1.0e-3, grid=None):
         self.n, self.npz, self.seed = n, npz, seed
-        grid = CubedSphereGrid(n, 3)
+        grid = CubedSphereGrid(n, 3) if grid is None else grid
         st = baroclinic_state(grid, npz, seed=seed, noise=noise)
         self.grid_data = GridData(grid, npz, precision=precision)
         gi = self.grid_data.grid_indexing
@@ -41,8 +41,20 @@ class Member:
             0, False, False, baroclinic_acoustic_config(n_split=n_split), st["ak"], st["bk"], st["pfull"], state.phis,
         )
         self.cell_levels = 6 * n * n * npz
+        self._initial = None
 
-    def step(self):
+    def keep_initial(self):
+        """Keep a device copy of the current state for ``reset``."""
+        self._initial = {k: getattr(self.state, k).clone() for k in _lib.DYCORE_FIELDS}
+
+    def reset(self):
+        """Copy the kept state back (device to device, capturable)."""
+        for k, t in self._initial.items():
+            getattr(self.state, k).copy_(t)
+
+    def step(self, reset=False):
+        if reset:
+            self.reset()
         self.dynamics(self.state)
 
     def close(self):
@@ -54,24 +66,35 @@ class Ensemble:
 
     def __init__(self, members, precision="f64", n_split=6):
         self.n_split = n_split
-        self.members = [Member(n, npz, seed, precision, n_split) for n, npz, seed in members]
+        grids = {}
+        self.members = []
+        for n, npz, seed in members:
+            if n not in grids:
+                grids[n] = CubedSphereGrid(n, 3)
+            self.members.append(Member(n, npz, seed, precision, n_split, grid=grids[n]))
 
     @property
     def cell_levels(self):
         return sum(m.cell_levels for m in self.members)
 
-    def step(self):
+    def keep_initial(self):
         for m in self.members:
-            m.step()
+            m.keep_initial()
 
-    def capture(self):
+    def step(self, reset=False):
+        """One AcousticDynamics call per member; with ``reset`` every member
+        first returns to its kept state (``keep_initial``)."""
+        for m in self.members:
+            m.step(reset)
+
+    def capture(self, reset=False):
         """One CUDA graph of a whole ensemble step.  Every member must have
         stepped eagerly once (the per-level Rayleigh factors are uploaded by
         the first call); replaying the graph advances all members."""
         graph = torch.cuda.CUDAGraph()
         torch.cuda.synchronize()
         with torch.cuda.graph(graph):
-            self.step()
+            self.step(reset)
         return graph
 
     def close(self):

@@ -160,3 +160,25 @@ def baroclinic_state(grid: CubedSphereGrid, nz, seed=0, noise=1.0e-3, ntracers=4
     apply_scalar_table(st["phis"], tc)
     apply_vector_tables(st["u"], st["v"], vector_tables(n, h, (1, 0), (0, 1), h))
     return st
+
+
+def resting_state(grid: CubedSphereGrid, nz, temperature=280.0):
+    """A dry isothermal atmosphere at rest over a flat surface, in the layout
+    of ``baroclinic_state``: every column is the same hydrostatic column
+    (delz from the interface log-pressures, pkz from the layer's log-mean
+    pressure), u = v = w = 0 and phis = 0.  Acoustic substeps must leave the
+    winds at zero and delp unchanged."""
+    st = baroclinic_state(grid, nz, seed=0, noise=0.0, ntracers=0)
+    pe_col = st["pe"][0, 0, 0, :]
+    dlnp = np.log(pe_col[1:] / pe_col[:-1])
+    delp_col = np.diff(pe_col)
+    cappa = C.RDGAS / (C.RDGAS + C.CV_AIR)
+    delz = -C.RDGAS * temperature / C.GRAV * dlnp
+    pkz = np.exp(cappa * np.log(delp_col / dlnp))
+    cols = {"delz": delz, "pkz": pkz, "pt": temperature / pkz, "cappa": np.full(nz, cappa),
+            "q_con": np.zeros(nz)}
+    for name, col in cols.items():
+        st[name][..., :nz] = col
+    for name in ("u", "v", "w", "phis"):
+        st[name][...] = 0.0
+    return st

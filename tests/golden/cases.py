@@ -186,3 +186,22 @@ def acoustics_case(n=12, nz=8, seed=41, n_split=2):
 
 
 CASES["acoustics"] = acoustics_case
+
+
+def resting_case(n=12, nz=8, n_split=2):
+    """An acoustics case on a dry isothermal atmosphere at rest over a flat
+    surface (identical hydrostatic columns, zero winds)."""
+    from fv3core_b200.initial_state import resting_state
+
+    st = resting_state(grid_for(n), nz)
+    shp = st["delp"].shape
+    case = {name: np.array(st[name], copy=True) for name in ACOUSTIC_STATE if name in st}
+    case["wsd"] = np.zeros(shp[:3])
+    for name in ("omga", "ua", "va", "uc", "vc", "mfxd", "mfyd", "cxd", "cyd", "diss_estd"):
+        case[name] = np.zeros(shp)
+    case.update(
+        ak=np.asarray(st["ak"], dtype=np.float64), bk=np.asarray(st["bk"], dtype=np.float64),
+        pfull=np.asarray(st["pfull"], dtype=np.float64), ptop=st["ptop"], ks=st["ks"],
+        mdt=37.5 * n_split, n_map=1, akap=C.KAPPA, n_split=n_split,
+    )
+    return case

@@ -1,8 +1,16 @@
 """The mixed-precision build (FP32 fields and bulk arithmetic, FP64 column
-solves) against the FP64 build on the same state: one AcousticDynamics call
+solves and column sums) against the FP64 build: one AcousticDynamics call
 with n_split = 6 (the acoustic part of one dynamics step of the baroclinic
-configuration).  The target is a max relative error of 1e-4 in delp and pt;
-the other prognostic fields are reported with looser bounds."""
+configuration).
+
+Three comparisons separate the build's own error from the sensitivity of
+the state: ``mixed`` is the mixed build against FP64 from the same state;
+``floor`` is FP64 started from the state rounded to FP32 (the mixed build's
+input) against FP64; ``arith`` is the mixed build against that FP64 run, so
+both start from identical numbers and only the arithmetic differs.  The
+target is 1e-4 max relative error in delp and pt; where FP32 rounding of
+the input alone moves FP64 by more than that (the C48 case: 1.3e-4 in pt),
+the bound is twice that floor."""
 import numpy as np
 import pytest
 
@@ -11,8 +19,8 @@ import cases
 H = 3
 
 
-def _rel(a, b, n, nz, extra=(0, 0)):
-    sl = (slice(None), slice(H, H + n + extra[0]), slice(H, H + n + extra[1]), slice(0, nz))
+def _rel(a, b, n, nz):
+    sl = (slice(None), slice(H, H + n), slice(H, H + n), slice(0, nz))
     a, b = a[sl], b[sl]
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-30)))
 
@@ -22,6 +30,11 @@ def _rms(a, b, n, nz):
     return float(np.sqrt(np.mean((a[sl] - b[sl]) ** 2)) / np.sqrt(np.mean(b[sl] ** 2)))
 
 
+def _rounded(case):
+    return {k: (v.astype(np.float32).astype(np.float64) if isinstance(v, np.ndarray) and v.ndim >= 2 else v)
+            for k, v in case.items()}
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("n,nz,seed", [(24, 79, 3), (48, 79, 8)])
 def test_mixed_matches_fp64_after_one_step(n, nz, seed):
@@ -29,10 +42,18 @@ def test_mixed_matches_fp64_after_one_step(n, nz, seed):
 
     case = cases.acoustics_case(n, nz, seed, n_split=6)
     ref = gpu_runs.run_acoustics(case, n, nz, "f64")
+    ref_r = gpu_runs.run_acoustics(_rounded(case), n, nz, "f64")
     mix = gpu_runs.run_acoustics(case, n, nz, "f32")
-    errs = {k: _rel(mix[k], ref[k], n, nz) for k in ("delp", "pt", "q_con", "delz")}
+    fields = ("delp", "pt", "q_con", "delz")
+    mixed = {k: _rel(mix[k], ref[k], n, nz) for k in fields}
+    floor = {k: _rel(ref_r[k], ref[k], n, nz) for k in fields}
+    arith = {k: _rel(mix[k], ref_r[k], n, nz) for k in fields}
     rms = {k: _rms(mix[k], ref[k], n, nz) for k in ("u", "v", "w", "delp", "pt")}
-    print("max rel", errs, "rms rel", rms)
-    assert errs["delp"] <= 1e-4 and errs["pt"] <= 1e-4, errs
-    assert errs["q_con"] <= 1e-3 and errs["delz"] <= 1e-3, errs
+    print("max rel: mixed", mixed, "floor", floor, "arith", arith, "rms rel", rms)
+    # 1e-4, or twice what FP32 rounding of the input alone does to FP64
+    # where the state is more sensitive than that
+    for k in ("delp", "pt"):
+        bound = max(1e-4, 2 * floor[k])
+        assert mixed[k] <= bound and arith[k] <= bound, (k, mixed, arith, floor)
+    assert mixed["q_con"] <= 1e-3 and mixed["delz"] <= 1e-3, mixed
     assert rms["u"] <= 1e-3 and rms["v"] <= 1e-3 and rms["w"] <= 5e-2, rms
