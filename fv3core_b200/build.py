@@ -46,12 +46,14 @@ def _sources():
 def _headers_mtime():
     hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     hs += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE)]
+    hs.append(os.path.abspath(__file__))  # the flags live here
     return max((os.path.getmtime(h) for h in hs), default=0.0)
 
 
 VARIANTS = {
     "f64": (LIB, []),
-    "f32": (LIB_F32, ["-DFV3B_REAL_T=float"]),
+    # mixed precision: FP32 fields, CUDA's FP64 exp/log/pow in the column solves
+    "f32": (LIB_F32, ["-DFV3B_REAL_T=float", "-DFV3B_FAST_TRANSCENDENTALS"]),
 }
 
 

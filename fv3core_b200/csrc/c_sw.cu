@@ -18,6 +18,12 @@ constexpr real C1 = -RC(2.0) / RC(14.0), C2 = RC(11.0) / RC(14.0), C3 = RC(5.0) 
 constexpr real A1 = RC(9.0) / RC(16.0), A2 = -RC(1.0) / RC(16.0);
 constexpr real BIG = RC(1e30);
 
+// The only points corner_x can fill: i in {s-3, s-2, s-1, e+1, e+2, e+3}
+// (x = 0..5) and j in {js-1, je+1} (y = 0, 1); corner_y swaps the roles.
+// The corner passes launch over these 12 points per level and tile.
+__device__ __forceinline__ int corner_i6(const Dims& d, int x) { return x < 3 ? d.isc - 3 + x : d.iec + x - 2; }
+__device__ __forceinline__ int corner_j6(const Dims& d, int x) { return x < 3 ? d.jsc - 3 + x : d.jec + x - 2; }
+
 }  // namespace
 
 extern "C" int fv3b_c_sw(fv3b_ctx* ctx, real* delp, real* pt, const real* u, const real* v, real* w,
@@ -69,8 +75,9 @@ extern "C" int fv3b_c_sw(fv3b_ctx* ctx, real* delp, real* pt, const real* u, con
     }
   }));
   // fill_corners_x on utmp (3 cells, from vtmp) and ua (2 cells, from va)
-  FV3B_CHECK(launch_box(Box{s - 3, e + 4, js - 1, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+  FV3B_CHECK(launch_box(Box{0, 6, 0, 2, 0, nz}, st, [=] __device__(int t, int x, int y, int k) {
     PT_SETUP(d, t, k);
+    const int i = corner_i6(d, x), j = y == 0 ? js - 1 : je + 1;
     CornerRule r;
     if (corner_x(d, i, j, true, -RC(1.0), RC(1.0), RC(1.0), -RC(1.0), r)) W3(utmp, i, j) = r.mult * F3(vtmp, i + r.di, j + r.dj);
     if (corner_x(d, i, j, false, -RC(1.0), RC(1.0), RC(1.0), -RC(1.0), r)) W3(ua, i, j) = r.mult * F3(va, i + r.di, j + r.dj);
@@ -102,8 +109,9 @@ extern "C" int fv3b_c_sw(fv3b_ctx* ctx, real* delp, real* pt, const real* u, con
     }
   }));
   // fill_corners_y on vtmp (3 cells, from utmp) and va (2 cells, from ua)
-  FV3B_CHECK(launch_box(Box{s - 1, e + 2, js - 3, je + 4, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+  FV3B_CHECK(launch_box(Box{0, 6, 0, 2, 0, nz}, st, [=] __device__(int t, int x, int y, int k) {
     PT_SETUP(d, t, k);
+    const int i = y == 0 ? s - 1 : e + 1, j = corner_j6(d, x);
     CornerRule r;
     if (corner_y(d, i, j, true, -RC(1.0), RC(1.0), RC(1.0), -RC(1.0), r)) W3(vtmp, i, j) = r.mult * F3(utmp, i + r.di, j + r.dj);
     if (corner_y(d, i, j, false, -RC(1.0), RC(1.0), RC(1.0), -RC(1.0), r)) W3(va, i, j) = r.mult * F3(ua, i + r.di, j + r.dj);
@@ -188,8 +196,9 @@ extern "C" int fv3b_c_sw(fv3b_ctx* ctx, real* delp, real* pt, const real* u, con
       W3(vt, i, j) = y > 0 ? dt2 * y * F2(g.dx, i, j) * F2(g.sin_sg4, i, j - 1) : dt2 * y * F2(g.dx, i, j) * F2(g.sin_sg2, i, j);
     }
   }));
-  FV3B_CHECK(launch_box(Box{s - 2, e + 3, js - 1, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+  FV3B_CHECK(launch_box(Box{0, 6, 0, 2, 0, nz}, st, [=] __device__(int t, int x, int y, int k) {
     PT_SETUP(d, t, k);
+    const int i = corner_i6(d, x), j = y == 0 ? js - 1 : je + 1;
     CornerRule r;
     if (corner_x(d, i, j, false, RC(1.0), RC(1.0), RC(1.0), RC(1.0), r)) {
       real a = F3(delp, i + r.di, j + r.dj), b = F3(pt, i + r.di, j + r.dj), c = F3(w, i + r.di, j + r.dj);
@@ -210,8 +219,9 @@ extern "C" int fv3b_c_sw(fv3b_ctx* ctx, real* delp, real* pt, const real* u, con
     W3(tfx2, i, j) = fx1 * F3(w, ii, j);
   }));
   // fill_corners_y on delp, pt, w
-  FV3B_CHECK(launch_box(Box{s - 1, e + 2, js - 2, je + 3, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+  FV3B_CHECK(launch_box(Box{0, 6, 0, 2, 0, nz}, st, [=] __device__(int t, int x, int y, int k) {
     PT_SETUP(d, t, k);
+    const int i = y == 0 ? s - 1 : e + 1, j = corner_j6(d, x);
     CornerRule r;
     if (corner_y(d, i, j, false, RC(1.0), RC(1.0), RC(1.0), RC(1.0), r)) {
       real a = F3(delp, i + r.di, j + r.dj), b = F3(pt, i + r.di, j + r.dj), c = F3(w, i + r.di, j + r.dj);

@@ -206,10 +206,16 @@ cudaError_t fxadv(const Dims d, const fv3b_metrics g, const real* uc, const real
 }
 
 // ---------------------------------------------------------------- corner fills, sequential per level
-// fill_corners_bgrid_{x,y} (corners.py:598-722) on levels [k0, k1)
+// fill_corners_bgrid_{x,y} (corners.py:598-722) on levels [k0, k1).  The
+// rules only touch the four 3 x 3 blocks i in [s-3, s-1] or [e+2, e+4],
+// j in [js-3, js-1] or [je+2, je+4], so the launch covers those 36 points
+// (x = block * 3 + column, y = row).
 cudaError_t fill_bgrid(const Dims d, real* q, bool xdir, int k0, int k1, cudaStream_t st) {
-  return launch_box(Box{0, d.ni, 0, d.nj, k0, k1}, st, [=] __device__(int t, int i, int j, int k) {
+  return launch_box(Box{0, 12, 0, 3, k0, k1}, st, [=] __device__(int t, int x, int y, int k) {
     PT_SETUP(d, t, k);
+    const int c = x / 3, a = x % 3;
+    const int i = (c == 0 || c == 2) ? d.isc - 3 + a : d.iec + 2 + a;
+    const int j = c < 2 ? d.jsc - 3 + y : d.jec + 2 + y;
     int si, sj;
     bool hit = xdir ? bgrid_corner_x(d, i, j, si, sj) : bgrid_corner_y(d, i, j, si, sj);
     if (hit) W3(q, i, j) = F3(q, si, sj);

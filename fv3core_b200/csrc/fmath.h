@@ -131,7 +131,23 @@ __host__ __device__ __forceinline__ double exp_dd(double xh, double xl) {
   return scale2(exp_reduced(rh, rl), k);
 }
 
-__host__ __device__ __forceinline__ double fm_exp(double x) { return exp_dd(x, 0.0); }
+// The mixed-precision library is compiled with FV3B_FAST_TRANSCENDENTALS:
+// it has no last-bit parity target, so its device code calls CUDA's FP64
+// exp, log and pow, which take a fraction of the instructions of the
+// double-double forms below.
+#if defined(FV3B_FAST_TRANSCENDENTALS) && defined(__CUDA_ARCH__)
+#define FV3B_FM_FAST 1
+#else
+#define FV3B_FM_FAST 0
+#endif
+
+__host__ __device__ __forceinline__ double fm_exp(double x) {
+#if FV3B_FM_FAST
+  return ::exp(x);
+#else
+  return exp_dd(x, 0.0);
+#endif
+}
 
 // log(x) as hi + lo (x positive, finite, normal or subnormal)
 __host__ __device__ __forceinline__ void log_dd(double x, double& hi, double& lo) {
@@ -179,6 +195,9 @@ __host__ __device__ __forceinline__ void log_dd(double x, double& hi, double& lo
 }
 
 __host__ __device__ __forceinline__ double fm_log(double x) {
+#if FV3B_FM_FAST
+  return ::log(x);
+#endif
   if (x != x) return x;
   if (x < 0.0) return from_bits(0x7ff8000000000000ull);
   if (x == 0.0) return -from_bits(0x7ff0000000000000ull);
@@ -191,6 +210,9 @@ __host__ __device__ __forceinline__ double fm_log(double x) {
 // x^y = exp(y log x) with log x and the product carried in double-double
 // (x > 0; x == 0 gives 0 for y > 0, 1 for y == 0, inf for y < 0; x < 0 NaN)
 __host__ __device__ __forceinline__ double fm_pow(double x, double y) {
+#if FV3B_FM_FAST
+  return ::pow(x, y);
+#endif
   if (x != x || y != y) return x + y;
   if (x == 0.0) return y > 0.0 ? 0.0 : (y == 0.0 ? 1.0 : from_bits(0x7ff0000000000000ull));
   if (x < 0.0) return from_bits(0x7ff8000000000000ull);

@@ -55,10 +55,10 @@ __device__ __forceinline__ real qy_at(const Dims& d, const real* q, int t, int i
   return q[idx3(d, t, i, j, k)];
 }
 struct LineQY {
-  const Dims* d;
+  Dims d;
   const real* q;
   int t, i, j, k;
-  __device__ __forceinline__ real operator()(int o) const { return qy_at(*d, q, t, i, j + o, k); }
+  __device__ __forceinline__ real operator()(int o) const { return qy_at(d, q, t, i, j + o, k); }
 };
 
 // compute_al (xppm.py:148-181) for the cell at offset o of the line; pos is
@@ -78,6 +78,15 @@ __device__ __forceinline__ real ppm_al(const Q& q, const A& dxa, int o, int pos,
 // line.  Away from the tile edges (no offset on an edge row) the six cells
 // are loaded once and the interior formula is used; otherwise each value
 // takes ppm_al's edge rules.  Same operations in the same order either way.
+// The edge-row case (the rows next to tile edges).  Kept inline: an
+// out-of-line version measured slower.
+template <typename Q, typename A>
+__device__ __forceinline__ void ppm_al3_edges(const Q q, const A dxa, int pos, int s, int e, real* al) {
+  al[0] = ppm_al(q, dxa, -1, pos, s, e);
+  al[1] = ppm_al(q, dxa, 0, pos, s, e);
+  al[2] = ppm_al(q, dxa, 1, pos, s, e);
+}
+
 template <typename Q, typename A>
 __device__ __forceinline__ void ppm_al3(const Q& q, const A& dxa, int pos, int s, int e, real& alm, real& al0,
                                         real& alp) {
@@ -88,9 +97,11 @@ __device__ __forceinline__ void ppm_al3(const Q& q, const A& dxa, int pos, int s
     alp = PPM_P1 * (q0 + q1) + PPM_P2 * (q_1 + q2);
     return;
   }
-  alm = ppm_al(q, dxa, -1, pos, s, e);
-  al0 = ppm_al(q, dxa, 0, pos, s, e);
-  alp = ppm_al(q, dxa, 1, pos, s, e);
+  real al[3];
+  ppm_al3_edges(q, dxa, pos, s, e, al);
+  alm = al[0];
+  al0 = al[1];
+  alp = al[2];
 }
 
 __device__ __forceinline__ bool ppm_smooth(real bl, real b0, real br, int mord) {
@@ -142,20 +153,20 @@ inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a
   cudaError_t err;
   // inner PPM: fy_mean on [is-3, ie+4] x [js, je+1], fx_mean on [is, ie+1] x [js-3, je+4]
   err = launch_box(Box{s - 3, e + 5, js - 3, je + 5, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
-    if (i >= s - 3 && i < e + 5 && j >= js && j < je + 2) {
+    const idx_t o = idx3(d, t, i, j, k);
+    const bool do_y = j >= js && j < je + 2, do_x = i >= s && i < e + 2;
+    real fy = RC(0.0), fx = RC(0.0);  // both before either store (shared q loads)
+    if (do_y) {
       auto dya = line2<1>(d, g.dya, t, i, j);
-      const idx_t o = idx3(d, t, i, j, k);
       if (i >= s && i <= e) {  // no cube-corner point on this line: plain reads
-        a.fy_mean[o] = ppm_flux(line3<1>(d, a.q_base, t, i, j, k), dya, a.cry[o], j, js, je, mord_in);
+        fy = ppm_flux(line3<1>(d, a.q_base, t, i, j, k), dya, a.cry[o], j, js, je, mord_in);
       } else {
-        a.fy_mean[o] = ppm_flux(LineQY{&d, a.q_base, t, i, j, k}, dya, a.cry[o], j, js, je, mord_in);
+        fy = ppm_flux(LineQY{d, a.q_base, t, i, j, k}, dya, a.cry[o], j, js, je, mord_in);
       }
     }
-    if (i >= s && i < e + 2 && j >= js - 3 && j < je + 5) {
-      auto q = line3<0>(d, a.q_base, t, i, j, k);
-      auto dxa = line2<0>(d, g.dxa, t, i, j);
-      a.fx_mean[idx3(d, t, i, j, k)] = ppm_flux(q, dxa, a.crx[idx3(d, t, i, j, k)], i, s, e, mord_in);
-    }
+    if (do_x) fx = ppm_flux(line3<0>(d, a.q_base, t, i, j, k), line2<0>(d, g.dxa, t, i, j), a.crx[o], i, s, e, mord_in);
+    if (do_y) a.fy_mean[o] = fy;
+    if (do_x) a.fx_mean[o] = fx;
   });
   if (err != cudaSuccess) return err;
   // q_i (fvtp2d.py:33-47) on [0, n+6) x [js, je+4), q_j (50-60) on [is, ie+4) x [0, n+6)
@@ -179,19 +190,18 @@ inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a
   if (err != cudaSuccess) return err;
   // outer PPM and final_fluxes (fvtp2d.py:63-93) on [is, ie+1] x [js, je+1]
   return launch_box(Box{s, e + 2, js, je + 2, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
-    idx_t o = idx3(d, t, i, j, k);
+    const idx_t o = idx3(d, t, i, j, k);
+    real fx = RC(0.0), fy = RC(0.0);
     if (j <= je) {
-      auto q = line3<0>(d, a.q_adv_y, t, i, j, k);
-      auto dxa = line2<0>(d, g.dxa, t, i, j);
-      real xo = ppm_flux(q, dxa, a.crx[o], i, s, e, mord_out);
-      a.fx[o] = RC(0.5) * (xo + a.fx_mean[o]) * a.x_unit[o];
+      real xo = ppm_flux(line3<0>(d, a.q_adv_y, t, i, j, k), line2<0>(d, g.dxa, t, i, j), a.crx[o], i, s, e, mord_out);
+      fx = RC(0.5) * (xo + a.fx_mean[o]) * a.x_unit[o];
     }
     if (i <= e) {
-      auto q = line3<1>(d, a.q_adv_x, t, i, j, k);
-      auto dya = line2<1>(d, g.dya, t, i, j);
-      real yo = ppm_flux(q, dya, a.cry[o], j, js, je, mord_out);
-      a.fy[o] = RC(0.5) * (yo + a.fy_mean[o]) * a.y_unit[o];
+      real yo = ppm_flux(line3<1>(d, a.q_adv_x, t, i, j, k), line2<1>(d, g.dya, t, i, j), a.cry[o], j, js, je, mord_out);
+      fy = RC(0.5) * (yo + a.fy_mean[o]) * a.y_unit[o];
     }
+    if (j <= je) a.fx[o] = fx;
+    if (i <= e) a.fy[o] = fy;
   });
 }
 
@@ -231,7 +241,9 @@ __device__ __forceinline__ void deln_flux_point(const Dims& d, const fv3b_metric
                                                 int lo, int nk_, bool first, real* wx, real* wy, const D2F& D2) {
   PT_SETUP(d, t, k);
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
-  const bool corners = nk_ > 0;
+  // reads at (i-1, j), (i, j), (i, j-1) can only hit a corner block when
+  // i and j are both within one point of the tile's edge rows
+  const bool corners = nk_ > 0 && (i <= s || i >= e + 1) && (j <= js || j >= je + 1);
   auto d2x = [&](int ii, int jj) {
     int si, sj;
     if (corners && copy_corner_x(d, ii, jj, si, sj)) return D2(si, sj);
@@ -250,14 +262,12 @@ __device__ __forceinline__ void deln_flux_point(const Dims& d, const fv3b_metric
     fx_in = i >= s && i < e + 2 && j >= js && j < je + 1;
     fy_in = i >= s && i < e + 1 && j >= js && j < je + 2;
   }
-  if (fx_in) {
-    real v = F2(g.del6_v, i, j) * (d2x(i - 1, j) - d2x(i, j));
-    W3(wx, i, j) = first ? v : -v;
-  }
-  if (fy_in) {
-    real v = F2(g.del6_u, i, j) * (d2y(i, j - 1) - d2y(i, j));
-    W3(wy, i, j) = first ? v : -v;
-  }
+  // both fluxes before either store, so that the shared d2 reads are loaded once
+  real vx = RC(0.0), vy = RC(0.0);
+  if (fx_in) vx = F2(g.del6_v, i, j) * (d2x(i - 1, j) - d2x(i, j));
+  if (fy_in) vy = F2(g.del6_u, i, j) * (d2y(i, j - 1) - d2y(i, j));
+  if (fx_in) W3(wx, i, j) = first ? vx : -vx;
+  if (fy_in) W3(wy, i, j) = first ? vy : -vy;
 }
 
 // DelnFluxNoSG.__call__ (delnflux.py:1156-1207): del-n diffusive fluxes of q
