@@ -154,19 +154,18 @@ inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a
   // inner PPM: fy_mean on [is-3, ie+4] x [js, je+1], fx_mean on [is, ie+1] x [js-3, je+4]
   err = launch_box(Box{s - 3, e + 5, js - 3, je + 5, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
     const idx_t o = idx3(d, t, i, j, k);
-    const bool do_y = j >= js && j < je + 2, do_x = i >= s && i < e + 2;
-    real fy = RC(0.0), fx = RC(0.0);  // both before either store (shared q loads)
-    if (do_y) {
+    if (j >= js && j < je + 2) {
       auto dya = line2<1>(d, g.dya, t, i, j);
       if (i >= s && i <= e) {  // no cube-corner point on this line: plain reads
-        fy = ppm_flux(line3<1>(d, a.q_base, t, i, j, k), dya, a.cry[o], j, js, je, mord_in);
+        a.fy_mean[o] = ppm_flux(line3<1>(d, a.q_base, t, i, j, k), dya, a.cry[o], j, js, je, mord_in);
       } else {
-        fy = ppm_flux(LineQY{d, a.q_base, t, i, j, k}, dya, a.cry[o], j, js, je, mord_in);
+        a.fy_mean[o] = ppm_flux(LineQY{d, a.q_base, t, i, j, k}, dya, a.cry[o], j, js, je, mord_in);
       }
     }
-    if (do_x) fx = ppm_flux(line3<0>(d, a.q_base, t, i, j, k), line2<0>(d, g.dxa, t, i, j), a.crx[o], i, s, e, mord_in);
-    if (do_y) a.fy_mean[o] = fy;
-    if (do_x) a.fx_mean[o] = fx;
+    if (i >= s && i < e + 2) {
+      a.fx_mean[o] = ppm_flux(line3<0>(d, a.q_base, t, i, j, k), line2<0>(d, g.dxa, t, i, j), a.crx[o], i, s, e,
+                              mord_in);
+    }
   });
   if (err != cudaSuccess) return err;
   // q_i (fvtp2d.py:33-47) on [0, n+6) x [js, je+4), q_j (50-60) on [is, ie+4) x [0, n+6)
@@ -191,17 +190,14 @@ inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a
   // outer PPM and final_fluxes (fvtp2d.py:63-93) on [is, ie+1] x [js, je+1]
   return launch_box(Box{s, e + 2, js, je + 2, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
     const idx_t o = idx3(d, t, i, j, k);
-    real fx = RC(0.0), fy = RC(0.0);
     if (j <= je) {
       real xo = ppm_flux(line3<0>(d, a.q_adv_y, t, i, j, k), line2<0>(d, g.dxa, t, i, j), a.crx[o], i, s, e, mord_out);
-      fx = RC(0.5) * (xo + a.fx_mean[o]) * a.x_unit[o];
+      a.fx[o] = RC(0.5) * (xo + a.fx_mean[o]) * a.x_unit[o];
     }
     if (i <= e) {
       real yo = ppm_flux(line3<1>(d, a.q_adv_x, t, i, j, k), line2<1>(d, g.dya, t, i, j), a.cry[o], j, js, je, mord_out);
-      fy = RC(0.5) * (yo + a.fy_mean[o]) * a.y_unit[o];
+      a.fy[o] = RC(0.5) * (yo + a.fy_mean[o]) * a.y_unit[o];
     }
-    if (j <= je) a.fx[o] = fx;
-    if (i <= e) a.fy[o] = fy;
   });
 }
 
