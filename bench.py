@@ -42,6 +42,18 @@ def _env_rank():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(values, dist=None, device="cuda"):
+    """Element-wise maximum of per-rank timings.  Every rank calls it at the
+    same point with the same number of values (one all-reduce)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    import torch
+
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
 def _measured_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -309,13 +321,10 @@ def run_cuda(args):
     e2e_ms = e0.elapsed_time(e1) / e2e_steps
 
     # max over ranks
-    if dist is not None:
-        vals = [results[p]["ms"] for p in precisions] + [e2e_ms]
-        t = torch.tensor(vals, device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        for q, p in enumerate(precisions):
-            results[p]["ms"] = float(t[q])
-        e2e_ms = float(t[-1])
+    vals = max_over_ranks([results[p]["ms"] for p in precisions] + [e2e_ms], dist)
+    for q, p in enumerate(precisions):
+        results[p]["ms"] = vals[q]
+    e2e_ms = vals[-1]
     peak, peak_kind = _measured_peak()
 
     def roof(prec):
@@ -510,10 +519,7 @@ def run_ensemble(args):
     graph = ens.capture(reset=True)
     graph_ms, _, clocks = timed(graph.replay)
     graph_launches = eager_launches  # the graph replays the same kernels
-    if dist is not None:
-        t = torch.tensor([eager_ms, graph_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        eager_ms, graph_ms = float(t[0]), float(t[1])
+    eager_ms, graph_ms = max_over_ranks([eager_ms, graph_ms], dist)
     cells = ens.cell_levels * args.n_split * world
     line = {
         "metric": "ensemble acoustic-substep cell-levels/s", "value": cells / (graph_ms * 1e-3),
