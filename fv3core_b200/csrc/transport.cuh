@@ -232,9 +232,21 @@ __device__ __forceinline__ int nord_at(const real* nord, int k) { return (int)no
 // levels with nord = 0 the compute-domain faces), corner points mapped to
 // their copy sources first (fx_calc_stencil_nord / fy_calc_stencil_nord,
 // delnflux.py:183-233).  D2(i, j) gives d2 at a point.
+// DelnFlux's final step (add_diffusive_component / diffusive_damp,
+// delnflux.py:276-294) done by the pass that produces the final fluxes:
+// fx += fx2 (or 0.5 damp (mass(i-1) + mass(i)) fx2) on [is, ie+1] x
+// [js, je+1].  Points of that box the final pass does not compute take the
+// value the flux buffer already holds, as the separate stencil would.
+struct DelnCombine {
+  real* fx = nullptr;  // nullptr: no combine (DelnFluxNoSG)
+  real* fy = nullptr;
+  const real* mass = nullptr;
+};
+
 template <typename D2F>
 __device__ __forceinline__ void deln_flux_point(const Dims& d, const fv3b_metrics& g, int t, int i, int j, int k,
-                                                int lo, int nk_, bool first, real* wx, real* wy, const D2F& D2) {
+                                                int lo, int nk_, bool first, real* wx, real* wy, const D2F& D2,
+                                                const DelnCombine& cb = DelnCombine{}, const real* damp = nullptr) {
   PT_SETUP(d, t, k);
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
   // reads at (i-1, j), (i, j), (i, j-1) can only hit a corner block when
@@ -262,8 +274,22 @@ __device__ __forceinline__ void deln_flux_point(const Dims& d, const fv3b_metric
   real vx = RC(0.0), vy = RC(0.0);
   if (fx_in) vx = F2(g.del6_v, i, j) * (d2x(i - 1, j) - d2x(i, j));
   if (fy_in) vy = F2(g.del6_u, i, j) * (d2y(i, j - 1) - d2y(i, j));
-  if (fx_in) W3(wx, i, j) = first ? vx : -vx;
-  if (fy_in) W3(wy, i, j) = first ? vy : -vy;
+  if (cb.fx == nullptr) {
+    if (fx_in) W3(wx, i, j) = first ? vx : -vx;
+    if (fy_in) W3(wy, i, j) = first ? vy : -vy;
+    return;
+  }
+  if (!(i >= s && i < e + 2 && j >= js && j < je + 2)) return;
+  const real fx2 = fx_in ? (first ? vx : -vx) : F3(wx, i, j);
+  const real fy2 = fy_in ? (first ? vy : -vy) : F3(wy, i, j);
+  if (cb.mass == nullptr) {
+    W3(cb.fx, i, j) = F3(cb.fx, i, j) + fx2;
+    W3(cb.fy, i, j) = F3(cb.fy, i, j) + fy2;
+  } else {
+    const real dk = damp[k];
+    W3(cb.fx, i, j) = F3(cb.fx, i, j) + RC(0.5) * dk * (F3(cb.mass, i - 1, j) + F3(cb.mass, i, j)) * fx2;
+    W3(cb.fy, i, j) = F3(cb.fy, i, j) + RC(0.5) * dk * (F3(cb.mass, i, j - 1) + F3(cb.mass, i, j)) * fy2;
+  }
 }
 
 // DelnFluxNoSG.__call__ (delnflux.py:1156-1207): del-n diffusive fluxes of q
@@ -285,7 +311,7 @@ __device__ __forceinline__ void deln_flux_point(const Dims& d, const fv3b_metric
 // on npz + 1 interface levels).
 inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const real* q, real* fx2, real* fy2,
                                  DelnCol col, real* ax, real* ay, bool mass_weighted, int nmax, cudaStream_t st,
-                                 int nlev = -1) {
+                                 int nlev = -1, DelnCombine cb = DelnCombine{}) {
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = nlev < 0 ? d.nz : nlev;
   // pass p writes (fx2, fy2) when nmax - p is even, so the last pass does
   auto out_x = [&](int p) { return ((nmax - p) % 2 == 0) ? fx2 : ax; };
@@ -303,8 +329,12 @@ inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const real*
                                      const real qv = q[b3 + jj * d.sj + ii];
                                      return mass_weighted ? qv : damp * qv;
                                    };
-                                   deln_flux_point(d, g, t, i, j, k, lo, nk_, true, nk_ > 0 ? wx : fx2,
-                                                   nk_ > 0 ? wy : fy2, D2);
+                                   // levels with nord = 0 (all levels when nmax = 0)
+                                   // end here: combine now if asked
+                                   if (nk_ > 0)
+                                     deln_flux_point(d, g, t, i, j, k, lo, nk_, true, wx, wy, D2);
+                                   else
+                                     deln_flux_point(d, g, t, i, j, k, lo, nk_, true, fx2, fy2, D2, cb, col.damp);
                                  });
     if (err != cudaSuccess) return err;
   }
@@ -325,7 +355,10 @@ inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const real*
                                      return (px[o] - px[o + 1] + py[o] - py[o + d.sj]) *
                                             g.rarea[b2 + jj * d.sj + ii] * col.rscale;
                                    };
-                                   deln_flux_point(d, g, t, i, j, k, lo, nk_, false, wx, wy, D2);
+                                   if (p == nmax)
+                                     deln_flux_point(d, g, t, i, j, k, lo, nk_, false, wx, wy, D2, cb, col.damp);
+                                   else
+                                     deln_flux_point(d, g, t, i, j, k, lo, nk_, false, wx, wy, D2);
                                  });
     if (err != cudaSuccess) return err;
   }
@@ -336,20 +369,11 @@ inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const real*
 // the cell corners of the compute domain.
 inline cudaError_t delnflux(const Dims d, const fv3b_metrics g, const real* q, real* fx, real* fy, DelnCol col,
                            const real* mass, real* fx2, real* fy2, real* ax, real* ay, int nmax, cudaStream_t st) {
-  cudaError_t err = delnflux_nosg(d, g, q, fx2, fy2, col, ax, ay, mass != nullptr, nmax, st);
-  if (err != cudaSuccess) return err;
-  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
-  return launch_box(Box{s, e + 2, js, je + 2, 0, d.nz}, st, [=] __device__(int t, int i, int j, int k) {
-    PT_SETUP(d, t, k);
-    if (mass == nullptr) {
-      W3(fx, i, j) = F3(fx, i, j) + F3(fx2, i, j);
-      W3(fy, i, j) = F3(fy, i, j) + F3(fy2, i, j);
-    } else {
-      real dk = col.damp[k];
-      W3(fx, i, j) = F3(fx, i, j) + RC(0.5) * dk * (F3(mass, i - 1, j) + F3(mass, i, j)) * F3(fx2, i, j);
-      W3(fy, i, j) = F3(fy, i, j) + RC(0.5) * dk * (F3(mass, i, j - 1) + F3(mass, i, j)) * F3(fy2, i, j);
-    }
-  });
+  DelnCombine cb;
+  cb.fx = fx;
+  cb.fy = fy;
+  cb.mass = mass;
+  return delnflux_nosg(d, g, q, fx2, fy2, col, ax, ay, mass != nullptr, nmax, st, -1, cb);
 }
 
 

@@ -143,15 +143,15 @@ extern "C" int fv3b_update_dz_d(fv3b_ctx* ctx, const real* zs, real* zh, const r
   const real* beta = colp(ctx, COL_SPLINE_BETA);
   const real* gamma = colp(ctx, COL_SPLINE_GAMMA);
   // cubic_spline_interpolation_from_layer_center_to_interfaces
-  // (updatedzd.py:148-186) of the four flux fields over the full domain
-  FV3B_CHECK(launch_columns(0, full, 0, full, st, [=] __device__(int t, int i, int j) {
-    const real* src[4] = {crx, xfx, cry, yfx};
-    real* dst[4] = {crx_i, xfx_i, cry_i, yfx_i};
-    const idx_t o0 = idx3(d, t, i, j, 0);
+  // (updatedzd.py:148-186) of the four flux fields over the full domain;
+  // one thread per (field, column): the launch's i index runs over the four
+  // fields' column rows in turn, f = i / full
+  FV3B_CHECK(launch_columns(0, 4 * full, 0, full, st, [=] __device__(int t, int fi, int j) {
+    const int f = fi / full, i = fi % full;
+    const real* q = (f == 0 ? crx : f == 1 ? xfx : f == 2 ? cry : yfx) + idx3(d, t, i, j, 0);
+    real* out = (f == 0 ? crx_i : f == 1 ? xfx_i : f == 2 ? cry_i : yfx_i) + idx3(d, t, i, j, 0);
     const idx_t sk = d.sk;
-    for (int f = 0; f < 4; ++f) {
-      const real* q = src[f] + o0;
-      real* out = dst[f] + o0;
+    {
       real xt1 = RC(2.0) * gk[0] * (gk[0] + RC(1.0));
       real prev = (xt1 * q[0] + q[sk]) / beta[0];
       out[0] = prev;
