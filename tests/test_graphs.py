@@ -117,10 +117,10 @@ def test_ensemble_graph_matches_members_eager():
 def test_streamed_round_trips_match_sequential_calls():
     """StreamedAcoustics overlaps the copies of one state with the call on
     another; each host state must come back exactly as from a plain
-    copy-in / call / copy-out.  Both runs follow the same previous call:
-    like the reference's, the driver's temporaries keep values between
-    calls at points a call does not rewrite, so a call's result depends on
-    the call before it."""
+    copy-in / call / copy-out.  Both runs start from a fresh context and make
+    the same calls in the same order: like the reference's, the driver's
+    heat_source temporary accumulates over calls, so a call's pt depends on
+    every call before it."""
     import types
 
     import torch
@@ -131,37 +131,31 @@ def test_streamed_round_trips_match_sequential_calls():
 
     fields = cases.ACOUSTIC_STATE
     cases_in = [cases.acoustics_case(12, 8, seed, n_split=2) for seed in (31, 32, 33)]
-    gd, ad, st = gpu_runs.make_acoustics(cases_in[0], 12, 8)
-    ad(st)  # per-level factors
-    torch.cuda.synchronize()
+    gd_a, ad_a, st_a = gpu_runs.make_acoustics(cases_in[0], 12, 8)
     batches, expected = [], []
     for case in cases_in:
         host_in = {}
         for k in fields:
-            t = torch.from_numpy(np.ascontiguousarray(case[k].transpose(0, 3, 2, 1) if case[k].ndim == 4
-                                                      else case[k].transpose(0, 2, 1)))
-            host_in[k] = t.to(getattr(st, k).dtype).pin_memory()
+            a = case[k]
+            t = torch.from_numpy(np.ascontiguousarray(a.transpose(0, 3, 2, 1) if a.ndim == 4 else a.transpose(0, 2, 1)))
+            host_in[k] = t.to(getattr(st_a, k).dtype).pin_memory()
         host_out = {k: torch.empty_like(host_in[k]).pin_memory() for k in fields}
         batches.append((host_in, host_out))
-        # sequential reference
-        for k in fields:
-            getattr(st, k).copy_(host_in[k])
-        ad(st)
+        for k in fields:  # sequential: copy in, call, read back
+            getattr(st_a, k).copy_(host_in[k])
+        ad_a(st_a)
         torch.cuda.synchronize()
-        expected.append({k: getattr(st, k).cpu().clone() for k in fields})
-    # the same history as the sequential run: one call on the first case
-    for k in fields:
-        getattr(st, k).copy_(batches[0][0][k])
-    ad(st)
-    torch.cuda.synchronize()
-    st2 = types.SimpleNamespace(**vars(st))
+        expected.append({k: getattr(st_a, k).cpu().clone() for k in fields})
+    gd_a.close()
+    gd_b, ad_b, st_b = gpu_runs.make_acoustics(cases_in[0], 12, 8)
+    st_b2 = types.SimpleNamespace(**vars(st_b))
     for k in _lib.DYCORE_FIELDS:
-        setattr(st2, k, getattr(st, k).clone())
-    streamed = StreamedAcoustics(ad, [st, st2], fields, fields)
+        setattr(st_b2, k, getattr(st_b, k).clone())
+    streamed = StreamedAcoustics(ad_b, [st_b, st_b2], fields, fields)
     streamed.run(batches)
     streamed.synchronize()
     for (host_in, host_out), exp in zip(batches, expected):
         for k in fields:
             np.testing.assert_array_equal(np.nan_to_num(host_out[k].numpy(), nan=7.0),
                                           np.nan_to_num(exp[k].numpy(), nan=7.0), err_msg=k)
-    gd.close()
+    gd_b.close()
