@@ -26,6 +26,14 @@ constexpr double RGRAV = 1.0 / GRAV;
 constexpr double KAPPA = RDGAS / 1004.6;
 constexpr int MAXK = 128;
 
+// Requests the 128-byte line holding *p into L2 (PTX prefetch): the column
+// loops walk the levels one after another, so each loop asks for the inputs
+// a few levels ahead while it works on the current one.
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+constexpr int PF_AHEAD = 3;
+
 // Per-column inputs of the Sim1 solve (fv3core/stencils/sim1_solver.py:11-101).
 // K = number of interface levels (npz + 1).  DM(k): delta p / g; DP(k):
 // delta p, whose running sums from ptop are the edge pressures pem; W1(k): w
@@ -34,11 +42,11 @@ constexpr int MAXK = 128;
 // delivered through PE_OUT(k, value) in increasing k) and the new layer
 // depths through DZ_OUT(k, value) for k = K-2 .. 0 (bottom up).
 template <int NK, typename DMF, typename DPF, typename W1F, typename DZF, typename GMF, typename PTRF,
-          typename CP3F, typename PEOUT, typename DZOUT>
+          typename CP3F, typename PEOUT, typename DZOUT, typename PFF>
 __device__ __forceinline__ void sim1_column(int K, DMF DM, DPF DP, double ptop, W1F W1, DZF DZ, GMF GM, PTRF PTR,
                                             CP3F CP3, const double* pm, double* pp, double* gam, double* w,
                                             double wsr, double dt, double t1g, double rdt, double p_fac,
-                                            PEOUT PE_OUT, DZOUT DZ_OUT) {
+                                            PEOUT PE_OUT, DZOUT DZ_OUT, PFF PF) {
   // pe = exp(gm*log(-dm/dz*Rd*ptr)) - pm   (sim1_solver.py:27-29), on the fly
   auto pe1 = [&](int k) { return fm::fm_exp(GM(k) * fm::fm_log(-DM(k) / DZ(k) * RDGAS * PTR(k))) - pm[k]; };
   // forward elimination of the pressure system (sim1_solver.py:30-59)
@@ -49,6 +57,7 @@ __device__ __forceinline__ void sim1_column(int K, DMF DM, DPF DP, double ptop, 
   pp[1] = (K > 2 ? 3.0 * (pe_k + (DM(0) / DM(1)) * pe_k1) : 3.0 * pe_k) / bb0;
   double bet = bb0;
   for (int k = 1; k <= K - 2; ++k) {
+    PF(k + 1 + PF_AHEAD);
     pe_k = pe_k1;
     double grm = DM(k - 1) / DM(k);
     double g = grm / bet;
@@ -78,7 +87,10 @@ __device__ __forceinline__ void sim1_column(int K, DMF DM, DPF DP, double ptop, 
   double aak = AA(1, pem_run);
   bet = DM(0) - aak;
   w[0] = (DM(0) * W1(0) + dt * pp[1]) / bet;
+  PF(1);
+  PF(2);
   for (int k = 1; k <= K - 3; ++k) {
+    PF(k + 1 + PF_AHEAD);
     pem_run = pem_run + DP(k);  // pem[k + 1]
     double aak1 = AA(k + 1, pem_run);
     double g = aak / bet;
@@ -102,13 +114,17 @@ __device__ __forceinline__ void sim1_column(int K, DMF DM, DPF DP, double ptop, 
   double* pe = pp;
   pe[0] = 0.0;
   PE_OUT(0, 0.0);
+  PF(0);
+  PF(1);
   for (int k = 1; k < K; ++k) {
+    PF(k + PF_AHEAD);
     pe[k] = pe[k - 1] + DM(k - 1) * (w[k - 1] - W1(k - 1)) * rdt;
     PE_OUT(k, pe[k]);
   }
   // layer-mean perturbation and new dz (sim1_solver.py:96-105), bottom up
   double p1n = 0.0;
   for (int k = K - 2; k >= 0; --k) {
+    PF(k - PF_AHEAD);
     double p1;
     if (k == K - 2) {
       p1 = (pe[k] + 2.0 * pe[k + 1]) * 1.0 / 3.0;
@@ -148,6 +164,10 @@ struct RiemC {
     // running sums rebuilt where they are used
     double peg_k = ptop;
     for (int k = 0; k < K - 1; ++k) {
+      if (k + PF_AHEAD < K) {
+        prefetch_l2(delpc + o0 + (k + PF_AHEAD) * sk);
+        prefetch_l2(q_con + o0 + (k + PF_AHEAD) * sk);
+      }
       const double dmk = __ldg(&delpc[o0 + k * sk]);
       const double peg_next = peg_k + dmk * (1.0 - __ldg(&q_con[o0 + k * sk]));
       pm[k] = (peg_next - peg_k) / fm::fm_log(peg_next / peg_k);
@@ -173,8 +193,17 @@ struct RiemC {
       g = g - dz * GRAV;
       gz[o0 + k * sk] = g;
     };
+    auto PF = [&](int k) {
+      if (k < 0 || k >= K) return;
+      const idx_t o = o0 + k * sk;
+      prefetch_l2(delpc + o);
+      prefetch_l2(gz + o);
+      prefetch_l2(cappa + o);
+      prefetch_l2(ptc + o);
+      prefetch_l2(w3 + o);
+    };
     sim1_column<NK>(K, DM, DP, ptop, W1, DZ, GM, PTR, CP3, pm, pp, gam, w, ws[idx2(d, t, i, j)], dt2, t1g, rdt,
-                    p_fac, PE_OUT, DZ_OUT);
+                    p_fac, PE_OUT, DZ_OUT, PF);
   }
 };
 
@@ -213,6 +242,10 @@ struct Riem3 {
     }
     for (int k = 0; k < K - 1; ++k) {
       const idx_t o = o0 + k * sk;
+      if (k + PF_AHEAD < K) {
+        prefetch_l2(delp + o + PF_AHEAD * sk);
+        prefetch_l2(q_con + o + PF_AHEAD * sk);
+      }
       const double dmk = delp[o];
       const double pem_n = pem_k + dmk;
       const double peg_n = peg_k + dmk * (1.0 - q_con[o]);
@@ -247,8 +280,17 @@ struct Riem3 {
       z = z - dz;
       zh[o0 + k * sk] = z;
     };
+    auto PF = [&](int k) {
+      if (k < 0 || k >= K) return;
+      const idx_t o = o0 + k * sk;
+      prefetch_l2(delp + o);
+      prefetch_l2(zh + o);
+      prefetch_l2(cappa + o);
+      prefetch_l2(pt + o);
+      prefetch_l2(w_io + o);
+    };
     sim1_column<NK>(K, DM, DP, ptop, W1, DZ, GM, PTR, CP3, pm, pp, gam, w, wsd[idx2(d, t, i, j)], dt, t1g, rdt,
-                    p_fac, PE_OUT, DZ_OUT);
+                    p_fac, PE_OUT, DZ_OUT, PF);
     for (int k = 0; k < K - 1; ++k) w_io[o0 + k * sk] = w[k];
   }
 };
