@@ -197,6 +197,12 @@ def _max_rel(a, b, n, npz):
     return float((torch.abs(a - b) / torch.clamp(torch.abs(b), min=1e-30)).max())
 
 
+def _rms_rel(a, b, n, npz):
+    """RMS of the difference over RMS of the reference, compute domain."""
+    a, b = _compute(a, n, npz).double(), _compute(b, n, npz).double()
+    return float(((a - b) ** 2).mean().sqrt() / (b ** 2).mean().sqrt())
+
+
 def run_cuda(args):
     import torch
 
@@ -253,8 +259,9 @@ def run_cuda(args):
         problems["f32"][1](s32)
         problems["f64"][1](s64)
         barrier()
-        ref = {k: getattr(s64, k).clone() for k in fields}
+        ref = {k: getattr(s64, k).clone() for k in fields + ("u", "v", "w")}
         mixed = {k: _max_rel(getattr(s32, k), ref[k], n, npz) for k in fields}
+        mixed_rms = {k: _rms_rel(getattr(s32, k), ref[k], n, npz) for k in fields + ("u", "v", "w")}
         for k, t in initial["f64"].items():
             getattr(s64, k).copy_(t.float())
         problems["f64"][1](s64)
@@ -263,10 +270,10 @@ def run_cuda(args):
         arith = {k: _max_rel(getattr(s32, k), getattr(s64, k), n, npz) for k in fields}
         del ref
         mixed_error = {
-            "mixed_vs_fp64": mixed, "fp64_from_fp32_rounded_input_vs_fp64": floor,
+            "mixed_vs_fp64": mixed, "mixed_vs_fp64_rms": mixed_rms, "fp64_from_fp32_rounded_input_vs_fp64": floor,
             "mixed_vs_fp64_from_same_input": arith,
             "after": "one AcousticDynamics call (n_split acoustic substeps) from the same state; max relative "
-                     "error over the compute domain",
+                     "error over the compute domain (rms: RMS difference over RMS of the FP64 field)",
         }
 
     results = {}

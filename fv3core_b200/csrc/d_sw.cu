@@ -448,7 +448,9 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, real* delpc, real* delp, real* ptc, real
                          real* w, real* uc, real* vc, const real* ua, const real* va, real* divgd,
                          real* mfx, real* mfy, real* cx, real* cy, real* crx, real* cry, real* xfx,
                          real* yfx, real* q_con, const real* zh, real* heat_source, real* diss_est,
-                         double dt, void* stream) {
+                         double dt_in, void* stream) {
+  // the build's precision inside the kernels (the same value in FP64 builds)
+  const real dt = static_cast<real>(dt_in);
   FV3B_REQUIRE(ctx && delpc && delp && ptc && pt && u && v && w && uc && vc && ua && va && divgd && mfx && mfy &&
                    cx && cy && crx && cry && xfx && yfx && q_con && zh && heat_source && diss_est,
                "fv3b_d_sw: null argument");

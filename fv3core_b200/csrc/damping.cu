@@ -117,7 +117,9 @@ extern "C" int fv3b_ray_fast(fv3b_ctx* ctx, real* u, real* v, real* w, const dou
 // compute domain plus nt = ntimes-1-n halo rows.  The reference's corner
 // copies of its scratch q (copy_corners_x before the x fluxes, _y before
 // the y fluxes and the copy back) are reads through the corner rules.
-extern "C" int fv3b_del2cubed(fv3b_ctx* ctx, real* qdel, double cd, int nmax, void* stream) {
+extern "C" int fv3b_del2cubed(fv3b_ctx* ctx, real* qdel, double cd_in, int nmax, void* stream) {
+  // the build's precision inside the kernels (the same value in FP64 builds)
+  const real cd = static_cast<real>(cd_in);
   FV3B_REQUIRE(ctx && qdel, "fv3b_del2cubed: null argument");
   const Dims d = ctx->d;
   const fv3b_metrics g = ctx->m;
@@ -186,8 +188,10 @@ extern "C" int fv3b_del2cubed(fv3b_ctx* ctx, real* qdel, double cd, int nmax, vo
 // compute_pkz_tempadjust (temperature_adjust.py:8-44) on the compute domain,
 // levels [0, nk_heat).
 extern "C" int fv3b_pkz_tempadjust(fv3b_ctx* ctx, const real* delp, const real* delz, const real* cappa,
-                                   const real* heat_source, real* pt, real* pkz, double delt_time_factor,
+                                   const real* heat_source, real* pt, real* pkz, double delt_time_factor_in,
                                    int nk_heat, void* stream) {
+  // the build's precision inside the kernels (the same value in FP64 builds)
+  const real delt_time_factor = static_cast<real>(delt_time_factor_in);
   FV3B_REQUIRE(ctx && delp && delz && cappa && heat_source && pt && pkz, "fv3b_pkz_tempadjust: null argument");
   const Dims d = ctx->d;
   FV3B_REQUIRE(nk_heat >= 0 && nk_heat <= d.nz, "fv3b_pkz_tempadjust: nk_heat out of range");

@@ -64,7 +64,9 @@ cudaError_t scratch_address(real** out) {
 }  // namespace
 
 extern "C" int fv3b_del2cubed_noalloc(const fv3b_grid_dims* dims, const fv3b_metrics* metrics, real* qdel,
-                                      double cd, int nmax, void* stream) {
+                                      double cd_in, int nmax, void* stream) {
+  // the build's precision inside the kernels (the same value in FP64 builds)
+  const real cd = static_cast<real>(cd_in);
   FV3B_REQUIRE(dims && metrics && qdel, "fv3b_del2cubed_noalloc: null argument");
   FV3B_REQUIRE(dims->npx >= 4 && dims->n_halo == 3 && dims->npz >= 1,
                "fv3b_del2cubed_noalloc: need npx >= 4, n_halo == 3, npz >= 1");

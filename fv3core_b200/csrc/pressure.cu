@@ -15,7 +15,9 @@ using namespace fv3b;
 
 // p_grad_c_stencil, nonhydrostatic (wk = delpc), on [is, ie+1] x [js, je+1].
 extern "C" int fv3b_p_grad_c(fv3b_ctx* ctx, real* uc, real* vc, const real* delpc, const real* pkc,
-                             const real* gz, double dt2, void* stream) {
+                             const real* gz, double dt2_in, void* stream) {
+  // the build's precision inside the kernels (the same value in FP64 builds)
+  const real dt2 = static_cast<real>(dt2_in);
   FV3B_REQUIRE(ctx && uc && vc && delpc && pkc && gz, "fv3b_p_grad_c: null argument");
   const Dims d = ctx->d;
   const fv3b_metrics g = ctx->m;
@@ -39,7 +41,9 @@ extern "C" int fv3b_p_grad_c(fv3b_ctx* ctx, real* uc, real* vc, const real* delp
 // the B-grid delp goes to scratch.  set_k0_and_calc_wk is folded into the
 // wind update: level 0 of pp and pk3 is read as its new value (0, ptop^akap).
 extern "C" int fv3b_nh_p_grad(fv3b_ctx* ctx, real* u, real* v, real* pp, real* gz, real* pk3,
-                              real* delp, double dt, double ptop, double akap, void* stream) {
+                              real* delp, double dt_in, double ptop, double akap, void* stream) {
+  // the build's precision inside the kernels (the same value in FP64 builds)
+  const real dt = static_cast<real>(dt_in);
   FV3B_REQUIRE(ctx && u && v && pp && gz && pk3 && delp, "fv3b_nh_p_grad: null argument");
   const Dims d = ctx->d;
   const fv3b_metrics g = ctx->m;
@@ -51,7 +55,7 @@ extern "C" int fv3b_nh_p_grad(fv3b_ctx* ctx, real* u, real* v, real* pp, real* g
   // reference's copy passes.
   real *wk1 = ctx->ws[0], *qx = ctx->ws[1], *qy = ctx->ws[2], *edges = ctx->ws[3];
   real *pp_b = ctx->ws[4], *pk3_b = ctx->ws[5], *gz_b = ctx->ws[6];
-  const double ptk = pow(ptop, akap);
+  const real ptk = static_cast<real>(pow(ptop, akap));
   FV3B_CHECK(a2b_ord4(d, g, pp, pp_b, qx, qy, edges, 1, nk, st, false));
   FV3B_CHECK(a2b_ord4(d, g, pk3, pk3_b, qx, qy, edges, 1, nk, st, false));
   FV3B_CHECK(a2b_ord4(d, g, gz, gz_b, qx, qy, edges, 0, nk, st, false));

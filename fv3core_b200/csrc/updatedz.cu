@@ -39,7 +39,9 @@ __device__ __forceinline__ real p_weighted(const real* dp0, int k, int nk, real 
 
 // UpdateGeopotentialHeightOnCGrid.__call__ (updatedzc.py:123-163).
 extern "C" int fv3b_update_dz_c(fv3b_ctx* ctx, const real* dp_ref, const real* zs, const real* ut,
-                                const real* vt, real* gz, real* ws, double dt, void* stream) {
+                                const real* vt, real* gz, real* ws, double dt_in, void* stream) {
+  // the build's precision inside the kernels (the same value in FP64 builds)
+  const real dt = static_cast<real>(dt_in);
   FV3B_REQUIRE(ctx && dp_ref && zs && ut && vt && gz && ws, "fv3b_update_dz_c: null argument");
   const Dims d = ctx->d;
   const fv3b_metrics g = ctx->m;
@@ -127,7 +129,9 @@ extern "C" int fv3b_update_dz_d_setup(fv3b_ctx* ctx, const double* dp_ref_host, 
 
 // UpdateHeightOnDGrid.__call__ (updatedzd.py:323-393).
 extern "C" int fv3b_update_dz_d(fv3b_ctx* ctx, const real* zs, real* zh, const real* crx, const real* cry,
-                                const real* xfx, const real* yfx, real* wsd, double dt, void* stream) {
+                                const real* xfx, const real* yfx, real* wsd, double dt_in, void* stream) {
+  // the build's precision inside the kernels (the same value in FP64 builds)
+  const real dt = static_cast<real>(dt_in);
   FV3B_REQUIRE(ctx && zs && zh && crx && cry && xfx && yfx && wsd, "fv3b_update_dz_d: null argument");
   FV3B_REQUIRE(ctx->dzd_ready, "fv3b_update_dz_d: call fv3b_update_dz_d_setup first");
   const Dims d = ctx->d;
