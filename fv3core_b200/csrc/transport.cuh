@@ -292,6 +292,87 @@ __device__ __forceinline__ void deln_flux_point(const Dims& d, const fv3b_metric
   }
 }
 
+// A later del-n pass (p >= 1) as a tiled kernel: a 32 x 4 block of one
+// level computes the d2 values its fluxes read (its own points plus the row
+// below and the column to the left) once into shared memory, instead of
+// each thread recomputing three of them.  Blocks that touch a cube-corner
+// zone take the per-point path (corner sources may lie outside the tile).
+// Same operations in the same order either way.
+struct DelnIterArgs {
+  Dims d;
+  fv3b_metrics g;
+  DelnCol col;
+  const real* px;
+  const real* py;
+  real* wx;
+  real* wy;
+  DelnCombine cb;
+  int lo, i0, i1, j0, j1, nlev;
+  bool final_pass;
+};
+
+constexpr int DELN_TX = 32, DELN_TY = 4;
+
+static __global__ void __launch_bounds__(DELN_TX* DELN_TY) deln_iter_kernel(const DelnIterArgs a) {
+  __shared__ real sd2[DELN_TY + 1][DELN_TX + 1];  // rows jb-1.., columns ib-1..
+  const Dims& d = a.d;
+  const int t = blockIdx.z / a.nlev, k = blockIdx.z % a.nlev;
+  const int nk_ = nord_at(a.col.nord, k);
+  if (nk_ == 0) return;  // whole block: one level
+  const int ib = a.i0 + blockIdx.x * DELN_TX, jb = a.j0 + blockIdx.y * DELN_TY;
+  const int i = ib + threadIdx.x, j = jb + threadIdx.y;
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
+  const idx_t b3 = t * d.st + k * d.sk, b2 = t * d.st2;
+  auto D2 = [&](int ii, int jj) {
+    const idx_t o = b3 + jj * d.sj + ii;
+    return (a.px[o] - a.px[o + 1] + a.py[o] - a.py[o + d.sj]) * a.g.rarea[b2 + jj * d.sj + ii] * a.col.rscale;
+  };
+  const bool near_corner = (ib <= s || ib + DELN_TX - 1 >= e + 1) && (jb <= js || jb + DELN_TY - 1 >= je + 1);
+  if (near_corner) {
+    if (i < a.i1 && j < a.j1) {
+      if (a.final_pass)
+        deln_flux_point(d, a.g, t, i, j, k, a.lo, nk_, false, a.wx, a.wy, D2, a.cb, a.col.damp);
+      else
+        deln_flux_point(d, a.g, t, i, j, k, a.lo, nk_, false, a.wx, a.wy, D2);
+    }
+    return;
+  }
+  // d2 at points whose four flux reads stay inside the arrays; others unused
+  auto D2_safe = [&](int ii, int jj) {
+    return (ii >= 0 && jj >= 0 && ii + 1 < d.ni && jj + 1 < d.nj) ? D2(ii, jj) : RC(0.0);
+  };
+  sd2[threadIdx.y + 1][threadIdx.x + 1] = D2_safe(i, j);
+  if (threadIdx.y == 0) sd2[0][threadIdx.x + 1] = D2_safe(i, jb - 1);
+  if (threadIdx.x == 0) sd2[threadIdx.y + 1][0] = D2_safe(ib - 1, j);
+  __syncthreads();
+  if (!(i < a.i1 && j < a.j1)) return;
+  PT_SETUP(d, t, k);
+  const int lo = a.lo;
+  const bool fx_in = i >= s - lo && i < e + 2 + lo && j >= js - lo && j < je + 1 + lo;
+  const bool fy_in = i >= s - lo && i < e + 1 + lo && j >= js - lo && j < je + 2 + lo;
+  const real d2c = sd2[threadIdx.y + 1][threadIdx.x + 1];
+  real vx = RC(0.0), vy = RC(0.0);
+  if (fx_in) vx = F2(a.g.del6_v, i, j) * (sd2[threadIdx.y + 1][threadIdx.x] - d2c);
+  if (fy_in) vy = F2(a.g.del6_u, i, j) * (sd2[threadIdx.y][threadIdx.x + 1] - d2c);
+  const DelnCombine& cb = a.cb;
+  if (!a.final_pass || cb.fx == nullptr) {
+    if (fx_in) W3(a.wx, i, j) = -vx;
+    if (fy_in) W3(a.wy, i, j) = -vy;
+    return;
+  }
+  if (!(i >= s && i < e + 2 && j >= js && j < je + 2)) return;
+  const real fx2 = fx_in ? -vx : F3(a.wx, i, j);
+  const real fy2 = fy_in ? -vy : F3(a.wy, i, j);
+  if (cb.mass == nullptr) {
+    W3(cb.fx, i, j) = F3(cb.fx, i, j) + fx2;
+    W3(cb.fy, i, j) = F3(cb.fy, i, j) + fy2;
+  } else {
+    const real dk = a.col.damp[k];
+    W3(cb.fx, i, j) = F3(cb.fx, i, j) + RC(0.5) * dk * (F3(cb.mass, i - 1, j) + F3(cb.mass, i, j)) * fx2;
+    W3(cb.fy, i, j) = F3(cb.fy, i, j) + RC(0.5) * dk * (F3(cb.mass, i, j - 1) + F3(cb.mass, i, j)) * fy2;
+  }
+}
+
 // DelnFluxNoSG.__call__ (delnflux.py:1156-1207): del-n diffusive fluxes of q
 // into fx2/fy2.  Corner copies of d2 are applied on read (a point of a
 // corner block reads its copy source), which gives the values the reference
@@ -343,23 +424,12 @@ inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const real*
   // (fx/fy_calc_stencil_column)
   for (int p = 1; p <= nmax; ++p) {
     const int lo = nmax - p;
-    const real *px = out_x(p - 1), *py = out_y(p - 1);
-    real *wx = out_x(p), *wy = out_y(p);
-    cudaError_t err = launch_box(Box{s - lo, e + 2 + lo, js - lo, je + 2 + lo, 0, nz}, st,
-                                 [=] __device__(int t, int i, int j, int k) {
-                                   const int nk_ = nord_at(col.nord, k);
-                                   if (nk_ == 0) return;
-                                   const idx_t b3 = t * d.st + k * d.sk, b2 = t * d.st2;
-                                   auto D2 = [&](int ii, int jj) {
-                                     const idx_t o = b3 + jj * d.sj + ii;
-                                     return (px[o] - px[o + 1] + py[o] - py[o + d.sj]) *
-                                            g.rarea[b2 + jj * d.sj + ii] * col.rscale;
-                                   };
-                                   if (p == nmax)
-                                     deln_flux_point(d, g, t, i, j, k, lo, nk_, false, wx, wy, D2, cb, col.damp);
-                                   else
-                                     deln_flux_point(d, g, t, i, j, k, lo, nk_, false, wx, wy, D2);
-                                 });
+    DelnIterArgs a{d, g, col, out_x(p - 1), out_y(p - 1), out_x(p), out_y(p), cb,
+                   lo, s - lo, e + 2 + lo, js - lo, je + 2 + lo, nz, p == nmax};
+    const dim3 grid((a.i1 - a.i0 + DELN_TX - 1) / DELN_TX, (a.j1 - a.j0 + DELN_TY - 1) / DELN_TY, 6 * nz);
+    deln_iter_kernel<<<grid, dim3(DELN_TX, DELN_TY, 1), 0, st>>>(a);
+    note_launch();
+    cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return err;
   }
   return cudaSuccess;
