@@ -9,9 +9,17 @@ the whole cube, on a Jablonowski-Williamson baroclinic-wave state with seeded
 noise (synthetic data).  ``value`` is cell-levels advanced per second per
 substep (6 * 384^2 * 79 cell-levels x n_split per step), device-timed with
 CUDA events, inputs resident in HBM (every 3-D field is 0.59 GB, far larger
-than the 126 MB L2, so no flush is needed).  ``e2e`` times the same call
-through the package's public API with the state copied in from pinned host
-memory and the results copied back every step.
+than the 126 MB L2, so no flush is needed); every step restarts from the
+initial state (a device-to-device copy outside the step's events).  ``e2e``
+times the same call through the package's public API with the state copied
+in from pinned host memory and the results copied back every step, streamed
+(two device states, the copies of one step overlapping the call of another;
+``e2e.sequential`` is the one-stream loop).  ``roofline.traffic`` is the DRAM
+traffic of a call as measured by ncu.
+
+``--workload ensemble`` times the mixed-resolution ensemble (16 x C48 L79,
+8 x C96 L79, 4 x C192 L63), one CUDA graph per ensemble step against eager
+launches.
 
 Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
 N > 1 runs under torch.distributed.run: every rank advances its own replica

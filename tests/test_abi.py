@@ -49,6 +49,22 @@ def test_version_and_error_reporting_without_gpu():
     assert rc == 1 and b"null argument" in L.fv3b_last_error()
 
 
+def test_oversized_grid_is_rejected_before_any_cuda_call():
+    import ctypes
+
+    from fv3core_b200 import _lib
+
+    L = _lib.lib()
+    L.fv3b_ctx_create.argtypes = [ctypes.POINTER(_lib.GridDims), ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    L.fv3b_ctx_create.restype = ctypes.c_int
+    # a 3-D field of 6 x 126 x 4103^2 elements does not fit 32-bit offsets
+    dims = _lib.GridDims(4096, 3, 125, 0)
+    metrics = ctypes.create_string_buffer(4096)
+    out = ctypes.c_void_p()
+    rc = L.fv3b_ctx_create(ctypes.byref(dims), metrics, ctypes.byref(out))
+    assert rc == 1 and b"2^31" in L.fv3b_last_error()
+
+
 def test_launch_shape_setting_without_gpu():
     from fv3core_b200 import _lib
 
