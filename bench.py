@@ -597,6 +597,75 @@ def run_ensemble(args):
         dist.destroy_process_group()
 
 
+def run_adjoint(args):
+    """Cost of the hand-written adjoint of RiemannSolver3 (the stage of the
+    acoustic substep that has one): forward alone against forward + backward
+    through torch autograd, C48 L79 FP64 by default."""
+    import numpy as np
+    import torch
+
+    from fv3core_b200.adjoint import riem_solver3
+    from fv3core_b200.grid import CubedSphereGrid
+    from fv3core_b200.initial_state import baroclinic_state
+    from fv3core_b200.storage import GridIndexing, to_device
+
+    rank, world, local = _env_rank()
+    torch.cuda.set_device(local)
+    n, npz = args.adj_n, args.npz
+    st = baroclinic_state(CubedSphereGrid(n, 3), npz, seed=7)
+    gi = GridIndexing((n, n, npz), 3)
+    dev = {k: to_device(st[k]) for k in ("w", "delp", "pt", "cappa", "q_con")}
+    zs = st["phis"] * (1.0 / 9.80665)
+    zh = np.zeros_like(st["delz"])
+    zh[..., npz] = zs
+    for k in range(npz - 1, -1, -1):
+        zh[..., k] = zh[..., k + 1] - st["delz"][..., k]
+    dev["zh"], dev["zs"], dev["wsd"] = to_device(zh), to_device(zs), to_device(np.zeros_like(zs))
+    dt, ptop, p_fac = 225.0 / 6, float(st["ptop"]), 0.05
+    gen = torch.Generator(device="cuda").manual_seed(1)
+    gw = torch.randn(dev["w"].shape, dtype=torch.float64, device="cuda", generator=gen)
+    gdz = 1e-2 * torch.randn(dev["w"].shape, dtype=torch.float64, device="cuda", generator=gen)
+    x = {k: dev[k].clone().requires_grad_(True) for k in ("w", "zh", "delp", "pt")}
+
+    def fwd():
+        with torch.no_grad():
+            return riem_solver3(dev["w"], dev["zh"], dev["delp"], dev["pt"], dev["cappa"], dev["zs"], dev["wsd"],
+                                dev["q_con"], gi, dt, ptop, p_fac)
+
+    def fwd_bwd():
+        a, b = riem_solver3(x["w"], x["zh"], x["delp"], x["pt"], dev["cappa"], dev["zs"], dev["wsd"], dev["q_con"],
+                            gi, dt, ptop, p_fac)
+        ((a * gw).sum() + (b * gdz).sum()).backward()
+
+    def timed(f):
+        for _ in range(args.warmup):
+            f()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            f()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    torch.cuda.reset_peak_memory_stats()
+    t_f = timed(fwd)
+    t_fb = timed(fwd_bwd)
+    peak = torch.cuda.max_memory_allocated()
+    line = {
+        "metric": f"RiemannSolver3 adjoint/forward time ratio (C{n} L{npz})", "value": t_fb / t_f,
+        "unit": "ratio", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_fb,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded baroclinic-wave state)",
+        "config": {"workload": f"RiemannSolver3 column solve, C{n} L{npz}, forward vs forward + hand-written "
+                               "adjoint through torch.autograd (the only stage with an adjoint so far)",
+                   "forward_ms": t_f, "forward_backward_ms": t_fb, "peak_memory_bytes": peak},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -614,8 +683,10 @@ def main():
     ap.add_argument("--ref-n", type=int, default=24, help="resolution of the reference arm's per-worker sample")
     ap.add_argument("--ref-max-workers", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["acoustics", "ensemble"], default="acoustics",
-                    help="ensemble: the mixed-resolution ensemble with CUDA-graph steps")
+    ap.add_argument("--workload", choices=["acoustics", "ensemble", "adjoint"], default="acoustics",
+                    help="ensemble: the mixed-resolution ensemble with CUDA-graph steps; adjoint: the "
+                         "RiemannSolver3 adjoint's cost")
+    ap.add_argument("--adj-n", type=int, default=48, help="adjoint workload: cube resolution")
     ap.add_argument("--members", default="16x48x79,8x96x79,4x192x63")
     ap.add_argument("--autotune", action="store_true", help="ensemble: pick the launch shape by timing first")
     args = ap.parse_args()
@@ -625,6 +696,8 @@ def main():
         run_reference(args)
     elif args.workload == "ensemble":
         run_ensemble(args)
+    elif args.workload == "adjoint":
+        run_adjoint(args)
     else:
         run_cuda(args)
 

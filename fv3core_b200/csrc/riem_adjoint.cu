@@ -1,0 +1,53 @@
+// fv3b_riem_solver3_adjoint: the column adjoint of riem_adjoint.h over the
+// compute-domain columns, one thread per column.  The per-level forward
+// values and adjoints live in the thread's local memory (about 50 arrays of
+// the level bucket), so this kernel favours simplicity over speed.
+#include "common.cuh"
+#include "riem_adjoint.h"
+
+namespace fv3b {
+namespace {
+
+struct Riem3AdjArgs {
+  double dt, ptop, p_fac;
+  const real *cappa, *wsd, *q_con, *delp, *pt, *zh, *w, *gw_out, *gdz_out;
+  real *g_w, *g_zh, *g_delp, *g_pt;
+};
+
+template <int NK>
+cudaError_t launch_adjoint(const Dims& d, cudaStream_t s, const Riem3AdjArgs a) {
+  const Dims dd = d;
+  return launch_columns(d.isc, d.iec + 1, d.jsc, d.jec + 1, s, [=] __device__(int t, int i, int j) {
+    const idx_t o = idx3(dd, t, i, j, 0);
+    adj::riem3_column_adjoint<NK, real, real>(dd.nk, dd.sk, a.dt, a.ptop, a.p_fac, (double)a.wsd[idx2(dd, t, i, j)],
+                                              a.w + o, a.zh + o, a.delp + o, a.pt + o, a.cappa + o, a.q_con + o,
+                                              a.gw_out + o, a.gdz_out + o, a.g_w + o, a.g_zh + o, a.g_delp + o,
+                                              a.g_pt + o);
+  }, 64);
+}
+
+}  // namespace
+}  // namespace fv3b
+
+using namespace fv3b;
+
+extern "C" int fv3b_riem_solver3_adjoint(const fv3b_grid_dims* dims, double dt, double ptop, double p_fac,
+                                         const real* cappa, const real* wsd, const real* q_con, const real* delp,
+                                         const real* pt, const real* zh, const real* w, const real* gw_out,
+                                         const real* gdz_out, real* g_w, real* g_zh, real* g_delp, real* g_pt,
+                                         void* stream) {
+  FV3B_REQUIRE(dims && cappa && wsd && q_con && delp && pt && zh && w && gw_out && gdz_out && g_w && g_zh && g_delp &&
+                   g_pt,
+               "fv3b_riem_solver3_adjoint: null argument");
+  FV3B_REQUIRE(dims_fit(dims), "fv3b_riem_solver3_adjoint: a 3-D field of the six tiles must hold fewer than 2^31 elements");
+  const Dims d = make_dims(dims);
+  FV3B_REQUIRE(d.nk >= 4 && d.nk <= 128, "fv3b_riem_solver3_adjoint: npz must be in 3..127");
+  const Riem3AdjArgs a{dt, ptop, p_fac, cappa, wsd, q_con, delp, pt, zh, w, gw_out, gdz_out, g_w, g_zh, g_delp, g_pt};
+  cudaStream_t s = (cudaStream_t)stream;
+  if (d.nk <= 16) FV3B_CHECK(launch_adjoint<16>(d, s, a));
+  else if (d.nk <= 32) FV3B_CHECK(launch_adjoint<32>(d, s, a));
+  else if (d.nk <= 64) FV3B_CHECK(launch_adjoint<64>(d, s, a));
+  else if (d.nk <= 80) FV3B_CHECK(launch_adjoint<80>(d, s, a));
+  else FV3B_CHECK(launch_adjoint<128>(d, s, a));
+  return FV3B_OK;
+}

@@ -1,0 +1,295 @@
+// Hand-written adjoint (reverse mode) of RiemannSolver3's column solve:
+// the precompute of riem_solver3.py:24-67 and Sim1Solver
+// (sim1_solver.py:11-105) for one column, differentiated with respect to
+// the inputs w, zh, delp and pt (cappa, q_con and the surface w are held
+// fixed).  The outputs are the new w and the new layer depths delz.  Written
+// for both the device and the host (the tests build it with g++ and compare
+// with torch autograd of a PyTorch-ops restatement).
+//
+// The forward values are recomputed first, with the same operations as the
+// solver (the library's exp and log), and kept in per-level arrays; the
+// reverse sweep then runs every forward step backwards.  The branch of the
+// pressure floor (maxp) is taken as the forward took it.  Columns need at
+// least four interface levels (three layers).
+#pragma once
+
+#include "fmath.h"
+
+namespace fv3b {
+namespace adj {
+
+constexpr double A_RDGAS = 287.05;
+constexpr double A_GRAV = 9.80665;
+constexpr double A_RGRAV = 1.0 / A_GRAV;
+
+// One column with K interface levels (N = K - 1 layers); every pointer
+// steps sk elements per level.  Inputs w, zh, delp, pt, cappa, q_con; the
+// cotangents gw_out (of the new w) and gdz_out (of the new delz); results
+// g_w, g_delp, g_pt on layers and g_zh on interfaces (overwritten).
+template <int NK, typename R, typename G>
+__host__ __device__ inline void riem3_column_adjoint(int K, long long sk, double dt, double ptop, double p_fac,
+                                                     double wsr, const R* w, const R* zh, const R* delp,
+                                                     const R* pt, const R* cappa, const R* q_con,
+                                                     const G* gw_out, const G* gdz_out, G* g_w, G* g_zh,
+                                                     G* g_delp, G* g_pt) {
+  const int N = K - 1;
+  double DM[NK], DZ[NK], GM[NK], PT[NK], CP3[NK], W1[NK];
+  double pem[NK], peg[NK], lg[NK], pm[NK], Xv[NK], Yv[NK], pe1[NK];
+  double grat[NK], bb[NK], dd[NK], bet[NK], gam[NK], pp[NK], ppb[NK], aa[NK];
+  double betw[NK], gw[NK], wpre[NK], wf[NK], pe[NK], p1[NK], maxp[NK], Ev[NK], dzv[NK];
+  bool floor_branch[NK];
+  // ---------------------------------------------------------------- forward
+  for (int k = 0; k < N; ++k) {
+    const double dp = delp[k * sk];
+    DM[k] = dp * A_RGRAV;
+    DZ[k] = (double)zh[(k + 1) * sk] - (double)zh[k * sk];
+    GM[k] = 1.0 / (1.0 - (double)cappa[k * sk]);
+    PT[k] = pt[k * sk];
+    CP3[k] = cappa[k * sk];
+    W1[k] = w[k * sk];
+  }
+  pem[0] = ptop;
+  peg[0] = ptop;
+  lg[0] = fm::fm_log(ptop);
+  for (int k = 0; k < N; ++k) {
+    const double dp = delp[k * sk];
+    pem[k + 1] = pem[k] + dp;
+    peg[k + 1] = peg[k] + dp * (1.0 - (double)q_con[k * sk]);
+    lg[k + 1] = fm::fm_log(peg[k + 1]);
+    pm[k] = (peg[k + 1] - peg[k]) / (lg[k + 1] - lg[k]);
+  }
+  for (int k = 0; k < N; ++k) {
+    Xv[k] = -DM[k] / DZ[k] * A_RDGAS * PT[k];
+    Yv[k] = fm::fm_exp(GM[k] * fm::fm_log(Xv[k]));
+    pe1[k] = Yv[k] - pm[k];
+  }
+  for (int k = 0; k < N - 1; ++k) {
+    grat[k] = DM[k] / DM[k + 1];
+    bb[k] = 2.0 * (1.0 + grat[k]);
+    dd[k] = 3.0 * (pe1[k] + grat[k] * pe1[k + 1]);
+  }
+  bb[N - 1] = 2.0;
+  dd[N - 1] = 3.0 * pe1[N - 1];
+  bet[0] = bb[0];
+  for (int k = 1; k < N; ++k) {
+    gam[k] = grat[k - 1] / bet[k - 1];
+    bet[k] = bb[k] - gam[k];
+  }
+  pp[0] = 0.0;
+  pp[1] = dd[0] / bet[0];
+  for (int k = 2; k <= N; ++k) pp[k] = (dd[k - 1] - pp[k - 1]) / bet[k - 1];
+  ppb[N] = pp[N];
+  ppb[0] = pp[0];
+  for (int k = N - 1; k >= 1; --k) ppb[k] = pp[k] - gam[k] * ppb[k + 1];
+  const double t1g = 2.0 * dt * dt, rdt = 1.0 / dt;
+  for (int k = 1; k < N; ++k) aa[k] = t1g * 0.5 * (GM[k - 1] + GM[k]) / (DZ[k - 1] + DZ[k]) * (pem[k] + ppb[k]);
+  betw[0] = DM[0] - aa[1];
+  wpre[0] = (DM[0] * W1[0] + dt * ppb[1]) / betw[0];
+  for (int k = 1; k < N - 1; ++k) {
+    gw[k] = aa[k] / betw[k - 1];
+    betw[k] = DM[k] - (aa[k] + aa[k + 1] + aa[k] * gw[k]);
+    wpre[k] = (DM[k] * W1[k] + dt * (ppb[k + 1] - ppb[k]) - aa[k] * wpre[k - 1]) / betw[k];
+  }
+  const int kl = N - 1;
+  const double p1t = t1g * GM[kl] / DZ[kl] * (pem[kl + 1] + ppb[kl + 1]);
+  gw[kl] = aa[kl] / betw[kl - 1];
+  betw[kl] = DM[kl] - (aa[kl] + p1t + aa[kl] * gw[kl]);
+  wpre[kl] = (DM[kl] * W1[kl] + dt * (ppb[kl + 1] - ppb[kl]) - p1t * wsr - aa[kl] * wpre[kl - 1]) / betw[kl];
+  wf[N - 1] = wpre[N - 1];
+  for (int k = N - 2; k >= 0; --k) wf[k] = wpre[k] - gw[k + 1] * wf[k + 1];
+  pe[0] = 0.0;
+  for (int k = 1; k <= N; ++k) pe[k] = pe[k - 1] + DM[k - 1] * (wf[k - 1] - W1[k - 1]) * rdt;
+  p1[N - 1] = (pe[N - 1] + 2.0 * pe[N]) * 1.0 / 3.0;
+  for (int k = N - 2; k >= 0; --k)
+    p1[k] = (pe[k] + bb[k] * pe[k + 1] + grat[k] * pe[k + 2]) * 1.0 / 3.0 - grat[k] * p1[k + 1];
+  for (int k = 0; k < N; ++k) {
+    floor_branch[k] = p_fac * DM[k] > p1[k] + pm[k];
+    maxp[k] = floor_branch[k] ? p_fac * pm[k] : p1[k] + pm[k];
+    Ev[k] = fm::fm_exp((CP3[k] - 1.0) * fm::fm_log(maxp[k]));
+    dzv[k] = -DM[k] * A_RDGAS * PT[k] * Ev[k];
+  }
+  // ---------------------------------------------------------------- reverse
+  double aDM[NK], aDZ[NK], aPT[NK], aW1[NK], aPEM[NK], aPEG[NK], aPM[NK], aPE1[NK];
+  double aGR[NK], aBB[NK], aDD[NK], aBET[NK], aGAM[NK], aPP[NK], aPPB[NK], aAA[NK];
+  double aBETW[NK], aGW[NK], aW[NK], aWF[NK], aPE[NK], aP1[NK];
+  for (int k = 0; k < NK; ++k) {
+    aDM[k] = aDZ[k] = aPT[k] = aW1[k] = aPEM[k] = aPEG[k] = aPM[k] = aPE1[k] = 0.0;
+    aGR[k] = aBB[k] = aDD[k] = aBET[k] = aGAM[k] = aPP[k] = aPPB[k] = aAA[k] = 0.0;
+    aBETW[k] = aGW[k] = aW[k] = aWF[k] = aPE[k] = aP1[k] = 0.0;
+  }
+  // dz = -DM Rd PT exp((cp3 - 1) log(maxp)); maxp on the forward's branch
+  for (int k = 0; k < N; ++k) {
+    const double a = gdz_out[k * sk];
+    aDM[k] += a * (-A_RDGAS * PT[k] * Ev[k]);
+    aPT[k] += a * (-DM[k] * A_RDGAS * Ev[k]);
+    const double amax = a * dzv[k] * (CP3[k] - 1.0) / maxp[k];
+    if (floor_branch[k]) {
+      aPM[k] += amax * p_fac;
+    } else {
+      aP1[k] += amax;
+      aPM[k] += amax;
+    }
+  }
+  // p1 recurrence (computed downwards, so its adjoint runs upwards)
+  for (int k = 0; k <= N - 2; ++k) {
+    const double a = aP1[k];
+    aPE[k] += a / 3.0;
+    aPE[k + 1] += a * bb[k] / 3.0;
+    aPE[k + 2] += a * grat[k] / 3.0;
+    aBB[k] += a * pe[k + 1] / 3.0;
+    aGR[k] += a * (pe[k + 2] / 3.0 - p1[k + 1]);
+    aP1[k + 1] += -a * grat[k];
+  }
+  aPE[N - 1] += aP1[N - 1] / 3.0;
+  aPE[N] += aP1[N - 1] * 2.0 / 3.0;
+  // pe[k] = pe[k-1] + DM[k-1] (wf[k-1] - W1[k-1]) rdt
+  for (int k = 0; k < N; ++k) aWF[k] = gw_out[k * sk];
+  for (int k = N; k >= 1; --k) {
+    const double a = aPE[k];
+    aPE[k - 1] += a;
+    aDM[k - 1] += a * (wf[k - 1] - W1[k - 1]) * rdt;
+    aWF[k - 1] += a * DM[k - 1] * rdt;
+    aW1[k - 1] -= a * DM[k - 1] * rdt;
+  }
+  // back substitution of w (downwards, adjoint upwards)
+  for (int k = 0; k <= N - 2; ++k) {
+    aW[k] += aWF[k];
+    aGW[k + 1] += -aWF[k] * wf[k + 1];
+    aWF[k + 1] += -aWF[k] * gw[k + 1];
+  }
+  aW[N - 1] += aWF[N - 1];
+  // forward sweep of the w system, last level first
+  {
+    const int k = kl;
+    const double anum = aW[k] / betw[k];
+    aBETW[k] += -aW[k] * wpre[k] / betw[k];
+    aDM[k] += anum * W1[k];
+    aW1[k] += anum * DM[k];
+    aPPB[k + 1] += anum * dt;
+    aPPB[k] -= anum * dt;
+    double ap1t = -anum * wsr;
+    aAA[k] += -anum * wpre[k - 1];
+    aW[k - 1] += -anum * aa[k];
+    const double ab = aBETW[k];
+    aDM[k] += ab;
+    aAA[k] += -ab * (1.0 + gw[k]);
+    ap1t += -ab;
+    aGW[k] += -ab * aa[k];
+    aAA[k] += aGW[k] / betw[k - 1];
+    aBETW[k - 1] += -aGW[k] * gw[k] / betw[k - 1];
+    const double c = t1g * GM[k] / DZ[k];
+    aDZ[k] += -ap1t * p1t / DZ[k];
+    aPEM[k + 1] += ap1t * c;
+    aPPB[k + 1] += ap1t * c;
+  }
+  for (int k = N - 2; k >= 1; --k) {
+    const double anum = aW[k] / betw[k];
+    aBETW[k] += -aW[k] * wpre[k] / betw[k];
+    aDM[k] += anum * W1[k];
+    aW1[k] += anum * DM[k];
+    aPPB[k + 1] += anum * dt;
+    aPPB[k] -= anum * dt;
+    aAA[k] += -anum * wpre[k - 1];
+    aW[k - 1] += -anum * aa[k];
+    const double ab = aBETW[k];
+    aDM[k] += ab;
+    aAA[k] += -ab * (1.0 + gw[k]);
+    aAA[k + 1] += -ab;
+    aGW[k] += -ab * aa[k];
+    aAA[k] += aGW[k] / betw[k - 1];
+    aBETW[k - 1] += -aGW[k] * gw[k] / betw[k - 1];
+  }
+  {
+    const double anum = aW[0] / betw[0];
+    aBETW[0] += -aW[0] * wpre[0] / betw[0];
+    aDM[0] += anum * W1[0];
+    aW1[0] += anum * DM[0];
+    aPPB[1] += anum * dt;
+    aDM[0] += aBETW[0];
+    aAA[1] += -aBETW[0];
+  }
+  // aa[k] = t1g 0.5 (GM[k-1] + GM[k]) / (DZ[k-1] + DZ[k]) (pem[k] + ppb[k])
+  for (int k = 1; k < N; ++k) {
+    const double S = DZ[k - 1] + DZ[k];
+    const double c = t1g * 0.5 * (GM[k - 1] + GM[k]);
+    const double aS = -aAA[k] * aa[k] / S;
+    aDZ[k - 1] += aS;
+    aDZ[k] += aS;
+    const double aP = aAA[k] * c / S;
+    aPEM[k] += aP;
+    aPPB[k] += aP;
+  }
+  // back substitution of pp (downwards, adjoint upwards)
+  for (int k = 1; k <= N - 1; ++k) {
+    aPP[k] += aPPB[k];
+    aGAM[k] += -aPPB[k] * ppb[k + 1];
+    aPPB[k + 1] += -aPPB[k] * gam[k];
+  }
+  aPP[N] += aPPB[N];
+  // forward recurrence of pp
+  for (int k = N; k >= 2; --k) {
+    const double a = aPP[k];
+    aDD[k - 1] += a / bet[k - 1];
+    aPP[k - 1] += -a / bet[k - 1];
+    aBET[k - 1] += -a * pp[k] / bet[k - 1];
+  }
+  aDD[0] += aPP[1] / bet[0];
+  aBET[0] += -aPP[1] * pp[1] / bet[0];
+  // gam[k] = grat[k-1] / bet[k-1]; bet[k] = bb[k] - gam[k]
+  for (int k = N - 1; k >= 1; --k) {
+    aBB[k] += aBET[k];
+    aGAM[k] += -aBET[k];
+    aGR[k - 1] += aGAM[k] / bet[k - 1];
+    aBET[k - 1] += -aGAM[k] * gam[k] / bet[k - 1];
+  }
+  aBB[0] += aBET[0];
+  // bb, dd from grat and pe1; grat from DM
+  for (int k = 0; k < N - 1; ++k) {
+    aGR[k] += 2.0 * aBB[k];
+    aPE1[k] += 3.0 * aDD[k];
+    aGR[k] += 3.0 * aDD[k] * pe1[k + 1];
+    aPE1[k + 1] += 3.0 * aDD[k] * grat[k];
+  }
+  aPE1[N - 1] += 3.0 * aDD[N - 1];
+  for (int k = 0; k < N - 1; ++k) {
+    aDM[k] += aGR[k] / DM[k + 1];
+    aDM[k + 1] += -aGR[k] * grat[k] / DM[k + 1];
+  }
+  // pe1 = exp(GM log X) - pm, X = -DM / DZ Rd PT
+  for (int k = 0; k < N; ++k) {
+    const double aX = aPE1[k] * GM[k] * Yv[k] / Xv[k];
+    aPM[k] += -aPE1[k];
+    aDM[k] += aX * (-A_RDGAS * PT[k] / DZ[k]);
+    aDZ[k] += aX * (DM[k] * A_RDGAS * PT[k] / (DZ[k] * DZ[k]));
+    aPT[k] += aX * (-DM[k] * A_RDGAS / DZ[k]);
+  }
+  // pm = (peg[k+1] - peg[k]) / (log peg[k+1] - log peg[k]); peg[0] = ptop fixed
+  for (int k = 0; k < N; ++k) {
+    const double den = lg[k + 1] - lg[k];
+    const double anum = aPM[k] / den;
+    const double aden = -aPM[k] * pm[k] / den;
+    aPEG[k + 1] += anum + aden / peg[k + 1];
+    aPEG[k] += -anum - aden / peg[k];
+  }
+  // running sums of delp: peg (moist) and pem
+  double a_dp[NK];
+  for (int k = 0; k < NK; ++k) a_dp[k] = 0.0;
+  for (int k = N - 1; k >= 0; --k) {
+    aPEG[k] += aPEG[k + 1];
+    a_dp[k] += aPEG[k + 1] * (1.0 - (double)q_con[k * sk]);
+    aPEM[k] += aPEM[k + 1];
+    a_dp[k] += aPEM[k + 1];
+  }
+  // DM = delp / g, DZ = zh[k+1] - zh[k]
+  for (int k = 0; k <= N; ++k) g_zh[k * sk] = 0.0;
+  for (int k = 0; k < N; ++k) {
+    g_delp[k * sk] = a_dp[k] + aDM[k] * A_RGRAV;
+    g_pt[k * sk] = aPT[k];
+    g_w[k * sk] = aW1[k];
+    g_zh[(k + 1) * sk] += aDZ[k];
+    g_zh[k * sk] -= aDZ[k];
+  }
+}
+
+}  // namespace adj
+}  // namespace fv3b

@@ -179,6 +179,23 @@ int fv3b_riem_solver3(const fv3b_grid_dims* dims, int last_call, double dt, doub
                       fv3b_real* ppe, fv3b_real* pk3, fv3b_real* pk, fv3b_real* peln, fv3b_real* w, void* stream);
 
 /*
+ * Adjoint of fv3b_riem_solver3's column solve (no reference counterpart: the
+ * reference has no derivatives).  For the compute-domain columns, given the
+ * solver's inputs w, zh, delp, pt (held fixed: cappa, q_con, wsd) and the
+ * cotangents gw_out of the new w and gdz_out of the new delz (layer levels
+ * 0..npz-1), writes the gradients g_w, g_delp, g_pt (layers) and g_zh
+ * (interfaces 0..npz) of <gw_out, w_new> + <gdz_out, delz_new>.  The
+ * branch of the pressure floor is the forward's.  Needs npz >= 3.  It
+ * recomputes the forward column in the thread's local memory: correct, not
+ * yet fast.
+ */
+int fv3b_riem_solver3_adjoint(const fv3b_grid_dims* dims, double dt, double ptop, double p_fac,
+                              const fv3b_real* cappa, const fv3b_real* wsd, const fv3b_real* q_con,
+                              const fv3b_real* delp, const fv3b_real* pt, const fv3b_real* zh, const fv3b_real* w,
+                              const fv3b_real* gw_out, const fv3b_real* gdz_out, fv3b_real* g_w, fv3b_real* g_zh,
+                              fv3b_real* g_delp, fv3b_real* g_pt, void* stream);
+
+/*
  * UpdateGeopotentialHeightOnCGrid.__call__ (fv3core/stencils/updatedzc.py:123-163).
  * dp_ref: device [npz+1] reference layer thickness; zs, ws: 2-D.
  * In: ut, vt.  In/out: gz (interface heights).  Out: ws.

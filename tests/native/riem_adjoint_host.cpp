@@ -1,0 +1,16 @@
+// Host build of the RiemannSolver3 column adjoint (fv3core_b200/csrc/riem_adjoint.h)
+// for the CPU tests: columns are rows of [ncol][K] arrays.
+#include "../../fv3core_b200/csrc/riem_adjoint.h"
+
+extern "C" void riem3_adjoint_columns(int ncol, int K, double dt, double ptop, double p_fac, const double* wsr,
+                                      const double* w, const double* zh, const double* delp, const double* pt,
+                                      const double* cappa, const double* q_con, const double* gw,
+                                      const double* gdz, double* g_w, double* g_zh, double* g_delp,
+                                      double* g_pt) {
+  for (int c = 0; c < ncol; ++c) {
+    const long long o = (long long)c * K;
+    fv3b::adj::riem3_column_adjoint<128, double, double>(K, 1, dt, ptop, p_fac, wsr[c], w + o, zh + o, delp + o,
+                                                         pt + o, cappa + o, q_con + o, gw + o, gdz + o, g_w + o,
+                                                         g_zh + o, g_delp + o, g_pt + o);
+  }
+}
