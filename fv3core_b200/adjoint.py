@@ -1,16 +1,20 @@
-"""Differentiable RiemannSolver3: the vertically implicit acoustic solve
-(reference ``fv3core/stencils/riem_solver3.py:145-242`` with
-``sim1_solver.py``) as a ``torch.autograd.Function`` whose backward pass is
-the library's hand-written adjoint (``fv3b_riem_solver3_adjoint``).
+"""Differentiable vertically implicit solvers: RiemannSolver3 (reference
+``fv3core/stencils/riem_solver3.py:145-242``) and RiemannSolverC
+(``riem_solver_c.py:106-165``), both with ``sim1_solver.py``, as
+``torch.autograd.Function`` s whose backward passes are the library's
+hand-written adjoints (``fv3b_riem_solver3_adjoint``,
+``fv3b_riem_solver_c_adjoint``).
 
-This is the first stage of the acoustic substep with an adjoint; the other
-stages have none yet, so a whole substep cannot be differentiated.
+These are the stages of the acoustic substep with an adjoint so far; the
+others have none yet, so a whole substep cannot be differentiated.
 
 ``riem_solver3(w, zh, delp, pt, cappa, zs, wsd, q_con, grid_indexing, dt,
-ptop, p_fac)`` returns the new (w, delz) of the compute-domain columns
-without changing its inputs; gradients flow to w, zh, delp and pt (cappa,
-q_con and the surface terms are held fixed).  Fields are device tensors in
-the kernel layout of ``grid_indexing``.
+ptop, p_fac)`` returns the new (w, delz) of the compute-domain columns;
+``riem_solver_c(w3, gz, delpc, ptc, cappa, hs, ws, q_con, grid_indexing,
+dt2, ptop, p_fac)`` returns the new (pef, gz) of the columns is-1..ie+1.
+Neither changes its inputs; gradients flow to the first four arguments
+(cappa, q_con and the surface terms are held fixed).  Fields are device
+tensors in the kernel layout of ``grid_indexing``.
 """
 import torch
 
@@ -64,3 +68,48 @@ def riem_solver3(w, zh, delp, pt, cappa, zs, wsd, q_con, grid_indexing, dt, ptop
     """New (w, delz) of RiemannSolver3 on the compute domain, differentiable
     with respect to w, zh, delp and pt."""
     return RiemannSolver3Function.apply(w, zh, delp, pt, cappa, zs, wsd, q_con, grid_indexing, dt, ptop, p_fac)
+
+
+class RiemannSolverCFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, w3, gz, delpc, ptc, cappa, hs, ws, q_con, gi, dt2, ptop, p_fac):
+        f3 = lambda t, n: check_field(t, gi, "3d", n)  # noqa: E731
+        gz_new = gz.detach().clone()
+        pef = torch.zeros_like(gz_new)
+        _lib.call(
+            "fv3b_riem_solver_c", gi.dims(), float(dt2), float(ptop), float(p_fac), f3(cappa, "cappa"),
+            check_field(hs, gi, "2d", "hs"), check_field(ws, gi, "2d", "ws"), f3(ptc, "ptc"), f3(q_con, "q_con"),
+            f3(delpc, "delpc"), f3(gz_new, "gz"), f3(pef, "pef"), f3(w3, "w3"), stream_ptr(),
+            precision=gi.precision,
+        )
+        ctx.save_for_backward(w3.detach(), gz.detach(), delpc.detach(), ptc.detach(), cappa, ws, q_con)
+        ctx.params = (gi, float(dt2), float(ptop), float(p_fac))
+        return pef, gz_new
+
+    @staticmethod
+    def backward(ctx, g_pef, g_gz):
+        w3, gz, delpc, ptc, cappa, ws, q_con = ctx.saved_tensors
+        gi, dt2, ptop, p_fac = ctx.params
+        f3 = lambda t, n: check_field(t, gi, "3d", n)  # noqa: E731
+        gpef_out = torch.zeros_like(gz) if g_pef is None else g_pef.contiguous()
+        ggz_out = torch.zeros_like(gz) if g_gz is None else g_gz.contiguous()
+        grads = [torch.zeros_like(gz) for _ in range(4)]  # w3, gz, delpc, ptc
+        _lib.call(
+            "fv3b_riem_solver_c_adjoint", gi.dims(), dt2, ptop, p_fac, f3(cappa, "cappa"),
+            check_field(ws, gi, "2d", "ws"), f3(q_con, "q_con"), f3(delpc, "delpc"), f3(ptc, "ptc"),
+            f3(gz, "gz"), f3(w3, "w3"), f3(gpef_out, "gpef_out"), f3(ggz_out, "ggz_out"), f3(grads[0], "g_w3"),
+            f3(grads[1], "g_gz"), f3(grads[2], "g_delpc"), f3(grads[3], "g_ptc"), stream_ptr(),
+            precision=gi.precision,
+        )
+        # gz outside the solved columns is gz itself: the gradient passes through
+        h, n = gi.n_halo, gi.n
+        solved = torch.zeros_like(gz, dtype=torch.bool)
+        solved[:, :, h - 1:h + n + 1, h - 1:h + n + 1] = True
+        grads[1] = grads[1] + torch.where(solved, torch.zeros_like(ggz_out), ggz_out)
+        return grads[0], grads[1], grads[2], grads[3], None, None, None, None, None, None, None, None
+
+
+def riem_solver_c(w3, gz, delpc, ptc, cappa, hs, ws, q_con, grid_indexing, dt2, ptop, p_fac):
+    """New (pef, gz) of RiemannSolverC on the columns is-1..ie+1,
+    differentiable with respect to w3, gz, delpc and ptc."""
+    return RiemannSolverCFunction.apply(w3, gz, delpc, ptc, cappa, hs, ws, q_con, grid_indexing, dt2, ptop, p_fac)

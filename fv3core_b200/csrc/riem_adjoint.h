@@ -1,10 +1,10 @@
-// Hand-written adjoint (reverse mode) of RiemannSolver3's column solve:
-// the precompute of riem_solver3.py:24-67 and Sim1Solver
-// (sim1_solver.py:11-105) for one column, differentiated with respect to
-// the inputs w, zh, delp and pt (cappa, q_con and the surface w are held
-// fixed).  The outputs are the new w and the new layer depths delz.  Written
-// for both the device and the host (the tests build it with g++ and compare
-// with torch autograd of a PyTorch-ops restatement).
+// Hand-written adjoints (reverse mode) of the two vertically implicit
+// solvers' column work: Sim1Solver (sim1_solver.py:11-105) shared by both,
+// with the precompute and finalize of RiemannSolver3 (riem_solver3.py:24-67)
+// and of RiemannSolverC (riem_solver_c.py:13-64).  cappa, q_con and the
+// surface terms are held fixed.  Written for both the device and the host
+// (the tests build it with g++ and compare with torch autograd of a
+// PyTorch-ops restatement).
 //
 // The forward values are recomputed first, with the same operations as the
 // solver (the library's exp and log), and kept in per-level arrays; the
@@ -22,42 +22,24 @@ constexpr double A_RDGAS = 287.05;
 constexpr double A_GRAV = 9.80665;
 constexpr double A_RGRAV = 1.0 / A_GRAV;
 
-// One column with K interface levels (N = K - 1 layers); every pointer
-// steps sk elements per level.  Inputs w, zh, delp, pt, cappa, q_con; the
-// cotangents gw_out (of the new w) and gdz_out (of the new delz); results
-// g_w, g_delp, g_pt on layers and g_zh on interfaces (overwritten).
-template <int NK, typename R, typename G>
-__host__ __device__ inline void riem3_column_adjoint(int K, long long sk, double dt, double ptop, double p_fac,
-                                                     double wsr, const R* w, const R* zh, const R* delp,
-                                                     const R* pt, const R* cappa, const R* q_con,
-                                                     const G* gw_out, const G* gdz_out, G* g_w, G* g_zh,
-                                                     G* g_delp, G* g_pt) {
-  const int N = K - 1;
-  double DM[NK], DZ[NK], GM[NK], PT[NK], CP3[NK], W1[NK];
-  double pem[NK], peg[NK], lg[NK], pm[NK], Xv[NK], Yv[NK], pe1[NK];
+// Sim1Solver's adjoint for one column of N layers (N + 1 interfaces).
+// Forward inputs: DM (delta p / g), DZ (layer depths), GM = 1 / (1 - cappa),
+// PT, CP3 (cappa), W1 (w at the start), pem (edge pressures, N + 1) and pm
+// (layer-mean pressures).  Forward outputs: w (aWF_in is its cotangent), the
+// pressure perturbation pe at interfaces 0..N (aPE_in) and dz (aDZ_in).
+// The adjoints of the inputs are added into aDM, aDZ, aPT, aW1, aPEM, aPM.
+template <int NK>
+__host__ __device__ inline void sim1_column_adjoint(int N, const double* DM, const double* DZ, const double* GM,
+                                                    const double* PT, const double* CP3, const double* W1,
+                                                    const double* pem, const double* pm, double wsr, double dt,
+                                                    double p_fac, const double* aWF_in, const double* aPE_in,
+                                                    const double* aDZ_in, double* aDM, double* aDZ, double* aPT,
+                                                    double* aW1, double* aPEM, double* aPM) {
+  double Xv[NK], Yv[NK], pe1[NK];
   double grat[NK], bb[NK], dd[NK], bet[NK], gam[NK], pp[NK], ppb[NK], aa[NK];
   double betw[NK], gw[NK], wpre[NK], wf[NK], pe[NK], p1[NK], maxp[NK], Ev[NK], dzv[NK];
   bool floor_branch[NK];
   // ---------------------------------------------------------------- forward
-  for (int k = 0; k < N; ++k) {
-    const double dp = delp[k * sk];
-    DM[k] = dp * A_RGRAV;
-    DZ[k] = (double)zh[(k + 1) * sk] - (double)zh[k * sk];
-    GM[k] = 1.0 / (1.0 - (double)cappa[k * sk]);
-    PT[k] = pt[k * sk];
-    CP3[k] = cappa[k * sk];
-    W1[k] = w[k * sk];
-  }
-  pem[0] = ptop;
-  peg[0] = ptop;
-  lg[0] = fm::fm_log(ptop);
-  for (int k = 0; k < N; ++k) {
-    const double dp = delp[k * sk];
-    pem[k + 1] = pem[k] + dp;
-    peg[k + 1] = peg[k] + dp * (1.0 - (double)q_con[k * sk]);
-    lg[k + 1] = fm::fm_log(peg[k + 1]);
-    pm[k] = (peg[k + 1] - peg[k]) / (lg[k + 1] - lg[k]);
-  }
   for (int k = 0; k < N; ++k) {
     Xv[k] = -DM[k] / DZ[k] * A_RDGAS * PT[k];
     Yv[k] = fm::fm_exp(GM[k] * fm::fm_log(Xv[k]));
@@ -109,17 +91,16 @@ __host__ __device__ inline void riem3_column_adjoint(int K, long long sk, double
     dzv[k] = -DM[k] * A_RDGAS * PT[k] * Ev[k];
   }
   // ---------------------------------------------------------------- reverse
-  double aDM[NK], aDZ[NK], aPT[NK], aW1[NK], aPEM[NK], aPEG[NK], aPM[NK], aPE1[NK];
-  double aGR[NK], aBB[NK], aDD[NK], aBET[NK], aGAM[NK], aPP[NK], aPPB[NK], aAA[NK];
+  double aPE1[NK], aGR[NK], aBB[NK], aDD[NK], aBET[NK], aGAM[NK], aPP[NK], aPPB[NK], aAA[NK];
   double aBETW[NK], aGW[NK], aW[NK], aWF[NK], aPE[NK], aP1[NK];
   for (int k = 0; k < NK; ++k) {
-    aDM[k] = aDZ[k] = aPT[k] = aW1[k] = aPEM[k] = aPEG[k] = aPM[k] = aPE1[k] = 0.0;
-    aGR[k] = aBB[k] = aDD[k] = aBET[k] = aGAM[k] = aPP[k] = aPPB[k] = aAA[k] = 0.0;
-    aBETW[k] = aGW[k] = aW[k] = aWF[k] = aPE[k] = aP1[k] = 0.0;
+    aPE1[k] = aGR[k] = aBB[k] = aDD[k] = aBET[k] = aGAM[k] = aPP[k] = aPPB[k] = aAA[k] = 0.0;
+    aBETW[k] = aGW[k] = aW[k] = aWF[k] = aP1[k] = 0.0;
+    aPE[k] = k <= N ? aPE_in[k] : 0.0;
   }
   // dz = -DM Rd PT exp((cp3 - 1) log(maxp)); maxp on the forward's branch
   for (int k = 0; k < N; ++k) {
-    const double a = gdz_out[k * sk];
+    const double a = aDZ_in[k];
     aDM[k] += a * (-A_RDGAS * PT[k] * Ev[k]);
     aPT[k] += a * (-DM[k] * A_RDGAS * Ev[k]);
     const double amax = a * dzv[k] * (CP3[k] - 1.0) / maxp[k];
@@ -143,7 +124,7 @@ __host__ __device__ inline void riem3_column_adjoint(int K, long long sk, double
   aPE[N - 1] += aP1[N - 1] / 3.0;
   aPE[N] += aP1[N - 1] * 2.0 / 3.0;
   // pe[k] = pe[k-1] + DM[k-1] (wf[k-1] - W1[k-1]) rdt
-  for (int k = 0; k < N; ++k) aWF[k] = gw_out[k * sk];
+  for (int k = 0; k < N; ++k) aWF[k] = aWF_in[k];
   for (int k = N; k >= 1; --k) {
     const double a = aPE[k];
     aPE[k - 1] += a;
@@ -263,24 +244,74 @@ __host__ __device__ inline void riem3_column_adjoint(int K, long long sk, double
     aDZ[k] += aX * (DM[k] * A_RDGAS * PT[k] / (DZ[k] * DZ[k]));
     aPT[k] += aX * (-DM[k] * A_RDGAS / DZ[k]);
   }
-  // pm = (peg[k+1] - peg[k]) / (log peg[k+1] - log peg[k]); peg[0] = ptop fixed
+}
+
+// Adjoint of the layer-mean pressures pm = (peg[k+1] - peg[k]) / L with
+// L = log(peg[k+1]) - log(peg[k]) (or log of their ratio: the same
+// derivatives) and of the running sums peg (moist) and pem over delp; adds
+// the result to a_dp.  peg[0] = pem[0] = ptop is fixed.
+template <int NK>
+__host__ __device__ inline void column_sums_adjoint(int N, const double* peg, const double* L, const double* pm,
+                                                    const double* qc, double* aPM, double* aPEM, double* a_dp) {
+  double aPEG[NK];
+  for (int k = 0; k < NK; ++k) aPEG[k] = 0.0;
   for (int k = 0; k < N; ++k) {
-    const double den = lg[k + 1] - lg[k];
-    const double anum = aPM[k] / den;
-    const double aden = -aPM[k] * pm[k] / den;
+    const double anum = aPM[k] / L[k];
+    const double aden = -aPM[k] * pm[k] / L[k];
     aPEG[k + 1] += anum + aden / peg[k + 1];
     aPEG[k] += -anum - aden / peg[k];
   }
-  // running sums of delp: peg (moist) and pem
-  double a_dp[NK];
-  for (int k = 0; k < NK; ++k) a_dp[k] = 0.0;
   for (int k = N - 1; k >= 0; --k) {
     aPEG[k] += aPEG[k + 1];
-    a_dp[k] += aPEG[k + 1] * (1.0 - (double)q_con[k * sk]);
+    a_dp[k] += aPEG[k + 1] * (1.0 - qc[k]);
     aPEM[k] += aPEM[k + 1];
     a_dp[k] += aPEM[k + 1];
   }
-  // DM = delp / g, DZ = zh[k+1] - zh[k]
+}
+
+// RiemannSolver3's column (riem_solver3.py:24-67 + sim1): one column with K
+// interface levels (N = K - 1 layers); every pointer steps sk elements per
+// level.  Inputs w, zh, delp, pt, cappa, q_con; the cotangents gw_out (of
+// the new w) and gdz_out (of the new delz); results g_w, g_delp, g_pt on
+// layers and g_zh on interfaces (overwritten).
+template <int NK, typename R, typename G>
+__host__ __device__ inline void riem3_column_adjoint(int K, long long sk, double dt, double ptop, double p_fac,
+                                                     double wsr, const R* w, const R* zh, const R* delp,
+                                                     const R* pt, const R* cappa, const R* q_con,
+                                                     const G* gw_out, const G* gdz_out, G* g_w, G* g_zh,
+                                                     G* g_delp, G* g_pt) {
+  const int N = K - 1;
+  double DM[NK], DZ[NK], GM[NK], PT[NK], CP3[NK], W1[NK], QC[NK];
+  double pem[NK], peg[NK], lg[NK], L[NK], pm[NK];
+  for (int k = 0; k < N; ++k) {
+    DM[k] = (double)delp[k * sk] * A_RGRAV;
+    DZ[k] = (double)zh[(k + 1) * sk] - (double)zh[k * sk];
+    GM[k] = 1.0 / (1.0 - (double)cappa[k * sk]);
+    PT[k] = pt[k * sk];
+    CP3[k] = cappa[k * sk];
+    W1[k] = w[k * sk];
+    QC[k] = q_con[k * sk];
+  }
+  pem[0] = ptop;
+  peg[0] = ptop;
+  lg[0] = fm::fm_log(ptop);
+  for (int k = 0; k < N; ++k) {
+    const double dp = delp[k * sk];
+    pem[k + 1] = pem[k] + dp;
+    peg[k + 1] = peg[k] + dp * (1.0 - QC[k]);
+    lg[k + 1] = fm::fm_log(peg[k + 1]);
+    L[k] = lg[k + 1] - lg[k];
+    pm[k] = (peg[k + 1] - peg[k]) / L[k];
+  }
+  double aDM[NK], aDZ[NK], aPT[NK], aW1[NK], aPEM[NK], aPM[NK], aWF[NK], aPE[NK], aDZo[NK], a_dp[NK];
+  for (int k = 0; k < NK; ++k) aDM[k] = aDZ[k] = aPT[k] = aW1[k] = aPEM[k] = aPM[k] = aPE[k] = a_dp[k] = 0.0;
+  for (int k = 0; k < N; ++k) {
+    aWF[k] = gw_out[k * sk];
+    aDZo[k] = gdz_out[k * sk];
+  }
+  sim1_column_adjoint<NK>(N, DM, DZ, GM, PT, CP3, W1, pem, pm, wsr, dt, p_fac, aWF, aPE, aDZo, aDM, aDZ, aPT, aW1,
+                          aPEM, aPM);
+  column_sums_adjoint<NK>(N, peg, L, pm, QC, aPM, aPEM, a_dp);
   for (int k = 0; k <= N; ++k) g_zh[k * sk] = 0.0;
   for (int k = 0; k < N; ++k) {
     g_delp[k * sk] = a_dp[k] + aDM[k] * A_RGRAV;
@@ -288,6 +319,68 @@ __host__ __device__ inline void riem3_column_adjoint(int K, long long sk, double
     g_w[k * sk] = aW1[k];
     g_zh[(k + 1) * sk] += aDZ[k];
     g_zh[k * sk] -= aDZ[k];
+  }
+}
+
+// RiemannSolverC's column (riem_solver_c.py:13-64 + sim1): inputs w3, gz
+// (interface heights), delpc, ptc, cappa, q_con, the surface height hs and
+// ws; outputs pef (pe + pem on interfaces 1..N, ptop on top) and gz
+// (hs at the bottom, gz[k] = gz[k+1] - dz[k] g).  Cotangents gpef_out,
+// ggz_out on interfaces; results g_w3, g_delpc, g_ptc on layers and g_gz on
+// interfaces (the input heights).
+template <int NK, typename R, typename G>
+__host__ __device__ inline void riemc_column_adjoint(int K, long long sk, double dt2, double ptop, double p_fac,
+                                                     double wsr, const R* w3, const R* gz, const R* delpc,
+                                                     const R* ptc, const R* cappa, const R* q_con,
+                                                     const G* gpef_out, const G* ggz_out, G* g_w3, G* g_gz,
+                                                     G* g_delpc, G* g_ptc) {
+  const int N = K - 1;
+  double DM[NK], DZ[NK], GM[NK], PT[NK], CP3[NK], W1[NK], QC[NK];
+  double pem[NK], peg[NK], L[NK], pm[NK];
+  for (int k = 0; k < N; ++k) {
+    DM[k] = (double)delpc[k * sk] / A_GRAV;
+    DZ[k] = (double)gz[(k + 1) * sk] - (double)gz[k * sk];
+    GM[k] = 1.0 / (1.0 - (double)cappa[k * sk]);
+    PT[k] = ptc[k * sk];
+    CP3[k] = cappa[k * sk];
+    W1[k] = w3[k * sk];
+    QC[k] = q_con[k * sk];
+  }
+  pem[0] = ptop;
+  peg[0] = ptop;
+  for (int k = 0; k < N; ++k) {
+    const double dp = delpc[k * sk];
+    pem[k + 1] = pem[k] + dp;
+    peg[k + 1] = peg[k] + dp * (1.0 - QC[k]);
+    L[k] = fm::fm_log(peg[k + 1] / peg[k]);
+    pm[k] = (peg[k + 1] - peg[k]) / L[k];
+  }
+  double aDM[NK], aDZ[NK], aPT[NK], aW1[NK], aPEM[NK], aPM[NK], aWF[NK], aPE[NK], aDZo[NK], a_dp[NK];
+  for (int k = 0; k < NK; ++k) {
+    aDM[k] = aDZ[k] = aPT[k] = aW1[k] = aPEM[k] = aPM[k] = aWF[k] = aPE[k] = aDZo[k] = a_dp[k] = 0.0;
+  }
+  // pef[k] = pe[k] + pem[k] for k >= 1
+  for (int k = 1; k <= N; ++k) {
+    aPE[k] = gpef_out[k * sk];
+    aPEM[k] += gpef_out[k * sk];
+  }
+  // gz[k] = hs - g sum_{m >= k} dz[m]: dz[m] collects -g times the
+  // cotangents of gz[0..m]
+  double acc = 0.0;
+  for (int m = 0; m < N; ++m) {
+    acc += ggz_out[m * sk];
+    aDZo[m] = -A_GRAV * acc;
+  }
+  sim1_column_adjoint<NK>(N, DM, DZ, GM, PT, CP3, W1, pem, pm, wsr, dt2, p_fac, aWF, aPE, aDZo, aDM, aDZ, aPT, aW1,
+                          aPEM, aPM);
+  column_sums_adjoint<NK>(N, peg, L, pm, QC, aPM, aPEM, a_dp);
+  for (int k = 0; k <= N; ++k) g_gz[k * sk] = 0.0;
+  for (int k = 0; k < N; ++k) {
+    g_delpc[k * sk] = a_dp[k] + aDM[k] / A_GRAV;
+    g_ptc[k * sk] = aPT[k];
+    g_w3[k * sk] = aW1[k];
+    g_gz[(k + 1) * sk] += aDZ[k];
+    g_gz[k * sk] -= aDZ[k];
   }
 }
 

@@ -196,6 +196,20 @@ int fv3b_riem_solver3_adjoint(const fv3b_grid_dims* dims, double dt, double ptop
                               fv3b_real* g_delp, fv3b_real* g_pt, void* stream);
 
 /*
+ * Adjoint of fv3b_riem_solver_c (no reference counterpart).  For the columns
+ * is-1..ie+1 x js-1..je+1, given the solver's inputs w3, gz, delpc, ptc
+ * (held fixed: cappa, q_con, ws, hs) and the cotangents gpef_out, ggz_out
+ * of its outputs pef and gz (interfaces 0..npz), writes the gradients g_w3,
+ * g_delpc, g_ptc (layers) and g_gz (the input heights, interfaces).  Same
+ * conditions as fv3b_riem_solver3_adjoint.
+ */
+int fv3b_riem_solver_c_adjoint(const fv3b_grid_dims* dims, double dt2, double ptop, double p_fac,
+                               const fv3b_real* cappa, const fv3b_real* ws, const fv3b_real* q_con,
+                               const fv3b_real* delpc, const fv3b_real* ptc, const fv3b_real* gz, const fv3b_real* w3,
+                               const fv3b_real* gpef_out, const fv3b_real* ggz_out, fv3b_real* g_w3,
+                               fv3b_real* g_gz, fv3b_real* g_delpc, fv3b_real* g_ptc, void* stream);
+
+/*
  * UpdateGeopotentialHeightOnCGrid.__call__ (fv3core/stencils/updatedzc.py:123-163).
  * dp_ref: device [npz+1] reference layer thickness; zs, ws: 2-D.
  * In: ut, vt.  In/out: gz (interface heights).  Out: ws.

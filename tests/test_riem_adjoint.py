@@ -79,6 +79,65 @@ def test_host_adjoint_matches_torch_autograd(host_adjoint):
         assert err <= 1e-12, (k, err)
 
 
+def riemc_case(n=12, nz=16, seed=11):
+    """The RiemannSolverC case's columns (is-1..ie+1, js-1..je+1) as [ncol, K]."""
+    case = cases.riem_solver_c_case(n, nz, seed)
+    sl = (slice(None), slice(H - 1, H + n + 1), slice(H - 1, H + n + 1))
+    cols = {k: np.ascontiguousarray(case[k][sl].reshape(6 * (n + 2) ** 2, -1))
+            for k in ("w3", "gz", "delpc", "ptc", "cappa", "q_con")}
+    cols["hs"] = np.ascontiguousarray(case["hs"][sl].reshape(-1))
+    cols["ws"] = np.ascontiguousarray(case["ws"][sl].reshape(-1))
+    return case, cols, dict(dt2=case["dt2"], ptop=float(case["ptop"]), p_fac=case["p_fac"])
+
+
+def riemc_torch(cols, par, requires_grad=False):
+    T = {k: torch.from_numpy(v.copy()) for k, v in cols.items()}
+    if requires_grad:
+        for k in ("w3", "gz", "delpc", "ptc"):
+            T[k].requires_grad_(True)
+    pef, gz = torch_riem3.riemc_columns(T["w3"], T["gz"], T["delpc"], T["ptc"], T["cappa"], T["q_con"], T["hs"],
+                                        T["ws"], par["dt2"], par["ptop"], par["p_fac"])
+    return T, pef, gz
+
+
+def test_riemc_restatement_matches_oracle():
+    from oracle.riem_solver_c import riem_solver_c
+
+    n, nz = 12, 16
+    case, cols, par = riemc_case(n, nz)
+    ref = {k: (np.array(v, copy=True) if isinstance(v, np.ndarray) else v) for k, v in case.items()}
+    for t in range(6):
+        riem_solver_c(ref["dt2"], ref["cappa"][t], ref["ptop"], ref["hs"][t], ref["ws"][t], ref["ptc"][t],
+                      ref["q_con"][t], ref["delpc"][t], ref["gz"][t], ref["pef"][t], ref["w3"][t], ref["p_fac"], n, nz)
+    _, pef, gz = riemc_torch(cols, par)
+    sl = (slice(None), slice(H - 1, H + n + 1), slice(H - 1, H + n + 1))
+    for name, mine in (("pef", pef), ("gz", gz)):
+        want = ref[name][sl].reshape(6 * (n + 2) ** 2, -1)
+        err = np.max(np.abs(mine.detach().numpy() - want) / np.maximum(np.abs(want), 1e-30))
+        assert err <= 1e-11, (name, err)
+
+
+def test_host_riemc_adjoint_matches_torch_autograd(host_adjoint):
+    _, cols, par = riemc_case()
+    ncol, K = cols["gz"].shape
+    rng = np.random.default_rng(12)
+    gpef = rng.standard_normal((ncol, K)) * 1e-3
+    ggz = rng.standard_normal((ncol, K))
+    T, pef, gz = riemc_torch(cols, par, requires_grad=True)
+    ((pef * torch.from_numpy(gpef)).sum() + (gz * torch.from_numpy(ggz)).sum()).backward()
+    out = {k: np.zeros((ncol, K)) for k in ("w3", "gz", "delpc", "ptc")}
+    f = host_adjoint.riemc_adjoint_columns
+    f.restype = None
+    f(ctypes.c_int(ncol), ctypes.c_int(K), ctypes.c_double(par["dt2"]), ctypes.c_double(par["ptop"]),
+      ctypes.c_double(par["p_fac"]), _ptr(cols["ws"]), _ptr(cols["w3"]), _ptr(cols["gz"]), _ptr(cols["delpc"]),
+      _ptr(cols["ptc"]), _ptr(cols["cappa"]), _ptr(cols["q_con"]), _ptr(gpef), _ptr(ggz),
+      _ptr(out["w3"]), _ptr(out["gz"]), _ptr(out["delpc"]), _ptr(out["ptc"]))
+    for k, width in (("w3", K - 1), ("gz", K), ("delpc", K - 1), ("ptc", K - 1)):
+        a, b = out[k][:, :width], T[k].grad.numpy()[:, :width]
+        err = np.max(np.abs(a - b)) / np.max(np.abs(b))
+        assert err <= 1e-12, (k, err)
+
+
 def test_torch_restatement_gradients_match_finite_differences():
     cols, par = riem3_case(n=4, nz=8, seed=9)
     ncol, K = cols["zh"].shape
@@ -195,3 +254,35 @@ def test_gpu_adjoint_matches_finite_differences_of_the_gpu_forward():
         fd = float((lp - lm) / (2 * eps))
         ad = sum(float((x[k].grad * d[k]).sum()) for k in x)
         assert abs(fd - ad) <= 1e-5 * abs(ad), (trial, fd, ad)
+
+
+@pytest.mark.gpu
+def test_gpu_riemc_adjoint_matches_torch_autograd():
+    from fv3core_b200.adjoint import riem_solver_c
+    from fv3core_b200.storage import GridIndexing, to_device, to_host
+
+    n, nz = 12, 16
+    case, cols, par = riemc_case(n, nz)
+    gi = GridIndexing((n, n, nz), H)
+    dev = {k: to_device(case[k]) for k in ("w3", "gz", "delpc", "ptc", "cappa", "q_con", "hs", "ws")}
+    for k in ("w3", "gz", "delpc", "ptc"):
+        dev[k].requires_grad_(True)
+    pef, gz = riem_solver_c(dev["w3"], dev["gz"], dev["delpc"], dev["ptc"], dev["cappa"], dev["hs"], dev["ws"],
+                            dev["q_con"], gi, par["dt2"], par["ptop"], par["p_fac"])
+    gen = torch.Generator(device="cuda").manual_seed(2)
+    gpef = 1e-3 * torch.randn(pef.shape, dtype=pef.dtype, device="cuda", generator=gen)
+    ggz = torch.randn(gz.shape, dtype=gz.dtype, device="cuda", generator=gen)
+    ((pef * gpef).sum() + (gz * ggz).sum()).backward()
+    sl = (slice(None), slice(H - 1, H + n + 1), slice(H - 1, H + n + 1))
+
+    def cols_of(t):
+        return to_host(t)[sl].reshape(6 * (n + 2) ** 2, -1)
+
+    T, pef_t, gz_t = riemc_torch(cols, par, requires_grad=True)
+    ((pef_t * torch.from_numpy(cols_of(gpef))).sum() + (gz_t * torch.from_numpy(cols_of(ggz))).sum()).backward()
+    K = nz + 1
+    for k, width in (("w3", K - 1), ("gz", K), ("delpc", K - 1), ("ptc", K - 1)):
+        a = cols_of(dev[k].grad)[:, :width]
+        b = T[k].grad.numpy()[:, :width]
+        err = np.max(np.abs(a - b)) / np.max(np.abs(b))
+        assert err <= 1e-10, (k, err)
