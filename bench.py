@@ -598,9 +598,10 @@ def run_ensemble(args):
 
 
 def run_adjoint(args):
-    """Cost of the hand-written adjoint of RiemannSolver3 (the stage of the
-    acoustic substep that has one): forward alone against forward + backward
-    through torch autograd, C48 L79 FP64 by default."""
+    """Cost of the hand-written adjoint of RiemannSolver3 (with
+    RiemannSolverC, the stages of the acoustic substep that have one so far):
+    forward alone against forward + backward through torch autograd, C48 L79
+    FP64 by default."""
     import numpy as np
     import torch
 
@@ -659,7 +660,7 @@ def run_adjoint(args):
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded baroclinic-wave state)",
         "config": {"workload": f"RiemannSolver3 column solve, C{n} L{npz}, forward vs forward + hand-written "
-                               "adjoint through torch.autograd (the only stage with an adjoint so far)",
+                               "adjoint through torch.autograd (the Riemann solvers are the stages with an adjoint so far)",
                    "forward_ms": t_f, "forward_backward_ms": t_fb, "peak_memory_bytes": peak},
     }
     if rank == 0:
