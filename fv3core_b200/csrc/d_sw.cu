@@ -54,32 +54,30 @@ cudaError_t fxadv(const Dims d, const fv3b_metrics g, const real* uc, const real
     W3(vcc, i, j) = vn;
   });
   if (err != cudaSuccess) return err;
-  // vc_contra_y_edge + vc_contra_x_edge (fxadv.py:97-150)
-  err = launch_box(Box{0, full, 0, full, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+  // vc_contra_y_edge + vc_contra_x_edge (fxadv.py:97-150).  Only two kinds of
+  // points change: the rows js and je+1 (every i) and, on the columns
+  // is-1, is, ie, ie+1, the rows js+2 .. je-1; the two sets are disjoint
+  // and each point reads only ucc and vc, so two small launches replace a
+  // pass over the whole domain.
+  err = launch_box(Box{0, full, 0, 2, 0, nz}, st, [=] __device__(int t, int i, int y, int k) {
     PT_SETUP(d, t, k);
-    real vn = F3(vcc, i, j);
-    bool ycol = (i >= s - 1 && i < s + 1) || (i >= e && i < e + 2);
-    if (ycol && j >= js && j < je + 2) {
-      bool keep = (j >= js && j < js + 2) || (j >= je && j < je + 2);
-      if (!keep) {
-        real uu = RC(0.25) * (F3(ucc, i, j - 1) + F3(ucc, i + 1, j - 1) + F3(ucc, i, j) + F3(ucc, i + 1, j));
-        vn = (F3(vc, i, j) - uu * F2(g.cosa_v, i, j)) * RC(1.0);
-      }
-    }
-    if (j == js || j == je + 1) {
-      real y = F3(vc, i, j);
-      vn = y > 0 ? y / F2(g.sin_sg4, i, j - 1) : y / F2(g.sin_sg2, i, j);
-    }
-    W3(vcc, i, j) = vn;
+    const int j = y == 0 ? js : je + 1;
+    real vy = F3(vc, i, j);
+    W3(vcc, i, j) = vy > 0 ? vy / F2(g.sin_sg4, i, j - 1) : vy / F2(g.sin_sg2, i, j);
   });
   if (err != cudaSuccess) return err;
-  // uc_contra_x_edge (fxadv.py:74-94)
-  err = launch_box(Box{s, e + 2, js - 1, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+  err = launch_box(Box{0, 4, js + 2, je, 0, nz}, st, [=] __device__(int t, int x, int j, int k) {
     PT_SETUP(d, t, k);
-    bool rows = (j >= js - 1 && j < js + 1) || (j >= je && j < je + 2);
-    if (!rows) return;
-    bool keep = (i >= s && i < s + 2) || (i >= e && i < e + 2);
-    if (keep) return;
+    const int i = x < 2 ? s - 1 + x : e + x - 2;
+    real uu = RC(0.25) * (F3(ucc, i, j - 1) + F3(ucc, i + 1, j - 1) + F3(ucc, i, j) + F3(ucc, i + 1, j));
+    W3(vcc, i, j) = (F3(vc, i, j) - uu * F2(g.cosa_v, i, j)) * RC(1.0);
+  });
+  if (err != cudaSuccess) return err;
+  // uc_contra_x_edge (fxadv.py:74-94): rows js-1, js, je, je+1, columns
+  // is+2 .. ie-1
+  err = launch_box(Box{s + 2, e, 0, 4, 0, nz}, st, [=] __device__(int t, int i, int y, int k) {
+    PT_SETUP(d, t, k);
+    const int j = y < 2 ? js - 1 + y : je + y - 2;
     real vv = RC(0.25) * (F3(vcc, i - 1, j) + F3(vcc, i, j) + F3(vcc, i - 1, j + 1) + F3(vcc, i, j + 1));
     W3(ucc, i, j) = (F3(uc, i, j) - vv * F2(g.cosa_u, i, j)) * RC(1.0);
   });
