@@ -7,6 +7,8 @@
   the mismatch of the tile-edge fluxes, which each side of an edge computes
   on its own (the oracle measures that level at C12 L8: 6.9e-9 relative
   after two substeps).
+* Symmetry: on a zonally symmetric state the two first equatorial tiles stay
+  alike.
 
 The oracle checks hold on the CPU; the GPU checks run the same properties
 at the full C384 L79 size, where the oracle is too slow to compare against.
@@ -49,6 +51,32 @@ def test_oracle_conserves_mass_up_to_edge_fluxes():
     area = np.asarray(cases.grid_for(n).area)
     m0, m1 = _mass(case["delp"], area, n, nz), _mass(out["delp"], area, n, nz)
     assert abs(m1 - m0) / m0 <= 2e-8
+
+
+def test_oracle_equatorial_tiles_agree_on_a_zonal_state():
+    """The two first equatorial tiles carry identical grids (to rounding) and,
+    for a zonally symmetric state (the baroclinic jet without noise or
+    tracers), identical fields; after a call they must still agree up to the
+    substep's amplification of that rounding.  A halo exchanged with the
+    wrong neighbour, orientation or vector sign breaks this at O(1)."""
+    import oracle_runs
+    from fv3core_b200 import constants as C
+    from fv3core_b200.initial_state import baroclinic_state
+
+    n, nz = 12, 8
+    st = baroclinic_state(cases.grid_for(n), nz, seed=0, noise=0.0, ntracers=0)
+    shp = st["delp"].shape
+    case = {k: np.array(st[k], copy=True) for k in cases.ACOUSTIC_STATE if k in st}
+    case["wsd"] = np.zeros(shp[:3])
+    for k in ("omga", "ua", "va", "uc", "vc", "mfxd", "mfyd", "cxd", "cyd", "diss_estd"):
+        case[k] = np.zeros(shp)
+    case.update(ak=np.asarray(st["ak"]), bk=np.asarray(st["bk"]), pfull=np.asarray(st["pfull"]),
+                ptop=st["ptop"], ks=st["ks"], mdt=75.0, n_map=1, akap=C.KAPPA, n_split=2)
+    out = oracle_runs.run_acoustics(case, n, nz)
+    bounds = {"u": 1e-5, "v": 1e-5, "delp": 1e-6, "pt": 1e-6, "delz": 1e-6, "w": 1e-2}
+    for k, bound in bounds.items():
+        a, b = _c(out[k][0:1], n, nz), _c(out[k][1:2], n, nz)
+        assert np.max(np.abs(a - b)) <= bound * np.max(np.abs(b)), k
 
 
 # ---------------------------------------------------------------- full size
