@@ -13,6 +13,11 @@ int main(int argc, char** argv) {
       if (fv3b::copy_corner_y(d, i, j, si, sj)) printf("cy %d %d %d %d\n", i, j, si, sj);
       if (fv3b::bgrid_corner_x(d, i, j, si, sj)) printf("bx %d %d %d %d\n", i, j, si, sj);
       if (fv3b::bgrid_corner_y(d, i, j, si, sj)) printf("by %d %d %d %d\n", i, j, si, sj);
+      fv3b::CornerRule r;
+      if (fv3b::corner_x(d, i, j, true, 1.0, 1.0, 1.0, 1.0, r)) printf("x3 %d %d %d %d\n", i, j, i + r.di, j + r.dj);
+      if (fv3b::corner_x(d, i, j, false, 1.0, 1.0, 1.0, 1.0, r)) printf("x2 %d %d %d %d\n", i, j, i + r.di, j + r.dj);
+      if (fv3b::corner_y(d, i, j, true, 1.0, 1.0, 1.0, 1.0, r)) printf("y3 %d %d %d %d\n", i, j, i + r.di, j + r.dj);
+      if (fv3b::corner_y(d, i, j, false, 1.0, 1.0, 1.0, 1.0, r)) printf("y2 %d %d %d %d\n", i, j, i + r.di, j + r.dj);
     }
   return 0;
 }
