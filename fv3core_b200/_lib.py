@@ -49,6 +49,7 @@ CTX_SIGNATURES = {
     "fv3b_update_dz_d_setup": [P, ctypes.c_int],
     "fv3b_update_dz_d": [P] * 7 + [D, P],
     "fv3b_p_grad_c": [P] * 5 + [D, P],
+    "fv3b_p_grad_c_adjoint": [P] * 8 + [D, P],
     "fv3b_nh_p_grad": [P] * 6 + [D, D, D, P],
     "fv3b_edge_pe": [P, P, D, P],
     "fv3b_pk3_halo": [P, P, D, D, P],

@@ -5,6 +5,10 @@
 hand-written adjoints (``fv3b_riem_solver3_adjoint``,
 ``fv3b_riem_solver_c_adjoint``).
 
+``p_grad_c(uc, vc, delpc, pkc, gz, stencil_factory, dt2)`` (reference
+``dyn_core.py:101-145``) returns the new (uc, vc), its backward pass being
+``fv3b_p_grad_c_adjoint``.
+
 These are the stages of the acoustic substep with an adjoint so far; the
 others have none yet, so a whole substep cannot be differentiated.
 
@@ -19,6 +23,7 @@ tensors in the kernel layout of ``grid_indexing``.
 import torch
 
 from . import _lib
+from .stencils._common import context
 from .storage import check_field, stream_ptr
 
 
@@ -113,3 +118,37 @@ def riem_solver_c(w3, gz, delpc, ptc, cappa, hs, ws, q_con, grid_indexing, dt2, 
     """New (pef, gz) of RiemannSolverC on the columns is-1..ie+1,
     differentiable with respect to w3, gz, delpc and ptc."""
     return RiemannSolverCFunction.apply(w3, gz, delpc, ptc, cappa, hs, ws, q_con, grid_indexing, dt2, ptop, p_fac)
+
+
+class PGradCFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, uc, vc, delpc, pkc, gz, stencil_factory, dt2):
+        gi = stencil_factory.grid_indexing
+        f3 = lambda t, n: check_field(t, gi, "3d", n)  # noqa: E731
+        uc_new, vc_new = uc.detach().clone(), vc.detach().clone()
+        _lib.call_ctx("fv3b_p_grad_c", context(stencil_factory), f3(uc_new, "uc"), f3(vc_new, "vc"),
+                      f3(delpc, "delpc"), f3(pkc, "pkc"), f3(gz, "gz"), float(dt2), stream_ptr())
+        ctx.save_for_backward(delpc.detach(), pkc.detach(), gz.detach())
+        ctx.params = (stencil_factory, float(dt2))
+        return uc_new, vc_new
+
+    @staticmethod
+    def backward(ctx, g_uc, g_vc):
+        delpc, pkc, gz = ctx.saved_tensors
+        stencil_factory, dt2 = ctx.params
+        gi = stencil_factory.grid_indexing
+        f3 = lambda t, n: check_field(t, gi, "3d", n)  # noqa: E731
+        g_uc = torch.zeros_like(delpc) if g_uc is None else g_uc.contiguous()
+        g_vc = torch.zeros_like(delpc) if g_vc is None else g_vc.contiguous()
+        grads = [torch.zeros_like(delpc) for _ in range(3)]  # delpc, pkc, gz
+        _lib.call_ctx("fv3b_p_grad_c_adjoint", context(stencil_factory), f3(delpc, "delpc"), f3(pkc, "pkc"),
+                      f3(gz, "gz"), f3(g_uc, "gu"), f3(g_vc, "gv"), f3(grads[0], "g_delpc"), f3(grads[1], "g_pkc"),
+                      f3(grads[2], "g_gz"), dt2, stream_ptr())
+        # the winds only gain increments: their gradients pass through
+        return g_uc, g_vc, grads[0], grads[1], grads[2], None, None
+
+
+def p_grad_c(uc, vc, delpc, pkc, gz, stencil_factory, dt2):
+    """New (uc, vc) of p_grad_c_stencil, differentiable with respect to all
+    five fields."""
+    return PGradCFunction.apply(uc, vc, delpc, pkc, gz, stencil_factory, dt2)

@@ -237,6 +237,18 @@ int fv3b_p_grad_c(fv3b_ctx* ctx, fv3b_real* uc, fv3b_real* vc, const fv3b_real* 
                   const fv3b_real* gz, double dt2, void* stream);
 
 /*
+ * Adjoint of fv3b_p_grad_c (no reference counterpart).  Given the inputs
+ * delpc, pkc, gz of the forward call and the cotangents gu, gv of the new
+ * uc, vc, writes the gradients g_delpc, g_pkc, g_gz of <gu, uc_new> +
+ * <gv, vc_new> on [is-1, ie+1] x [js-1, je+1] x levels 0..npz (g_delpc is
+ * 0 on level npz); the caller zeroes the points outside that box.  The
+ * gradients of uc and vc are gu and gv themselves.
+ */
+int fv3b_p_grad_c_adjoint(fv3b_ctx* ctx, const fv3b_real* delpc, const fv3b_real* pkc, const fv3b_real* gz,
+                          const fv3b_real* gu, const fv3b_real* gv, fv3b_real* g_delpc, fv3b_real* g_pkc,
+                          fv3b_real* g_gz, double dt2, void* stream);
+
+/*
  * NonHydrostaticPressureGradient.__call__ (fv3core/stencils/nh_p_grad.py:147-206).
  * pp, pk3 and gz are replaced by their B-grid values, as in the reference.
  */
