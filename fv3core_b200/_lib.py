@@ -35,8 +35,8 @@ class GridDims(ctypes.Structure):
 SIGNATURES = {
     "fv3b_riem_solver_c": [D, D, D, P, P, P, P, P, P, P, P, P, P],
     "fv3b_riem_solver3": [ctypes.c_int, D, D, D] + [P] * 14 + [P],
-    "fv3b_riem_solver3_adjoint": [D, D, D] + [P] * 13 + [P],
-    "fv3b_riem_solver_c_adjoint": [D, D, D] + [P] * 13 + [P],
+    "fv3b_riem_solver3_adjoint": [D, D, D] + [P] * 14 + [P],
+    "fv3b_riem_solver_c_adjoint": [D, D, D] + [P] * 14 + [P],
     "fv3b_del2cubed_noalloc": [P, P, D, ctypes.c_int, P],
 }
 

@@ -17,7 +17,8 @@ ptop, p_fac)`` returns the new (w, delz) of the compute-domain columns;
 ``riem_solver_c(w3, gz, delpc, ptc, cappa, hs, ws, q_con, grid_indexing,
 dt2, ptop, p_fac)`` returns the new (pef, gz) of the columns is-1..ie+1.
 Neither changes its inputs; gradients flow to the first four arguments
-(cappa, q_con and the surface terms are held fixed).  Fields are device
+and to the surface w (wsd, ws); cappa, q_con and the surface heights are
+held fixed.  Fields are device
 tensors in the kernel layout of ``grid_indexing``.
 """
 import torch
@@ -42,7 +43,7 @@ class RiemannSolver3Function(torch.autograd.Function):
             f3(scratch[1], "ppe"), f3(scratch[2], "pk3"), f3(scratch[3], "pk"), f3(scratch[4], "peln"),
             f3(w_new, "w"), stream_ptr(), precision=gi.precision,
         )
-        ctx.save_for_backward(w.detach(), zh.detach(), delp.detach(), pt.detach(), cappa, wsd, q_con)
+        ctx.save_for_backward(w.detach(), zh.detach(), delp.detach(), pt.detach(), cappa, wsd.detach(), q_con)
         ctx.params = (gi, float(dt), float(ptop), float(p_fac))
         return w_new, delz
 
@@ -54,11 +55,13 @@ class RiemannSolver3Function(torch.autograd.Function):
         gw_out = torch.zeros_like(w) if g_w_new is None else g_w_new.contiguous()
         gdz_out = torch.zeros_like(w) if g_delz is None else g_delz.contiguous()
         grads = [torch.zeros_like(w) for _ in range(4)]  # w, zh, delp, pt
+        g_wsd = torch.zeros_like(wsd)
         _lib.call(
             "fv3b_riem_solver3_adjoint", gi.dims(), dt, ptop, p_fac, f3(cappa, "cappa"),
             check_field(wsd, gi, "2d", "wsd"), f3(q_con, "q_con"), f3(delp, "delp"), f3(pt, "pt"), f3(zh, "zh"),
             f3(w, "w"), f3(gw_out, "gw_out"), f3(gdz_out, "gdz_out"), f3(grads[0], "g_w"), f3(grads[1], "g_zh"),
-            f3(grads[2], "g_delp"), f3(grads[3], "g_pt"), stream_ptr(), precision=gi.precision,
+            f3(grads[2], "g_delp"), f3(grads[3], "g_pt"), check_field(g_wsd, gi, "2d", "g_wsd"), stream_ptr(),
+            precision=gi.precision,
         )
         # w_new is w itself outside the solved points (other columns, the
         # bottom interface level): there the gradient passes through
@@ -66,12 +69,12 @@ class RiemannSolver3Function(torch.autograd.Function):
         solved = torch.zeros_like(w, dtype=torch.bool)
         solved[:, :nz, h:h + n, h:h + n] = True
         grads[0] = torch.where(solved, grads[0], gw_out)
-        return grads[0], grads[1], grads[2], grads[3], None, None, None, None, None, None, None, None
+        return grads[0], grads[1], grads[2], grads[3], None, None, g_wsd, None, None, None, None, None
 
 
 def riem_solver3(w, zh, delp, pt, cappa, zs, wsd, q_con, grid_indexing, dt, ptop, p_fac):
     """New (w, delz) of RiemannSolver3 on the compute domain, differentiable
-    with respect to w, zh, delp and pt."""
+    with respect to w, zh, delp, pt and wsd."""
     return RiemannSolver3Function.apply(w, zh, delp, pt, cappa, zs, wsd, q_con, grid_indexing, dt, ptop, p_fac)
 
 
@@ -87,7 +90,7 @@ class RiemannSolverCFunction(torch.autograd.Function):
             f3(delpc, "delpc"), f3(gz_new, "gz"), f3(pef, "pef"), f3(w3, "w3"), stream_ptr(),
             precision=gi.precision,
         )
-        ctx.save_for_backward(w3.detach(), gz.detach(), delpc.detach(), ptc.detach(), cappa, ws, q_con)
+        ctx.save_for_backward(w3.detach(), gz.detach(), delpc.detach(), ptc.detach(), cappa, ws.detach(), q_con)
         ctx.params = (gi, float(dt2), float(ptop), float(p_fac))
         return pef, gz_new
 
@@ -99,24 +102,25 @@ class RiemannSolverCFunction(torch.autograd.Function):
         gpef_out = torch.zeros_like(gz) if g_pef is None else g_pef.contiguous()
         ggz_out = torch.zeros_like(gz) if g_gz is None else g_gz.contiguous()
         grads = [torch.zeros_like(gz) for _ in range(4)]  # w3, gz, delpc, ptc
+        g_ws = torch.zeros_like(ws)
         _lib.call(
             "fv3b_riem_solver_c_adjoint", gi.dims(), dt2, ptop, p_fac, f3(cappa, "cappa"),
             check_field(ws, gi, "2d", "ws"), f3(q_con, "q_con"), f3(delpc, "delpc"), f3(ptc, "ptc"),
             f3(gz, "gz"), f3(w3, "w3"), f3(gpef_out, "gpef_out"), f3(ggz_out, "ggz_out"), f3(grads[0], "g_w3"),
-            f3(grads[1], "g_gz"), f3(grads[2], "g_delpc"), f3(grads[3], "g_ptc"), stream_ptr(),
-            precision=gi.precision,
+            f3(grads[1], "g_gz"), f3(grads[2], "g_delpc"), f3(grads[3], "g_ptc"), check_field(g_ws, gi, "2d", "g_ws"),
+            stream_ptr(), precision=gi.precision,
         )
         # gz outside the solved columns is gz itself: the gradient passes through
         h, n = gi.n_halo, gi.n
         solved = torch.zeros_like(gz, dtype=torch.bool)
         solved[:, :, h - 1:h + n + 1, h - 1:h + n + 1] = True
         grads[1] = grads[1] + torch.where(solved, torch.zeros_like(ggz_out), ggz_out)
-        return grads[0], grads[1], grads[2], grads[3], None, None, None, None, None, None, None, None
+        return grads[0], grads[1], grads[2], grads[3], None, None, g_ws, None, None, None, None, None
 
 
 def riem_solver_c(w3, gz, delpc, ptc, cappa, hs, ws, q_con, grid_indexing, dt2, ptop, p_fac):
     """New (pef, gz) of RiemannSolverC on the columns is-1..ie+1,
-    differentiable with respect to w3, gz, delpc and ptc."""
+    differentiable with respect to w3, gz, delpc, ptc and ws."""
     return RiemannSolverCFunction.apply(w3, gz, delpc, ptc, cappa, hs, ws, q_con, grid_indexing, dt2, ptop, p_fac)
 
 

@@ -1,8 +1,8 @@
 // Hand-written adjoints (reverse mode) of the two vertically implicit
 // solvers' column work: Sim1Solver (sim1_solver.py:11-105) shared by both,
 // with the precompute and finalize of RiemannSolver3 (riem_solver3.py:24-67)
-// and of RiemannSolverC (riem_solver_c.py:13-64).  cappa, q_con and the
-// surface terms are held fixed.  Written for both the device and the host
+// and of RiemannSolverC (riem_solver_c.py:13-64).  Written for both the
+// device and the host
 // (the tests build it with g++ and compare with torch autograd of a
 // PyTorch-ops restatement).
 //
@@ -10,7 +10,8 @@
 // solver (the library's exp and log), and kept in per-level arrays; the
 // reverse sweep then runs every forward step backwards.  The branch of the
 // pressure floor (maxp) is taken as the forward took it.  Columns need at
-// least four interface levels (three layers).
+// least four interface levels (three layers).  cappa, q_con and the
+// surface height are held fixed; the surface w has its gradient.
 #pragma once
 
 #include "fmath.h"
@@ -27,14 +28,15 @@ constexpr double A_RGRAV = 1.0 / A_GRAV;
 // PT, CP3 (cappa), W1 (w at the start), pem (edge pressures, N + 1) and pm
 // (layer-mean pressures).  Forward outputs: w (aWF_in is its cotangent), the
 // pressure perturbation pe at interfaces 0..N (aPE_in) and dz (aDZ_in).
-// The adjoints of the inputs are added into aDM, aDZ, aPT, aW1, aPEM, aPM.
+// The adjoints of the inputs are added into aDM, aDZ, aPT, aW1, aPEM, aPM
+// and *aWSR (the surface w).
 template <int NK>
 __host__ __device__ inline void sim1_column_adjoint(int N, const double* DM, const double* DZ, const double* GM,
                                                     const double* PT, const double* CP3, const double* W1,
                                                     const double* pem, const double* pm, double wsr, double dt,
                                                     double p_fac, const double* aWF_in, const double* aPE_in,
                                                     const double* aDZ_in, double* aDM, double* aDZ, double* aPT,
-                                                    double* aW1, double* aPEM, double* aPM) {
+                                                    double* aW1, double* aPEM, double* aPM, double* aWSR) {
   double Xv[NK], Yv[NK], pe1[NK];
   double grat[NK], bb[NK], dd[NK], bet[NK], gam[NK], pp[NK], ppb[NK], aa[NK];
   double betw[NK], gw[NK], wpre[NK], wf[NK], pe[NK], p1[NK], maxp[NK], Ev[NK], dzv[NK];
@@ -149,6 +151,7 @@ __host__ __device__ inline void sim1_column_adjoint(int N, const double* DM, con
     aPPB[k + 1] += anum * dt;
     aPPB[k] -= anum * dt;
     double ap1t = -anum * wsr;
+    *aWSR += -anum * p1t;
     aAA[k] += -anum * wpre[k - 1];
     aW[k - 1] += -anum * aa[k];
     const double ab = aBETW[k];
@@ -273,13 +276,13 @@ __host__ __device__ inline void column_sums_adjoint(int N, const double* peg, co
 // interface levels (N = K - 1 layers); every pointer steps sk elements per
 // level.  Inputs w, zh, delp, pt, cappa, q_con; the cotangents gw_out (of
 // the new w) and gdz_out (of the new delz); results g_w, g_delp, g_pt on
-// layers and g_zh on interfaces (overwritten).
+// layers, g_zh on interfaces and *g_wsr for the surface w (overwritten).
 template <int NK, typename R, typename G>
 __host__ __device__ inline void riem3_column_adjoint(int K, long long sk, double dt, double ptop, double p_fac,
                                                      double wsr, const R* w, const R* zh, const R* delp,
                                                      const R* pt, const R* cappa, const R* q_con,
                                                      const G* gw_out, const G* gdz_out, G* g_w, G* g_zh,
-                                                     G* g_delp, G* g_pt) {
+                                                     G* g_delp, G* g_pt, G* g_wsr) {
   const int N = K - 1;
   double DM[NK], DZ[NK], GM[NK], PT[NK], CP3[NK], W1[NK], QC[NK];
   double pem[NK], peg[NK], lg[NK], L[NK], pm[NK];
@@ -309,9 +312,11 @@ __host__ __device__ inline void riem3_column_adjoint(int K, long long sk, double
     aWF[k] = gw_out[k * sk];
     aDZo[k] = gdz_out[k * sk];
   }
+  double aWSR = 0.0;
   sim1_column_adjoint<NK>(N, DM, DZ, GM, PT, CP3, W1, pem, pm, wsr, dt, p_fac, aWF, aPE, aDZo, aDM, aDZ, aPT, aW1,
-                          aPEM, aPM);
+                          aPEM, aPM, &aWSR);
   column_sums_adjoint<NK>(N, peg, L, pm, QC, aPM, aPEM, a_dp);
+  *g_wsr = aWSR;
   for (int k = 0; k <= N; ++k) g_zh[k * sk] = 0.0;
   for (int k = 0; k < N; ++k) {
     g_delp[k * sk] = a_dp[k] + aDM[k] * A_RGRAV;
@@ -327,13 +332,13 @@ __host__ __device__ inline void riem3_column_adjoint(int K, long long sk, double
 // ws; outputs pef (pe + pem on interfaces 1..N, ptop on top) and gz
 // (hs at the bottom, gz[k] = gz[k+1] - dz[k] g).  Cotangents gpef_out,
 // ggz_out on interfaces; results g_w3, g_delpc, g_ptc on layers and g_gz on
-// interfaces (the input heights).
+// interfaces (the input heights), *g_wsr for the surface w ws.
 template <int NK, typename R, typename G>
 __host__ __device__ inline void riemc_column_adjoint(int K, long long sk, double dt2, double ptop, double p_fac,
                                                      double wsr, const R* w3, const R* gz, const R* delpc,
                                                      const R* ptc, const R* cappa, const R* q_con,
                                                      const G* gpef_out, const G* ggz_out, G* g_w3, G* g_gz,
-                                                     G* g_delpc, G* g_ptc) {
+                                                     G* g_delpc, G* g_ptc, G* g_wsr) {
   const int N = K - 1;
   double DM[NK], DZ[NK], GM[NK], PT[NK], CP3[NK], W1[NK], QC[NK];
   double pem[NK], peg[NK], L[NK], pm[NK];
@@ -371,9 +376,11 @@ __host__ __device__ inline void riemc_column_adjoint(int K, long long sk, double
     acc += ggz_out[m * sk];
     aDZo[m] = -A_GRAV * acc;
   }
+  double aWSR = 0.0;
   sim1_column_adjoint<NK>(N, DM, DZ, GM, PT, CP3, W1, pem, pm, wsr, dt2, p_fac, aWF, aPE, aDZo, aDM, aDZ, aPT, aW1,
-                          aPEM, aPM);
+                          aPEM, aPM, &aWSR);
   column_sums_adjoint<NK>(N, peg, L, pm, QC, aPM, aPEM, a_dp);
+  *g_wsr = aWSR;
   for (int k = 0; k <= N; ++k) g_gz[k * sk] = 0.0;
   for (int k = 0; k < N; ++k) {
     g_delpc[k * sk] = a_dp[k] + aDM[k] / A_GRAV;

@@ -181,33 +181,33 @@ int fv3b_riem_solver3(const fv3b_grid_dims* dims, int last_call, double dt, doub
 /*
  * Adjoint of fv3b_riem_solver3's column solve (no reference counterpart: the
  * reference has no derivatives).  For the compute-domain columns, given the
- * solver's inputs w, zh, delp, pt (held fixed: cappa, q_con, wsd) and the
+ * solver's inputs w, zh, delp, pt, wsd (held fixed: cappa, q_con) and the
  * cotangents gw_out of the new w and gdz_out of the new delz (layer levels
- * 0..npz-1), writes the gradients g_w, g_delp, g_pt (layers) and g_zh
- * (interfaces 0..npz) of <gw_out, w_new> + <gdz_out, delz_new>.  The
- * branch of the pressure floor is the forward's.  Needs npz >= 3.  It
- * recomputes the forward column in the thread's local memory: correct, not
- * yet fast.
+ * 0..npz-1), writes the gradients g_w, g_delp, g_pt (layers), g_zh
+ * (interfaces 0..npz) and g_wsd (2-D, the surface w) of <gw_out, w_new> +
+ * <gdz_out, delz_new>.  The branch of the pressure floor is the forward's.
+ * Needs npz >= 3.  It recomputes the forward column in the thread's local
+ * memory: correct, not yet fast.
  */
 int fv3b_riem_solver3_adjoint(const fv3b_grid_dims* dims, double dt, double ptop, double p_fac,
                               const fv3b_real* cappa, const fv3b_real* wsd, const fv3b_real* q_con,
                               const fv3b_real* delp, const fv3b_real* pt, const fv3b_real* zh, const fv3b_real* w,
                               const fv3b_real* gw_out, const fv3b_real* gdz_out, fv3b_real* g_w, fv3b_real* g_zh,
-                              fv3b_real* g_delp, fv3b_real* g_pt, void* stream);
+                              fv3b_real* g_delp, fv3b_real* g_pt, fv3b_real* g_wsd, void* stream);
 
 /*
  * Adjoint of fv3b_riem_solver_c (no reference counterpart).  For the columns
- * is-1..ie+1 x js-1..je+1, given the solver's inputs w3, gz, delpc, ptc
- * (held fixed: cappa, q_con, ws, hs) and the cotangents gpef_out, ggz_out
+ * is-1..ie+1 x js-1..je+1, given the solver's inputs w3, gz, delpc, ptc, ws
+ * (held fixed: cappa, q_con, hs) and the cotangents gpef_out, ggz_out
  * of its outputs pef and gz (interfaces 0..npz), writes the gradients g_w3,
- * g_delpc, g_ptc (layers) and g_gz (the input heights, interfaces).  Same
- * conditions as fv3b_riem_solver3_adjoint.
+ * g_delpc, g_ptc (layers), g_gz (the input heights, interfaces) and g_ws
+ * (2-D, the surface w).  Same conditions as fv3b_riem_solver3_adjoint.
  */
 int fv3b_riem_solver_c_adjoint(const fv3b_grid_dims* dims, double dt2, double ptop, double p_fac,
                                const fv3b_real* cappa, const fv3b_real* ws, const fv3b_real* q_con,
                                const fv3b_real* delpc, const fv3b_real* ptc, const fv3b_real* gz, const fv3b_real* w3,
                                const fv3b_real* gpef_out, const fv3b_real* ggz_out, fv3b_real* g_w3,
-                               fv3b_real* g_gz, fv3b_real* g_delpc, fv3b_real* g_ptc, void* stream);
+                               fv3b_real* g_gz, fv3b_real* g_delpc, fv3b_real* g_ptc, fv3b_real* g_ws, void* stream);
 
 /*
  * UpdateGeopotentialHeightOnCGrid.__call__ (fv3core/stencils/updatedzc.py:123-163).

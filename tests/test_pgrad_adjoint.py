@@ -157,3 +157,59 @@ def test_gpu_adjoint_matches_torch_autograd():
         b = ref[k]
         err = np.max(np.abs(a - b)) / np.max(np.abs(b))
         assert err <= 1e-12, (k, err)
+
+
+@pytest.mark.gpu
+def test_gpu_chain_riemann_c_then_p_grad_c_matches_torch_autograd():
+    # RiemannSolverC's pef and gz feed p_grad_c as pkc and gz (dyn_core.py
+    # acoustic loop): the two autograd Functions compose on the device
+    import gpu_runs
+    import torch_riem3
+    from test_riem_adjoint import riemc_case
+
+    from fv3core_b200.adjoint import p_grad_c, riem_solver_c
+    from fv3core_b200.storage import to_device
+
+    n, nz = 12, 16
+    K = nz + 1
+    case, cols, par = riemc_case(n, nz)
+    rng = np.random.default_rng(21)
+    shp = case["delpc"].shape
+    case["uc"], case["vc"] = 10 * rng.standard_normal(shp), 10 * rng.standard_normal(shp)
+    leaves = ("w3", "gz", "delpc", "ptc", "uc", "vc")
+    gd, sf = gpu_runs.device_grid(n, nz)
+    dev = {k: to_device(case[k]) for k in leaves + ("cappa", "q_con", "hs", "ws")}
+    for k in leaves:
+        dev[k].requires_grad_(True)
+    pef, gz = riem_solver_c(dev["w3"], dev["gz"], dev["delpc"], dev["ptc"], dev["cappa"], dev["hs"], dev["ws"],
+                            dev["q_con"], sf.grid_indexing, par["dt2"], par["ptop"], par["p_fac"])
+    uc, vc = p_grad_c(dev["uc"], dev["vc"], dev["delpc"], pef, gz, sf, par["dt2"])
+    gu, gv = rng.standard_normal(uc.shape), rng.standard_normal(vc.shape)
+    ((uc * torch.from_numpy(gu).cuda()).sum() + (vc * torch.from_numpy(gv).cuda()).sum()).backward()
+
+    # the same chain in torch ops on the host, with kernel-layout leaves
+    T = {k: torch.from_numpy(kernel_layout(case[k])).requires_grad_(True) for k in leaves}
+    R = slice(H - 1, H + n + 1)
+
+    def cols_of(t):
+        return t[:, :, R, R].permute(0, 3, 2, 1).reshape(6 * (n + 2) ** 2, -1)
+
+    def full_of(c):
+        return c.reshape(6, n + 2, n + 2, K).permute(0, 3, 2, 1)
+
+    fixed = {k: torch.from_numpy(cols[k]) for k in ("cappa", "q_con", "hs", "ws")}
+    pef_c, gz_c = torch_riem3.riemc_columns(cols_of(T["w3"]), cols_of(T["gz"]), cols_of(T["delpc"]),
+                                            cols_of(T["ptc"]), fixed["cappa"], fixed["q_con"], fixed["hs"],
+                                            fixed["ws"], par["dt2"], par["ptop"], par["p_fac"])
+    pef_t = torch.zeros_like(T["gz"])
+    pef_t[:, :, R, R] = full_of(pef_c)
+    gz_t = T["gz"].clone()
+    gz_t[:, :, R, R] = full_of(gz_c)
+    rdxc, rdyc = (torch.from_numpy(a) for a in _metrics(n))
+    f = {"uc": T["uc"], "vc": T["vc"], "delpc": T["delpc"], "pkc": pef_t, "gz": gz_t}
+    uc_t, vc_t = p_grad_c_torch(f, rdxc, rdyc, par["dt2"], n, nz)
+    ((uc_t * torch.from_numpy(gu)).sum() + (vc_t * torch.from_numpy(gv)).sum()).backward()
+    for k in leaves:
+        a, b = dev[k].grad.cpu().numpy(), T[k].grad.numpy()
+        err = np.max(np.abs(a - b)) / np.max(np.abs(b))
+        assert err <= 1e-10, (k, err)

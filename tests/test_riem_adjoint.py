@@ -33,14 +33,14 @@ def riem3_case(n=12, nz=8, seed=5):
 
 def torch_grads(cols, par, gw, gdz):
     T = {k: torch.from_numpy(v.copy()) for k, v in cols.items()}
-    for k in ("w", "zh", "delp", "pt"):
+    for k in ("w", "zh", "delp", "pt", "wsr"):
         T[k].requires_grad_(True)
     w_new, dz_new = torch_riem3.riem3_columns(T["w"], T["zh"], T["delp"], T["pt"], T["cappa"], T["q_con"], T["wsr"],
                                               par["dt"], par["ptop"], par["p_fac"])
     loss = (w_new * torch.from_numpy(gw)).sum() + (dz_new * torch.from_numpy(gdz)).sum()
     loss.backward()
     K = cols["zh"].shape[1]
-    return {k: T[k].grad.numpy() for k in ("w", "zh", "delp", "pt")}, K
+    return {k: T[k].grad.numpy() for k in ("w", "zh", "delp", "pt", "wsr")}, K
 
 
 @pytest.fixture(scope="module")
@@ -67,14 +67,15 @@ def test_host_adjoint_matches_torch_autograd(host_adjoint):
     gw_k = np.zeros((ncol, K)); gw_k[:, :K - 1] = gw
     gdz_k = np.zeros((ncol, K)); gdz_k[:, :K - 1] = gdz
     out = {k: np.zeros((ncol, K)) for k in ("w", "zh", "delp", "pt")}
+    out["wsr"] = np.zeros(ncol)
     f = host_adjoint.riem3_adjoint_columns
     f.restype = None
     f(ctypes.c_int(ncol), ctypes.c_int(K), ctypes.c_double(par["dt"]), ctypes.c_double(par["ptop"]),
       ctypes.c_double(par["p_fac"]), _ptr(cols["wsr"]), _ptr(cols["w"]), _ptr(cols["zh"]), _ptr(cols["delp"]),
       _ptr(cols["pt"]), _ptr(cols["cappa"]), _ptr(cols["q_con"]), _ptr(gw_k), _ptr(gdz_k),
-      _ptr(out["w"]), _ptr(out["zh"]), _ptr(out["delp"]), _ptr(out["pt"]))
-    for k, width in (("w", K - 1), ("zh", K), ("delp", K - 1), ("pt", K - 1)):
-        a, b = out[k][:, :width], ref[k][:, :width]
+      _ptr(out["w"]), _ptr(out["zh"]), _ptr(out["delp"]), _ptr(out["pt"]), _ptr(out["wsr"]))
+    for k, width in (("w", K - 1), ("zh", K), ("delp", K - 1), ("pt", K - 1), ("wsr", None)):
+        a, b = (out[k], ref[k]) if width is None else (out[k][:, :width], ref[k][:, :width])
         err = np.max(np.abs(a - b)) / np.max(np.abs(b))
         assert err <= 1e-12, (k, err)
 
@@ -93,7 +94,7 @@ def riemc_case(n=12, nz=16, seed=11):
 def riemc_torch(cols, par, requires_grad=False):
     T = {k: torch.from_numpy(v.copy()) for k, v in cols.items()}
     if requires_grad:
-        for k in ("w3", "gz", "delpc", "ptc"):
+        for k in ("w3", "gz", "delpc", "ptc", "ws"):
             T[k].requires_grad_(True)
     pef, gz = torch_riem3.riemc_columns(T["w3"], T["gz"], T["delpc"], T["ptc"], T["cappa"], T["q_con"], T["hs"],
                                         T["ws"], par["dt2"], par["ptop"], par["p_fac"])
@@ -126,14 +127,16 @@ def test_host_riemc_adjoint_matches_torch_autograd(host_adjoint):
     T, pef, gz = riemc_torch(cols, par, requires_grad=True)
     ((pef * torch.from_numpy(gpef)).sum() + (gz * torch.from_numpy(ggz)).sum()).backward()
     out = {k: np.zeros((ncol, K)) for k in ("w3", "gz", "delpc", "ptc")}
+    out["ws"] = np.zeros(ncol)
     f = host_adjoint.riemc_adjoint_columns
     f.restype = None
     f(ctypes.c_int(ncol), ctypes.c_int(K), ctypes.c_double(par["dt2"]), ctypes.c_double(par["ptop"]),
       ctypes.c_double(par["p_fac"]), _ptr(cols["ws"]), _ptr(cols["w3"]), _ptr(cols["gz"]), _ptr(cols["delpc"]),
       _ptr(cols["ptc"]), _ptr(cols["cappa"]), _ptr(cols["q_con"]), _ptr(gpef), _ptr(ggz),
-      _ptr(out["w3"]), _ptr(out["gz"]), _ptr(out["delpc"]), _ptr(out["ptc"]))
-    for k, width in (("w3", K - 1), ("gz", K), ("delpc", K - 1), ("ptc", K - 1)):
-        a, b = out[k][:, :width], T[k].grad.numpy()[:, :width]
+      _ptr(out["w3"]), _ptr(out["gz"]), _ptr(out["delpc"]), _ptr(out["ptc"]), _ptr(out["ws"]))
+    for k, width in (("w3", K - 1), ("gz", K), ("delpc", K - 1), ("ptc", K - 1), ("ws", None)):
+        b = T[k].grad.numpy()
+        a, b = (out[k], b) if width is None else (out[k][:, :width], b[:, :width])
         err = np.max(np.abs(a - b)) / np.max(np.abs(b))
         assert err <= 1e-12, (k, err)
 
@@ -153,7 +156,7 @@ def test_torch_restatement_gradients_match_finite_differences():
         return float((w_new.numpy() * gw).sum() + (dz_new.numpy() * gdz).sum())
 
     for trial in range(4):
-        d = {k: rng.standard_normal(cols[k].shape) * np.abs(cols[k]) for k in ("w", "zh", "delp", "pt")}
+        d = {k: rng.standard_normal(cols[k].shape) * np.abs(cols[k]) for k in ("w", "zh", "delp", "pt", "wsr")}
         eps = 1e-6
         cp = {k: v.copy() for k, v in cols.items()}
         cm = {k: v.copy() for k, v in cols.items()}
@@ -200,7 +203,7 @@ def test_gpu_adjoint_matches_torch_autograd(n, nz, seed):
 
     dev, cols, par = _device_case(n, nz, seed)
     gi = GridIndexing((n, n, nz), H)
-    for k in ("w", "zh", "delp", "pt"):
+    for k in ("w", "zh", "delp", "pt", "wsd"):
         dev[k].requires_grad_(True)
     w_new, dz_new = riem_solver3(dev["w"], dev["zh"], dev["delp"], dev["pt"], dev["cappa"], dev["zs"], dev["wsd"],
                                  dev["q_con"], gi, par["dt"], par["ptop"], par["p_fac"])
@@ -216,9 +219,14 @@ def test_gpu_adjoint_matches_torch_autograd(n, nz, seed):
         b = ref[k][:, :width]
         err = np.max(np.abs(a - b)) / np.max(np.abs(b))
         assert err <= 1e-10, (k, err)
-    # outside the solved points w passes through
     from fv3core_b200.storage import to_host
 
+    g_wsd = to_host(dev["wsd"].grad)
+    err = np.max(np.abs(g_wsd[:, H:H + n, H:H + n].reshape(-1) - ref["wsr"])) / np.max(np.abs(ref["wsr"]))
+    assert err <= 1e-10, ("wsd", err)
+    g_wsd[:, H:H + n, H:H + n] = 0.0
+    assert not g_wsd.any()
+    # outside the solved points w passes through
     gw_h, gwgrad_h = to_host(gw), to_host(dev["w"].grad)
     outside = np.ones(gw_h.shape, bool)
     outside[:, H:H + n, H:H + n, :nz] = False
@@ -265,7 +273,7 @@ def test_gpu_riemc_adjoint_matches_torch_autograd():
     case, cols, par = riemc_case(n, nz)
     gi = GridIndexing((n, n, nz), H)
     dev = {k: to_device(case[k]) for k in ("w3", "gz", "delpc", "ptc", "cappa", "q_con", "hs", "ws")}
-    for k in ("w3", "gz", "delpc", "ptc"):
+    for k in ("w3", "gz", "delpc", "ptc", "ws"):
         dev[k].requires_grad_(True)
     pef, gz = riem_solver_c(dev["w3"], dev["gz"], dev["delpc"], dev["ptc"], dev["cappa"], dev["hs"], dev["ws"],
                             dev["q_con"], gi, par["dt2"], par["ptop"], par["p_fac"])
@@ -286,3 +294,7 @@ def test_gpu_riemc_adjoint_matches_torch_autograd():
         b = T[k].grad.numpy()[:, :width]
         err = np.max(np.abs(a - b)) / np.max(np.abs(b))
         assert err <= 1e-10, (k, err)
+    g_ws = to_host(dev["ws"].grad)
+    b = T["ws"].grad.numpy()
+    err = np.max(np.abs(g_ws[sl].reshape(-1) - b)) / np.max(np.abs(b))
+    assert err <= 1e-10, ("ws", err)
