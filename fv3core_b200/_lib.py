@@ -46,6 +46,7 @@ CTX_SIGNATURES = {
     "fv3b_d_sw_setup": [P],
     "fv3b_d_sw": [P] * 24 + [D, P],
     "fv3b_update_dz_c": [P] * 6 + [D, P],
+    "fv3b_update_dz_c_adjoint": [P] * 9 + [D, P],
     "fv3b_update_dz_d_setup": [P, ctypes.c_int],
     "fv3b_update_dz_d": [P] * 7 + [D, P],
     "fv3b_p_grad_c": [P] * 5 + [D, P],

@@ -8,6 +8,9 @@ hand-written adjoints (``fv3b_riem_solver3_adjoint``,
 ``p_grad_c(uc, vc, delpc, pkc, gz, stencil_factory, dt2)`` (reference
 ``dyn_core.py:101-145``) returns the new (uc, vc), its backward pass being
 ``fv3b_p_grad_c_adjoint``.
+``update_dz_c(dp_ref, zs, ut, vt, gz, ws, stencil_factory, dt)`` (reference
+``updatedzc.py:123-163``) returns the new (gz, ws), its backward pass being
+``fv3b_update_dz_c_adjoint`` (dp_ref and zs held fixed).
 
 These are the stages of the acoustic substep with an adjoint so far; the
 others have none yet, so a whole substep cannot be differentiated.
@@ -156,3 +159,43 @@ def p_grad_c(uc, vc, delpc, pkc, gz, stencil_factory, dt2):
     """New (uc, vc) of p_grad_c_stencil, differentiable with respect to all
     five fields."""
     return PGradCFunction.apply(uc, vc, delpc, pkc, gz, stencil_factory, dt2)
+
+
+class UpdateDzCFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, ut, vt, gz, ws, dp_ref, zs, stencil_factory, dt):
+        gi = stencil_factory.grid_indexing
+        f3 = lambda t, n: check_field(t, gi, "3d", n)  # noqa: E731
+        gz_new, ws_new = gz.detach().clone(), ws.detach().clone()
+        _lib.call_ctx("fv3b_update_dz_c", context(stencil_factory), check_field(dp_ref, gi, "1d", "dp_ref"),
+                      check_field(zs, gi, "2d", "zs"), f3(ut, "ut"), f3(vt, "vt"), f3(gz_new, "gz"),
+                      check_field(ws_new, gi, "2d", "ws"), float(dt), stream_ptr())
+        ctx.save_for_backward(ut.detach(), vt.detach(), gz.detach(), dp_ref)
+        ctx.params = (stencil_factory, float(dt))
+        return gz_new, ws_new
+
+    @staticmethod
+    def backward(ctx, g_gz, g_ws):
+        ut, vt, gz, dp_ref = ctx.saved_tensors
+        stencil_factory, dt = ctx.params
+        gi = stencil_factory.grid_indexing
+        f3 = lambda t, n: check_field(t, gi, "3d", n)  # noqa: E731
+        g_gz = torch.zeros_like(gz) if g_gz is None else g_gz.contiguous()
+        m = gi.max_shape[0]
+        g_ws = torch.zeros((6, m, m), dtype=gz.dtype, device=gz.device) if g_ws is None else g_ws.contiguous()
+        grads = [torch.empty_like(gz) for _ in range(3)]  # gz, ut, vt
+        _lib.call_ctx("fv3b_update_dz_c_adjoint", context(stencil_factory), check_field(dp_ref, gi, "1d", "dp_ref"),
+                      f3(ut, "ut"), f3(vt, "vt"), f3(gz, "gz"), f3(g_gz, "g_gz_out"),
+                      check_field(g_ws, gi, "2d", "g_ws"), f3(grads[0], "g_gz"), f3(grads[1], "g_ut"),
+                      f3(grads[2], "g_vt"), dt, stream_ptr())
+        # ws keeps its value outside the updated box: there its gradient passes through
+        h, n = gi.n_halo, gi.n
+        g_ws_in = g_ws.clone()
+        g_ws_in[:, h - 1:h + n + 1, h - 1:h + n + 1] = 0.0
+        return grads[1], grads[2], grads[0], g_ws_in, None, None, None, None
+
+
+def update_dz_c(dp_ref, zs, ut, vt, gz, ws, stencil_factory, dt):
+    """New (gz, ws) of UpdateGeopotentialHeightOnCGrid, differentiable with
+    respect to ut, vt, gz and ws."""
+    return UpdateDzCFunction.apply(ut, vt, gz, ws, dp_ref, zs, stencil_factory, dt)

@@ -218,6 +218,19 @@ int fv3b_update_dz_c(fv3b_ctx* ctx, const fv3b_real* dp_ref, const fv3b_real* zs
                      fv3b_real* gz, fv3b_real* ws, double dt, void* stream);
 
 /*
+ * Adjoint of fv3b_update_dz_c (no reference counterpart).  gz is the input
+ * heights of the forward call (before it updated them), ut and vt its
+ * fluxes; g_gz_out and g_ws are the cotangents of the new gz (3-D) and ws
+ * (2-D).  Writes, on every point, the gradients g_gz (of the input heights,
+ * the pass-through outside the updated box included), g_ut and g_vt.
+ * dp_ref, zs and the areas are held fixed; the upwind choices and the DZ_MIN
+ * floor are the forward's.  Uses the context's workspace.
+ */
+int fv3b_update_dz_c_adjoint(fv3b_ctx* ctx, const fv3b_real* dp_ref, const fv3b_real* ut, const fv3b_real* vt,
+                             const fv3b_real* gz, const fv3b_real* g_gz_out, const fv3b_real* g_ws, fv3b_real* g_gz,
+                             fv3b_real* g_ut, fv3b_real* g_vt, double dt, void* stream);
+
+/*
  * UpdateHeightOnDGrid.__init__ (fv3core/stencils/updatedzd.py:189-320):
  * dp_ref_host is the host [npz+1] reference layer thickness (dp0), hord_tm
  * the PPM order of the height transport.  Needs
