@@ -597,11 +597,63 @@ def run_ensemble(args):
         dist.destroy_process_group()
 
 
+def _time_c_grid_chain(args, st, zh, dev, timed):
+    """Forward and forward + backward times (ms) of the C-grid vertical
+    chain of the acoustic loop (dyn_core.py): UpdateGeopotentialHeightOnCGrid,
+    RiemannSolverC and p_grad_c, through their torch.autograd Functions."""
+    import numpy as np
+    import torch
+
+    from fv3core_b200.adjoint import p_grad_c, riem_solver_c, update_dz_c
+    from fv3core_b200.grid import CubedSphereGrid
+    from fv3core_b200.grid_data import GridData
+    from fv3core_b200.stencil import StencilConfig, StencilFactory
+    from fv3core_b200.storage import to_device
+
+    n, npz = args.adj_n, args.npz
+    grid = CubedSphereGrid(n, 3)
+    gd = GridData(grid, npz)
+    sf = StencilFactory(StencilConfig(), gd.grid_indexing)
+    ak, bk = np.asarray(st["ak"]), np.asarray(st["bk"])
+    dp_ref = np.zeros(npz + 1)
+    dp_ref[:npz] = ak[1:] - ak[:-1] + (bk[1:] - bk[:-1]) * 1.0e5
+    area = np.asarray(grid.area)[:, :, :, None]
+    rng = np.random.default_rng(3)
+    c = {k: to_device(v) for k, v in {
+        "ut": 0.02 * area * rng.standard_normal(zh.shape), "vt": 0.02 * area * rng.standard_normal(zh.shape),
+        "uc": 10.0 * rng.standard_normal(zh.shape), "vc": 10.0 * rng.standard_normal(zh.shape),
+        "dp_ref": dp_ref, "zs": st["phis"] * (1.0 / 9.80665), "hs": st["phis"], "ws": np.zeros(st["phis"].shape),
+    }.items()}
+    base = {"ut": c["ut"], "vt": c["vt"], "gz": to_device(zh), "w3": dev["w"], "delpc": dev["delp"],
+            "ptc": dev["pt"], "uc": c["uc"], "vc": c["vc"]}
+    x = {k: v.clone().requires_grad_(True) for k, v in base.items()}
+    dt2, ptop, p_fac = 225.0 / 12, float(st["ptop"]), 0.05
+    gen = torch.Generator(device="cuda").manual_seed(2)
+    gu = torch.randn(c["uc"].shape, dtype=torch.float64, device="cuda", generator=gen)
+    gv = torch.randn(c["vc"].shape, dtype=torch.float64, device="cuda", generator=gen)
+
+    def chain(f):
+        gz1, ws1 = update_dz_c(c["dp_ref"], c["zs"], f["ut"], f["vt"], f["gz"], c["ws"], sf, dt2)
+        pef, gz2 = riem_solver_c(f["w3"], gz1, f["delpc"], f["ptc"], dev["cappa"], c["hs"], ws1, dev["q_con"],
+                                 sf.grid_indexing, dt2, ptop, p_fac)
+        return p_grad_c(f["uc"], f["vc"], f["delpc"], pef, gz2, sf, dt2)
+
+    def fwd():
+        with torch.no_grad():
+            return chain(base)
+
+    def fwd_bwd():
+        uc, vc = chain(x)
+        ((uc * gu).sum() + (vc * gv).sum()).backward()
+
+    return timed(fwd), timed(fwd_bwd)
+
+
 def run_adjoint(args):
-    """Cost of the hand-written adjoint of RiemannSolver3 (with
-    RiemannSolverC, the stages of the acoustic substep that have one so far):
-    forward alone against forward + backward through torch autograd, C48 L79
-    FP64 by default."""
+    """Cost of the hand-written adjoints: RiemannSolver3 alone, and the C-grid
+    chain UpdateGeopotentialHeightOnCGrid, RiemannSolverC, p_grad_c; forward
+    alone against forward + backward through torch autograd, C48 L79 FP64 by
+    default."""
     import numpy as np
     import torch
 
@@ -654,14 +706,18 @@ def run_adjoint(args):
     t_f = timed(fwd)
     t_fb = timed(fwd_bwd)
     peak = torch.cuda.max_memory_allocated()
+    chain_f, chain_fb = _time_c_grid_chain(args, st, zh, dev, timed)
     line = {
         "metric": f"RiemannSolver3 adjoint/forward time ratio (C{n} L{npz})", "value": t_fb / t_f,
         "unit": "ratio", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_fb,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded baroclinic-wave state)",
         "config": {"workload": f"RiemannSolver3 column solve, C{n} L{npz}, forward vs forward + hand-written "
-                               "adjoint through torch.autograd (the Riemann solvers are the stages with an adjoint so far)",
-                   "forward_ms": t_f, "forward_backward_ms": t_fb, "peak_memory_bytes": peak},
+                               "adjoint through torch.autograd",
+                   "forward_ms": t_f, "forward_backward_ms": t_fb, "peak_memory_bytes": peak,
+                   "c_grid_chain": {"stages": "UpdateGeopotentialHeightOnCGrid, RiemannSolverC, p_grad_c",
+                                    "forward_ms": chain_f, "forward_backward_ms": chain_fb,
+                                    "ratio": chain_fb / chain_f}},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
