@@ -49,6 +49,29 @@ def test_version_and_error_reporting_without_gpu():
     assert rc == 1 and b"null argument" in L.fv3b_last_error()
 
 
+def test_adjoint_entry_points_reject_bad_arguments_without_gpu():
+    import ctypes
+
+    from fv3core_b200 import _lib
+
+    L = _lib.lib()
+    # null context or field: rejected on the host before any CUDA call
+    for name, n_ptr in (("fv3b_p_grad_c_adjoint", 8), ("fv3b_update_dz_c_adjoint", 9)):
+        rc = getattr(L, name)(None, *([None] * n_ptr), 1.0, None)
+        assert rc == 1 and b"null argument" in L.fv3b_last_error(), name
+    # the column adjoints: nulls, then too few levels, then too many
+    buf = ctypes.create_string_buffer(8)
+    ptrs = [ctypes.addressof(buf)] * 14
+    for name in ("fv3b_riem_solver3_adjoint", "fv3b_riem_solver_c_adjoint"):
+        dims = _lib.GridDims(12, 3, 8, 0)
+        rc = getattr(L, name)(ctypes.byref(dims), 1.0, 1.0, 0.05, *([None] * 14), None)
+        assert rc == 1 and b"null argument" in L.fv3b_last_error(), name
+        for npz in (2, 128):
+            dims = _lib.GridDims(12, 3, npz, 0)
+            rc = getattr(L, name)(ctypes.byref(dims), 1.0, 1.0, 0.05, *ptrs, None)
+            assert rc == 1 and b"npz must be in 3..127" in L.fv3b_last_error(), (name, npz)
+
+
 def test_oversized_grid_is_rejected_before_any_cuda_call():
     import ctypes
 
