@@ -108,3 +108,74 @@ def test_transpose_dot_product_identity(host_a2b, n, nz, seed):
     reach = np.zeros(x.shape, bool)
     reach[:, :, H - 2:H + n + 3, H - 2:H + n + 3] = True
     assert not aty[~reach].any()
+
+
+# ---------------------------------------------------------------- nh_p_grad
+
+
+def nhp_case(n, nz, seed):
+    st = cases.base_state(n, nz, seed)
+    rng = np.random.default_rng(seed + 9)
+    shp = st["delp"].shape
+    f = {"u": st["u"].copy(), "v": st["v"].copy(), "pp": 10.0 * rng.standard_normal(shp),
+         "gz": cases.heights(st, nz) * 9.80665, "pk3": st["pk"] * (1 + 1e-5 * rng.standard_normal(shp)),
+         "delp": st["delp"].copy()}
+    return f, float(st["ptop"])
+
+
+OUTPUTS = ("u", "v", "pp", "pk3", "gz")
+
+
+def oracle_nh_p_grad(f, n, nz, dt, ptop):
+    """The oracle's stage on copies of f (oracle layout): the new fields."""
+    from oracle._util import Tile
+    from oracle.a2b_ord4 import A2BScratch
+    from oracle.dyn_core import nh_p_grad
+
+    from fv3core_b200 import constants as C
+
+    out = {k: np.array(v, copy=True) for k, v in f.items()}
+    T = Tile(n, nz)
+    shape = (T.m, T.m, T.nk)
+    for t in range(6):
+        scr = {"wk": np.full(shape, np.nan), "wk1": np.full(shape, np.nan), "a2b_k1": A2BScratch(shape),
+               "a2b_kbuffer": A2BScratch(shape), "a2b_kstandard": A2BScratch(shape)}
+        nh_p_grad(T, cases.metric_namespace(n, t), scr, out["u"][t], out["v"][t], out["pp"][t], out["gz"][t],
+                  out["pk3"][t], out["delp"][t], dt, ptop, C.KAPPA)
+    return out
+
+
+@pytest.mark.parametrize("n,nz,seed", [(12, 4, 3), (13, 3, 4)])
+def test_host_nh_p_grad_adjoint_matches_oracle_finite_differences(host_a2b, n, nz, seed):
+    from fv3core_b200 import constants as C
+
+    f, ptop = nhp_case(n, nz, seed)
+    dt = 37.5
+    rng = np.random.default_rng(seed)
+    cot = {k: rng.standard_normal(f[k].shape) for k in OUTPUTS}
+    cot["gz"] *= 1e-3
+    grid = HostGrid(n)
+    g = cases.grid_for(n)
+    rdx, rdy = kernel_layout(np.asarray(g.rdx)), kernel_layout(np.asarray(g.rdy))
+    kf = {k: kernel_layout(v) for k, v in f.items()}
+    kc = {k: kernel_layout(v) for k, v in cot.items()}
+    grads = {k: np.zeros_like(kf["u"]) for k in ("u", "v", "pp", "pk3", "gz", "delp")}
+    host_a2b.nhp_adjoint_host.restype = None
+    host_a2b.nhp_adjoint_host(
+        ctypes.c_int(n), ctypes.c_int(H), ctypes.c_int(nz), ctypes.c_double(dt), ctypes.c_double(ptop ** C.KAPPA),
+        *grid.args(), _ptr(rdx), _ptr(rdy), _ptr(kf["pp"]), _ptr(kf["pk3"]), _ptr(kf["gz"]), _ptr(kf["delp"]),
+        *[_ptr(kc[k]) for k in OUTPUTS], *[_ptr(grads[k]) for k in ("u", "v", "pp", "pk3", "gz", "delp")])
+    grads = {k: v.transpose(0, 3, 2, 1) for k, v in grads.items()}  # back to the oracle layout
+
+    def loss(x):
+        out = oracle_nh_p_grad(x, n, nz, dt, ptop)
+        return sum(float((out[k] * cot[k]).sum()) for k in OUTPUTS)
+
+    for trial in range(3):
+        dirs = {k: rng.standard_normal(v.shape) * (np.abs(v) + (10.0 if k == "pp" else 0.0)) for k, v in f.items()}
+        eps = 1e-6
+        lp = loss({k: f[k] + eps * dirs[k] for k in f})
+        lm = loss({k: f[k] - eps * dirs[k] for k in f})
+        fd = (lp - lm) / (2 * eps)
+        ad = sum(float((grads[k] * dirs[k]).sum()) for k in f)
+        assert abs(fd - ad) <= 1e-7 * abs(ad), (trial, fd, ad)
