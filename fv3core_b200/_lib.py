@@ -52,6 +52,7 @@ CTX_SIGNATURES = {
     "fv3b_p_grad_c": [P] * 5 + [D, P],
     "fv3b_p_grad_c_adjoint": [P] * 8 + [D, P],
     "fv3b_nh_p_grad": [P] * 6 + [D, D, D, P],
+    "fv3b_nh_p_grad_adjoint": [P] * 15 + [D, D, D, P],
     "fv3b_edge_pe": [P, P, D, P],
     "fv3b_pk3_halo": [P, P, D, D, P],
     "fv3b_ray_fast": [P] * 5 + [D, D, D, D, ctypes.c_int, P],

@@ -11,6 +11,10 @@ hand-written adjoints (``fv3b_riem_solver3_adjoint``,
 ``update_dz_c(dp_ref, zs, ut, vt, gz, ws, stencil_factory, dt)`` (reference
 ``updatedzc.py:123-163``) returns the new (gz, ws), its backward pass being
 ``fv3b_update_dz_c_adjoint`` (dp_ref and zs held fixed).
+``nh_p_grad(u, v, pp, gz, pk3, delp, stencil_factory, dt, ptop, akap)``
+(reference ``nh_p_grad.py:147-206``) returns the new (u, v, pp, gz, pk3),
+its backward pass being ``fv3b_nh_p_grad_adjoint`` (the wind update's
+adjoint and the transposes of the four a2b_ord4 interpolations).
 
 These are the stages of the acoustic substep with an adjoint so far; the
 others have none yet, so a whole substep cannot be differentiated.
@@ -199,3 +203,38 @@ def update_dz_c(dp_ref, zs, ut, vt, gz, ws, stencil_factory, dt):
     """New (gz, ws) of UpdateGeopotentialHeightOnCGrid, differentiable with
     respect to ut, vt, gz and ws."""
     return UpdateDzCFunction.apply(ut, vt, gz, ws, dp_ref, zs, stencil_factory, dt)
+
+
+class NhPGradFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, u, v, pp, gz, pk3, delp, stencil_factory, dt, ptop, akap):
+        gi = stencil_factory.grid_indexing
+        f3 = lambda t, n: check_field(t, gi, "3d", n)  # noqa: E731
+        out = [t.detach().clone() for t in (u, v, pp, gz, pk3)]
+        _lib.call_ctx("fv3b_nh_p_grad", context(stencil_factory), f3(out[0], "u"), f3(out[1], "v"),
+                      f3(out[2], "pp"), f3(out[3], "gz"), f3(out[4], "pk3"), f3(delp, "delp"), float(dt),
+                      float(ptop), float(akap), stream_ptr())
+        ctx.save_for_backward(pp.detach(), gz.detach(), pk3.detach(), delp.detach())
+        ctx.params = (stencil_factory, float(dt), float(ptop), float(akap))
+        return tuple(out)
+
+    @staticmethod
+    def backward(ctx, g_u, g_v, g_pp, g_gz, g_pk3):
+        pp, gz, pk3, delp = ctx.saved_tensors
+        stencil_factory, dt, ptop, akap = ctx.params
+        gi = stencil_factory.grid_indexing
+        f3 = lambda t, n: check_field(t, gi, "3d", n)  # noqa: E731
+        cot = [torch.zeros_like(pp) if g is None else g.contiguous() for g in (g_u, g_v, g_pp, g_gz, g_pk3)]
+        grads = [torch.empty_like(pp) for _ in range(6)]  # u, v, pp, gz, pk3, delp
+        _lib.call_ctx("fv3b_nh_p_grad_adjoint", context(stencil_factory), f3(pp, "pp"), f3(gz, "gz"),
+                      f3(pk3, "pk3"), f3(delp, "delp"), *[f3(c, n) for c, n in zip(cot, ("gu", "gv", "gpp", "ggz",
+                                                                                       "gpk3"))],
+                      *[f3(g, n) for g, n in zip(grads, ("g_u", "g_v", "g_pp", "g_gz", "g_pk3", "g_delp"))],
+                      dt, ptop, akap, stream_ptr())
+        return tuple(grads) + (None, None, None, None)
+
+
+def nh_p_grad(u, v, pp, gz, pk3, delp, stencil_factory, dt, ptop, akap):
+    """New (u, v, pp, gz, pk3) of NonHydrostaticPressureGradient,
+    differentiable with respect to u, v, pp, gz, pk3 and delp."""
+    return NhPGradFunction.apply(u, v, pp, gz, pk3, delp, stencil_factory, dt, ptop, akap)

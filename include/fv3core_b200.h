@@ -268,6 +268,20 @@ int fv3b_p_grad_c_adjoint(fv3b_ctx* ctx, const fv3b_real* delpc, const fv3b_real
 int fv3b_nh_p_grad(fv3b_ctx* ctx, fv3b_real* u, fv3b_real* v, fv3b_real* pp, fv3b_real* gz, fv3b_real* pk3, fv3b_real* delp,
                    double dt, double ptop, double akap, void* stream);
 
+/*
+ * Adjoint of fv3b_nh_p_grad (no reference counterpart).  pp, gz, pk3, delp
+ * are the forward call's inputs (before it replaced pp, gz, pk3 by their
+ * B-grid values); gu, gv, gpp, ggz, gpk3 the cotangents of its outputs u, v,
+ * pp, gz, pk3.  Writes, on every point, the gradients g_u, g_v, g_pp, g_gz,
+ * g_pk3 (pass-through outside what the stage writes included) and g_delp.
+ * Uses the context's workspace.
+ */
+int fv3b_nh_p_grad_adjoint(fv3b_ctx* ctx, const fv3b_real* pp, const fv3b_real* gz, const fv3b_real* pk3,
+                           const fv3b_real* delp, const fv3b_real* gu, const fv3b_real* gv, const fv3b_real* gpp,
+                           const fv3b_real* ggz, const fv3b_real* gpk3, fv3b_real* g_u, fv3b_real* g_v,
+                           fv3b_real* g_pp, fv3b_real* g_gz, fv3b_real* g_pk3, fv3b_real* g_delp, double dt,
+                           double ptop, double akap, void* stream);
+
 /* edge_pe (fv3core/stencils/pe_halo.py:6-33). */
 int fv3b_edge_pe(fv3b_ctx* ctx, fv3b_real* pe, const fv3b_real* delp, double ptop, void* stream);
 
