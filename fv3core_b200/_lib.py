@@ -61,6 +61,9 @@ CTX_SIGNATURES = {
     "fv3b_halo_update_scalar": [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P],
     "fv3b_halo_update_vector": [P, P, ctypes.c_int, ctypes.c_int, P],
     "fv3b_synchronize_vector_interfaces": [P, P, ctypes.c_int, P],
+    "fv3b_halo_update_scalar_adjoint": [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P],
+    "fv3b_halo_update_vector_adjoint": [P, P, ctypes.c_int, ctypes.c_int, P],
+    "fv3b_synchronize_vector_interfaces_adjoint": [P, P, ctypes.c_int, P],
     "fv3b_acoustics_setup": [P] * 6,
     "fv3b_acoustics": [P, P],
 }

@@ -15,6 +15,12 @@ hand-written adjoints (``fv3b_riem_solver3_adjoint``,
 (reference ``nh_p_grad.py:147-206``) returns the new (u, v, pp, gz, pk3),
 its backward pass being ``fv3b_nh_p_grad_adjoint`` (the wind update's
 adjoint and the transposes of the four a2b_ord4 interpolations).
+``halo_update_scalar(field, stencil_factory, stagger, n_halo, nlev)``,
+``halo_update_vector(x, y, stencil_factory, grid, nlev)`` and
+``synchronize_vector_interfaces(u, v, stencil_factory, nlev)`` are the halo
+calls the acoustic loop makes between stages, with their transposes
+(``fv3b_halo_update_*_adjoint``, ``fv3b_synchronize_vector_interfaces_adjoint``)
+as backward passes.
 
 These are the stages of the acoustic substep with an adjoint so far; the
 others have none yet, so a whole substep cannot be differentiated.
@@ -238,3 +244,88 @@ def nh_p_grad(u, v, pp, gz, pk3, delp, stencil_factory, dt, ptop, akap):
     """New (u, v, pp, gz, pk3) of NonHydrostaticPressureGradient,
     differentiable with respect to u, v, pp, gz, pk3 and delp."""
     return NhPGradFunction.apply(u, v, pp, gz, pk3, delp, stencil_factory, dt, ptop, akap)
+
+
+class HaloUpdateScalarFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, field, stencil_factory, stagger, n_halo, nlev):
+        gi = stencil_factory.grid_indexing
+        out = field.detach().clone()
+        _lib.call_ctx("fv3b_halo_update_scalar", context(stencil_factory), check_field(out, gi, "3d", "field"),
+                      int(stagger), int(n_halo), int(nlev), stream_ptr())
+        ctx.params = (stencil_factory, int(stagger), int(n_halo), int(nlev))
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        stencil_factory, stagger, n_halo, nlev = ctx.params
+        g = g.clone(memory_format=torch.contiguous_format)
+        _lib.call_ctx("fv3b_halo_update_scalar_adjoint", context(stencil_factory),
+                      check_field(g, stencil_factory.grid_indexing, "3d", "g"), stagger, n_halo, nlev, stream_ptr())
+        return g, None, None, None, None
+
+
+class HaloUpdateVectorFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, x, y, stencil_factory, grid, nlev):
+        gi = stencil_factory.grid_indexing
+        ox, oy = x.detach().clone(), y.detach().clone()
+        _lib.call_ctx("fv3b_halo_update_vector", context(stencil_factory), check_field(ox, gi, "3d", "x"),
+                      check_field(oy, gi, "3d", "y"), int(grid), int(nlev), stream_ptr())
+        ctx.params = (stencil_factory, int(grid), int(nlev))
+        return ox, oy
+
+    @staticmethod
+    def backward(ctx, gx, gy):
+        stencil_factory, grid, nlev = ctx.params
+        gi = stencil_factory.grid_indexing
+        m = gi.max_shape[0]
+        zeros = lambda: torch.zeros((6, gi.max_shape[2], m, m), dtype=gi.dtype, device="cuda")  # noqa: E731
+        gx = zeros() if gx is None else gx.clone(memory_format=torch.contiguous_format)
+        gy = zeros() if gy is None else gy.clone(memory_format=torch.contiguous_format)
+        _lib.call_ctx("fv3b_halo_update_vector_adjoint", context(stencil_factory), check_field(gx, gi, "3d", "gx"),
+                      check_field(gy, gi, "3d", "gy"), grid, nlev, stream_ptr())
+        return gx, gy, None, None, None
+
+
+class InterfaceSyncFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, u, v, stencil_factory, nlev):
+        gi = stencil_factory.grid_indexing
+        ou, ov = u.detach().clone(), v.detach().clone()
+        _lib.call_ctx("fv3b_synchronize_vector_interfaces", context(stencil_factory),
+                      check_field(ou, gi, "3d", "u"), check_field(ov, gi, "3d", "v"), int(nlev), stream_ptr())
+        ctx.params = (stencil_factory, int(nlev))
+        return ou, ov
+
+    @staticmethod
+    def backward(ctx, gu, gv):
+        stencil_factory, nlev = ctx.params
+        gi = stencil_factory.grid_indexing
+        m = gi.max_shape[0]
+        zeros = lambda: torch.zeros((6, gi.max_shape[2], m, m), dtype=gi.dtype, device="cuda")  # noqa: E731
+        gu = zeros() if gu is None else gu.clone(memory_format=torch.contiguous_format)
+        gv = zeros() if gv is None else gv.clone(memory_format=torch.contiguous_format)
+        _lib.call_ctx("fv3b_synchronize_vector_interfaces_adjoint", context(stencil_factory),
+                      check_field(gu, gi, "3d", "gu"), check_field(gv, gi, "3d", "gv"), nlev, stream_ptr())
+        return gu, gv, None, None
+
+
+def halo_update_scalar(field, stencil_factory, stagger=1, n_halo=3, nlev=None):
+    """The field after a scalar halo update (stagger 1 = cell centres,
+    0 = cell corners), differentiable."""
+    nlev = stencil_factory.grid_indexing.max_shape[2] if nlev is None else nlev
+    return HaloUpdateScalarFunction.apply(field, stencil_factory, stagger, n_halo, nlev)
+
+
+def halo_update_vector(x, y, stencil_factory, grid=0, nlev=None):
+    """The winds after a vector halo update (grid 0 = D, 1 = C),
+    differentiable."""
+    nlev = stencil_factory.grid_indexing.max_shape[2] if nlev is None else nlev
+    return HaloUpdateVectorFunction.apply(x, y, stencil_factory, grid, nlev)
+
+
+def synchronize_vector_interfaces(u, v, stencil_factory, nlev=None):
+    """The D-grid winds after synchronize_vector_interfaces, differentiable."""
+    nlev = stencil_factory.grid_indexing.max_shape[2] if nlev is None else nlev
+    return InterfaceSyncFunction.apply(u, v, stencil_factory, nlev)

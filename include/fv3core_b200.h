@@ -320,6 +320,18 @@ int fv3b_halo_update_vector(fv3b_ctx* ctx, fv3b_real* x, fv3b_real* y, int grid,
 int fv3b_synchronize_vector_interfaces(fv3b_ctx* ctx, fv3b_real* u, fv3b_real* v, int nlev, void* stream);
 
 /*
+ * Adjoints of the three halo calls above (no reference counterpart), in
+ * place: on entry the arrays hold the cotangents of the updated fields, on
+ * return those of the fields before the update (each halo point's
+ * cotangent added into its source, rotated like the forward copy, and the
+ * halo point zeroed).  Same arguments and conditions as the forward calls.
+ */
+int fv3b_halo_update_scalar_adjoint(fv3b_ctx* ctx, fv3b_real* g, int stagger, int n_halo, int nlev, void* stream);
+int fv3b_halo_update_vector_adjoint(fv3b_ctx* ctx, fv3b_real* gx, fv3b_real* gy, int grid, int nlev, void* stream);
+int fv3b_synchronize_vector_interfaces_adjoint(fv3b_ctx* ctx, fv3b_real* gu, fv3b_real* gv, int nlev,
+                                               void* stream);
+
+/*
  * AcousticDynamicsConfig (fv3core/_config.py:164-212) without the nested
  * RiemannConfig / D-grid config (p_fac comes from the Riemann config; the
  * D-grid namelist is passed separately).  Flags are 0/1.
