@@ -55,6 +55,8 @@ CTX_SIGNATURES = {
     "fv3b_nh_p_grad_adjoint": [P] * 15 + [D, D, D, P],
     "fv3b_edge_pe": [P, P, D, P],
     "fv3b_pk3_halo": [P, P, D, D, P],
+    "fv3b_edge_pe_adjoint": [P, P, P],
+    "fv3b_pk3_halo_adjoint": [P, P, P, D, D, P],
     "fv3b_ray_fast": [P] * 5 + [D, D, D, D, ctypes.c_int, P],
     "fv3b_del2cubed": [P, D, ctypes.c_int, P],
     "fv3b_pkz_tempadjust": [P] * 6 + [D, ctypes.c_int, P],

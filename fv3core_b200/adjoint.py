@@ -21,6 +21,10 @@ adjoint and the transposes of the four a2b_ord4 interpolations).
 calls the acoustic loop makes between stages, with their transposes
 (``fv3b_halo_update_*_adjoint``, ``fv3b_synchronize_vector_interfaces_adjoint``)
 as backward passes.
+``edge_pe(pe, delp, stencil_factory, ptop)`` and ``pk3_halo(pk3, delp,
+stencil_factory, ptop, akap)`` (reference ``pe_halo.py:6-33``,
+``pk3_halo.py:36-68``) are the halo-ring column sums, with
+``fv3b_edge_pe_adjoint`` / ``fv3b_pk3_halo_adjoint`` as backward passes.
 
 These are the stages of the acoustic substep with an adjoint so far; the
 others have none yet, so a whole substep cannot be differentiated.
@@ -329,3 +333,58 @@ def synchronize_vector_interfaces(u, v, stencil_factory, nlev=None):
     """The D-grid winds after synchronize_vector_interfaces, differentiable."""
     nlev = stencil_factory.grid_indexing.max_shape[2] if nlev is None else nlev
     return InterfaceSyncFunction.apply(u, v, stencil_factory, nlev)
+
+
+class EdgePeFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, pe, delp, stencil_factory, ptop):
+        gi = stencil_factory.grid_indexing
+        out = pe.detach().clone()
+        _lib.call_ctx("fv3b_edge_pe", context(stencil_factory), check_field(out, gi, "3d", "pe"),
+                      check_field(delp, gi, "3d", "delp"), float(ptop), stream_ptr())
+        ctx.params = stencil_factory
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        stencil_factory = ctx.params
+        gi = stencil_factory.grid_indexing
+        g = g.clone(memory_format=torch.contiguous_format)
+        g_delp = torch.empty_like(g)
+        _lib.call_ctx("fv3b_edge_pe_adjoint", context(stencil_factory), check_field(g, gi, "3d", "g_pe"),
+                      check_field(g_delp, gi, "3d", "g_delp"), stream_ptr())
+        return g, g_delp, None, None
+
+
+class Pk3HaloFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, pk3, delp, stencil_factory, ptop, akap):
+        gi = stencil_factory.grid_indexing
+        out = pk3.detach().clone()
+        _lib.call_ctx("fv3b_pk3_halo", context(stencil_factory), check_field(out, gi, "3d", "pk3"),
+                      check_field(delp, gi, "3d", "delp"), float(ptop), float(akap), stream_ptr())
+        ctx.save_for_backward(delp.detach())
+        ctx.params = (stencil_factory, float(ptop), float(akap))
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        (delp,) = ctx.saved_tensors
+        stencil_factory, ptop, akap = ctx.params
+        gi = stencil_factory.grid_indexing
+        g = g.clone(memory_format=torch.contiguous_format)
+        g_delp = torch.empty_like(g)
+        _lib.call_ctx("fv3b_pk3_halo_adjoint", context(stencil_factory), check_field(delp, gi, "3d", "delp"),
+                      check_field(g, gi, "3d", "g_pk3"), check_field(g_delp, gi, "3d", "g_delp"), ptop, akap,
+                      stream_ptr())
+        return g, g_delp, None, None, None
+
+
+def edge_pe(pe, delp, stencil_factory, ptop):
+    """pe after edge_pe (the one-cell ring), differentiable."""
+    return EdgePeFunction.apply(pe, delp, stencil_factory, ptop)
+
+
+def pk3_halo(pk3, delp, stencil_factory, ptop, akap):
+    """pk3 after PK3Halo (the two-cell ring), differentiable."""
+    return Pk3HaloFunction.apply(pk3, delp, stencil_factory, ptop, akap)

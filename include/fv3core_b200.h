@@ -289,6 +289,16 @@ int fv3b_edge_pe(fv3b_ctx* ctx, fv3b_real* pe, const fv3b_real* delp, double pto
 int fv3b_pk3_halo(fv3b_ctx* ctx, fv3b_real* pk3, const fv3b_real* delp, double ptop, double akap, void* stream);
 
 /*
+ * Adjoints of fv3b_edge_pe and fv3b_pk3_halo (no reference counterpart).
+ * g_pe / g_pk3 hold the cotangent of the new field on entry and that of the
+ * old field on return (zero where the stage overwrote it); g_delp is
+ * overwritten on every point.  pk3's needs npz <= 127.
+ */
+int fv3b_edge_pe_adjoint(fv3b_ctx* ctx, fv3b_real* g_pe, fv3b_real* g_delp, void* stream);
+int fv3b_pk3_halo_adjoint(fv3b_ctx* ctx, const fv3b_real* delp, fv3b_real* g_pk3, fv3b_real* g_delp, double ptop,
+                          double akap, void* stream);
+
+/*
  * RayleighDamping.__call__ (fv3core/stencils/ray_fast.py:169-192); the
  * constructor arguments rf_cutoff, tau, hydrostatic are passed per call.
  * dp and pfull are HOST arrays of npz values (the reference's K fields);
