@@ -25,6 +25,9 @@ as backward passes.
 stencil_factory, ptop, akap)`` (reference ``pe_halo.py:6-33``,
 ``pk3_halo.py:36-68``) are the halo-ring column sums, with
 ``fv3b_edge_pe_adjoint`` / ``fv3b_pk3_halo_adjoint`` as backward passes.
+``ray_fast(u, v, w, dp, pfull, stencil_factory, dt, ptop, rf_cutoff, tau)``
+(reference ``ray_fast.py:131-192``) returns the damped (u, v, w), with
+``fv3b_ray_fast_adjoint`` as its backward pass.
 
 These are the stages of the acoustic substep with an adjoint so far; the
 others have none yet, so a whole substep cannot be differentiated.
@@ -41,7 +44,7 @@ tensors in the kernel layout of ``grid_indexing``.
 import torch
 
 from . import _lib
-from .stencils._common import context
+from .stencils._common import context, host_column
 from .storage import check_field, stream_ptr
 
 
@@ -388,3 +391,33 @@ def edge_pe(pe, delp, stencil_factory, ptop):
 def pk3_halo(pk3, delp, stencil_factory, ptop, akap):
     """pk3 after PK3Halo (the two-cell ring), differentiable."""
     return Pk3HaloFunction.apply(pk3, delp, stencil_factory, ptop, akap)
+
+
+class RayFastFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, u, v, w, dp, pfull, stencil_factory, dt, ptop, rf_cutoff, tau):
+        gi = stencil_factory.grid_indexing
+        dp_h, pf_h = host_column(dp, gi.npz, "dp"), host_column(pfull, gi.npz, "pfull")
+        out = [t.detach().clone() for t in (u, v, w)]
+        args = (dp_h.ctypes.data, pf_h.ctypes.data, float(dt), float(ptop), float(rf_cutoff), float(tau), 0)
+        _lib.call_ctx("fv3b_ray_fast", context(stencil_factory), *[check_field(t, gi, "3d", n)
+                                                                  for t, n in zip(out, "uvw")], *args, stream_ptr())
+        ctx.params = (stencil_factory, dp_h, pf_h, args)
+        return tuple(out)
+
+    @staticmethod
+    def backward(ctx, gu, gv, gw):
+        stencil_factory, dp_h, pf_h, args = ctx.params
+        gi = stencil_factory.grid_indexing
+        m = gi.max_shape[0]
+        g = [torch.zeros((6, gi.max_shape[2], m, m), dtype=gi.dtype, device="cuda") if x is None
+             else x.clone(memory_format=torch.contiguous_format) for x in (gu, gv, gw)]
+        _lib.call_ctx("fv3b_ray_fast_adjoint", context(stencil_factory),
+                      *[check_field(t, gi, "3d", n) for t, n in zip(g, ("gu", "gv", "gw"))], *args, stream_ptr())
+        return g[0], g[1], g[2], None, None, None, None, None, None, None
+
+
+def ray_fast(u, v, w, dp, pfull, stencil_factory, dt, ptop, rf_cutoff, tau):
+    """The winds after RayleighDamping (nonhydrostatic), differentiable with
+    respect to u, v and w."""
+    return RayFastFunction.apply(u, v, w, dp, pfull, stencil_factory, dt, ptop, rf_cutoff, tau)

@@ -4,7 +4,8 @@
 //   HyperdiffusionDamping (fv3core/stencils/del2cubed.py), the del-2
 //     filter of the dissipation heat source;
 //   compute_pkz_tempadjust (fv3core/stencils/temperature_adjust.py), the
-//     temperature change from that heat.
+//     temperature change from that heat;
+// and the adjoint of the Rayleigh damping (ray_adjoint.h).
 #include <math.h>
 
 #include <vector>
@@ -12,6 +13,7 @@
 #include "corners.cuh"
 #include "ctx.cuh"
 #include "fmath.h"
+#include "ray_adjoint.h"
 #include "stencil.cuh"
 
 using namespace fv3b;
@@ -108,6 +110,35 @@ extern "C" int fv3b_ray_fast(fv3b_ctx* ctx, real* u, real* v, real* w, const dou
     if (j <= je) damp(v);
     if (do_w && i <= e && j <= je)
       for (int k = 0; k < k_rf; ++k) w[o0 + k * d.sk] = w[o0 + k * d.sk] * rf[k];
+  }));
+  return FV3B_OK;
+}
+
+// Adjoint of fv3b_ray_fast (no reference counterpart), in place on the
+// cotangents gu, gv, gw of the new winds.  The damping constants are those
+// the last fv3b_ray_fast call on this context derived; the arguments must
+// match that call's.
+extern "C" int fv3b_ray_fast_adjoint(fv3b_ctx* ctx, real* gu, real* gv, real* gw, const double* dp,
+                                     const double* pfull, double dt, double ptop, double rf_cutoff, double tau,
+                                     int hydrostatic, void* stream) {
+  FV3B_REQUIRE(ctx && gu && gv && gw && dp && pfull, "fv3b_ray_fast_adjoint: null argument");
+  const Dims d = ctx->d;
+  const RayState& rs = ctx->ray;
+  bool same = rs.ready && rs.dt == dt && rs.ptop == ptop && rs.rf_cutoff == rf_cutoff && rs.tau == tau;
+  for (int k = 0; same && k < d.nz; ++k) same = rs.dp[k] == dp[k] && rs.pfull[k] == pfull[k];
+  FV3B_REQUIRE(same, "fv3b_ray_fast_adjoint: call fv3b_ray_fast first with the same constants");
+  const int k_rf = rs.k_rf, k_nudge = rs.k_nudge;
+  if (k_rf == 0) return FV3B_OK;
+  const real* rf = colp(ctx, COL_RF);
+  const real* dm = colp(ctx, COL_RF_DM);
+  const real* dpc = colp(ctx, COL_DP_RAY);
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
+  const bool do_w = hydrostatic == 0;
+  FV3B_CHECK(launch_columns(s, e + 2, js, je + 2, (cudaStream_t)stream, [=] __device__(int t, int i, int j) {
+    const idx_t o0 = idx3(d, t, i, j, 0);
+    if (i <= e) adj::ray_column_adjoint<real>(k_rf, k_nudge, d.sk, rf, dm, dpc, gu + o0);
+    if (j <= je) adj::ray_column_adjoint<real>(k_rf, k_nudge, d.sk, rf, dm, dpc, gv + o0);
+    if (do_w && i <= e && j <= je) adj::ray_w_column_adjoint<real>(k_rf, d.sk, rf, gw + o0);
   }));
   return FV3B_OK;
 }

@@ -307,6 +307,16 @@ int fv3b_pk3_halo_adjoint(fv3b_ctx* ctx, const fv3b_real* delp, fv3b_real* g_pk3
 int fv3b_ray_fast(fv3b_ctx* ctx, fv3b_real* u, fv3b_real* v, fv3b_real* w, const double* dp, const double* pfull,
                   double dt, double ptop, double rf_cutoff, double tau, int hydrostatic, void* stream);
 
+/*
+ * Adjoint of fv3b_ray_fast (no reference counterpart), in place on the
+ * cotangents gu, gv, gw of the new winds.  Uses the damping constants of
+ * the last fv3b_ray_fast call on this context, whose arguments these must
+ * match (FV3B_ERR_ARGUMENT otherwise).
+ */
+int fv3b_ray_fast_adjoint(fv3b_ctx* ctx, fv3b_real* gu, fv3b_real* gv, fv3b_real* gw, const double* dp,
+                          const double* pfull, double dt, double ptop, double rf_cutoff, double tau, int hydrostatic,
+                          void* stream);
+
 /* HyperdiffusionDamping.__call__ (fv3core/stencils/del2cubed.py:152-181). */
 int fv3b_del2cubed(fv3b_ctx* ctx, fv3b_real* qdel, double cd, int nmax, void* stream);
 
