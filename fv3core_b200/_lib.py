@@ -60,6 +60,7 @@ CTX_SIGNATURES = {
     "fv3b_ray_fast": [P] * 5 + [D, D, D, D, ctypes.c_int, P],
     "fv3b_ray_fast_adjoint": [P] * 5 + [D, D, D, D, ctypes.c_int, P],
     "fv3b_del2cubed": [P, D, ctypes.c_int, P],
+    "fv3b_del2cubed_adjoint": [P, D, ctypes.c_int, P],
     "fv3b_pkz_tempadjust": [P] * 6 + [D, ctypes.c_int, P],
     "fv3b_halo_update_scalar": [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P],
     "fv3b_halo_update_vector": [P, P, ctypes.c_int, ctypes.c_int, P],

@@ -28,6 +28,9 @@ stencil_factory, ptop, akap)`` (reference ``pe_halo.py:6-33``,
 ``ray_fast(u, v, w, dp, pfull, stencil_factory, dt, ptop, rf_cutoff, tau)``
 (reference ``ray_fast.py:131-192``) returns the damped (u, v, w), with
 ``fv3b_ray_fast_adjoint`` as its backward pass.
+``del2cubed(qdel, stencil_factory, cd, nmax)`` (reference
+``del2cubed.py:152-181``) returns the filtered field, with
+``fv3b_del2cubed_adjoint`` as its backward pass.
 
 These are the stages of the acoustic substep with an adjoint so far; the
 others have none yet, so a whole substep cannot be differentiated.
@@ -421,3 +424,27 @@ def ray_fast(u, v, w, dp, pfull, stencil_factory, dt, ptop, rf_cutoff, tau):
     """The winds after RayleighDamping (nonhydrostatic), differentiable with
     respect to u, v and w."""
     return RayFastFunction.apply(u, v, w, dp, pfull, stencil_factory, dt, ptop, rf_cutoff, tau)
+
+
+class Del2CubedFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, qdel, stencil_factory, cd, nmax):
+        gi = stencil_factory.grid_indexing
+        out = qdel.detach().clone()
+        _lib.call_ctx("fv3b_del2cubed", context(stencil_factory), check_field(out, gi, "3d", "qdel"), float(cd),
+                      int(nmax), stream_ptr())
+        ctx.params = (stencil_factory, float(cd), int(nmax))
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        stencil_factory, cd, nmax = ctx.params
+        g = g.clone(memory_format=torch.contiguous_format)
+        _lib.call_ctx("fv3b_del2cubed_adjoint", context(stencil_factory),
+                      check_field(g, stencil_factory.grid_indexing, "3d", "gq"), cd, nmax, stream_ptr())
+        return g, None, None, None
+
+
+def del2cubed(qdel, stencil_factory, cd, nmax):
+    """The field after HyperdiffusionDamping, differentiable."""
+    return Del2CubedFunction.apply(qdel, stencil_factory, cd, nmax)

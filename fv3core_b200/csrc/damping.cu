@@ -5,13 +5,15 @@
 //     filter of the dissipation heat source;
 //   compute_pkz_tempadjust (fv3core/stencils/temperature_adjust.py), the
 //     temperature change from that heat;
-// and the adjoint of the Rayleigh damping (ray_adjoint.h).
+// and the adjoints of the Rayleigh damping (ray_adjoint.h) and of the
+// del-2 filter (del2cubed_adjoint.h).
 #include <math.h>
 
 #include <vector>
 
 #include "corners.cuh"
 #include "ctx.cuh"
+#include "del2cubed_adjoint.h"
 #include "fmath.h"
 #include "ray_adjoint.h"
 #include "stencil.cuh"
@@ -211,6 +213,39 @@ extern "C" int fv3b_del2cubed(fv3b_ctx* ctx, real* qdel, double cd_in, int nmax,
       if (i >= s - nt && i < e + 1 + nt && j >= js - nt && j < je + 1 + nt)
         qv = qv + cd * F2(g.rarea, i, j) * (F3(fx, i, j) - F3(fx, i + 1, j) + F3(fy, i, j) - F3(fy, i, j + 1));
       W3(qdel, i, j) = qv;
+    }));
+  }
+  return FV3B_OK;
+}
+
+// Adjoint of fv3b_del2cubed (no reference counterpart), in place on the
+// cotangent g of the filtered field: the passes transposed in reverse order
+// (del2cubed_adjoint.h), each scattering every point's cotangent onto the
+// inputs it read (atomic adds) in the workspace, then copied back.
+extern "C" int fv3b_del2cubed_adjoint(fv3b_ctx* ctx, real* gq, double cd_in, int nmax, void* stream) {
+  const real cd = static_cast<real>(cd_in);
+  FV3B_REQUIRE(ctx && gq, "fv3b_del2cubed_adjoint: null argument");
+  const Dims d = ctx->d;
+  const real *del6_u = ctx->m.del6_u, *del6_v = ctx->m.del6_v, *rarea = ctx->m.rarea;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int full = d.ni - 1, nz = d.nz;
+  real* nxt = ctx->ws[0];
+  const int ntimes = nmax < 3 ? nmax : 3;
+  for (int n = ntimes - 1; n >= 0; --n) {
+    const int nt = ntimes - (n + 1);
+    FV3B_CHECK(cudaMemsetAsync(nxt, 0, sizeof(real) * (size_t)6 * d.st, st));
+    FV3B_CHECK(launch_box(Box{0, d.ni, 0, d.nj, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+      const idx_t o = idx3(d, t, i, j, k);
+      if (i == full || j == full) {
+        atomicAdd(nxt + o, gq[o]);
+        return;
+      }
+      auto add = [&](idx_t oo, real v) { atomicAdd(nxt + oo, v); };
+      adj::d2c_pass_adjoint<real>(d, t, i, j, k, nt, cd, del6_u, del6_v, rarea, gq[o], add);
+    }));
+    FV3B_CHECK(launch_box(Box{0, d.ni, 0, d.nj, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+      const idx_t o = idx3(d, t, i, j, k);
+      gq[o] = nxt[o];
     }));
   }
   return FV3B_OK;

@@ -320,6 +320,13 @@ int fv3b_ray_fast_adjoint(fv3b_ctx* ctx, fv3b_real* gu, fv3b_real* gv, fv3b_real
 /* HyperdiffusionDamping.__call__ (fv3core/stencils/del2cubed.py:152-181). */
 int fv3b_del2cubed(fv3b_ctx* ctx, fv3b_real* qdel, double cd, int nmax, void* stream);
 
+/*
+ * Adjoint of fv3b_del2cubed (no reference counterpart), in place: gq holds
+ * the cotangent of the filtered field on entry and that of the field before
+ * the filter on return.  Uses the context's workspace.
+ */
+int fv3b_del2cubed_adjoint(fv3b_ctx* ctx, fv3b_real* gq, double cd, int nmax, void* stream);
+
 /* compute_pkz_tempadjust (fv3core/stencils/temperature_adjust.py:8-44) on
  * levels [0, nk_heat). */
 int fv3b_pkz_tempadjust(fv3b_ctx* ctx, const fv3b_real* delp, const fv3b_real* delz, const fv3b_real* cappa,
