@@ -62,6 +62,7 @@ CTX_SIGNATURES = {
     "fv3b_del2cubed": [P, D, ctypes.c_int, P],
     "fv3b_del2cubed_adjoint": [P, D, ctypes.c_int, P],
     "fv3b_pkz_tempadjust": [P] * 6 + [D, ctypes.c_int, P],
+    "fv3b_pkz_tempadjust_adjoint": [P] * 10 + [D, ctypes.c_int, P],
     "fv3b_halo_update_scalar": [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P],
     "fv3b_halo_update_vector": [P, P, ctypes.c_int, ctypes.c_int, P],
     "fv3b_synchronize_vector_interfaces": [P, P, ctypes.c_int, P],

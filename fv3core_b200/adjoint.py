@@ -31,6 +31,10 @@ stencil_factory, ptop, akap)`` (reference ``pe_halo.py:6-33``,
 ``del2cubed(qdel, stencil_factory, cd, nmax)`` (reference
 ``del2cubed.py:152-181``) returns the filtered field, with
 ``fv3b_del2cubed_adjoint`` as its backward pass.
+``pkz_tempadjust(delp, delz, cappa, heat_source, pt, pkz, stencil_factory,
+delt_time_factor, nk_heat)`` (reference ``temperature_adjust.py:8-44``)
+returns the new (pt, pkz), with ``fv3b_pkz_tempadjust_adjoint`` as its
+backward pass (cappa held fixed).
 
 These are the stages of the acoustic substep with an adjoint so far; the
 others have none yet, so a whole substep cannot be differentiated.
@@ -448,3 +452,39 @@ class Del2CubedFunction(torch.autograd.Function):
 def del2cubed(qdel, stencil_factory, cd, nmax):
     """The field after HyperdiffusionDamping, differentiable."""
     return Del2CubedFunction.apply(qdel, stencil_factory, cd, nmax)
+
+
+class PkzTempadjustFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, delp, delz, cappa, heat_source, pt, pkz, stencil_factory, delt_time_factor, nk_heat):
+        gi = stencil_factory.grid_indexing
+        f3 = lambda t, n: check_field(t, gi, "3d", n)  # noqa: E731
+        new_pt, new_pkz = pt.detach().clone(), pkz.detach().clone()
+        _lib.call_ctx("fv3b_pkz_tempadjust", context(stencil_factory), f3(delp, "delp"), f3(delz, "delz"),
+                      f3(cappa, "cappa"), f3(heat_source, "heat_source"), f3(new_pt, "pt"), f3(new_pkz, "pkz"),
+                      float(delt_time_factor), int(nk_heat), stream_ptr())
+        ctx.save_for_backward(delp.detach(), delz.detach(), cappa, heat_source.detach(), pt.detach())
+        ctx.params = (stencil_factory, float(delt_time_factor), int(nk_heat))
+        return new_pt, new_pkz
+
+    @staticmethod
+    def backward(ctx, g_pt, g_pkz):
+        delp, delz, cappa, heat_source, pt = ctx.saved_tensors
+        stencil_factory, dtf, nk_heat = ctx.params
+        gi = stencil_factory.grid_indexing
+        f3 = lambda t, n: check_field(t, gi, "3d", n)  # noqa: E731
+        g_pt = torch.zeros_like(pt) if g_pt is None else g_pt.clone(memory_format=torch.contiguous_format)
+        g_pkz = torch.zeros_like(pt) if g_pkz is None else g_pkz.clone(memory_format=torch.contiguous_format)
+        out = [torch.empty_like(pt) for _ in range(3)]  # delp, delz, heat_source
+        _lib.call_ctx("fv3b_pkz_tempadjust_adjoint", context(stencil_factory), f3(delp, "delp"), f3(delz, "delz"),
+                      f3(cappa, "cappa"), f3(heat_source, "heat_source"), f3(pt, "pt"), f3(g_pt, "g_pt"),
+                      f3(g_pkz, "g_pkz"), f3(out[0], "g_delp"), f3(out[1], "g_delz"), f3(out[2], "g_heat"), dtf,
+                      nk_heat, stream_ptr())
+        return out[0], out[1], None, out[2], g_pt, g_pkz, None, None, None
+
+
+def pkz_tempadjust(delp, delz, cappa, heat_source, pt, pkz, stencil_factory, delt_time_factor, nk_heat):
+    """New (pt, pkz) of compute_pkz_tempadjust, differentiable with respect
+    to delp, delz, heat_source, pt and pkz."""
+    return PkzTempadjustFunction.apply(delp, delz, cappa, heat_source, pt, pkz, stencil_factory, delt_time_factor,
+                                       nk_heat)

@@ -5,8 +5,9 @@
 //     filter of the dissipation heat source;
 //   compute_pkz_tempadjust (fv3core/stencils/temperature_adjust.py), the
 //     temperature change from that heat;
-// and the adjoints of the Rayleigh damping (ray_adjoint.h) and of the
-// del-2 filter (del2cubed_adjoint.h).
+// and the adjoints of the Rayleigh damping (ray_adjoint.h), of the del-2
+// filter (del2cubed_adjoint.h) and of the temperature adjustment
+// (tempadjust_adjoint.h).
 #include <math.h>
 
 #include <vector>
@@ -17,6 +18,7 @@
 #include "fmath.h"
 #include "ray_adjoint.h"
 #include "stencil.cuh"
+#include "tempadjust_adjoint.h"
 
 using namespace fv3b;
 
@@ -274,6 +276,41 @@ extern "C" int fv3b_pkz_tempadjust(fv3b_ctx* ctx, const real* delp, const real* 
     real deltmin = dtmp > RC(0.0) ? fabs(m) : -fabs(m);
     W3(pkz, i, j) = p;
     W3(pt, i, j) = F3(pt, i, j) + deltmin / p;
+  }));
+  return FV3B_OK;
+}
+
+// Adjoint of fv3b_pkz_tempadjust (no reference counterpart).  delp, delz,
+// cappa, heat_source and pt are the forward call's inputs; g_pt and g_pkz
+// hold the cotangents of the new pt and pkz on entry and those of the old
+// ones on return (pkz's zero where the stage overwrote it); g_delp, g_delz
+// and g_heat are overwritten on every point.  cappa is held fixed.
+extern "C" int fv3b_pkz_tempadjust_adjoint(fv3b_ctx* ctx, const real* delp, const real* delz, const real* cappa,
+                                           const real* heat_source, const real* pt, real* g_pt, real* g_pkz,
+                                           real* g_delp, real* g_delz, real* g_heat, double delt_time_factor_in,
+                                           int nk_heat, void* stream) {
+  const real delt_time_factor = static_cast<real>(delt_time_factor_in);
+  FV3B_REQUIRE(ctx && delp && delz && cappa && heat_source && pt && g_pt && g_pkz && g_delp && g_delz && g_heat,
+               "fv3b_pkz_tempadjust_adjoint: null argument");
+  const Dims d = ctx->d;
+  FV3B_REQUIRE(nk_heat >= 0 && nk_heat <= d.nz, "fv3b_pkz_tempadjust_adjoint: nk_heat out of range");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t bytes = sizeof(real) * (size_t)6 * d.st;
+  FV3B_CHECK(cudaMemsetAsync(g_delp, 0, bytes, st));
+  FV3B_CHECK(cudaMemsetAsync(g_delz, 0, bytes, st));
+  FV3B_CHECK(cudaMemsetAsync(g_heat, 0, bytes, st));
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
+  FV3B_CHECK(launch_box(Box{s, e + 1, js, je + 1, 0, nk_heat}, st, [=] __device__(int t, int i, int j, int k) {
+    const idx_t o = idx3(d, t, i, j, k);
+    const real lim = k == 0 ? delt_time_factor * RC(0.1) : (k == 1 ? delt_time_factor * RC(0.5) : delt_time_factor);
+    real a_dp, a_dz, a_pt, a_heat;
+    adj::tempadjust_point_adjoint<real>(delp[o], delz[o], pt[o], heat_source[o], cappa[o], lim, RDG, CV_AIR, g_pt[o],
+                                        g_pkz[o], a_dp, a_dz, a_pt, a_heat);
+    g_pt[o] = a_pt;
+    g_pkz[o] = RC(0.0);
+    g_delp[o] = a_dp;
+    g_delz[o] = a_dz;
+    g_heat[o] = a_heat;
   }));
   return FV3B_OK;
 }

@@ -334,6 +334,17 @@ int fv3b_pkz_tempadjust(fv3b_ctx* ctx, const fv3b_real* delp, const fv3b_real* d
                         void* stream);
 
 /*
+ * Adjoint of fv3b_pkz_tempadjust (no reference counterpart).  delp, delz,
+ * cappa, heat_source, pt: the forward call's inputs.  g_pt, g_pkz: the
+ * cotangents of the new pt, pkz on entry, of the old ones on return.
+ * g_delp, g_delz, g_heat: overwritten on every point.  cappa is held fixed.
+ */
+int fv3b_pkz_tempadjust_adjoint(fv3b_ctx* ctx, const fv3b_real* delp, const fv3b_real* delz, const fv3b_real* cappa,
+                                const fv3b_real* heat_source, const fv3b_real* pt, fv3b_real* g_pt, fv3b_real* g_pkz,
+                                fv3b_real* g_delp, fv3b_real* g_delz, fv3b_real* g_heat, double delt_time_factor,
+                                int nk_heat, void* stream);
+
+/*
  * Halo updates, replacing fv3gfs-util's HaloUpdater.update /
  * CubedSphereCommunicator.synchronize_vector_interfaces as the reference's
  * AcousticDynamics._HaloUpdaters use them (fv3core/stencils/dyn_core.py:216-286).
