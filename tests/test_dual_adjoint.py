@@ -1,0 +1,47 @@
+"""The dual-number adjoint scheme (fv3core_b200/csrc/dual.h), built for the
+host: p_grad_c's increments differentiated with duals give the gradients of
+the hand-written adjoint (fv3core_b200/csrc/pgrad_adjoint.h), which torch
+autograd checks in tests/test_pgrad_adjoint.py."""
+import ctypes
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from test_pgrad_adjoint import DT2, H, _metrics, kernel_layout, pgc_case
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _build(tmp_path_factory, name):
+    so = str(tmp_path_factory.mktemp(name) / f"{name}.so")
+    subprocess.check_call(["g++", "-O1", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-o", so,
+                           os.path.join(ROOT, "tests", "native", f"{name}.cpp")])
+    return ctypes.CDLL(so)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+@pytest.mark.parametrize("n,nz,seed", [(12, 8, 3), (7, 4, 4)])
+def test_dual_adjoint_matches_hand_written(tmp_path_factory, n, nz, seed):
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    dual = _build(tmp_path_factory, "dual_adjoint_host")
+    hand = _build(tmp_path_factory, "pgrad_adjoint_host")
+    case = {k: kernel_layout(v) for k, v in pgc_case(n, nz, seed).items()}
+    rng = np.random.default_rng(seed)
+    gu, gv = rng.standard_normal(case["uc"].shape), rng.standard_normal(case["uc"].shape)
+    rdxc, rdyc = _metrics(n)
+    results = []
+    for lib, name in ((dual, "pgc_dual_adjoint_host"), (hand, "pgc_adjoint_host")):
+        out = [np.zeros_like(gu) for _ in range(3)]
+        getattr(lib, name)(ctypes.c_int(n), ctypes.c_int(H), ctypes.c_int(nz), ctypes.c_double(DT2), _ptr(rdxc),
+                           _ptr(rdyc), _ptr(case["delpc"]), _ptr(case["pkc"]), _ptr(case["gz"]), _ptr(gu), _ptr(gv),
+                           *[_ptr(o) for o in out])
+        results.append(out)
+    for a, b in zip(*results):
+        assert np.max(np.abs(a - b)) <= 1e-13 * np.max(np.abs(b))
