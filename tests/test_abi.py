@@ -59,6 +59,20 @@ def test_adjoint_entry_points_reject_bad_arguments_without_gpu():
     for name, n_ptr in (("fv3b_p_grad_c_adjoint", 8), ("fv3b_update_dz_c_adjoint", 9)):
         rc = getattr(L, name)(None, *([None] * n_ptr), 1.0, None)
         assert rc == 1 and b"null argument" in L.fv3b_last_error(), name
+    null_calls = {
+        "fv3b_nh_p_grad_adjoint": [None] * 15 + [1.0, 1.0, 0.28, None],
+        "fv3b_halo_update_scalar_adjoint": [None, 1, 3, 1, None],
+        "fv3b_halo_update_vector_adjoint": [None, None, 0, 1, None],
+        "fv3b_synchronize_vector_interfaces_adjoint": [None, None, 1, None],
+        "fv3b_edge_pe_adjoint": [None, None, None],
+        "fv3b_pk3_halo_adjoint": [None, None, None, 1.0, 0.28, None],
+        "fv3b_ray_fast_adjoint": [None] * 5 + [1.0, 1.0, 1.0, 1.0, 0, None],
+        "fv3b_del2cubed_adjoint": [None, 1.0, 3, None],
+        "fv3b_pkz_tempadjust_adjoint": [None] * 10 + [1.0, 1, None],
+    }
+    for name, args in null_calls.items():
+        rc = getattr(L, name)(None, *args)
+        assert rc == 1 and b"null argument" in L.fv3b_last_error(), name
     # the column adjoints: nulls, then too few levels, then too many
     buf = ctypes.create_string_buffer(8)
     ptrs = [ctypes.addressof(buf)] * 14
