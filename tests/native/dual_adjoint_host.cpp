@@ -52,3 +52,74 @@ extern "C" void pgc_dual_adjoint_host(int n, int halo, int npz, double dt2, cons
             fv3b::adj::dual_point_adjoint<double>(f, cands, G, add);
           }
 }
+
+// The scheme on a branchy stage: UpdateGeopotentialHeightOnCGrid's
+// advected height (upwind choices, corner copies) over T, differentiated
+// with duals; for comparison with the scatter of uzc_point_adjoint
+// (fv3core_b200/csrc/updatedzc_adjoint.h).  g_new: the cotangents of the
+// heights before the floor; the results are accumulated into g_gz, g_ut,
+// g_vt.
+#include "../../fv3core_b200/csrc/updatedzc_adjoint.h"
+
+namespace {
+template <class T, class A>
+T uzc_value(const fv3b::Dims& d, int t, int i, int j, int k, const double* dp0, const double* area, const A& at) {
+  double w[4];
+  fv3b::adj::uzc_weights<double>(dp0, k, d.nk, w);
+  auto flux = [&](int a, int ii, int jj) {
+    T f(0.0);
+    for (int m = 0; m < 4; ++m) {
+      const int kk = k - 2 + m;
+      if (w[m] != 0.0 && kk >= 0 && kk < d.nk) f = f + w[m] * at(a, fv3b::idx3(d, t, ii, jj, kk));
+    }
+    return f;
+  };
+  const T xf0 = flux(1, i, j), xf1 = flux(1, i + 1, j), yf0 = flux(2, i, j), yf1 = flux(2, i, j + 1);
+  auto gzs = [&](int ii, int jj, bool xdir) { return at(0, fv3b::adj::uzc_source(d, t, ii, jj, k, xdir)); };
+  const T sx0 = gzs(xf0 > 0.0 ? i - 1 : i, j, true), sx1 = gzs(xf1 > 0.0 ? i : i + 1, j, true);
+  const T sy0 = gzs(i, yf0 > 0.0 ? j - 1 : j, false), sy1 = gzs(i, yf1 > 0.0 ? j : j + 1, false);
+  const double a = area[fv3b::idx2(d, t, i, j)];
+  return (gzs(i, j, false) * a + xf0 * sx0 - xf1 * sx1 + yf0 * sy0 - yf1 * sy1) / (a + xf0 - xf1 + yf0 - yf1);
+}
+}  // namespace
+
+extern "C" void uzc_dual_scatter_host(int n, int halo, int npz, const double* dp0, const double* area,
+                                      const double* ut, const double* vt, const double* gz, const double* g_new,
+                                      double* g_gz, double* g_ut, double* g_vt) {
+  fv3b_grid_dims g{n, halo, npz, 0};
+  const fv3b::Dims d = fv3b::make_dims(&g);
+  const double* arr[3] = {gz, ut, vt};
+  double* out[3] = {g_gz, g_ut, g_vt};
+  const idx_t S = (idx_t)6 * d.st;
+  for (int t = 0; t < 6; ++t)
+    for (int k = 0; k < d.nk; ++k)
+      for (int j = d.jsc - 1; j <= d.jec + 1; ++j)
+        for (int i = d.isc - 1; i <= d.iec + 1; ++i) {
+          // candidates: gz within two points (corner copies included), the
+          // fluxes' four layers at i, i+1 (ut) and j, j+1 (vt)
+          auto cands = [&](int m, idx_t& c) {
+            if (m < 25 * d.nk) {
+              const int ii = i - 2 + (m / d.nk) % 5, jj = j - 2 + m / (5 * d.nk), kk = m % d.nk;
+              if (kk != k) c = -1;
+              else c = fv3b::idx3(d, t, ii, jj, kk);
+              return true;
+            }
+            m -= 25 * d.nk;
+            if (m >= 16) return false;
+            const int a = 1 + m / 8, side = (m / 4) % 2, kk = k - 2 + m % 4;
+            if (kk < 0 || kk >= d.nk) {
+              c = -1;
+              return true;
+            }
+            c = a * S + fv3b::idx3(d, t, a == 1 ? i + side : i, a == 2 ? j + side : j, kk);
+            return true;
+          };
+          auto f = [&](idx_t c) {
+            if (c < 0) return D(0.0);
+            auto at = [&](int a, idx_t x) { return D(arr[a][x], a * S + x == c ? 1.0 : 0.0); };
+            return uzc_value<D>(d, t, i, j, k, dp0, area, at);
+          };
+          auto add = [&](idx_t c, double v) { out[c / S][c % S] += v; };
+          fv3b::adj::dual_point_adjoint<double>(f, cands, g_new[fv3b::idx3(d, t, i, j, k)], add);
+        }
+}

@@ -45,3 +45,41 @@ def test_dual_adjoint_matches_hand_written(tmp_path_factory, n, nz, seed):
         results.append(out)
     for a, b in zip(*results):
         assert np.max(np.abs(a - b)) <= 1e-13 * np.max(np.abs(b))
+
+
+@pytest.mark.parametrize("thin", [False, True])
+def test_dual_scheme_on_update_dz_c(tmp_path_factory, thin):
+    # a branchy stage (upwind choices, corner copies): the dual scatter of
+    # the advected heights' cotangents equals the hand-written one
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    import cases
+    from test_updatedzc_adjoint import DT2 as UDT, uzc_case
+
+    from test_updatedzc_adjoint import kernel_layout as kl
+
+    dual = _build(tmp_path_factory, "dual_adjoint_host")
+    hand = _build(tmp_path_factory, "updatedzc_adjoint_host")
+    n, nz = 12, 5
+    case = uzc_case(n, nz, 7, thin)
+    k = {name: kl(case[name]) for name in ("ut", "vt", "gz")}
+    area = kl(np.asarray(cases.grid_for(n).area))
+    rng = np.random.default_rng(2)
+    g_gz_out, g_ws = rng.standard_normal(k["gz"].shape), rng.standard_normal(kl(case["ws"]).shape)
+    hand_out = {name: np.zeros_like(k["gz"]) for name in ("gz", "ut", "vt", "hnew", "g_new")}
+    hand.uzc_adjoint_host.restype = None
+    hand.uzc_adjoint_host(ctypes.c_int(n), ctypes.c_int(H), ctypes.c_int(nz), ctypes.c_double(UDT),
+                          _ptr(case["dp_ref"]), _ptr(area), _ptr(k["ut"]), _ptr(k["vt"]), _ptr(k["gz"]),
+                          _ptr(g_gz_out), _ptr(g_ws), *[_ptr(hand_out[x]) for x in ("gz", "ut", "vt", "hnew",
+                                                                                      "g_new")])
+    mine = {name: np.zeros_like(k["gz"]) for name in ("gz", "ut", "vt")}
+    box = np.zeros(k["gz"].shape, bool)
+    box[:, :, H - 1:H + n + 1, H - 1:H + n + 1] = True
+    mine["gz"][~box] = g_gz_out[~box]  # the pass-through outside the updated box
+    dual.uzc_dual_scatter_host.restype = None
+    dual.uzc_dual_scatter_host(ctypes.c_int(n), ctypes.c_int(H), ctypes.c_int(nz), _ptr(case["dp_ref"]), _ptr(area),
+                               _ptr(k["ut"]), _ptr(k["vt"]), _ptr(k["gz"]), _ptr(hand_out["g_new"]),
+                               *[_ptr(mine[x]) for x in ("gz", "ut", "vt")])
+    for name in ("gz", "ut", "vt"):
+        b = hand_out[name]
+        assert np.max(np.abs(mine[name] - b)) <= 1e-12 * np.max(np.abs(b)), name
