@@ -12,9 +12,13 @@
 // so the memory is reserved when the library's module is loaded, not when
 // the call runs.
 //
-// Set-up: the first call on a device looks up the device address of the
-// scratch array (cudaGetSymbolAddress, with that device current) and keeps
-// it for later calls; make that first call before any stream capture.
+// Set-up: a call on a stream that is not being captured looks up the
+// device address of the scratch array (cudaGetSymbolAddress, with the
+// stream's device current) and keeps it per device; a call made during
+// stream capture uses the kept address, so the first call on a device must
+// come before any stream capture.  Looking the address up again on every
+// uncaptured call keeps it valid after a cudaDeviceReset, which reloads the
+// module at a new address.
 //
 // Sharing: there is one scratch array per device for the whole process, and
 // it keeps the contents of the last call.  Nothing in it has to start at
@@ -34,28 +38,36 @@ using namespace fv3b;
 
 namespace {
 
-// Scratch: three fields of at most FV3B_NOALLOC_FIELD_DOUBLES doubles each
-// (6 * (npz+1) * (n+7)^2 <= 1,500,000 covers C48 L79), 36 MB in total.
-constexpr long long FV3B_NOALLOC_FIELD_DOUBLES = 1500000;
-static __device__ __align__(256) real g_noalloc_scratch[3 * FV3B_NOALLOC_FIELD_DOUBLES];
+// Scratch: three fields of at most FV3B_NOALLOC_FIELD_ELEMS elements of
+// fv3b_real each (6 * (npz+1) * (n+7)^2 <= 1,500,000 covers C48 L79):
+// 36 MB in the FP64 build, 18 MB in the mixed-precision build.
+constexpr long long FV3B_NOALLOC_FIELD_ELEMS = 1500000;
+static __device__ __align__(256) real g_noalloc_scratch[3 * FV3B_NOALLOC_FIELD_ELEMS];
 
 constexpr int MAX_DEVICES = 64;
 std::mutex g_scratch_mutex;
 real* g_scratch_addr[MAX_DEVICES] = {nullptr};
 
-// Device address of the scratch array on the current device, looked up once
-// per device.
-cudaError_t scratch_address(real** out) {
+// Device address of the scratch array on the current device: looked up
+// afresh when the stream is not capturing, the kept one otherwise.
+cudaError_t scratch_address(cudaStream_t st, real** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(st, &cap);
+  if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (g_scratch_addr[dev] == nullptr) {
+  if (cap == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
     g_scratch_addr[dev] = static_cast<real*>(p);
+  } else if (g_scratch_addr[dev] == nullptr) {
+    // first call on this device inside a capture: the symbol lookup may load
+    // the module, which a capture does not allow
+    return cudaErrorStreamCaptureUnsupported;
   }
   *out = g_scratch_addr[dev];
   return cudaSuccess;
@@ -70,17 +82,17 @@ extern "C" int fv3b_del2cubed_noalloc(const fv3b_grid_dims* dims, const fv3b_met
   FV3B_REQUIRE(dims && metrics && qdel, "fv3b_del2cubed_noalloc: null argument");
   FV3B_REQUIRE(dims->npx >= 4 && dims->n_halo == 3 && dims->npz >= 1,
                "fv3b_del2cubed_noalloc: need npx >= 4, n_halo == 3, npz >= 1");
-  FV3B_REQUIRE(dims_fit(dims), "fv3b_del2cubed_noalloc: grid too large for the static scratch "
-                               "(6*(npz+1)*(npx+7)^2 must be <= 1500000 doubles)");
+  FV3B_REQUIRE(dims_fit(dims), "fv3b_del2cubed_noalloc: a 3-D field of the six tiles must hold fewer than "
+                               "2^31 elements");
   const Dims d = make_dims(dims);
-  FV3B_REQUIRE(d.st * 6 <= FV3B_NOALLOC_FIELD_DOUBLES,
+  FV3B_REQUIRE(d.st * 6 <= FV3B_NOALLOC_FIELD_ELEMS,
                "fv3b_del2cubed_noalloc: grid too large for the static scratch "
-               "(6*(npz+1)*(npx+7)^2 must be <= 1500000 doubles)");
+               "(6*(npz+1)*(npx+7)^2 must be <= 1500000 elements, i.e. at most C48 L79)");
   const fv3b_metrics g = *metrics;
   real* base = nullptr;
-  FV3B_CHECK(scratch_address(&base));
-  real *q = base, *fx = base + FV3B_NOALLOC_FIELD_DOUBLES, *fy = base + 2 * FV3B_NOALLOC_FIELD_DOUBLES;
   cudaStream_t st = (cudaStream_t)stream;
+  FV3B_CHECK(scratch_address(st, &base));
+  real *q = base, *fx = base + FV3B_NOALLOC_FIELD_ELEMS, *fy = base + 2 * FV3B_NOALLOC_FIELD_ELEMS;
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nz = d.nz;
   const int full = d.ni - 1;
   const int ntimes = nmax < 3 ? nmax : 3;

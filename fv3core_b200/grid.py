@@ -64,7 +64,11 @@ def _gc_dist(p, q):
 def _tangent(p, q):
     """Unit tangent at p of the great circle towards q."""
     t = q - np.sum(q * p, axis=-1, keepdims=True) * p
-    return t / np.linalg.norm(t, axis=-1, keepdims=True)
+    norm = np.linalg.norm(t, axis=-1, keepdims=True)
+    # Where q coincides with p (the halo points that fold onto a cube vertex)
+    # the tangent is undefined: those points hold NaN, set explicitly.
+    defined = norm > 0.0
+    return np.where(defined, t / np.where(defined, norm, 1.0), np.nan)
 
 
 def _cos_angle(p, q1, q2):

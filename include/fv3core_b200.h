@@ -423,15 +423,19 @@ fv3b_real* fv3b_acoustics_temporary(fv3b_ctx* ctx, const char* name);
  * fv3b_del2cubed (HyperdiffusionDamping, fv3core/stencils/del2cubed.py:152-181)
  * for callers that cannot let the library allocate device memory: it takes
  * no context (fv3b_ctx_create allocates the full stage workspace) and
- * allocates nothing; its scratch is a fixed file-scope device array reserved
- * when the library is loaded.  Grids with 6*(npz+1)*(npx+2*n_halo+1)^2 above
- * 1,500,000 (larger than C48 L79) are rejected with FV3B_ERR_ARGUMENT.  The
- * first call on a device looks up the scratch's device address (make it
- * before any stream capture).  The scratch is shared by every caller on a
- * device and keeps the last call's contents (nothing in it needs to start at
- * zero): calls must not overlap in time (issue them on one stream, or order
- * them).  metrics: as for
- * fv3b_ctx_create (del6_u, del6_v and rarea are read).
+ * allocates nothing; its scratch is a fixed file-scope device array of
+ * 3 x 1,500,000 elements of fv3b_real (36 MB in the FP64 build, 18 MB in the
+ * mixed-precision build), reserved on every device that loads the library.
+ * Grids with 6*(npz+1)*(npx+2*n_halo+1)^2 above 1,500,000 (larger than
+ * C48 L79) are rejected with FV3B_ERR_ARGUMENT.  A call on a stream that is
+ * not capturing looks up the scratch's device address (so the address stays
+ * valid after a cudaDeviceReset); a call during stream capture uses the
+ * address kept by the last uncaptured call on that device, so the first call
+ * on a device must come before any stream capture.  The scratch is shared by
+ * every caller on a device and keeps the last call's contents (nothing in it
+ * needs to start at zero): calls must not overlap in time (issue them on one
+ * stream, or order them).  metrics: as for fv3b_ctx_create (del6_u, del6_v
+ * and rarea are read).
  */
 int fv3b_del2cubed_noalloc(const fv3b_grid_dims* dims, const fv3b_metrics* metrics, fv3b_real* qdel, double cd, int nmax,
                            void* stream);

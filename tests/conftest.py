@@ -10,11 +10,6 @@ sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built library")
-    config.addinivalue_line(
-        "markers",
-        "gpu_pending: needs a CUDA GPU; checks device entry points that have not yet run on one "
-        "(select with -m gpu_pending; promoted to gpu once they pass)",
-    )
     config.addinivalue_line("markers", "slow: longer CPU test")
 
 
@@ -29,5 +24,5 @@ def pytest_collection_modifyitems(config, items):
         return
     skip = pytest.mark.skip(reason="no CUDA device")
     for item in items:
-        if "gpu" in item.keywords or "gpu_pending" in item.keywords:
+        if "gpu" in item.keywords:
             item.add_marker(skip)

@@ -186,6 +186,9 @@ def acoustics_case(n=12, nz=8, seed=41, n_split=2):
 
 
 CASES["acoustics"] = acoustics_case
+# the parity case of the plain FP64 method: C12 L79, one acoustic substep of
+# dt_acoustic = 225 / 6 s (n_split = 1, mdt = 37.5 s)
+CASES["acoustics_c12_l79"] = acoustics_case
 
 
 def resting_case(n=12, nz=8, n_split=2):

@@ -1,8 +1,8 @@
 """Generate golden fixtures by running the reference's own stencil classes.
 
-Run here (needs the reference checkout at /root/reference)::
+Run on a machine that holds the reference checkout::
 
-    python tests/golden/make_golden.py [case ...]
+    FV3CORE_REFERENCE=<checkout> python tests/golden/make_golden.py [case ...]
 
 For each case in ``cases.py`` the inputs are rebuilt deterministically, the
 reference class runs tile by tile (or, for the full substep, six tiles in
@@ -163,11 +163,29 @@ def run_acoustics(case, n, nz):
     return out, {"region": "full storage"}
 
 
+# fields of the C12 L79 fixture: the prognostic fields and the edge
+# pressures, on the compute domain (the full storages of 24 fields at L79
+# would make a 40 MB fixture)
+L79_FIELDS = {"u": (0, 1, 0), "v": (1, 0, 0), "w": (0, 0, 0), "delp": (0, 0, 0), "pt": (0, 0, 0),
+              "delz": (0, 0, 0), "q_con": (0, 0, 0), "pe": (0, 0, 1), "pk": (0, 0, 1), "peln": (0, 0, 1),
+              "pkz": (0, 0, 0)}
+
+
+def run_acoustics_compute(case, n, nz):
+    out, _ = run_acoustics(case, n, nz)
+    h = 3
+    res = {}
+    for name, (di, dj, dk) in L79_FIELDS.items():
+        res[name] = out[name][:, h:h + n + di, h:h + n + dj, :nz + dk]
+    return res, {"region": "compute domain (+1 on staggered axes)"}
+
+
 RUNNERS = {
     "acoustics": (run_acoustics, dict(n=12, nz=8, seed=41)),
     "d_sw": (run_d_sw, dict(n=12, nz=8, seed=31)),
     "c_sw": (run_c_sw, dict(n=12, nz=6, seed=21)),
     "riem_solver_c": (run_riem_solver_c, dict(n=12, nz=16, seed=11)),
+    "acoustics_c12_l79": (run_acoustics_compute, dict(n=12, nz=79, seed=7, n_split=1)),
 }
 
 

@@ -3,8 +3,10 @@
 The reference (fv3core, pure gtscript) needs gt4py v36 and fv3gfs-util,
 neither of which is installed.  ``gt4py_shim/`` holds a minimal gtscript
 interpreter with gt4py-numpy-backend semantics and the few fv3gfs.util names
-the hot path imports; with them the reference modules import from
-``/root/reference`` unchanged and their stencil classes execute.  Results are
+the hot path imports; with them the reference modules import unchanged from
+the checkout named by the ``FV3CORE_REFERENCE`` environment variable (the
+directory that holds the ``fv3core`` package) and their stencil classes
+execute.  Results are
 written as golden fixtures by ``make_golden.py``; nothing here is used on
 the GPU box or by the product.
 """
@@ -17,10 +19,20 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFERENCE = os.environ.get("FV3CORE_REFERENCE", "/root/reference")
+
+
+def reference_root():
+    """The reference checkout, from ``FV3CORE_REFERENCE`` (required)."""
+    root = os.environ.get("FV3CORE_REFERENCE")
+    if not root:
+        raise RuntimeError("set FV3CORE_REFERENCE to the reference checkout (the directory holding fv3core/)")
+    if not os.path.isdir(os.path.join(root, "fv3core")):
+        raise RuntimeError(f"FV3CORE_REFERENCE={root!r} holds no fv3core package")
+    return root
 
 
 def import_reference():
+    REFERENCE = reference_root()
     if HERE + "/gt4py_shim" not in sys.path:
         sys.path.insert(0, os.path.join(HERE, "gt4py_shim"))
     if REFERENCE not in sys.path:

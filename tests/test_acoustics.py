@@ -104,6 +104,117 @@ def test_gpu_against_numpy_transcendentals():
     assert max(errs.values()) <= 1e-7, errs
 
 
+L79_GOLDEN = os.path.join(HERE, "golden", "acoustics_c12_l79.npz")
+
+
+def _c12_l79():
+    """The golden C12 L79 case: one acoustic substep (n_split = 1, dt = 37.5 s)
+    of the seeded baroclinic-wave state, run by the reference itself."""
+    g = np.load(L79_GOLDEN)
+    n, nz, seed, n_split = (int(g["arg_" + k]) for k in ("n", "nz", "seed", "n_split"))
+    return g, n, nz, cases.acoustics_case(n, nz, seed, n_split=n_split)
+
+
+def _golden_fields(out, g, n, nz):
+    """``out`` cut to the fixture's compute-domain region of each field."""
+    res = {}
+    for name in g.files:
+        if name.startswith(("arg_", "meta_")):
+            continue
+        di, dj, dk = LAYOUT[name]
+        res[name] = out[name][:, H:H + n + di, H:H + n + dj, :nz + dk]
+    return res
+
+
+def test_oracle_matches_reference_golden_c12_l79():
+    """The oracle reproduces the reference's own C12 L79 substep bit for bit."""
+    g, n, nz, case = _c12_l79()
+    out = _golden_fields(oracle_runs.run_acoustics(case, n, nz), g, n, nz)
+    for k, v in out.items():
+        assert _same(v, g[k]), k
+
+
+# Bounds of the CUDA path against the reference's own arithmetic (numpy's
+# exp/log/power) on the C12 L79 substep.  The oracle with numpy's
+# transcendentals and the oracle with the kernels' own (both within 1 ulp)
+# differ on this case by (parity metric, compare_arr with near-zero 1e-18):
+# delp 1.9e-16, pt 2.7e-16, q_con 2.2e-16, delz 1.6e-13, pe 1.1e-16,
+# pk 9.4e-16, peln 2.0e-16, pkz 6.2e-14; w 5.7e-12; u 1.1e-10 (3.6e-9),
+# v 9.9e-11 (9.9e-10).  The bounds sit above those floors; the mass, heat,
+# pressure and height fields keep 1e-12.
+C12_L79_BOUNDS = {
+    "delp": (1e-12, 1e-12), "pt": (1e-12, 1e-12), "q_con": (1e-12, 1e-12), "delz": (1e-12, 1e-12),
+    "pe": (1e-12, 1e-12), "pk": (1e-12, 1e-12), "peln": (1e-12, 1e-12), "pkz": (1e-12, 1e-12),
+    "w": (5e-11, 5e-11), "u": (1e-9, 3e-8), "v": (1e-9, 1e-8),
+}
+
+
+def test_conditioning_bounds_c12_l79():
+    """The floors behind C12_L79_BOUNDS: the two transcendental flavours of
+    the oracle stay inside the bounds on the golden case."""
+    from oracle import _math
+
+    from metrics import max_rel_err
+
+    g, n, nz, case = _c12_l79()
+    a = _golden_fields(oracle_runs.run_acoustics(case, n, nz), g, n, nz)
+    with _math.device_math():
+        b = _golden_fields(oracle_runs.run_acoustics(case, n, nz), g, n, nz)
+    for k, (bp, bc) in C12_L79_BOUNDS.items():
+        assert parity_err(a[k], b[k]) <= bp and max_rel_err(a[k], b[k]) <= bc, k
+
+
+@pytest.mark.gpu
+def test_gpu_c12_l79_matches_oracle():
+    """The plain FP64 method at C12 L79, one substep: 1e-12 on every field
+    against the oracle with the kernels' exp/log/pow."""
+    import gpu_runs
+    from oracle import _math
+
+    _, n, nz, case = _c12_l79()
+    with _math.device_math():
+        ref = oracle_runs.run_acoustics(case, n, nz)
+    gpu = gpu_runs.run_acoustics(case, n, nz)
+    errs = _errors(gpu, ref, n, nz)
+    bad = {k: e for k, e in errs.items() if not e <= 1e-12}
+    assert not bad, bad
+
+
+@pytest.mark.gpu
+def test_gpu_c12_l79_against_reference_golden():
+    """The plain FP64 method at C12 L79 against the reference's own output
+    (the committed fixture), field by field, in both metrics: the parity
+    metric and the reference's compare_arr with near-zero 1e-18."""
+    import gpu_runs
+
+    from metrics import max_rel_err
+
+    g, n, nz, case = _c12_l79()
+    gpu = _golden_fields(gpu_runs.run_acoustics(case, n, nz), g, n, nz)
+    report = {k: (parity_err(gpu[k], g[k]), max_rel_err(gpu[k], g[k])) for k in C12_L79_BOUNDS}
+    print("C12 L79 vs reference (parity, compare_arr):", report)
+    bad = {k: e for k, e in report.items() if not (e[0] <= C12_L79_BOUNDS[k][0] and e[1] <= C12_L79_BOUNDS[k][1])}
+    assert not bad, bad
+
+
+@pytest.mark.gpu
+def test_gpu_c48_l79_full_call_matches_oracle():
+    """A whole AcousticDynamics call of the benchmark's namelist at C48 L79:
+    n_split = 6 substeps of dt_atmos = 225 s, 1e-12 on every field against
+    the oracle with the kernels' exp/log/pow."""
+    import gpu_runs
+    from oracle import _math
+
+    n, nz = 48, 79
+    case = cases.acoustics_case(n, nz, 13, n_split=6)
+    with _math.device_math():
+        ref = oracle_runs.run_acoustics(case, n, nz)
+    gpu = gpu_runs.run_acoustics(case, n, nz)
+    errs = _errors(gpu, ref, n, nz)
+    bad = {k: e for k, e in errs.items() if not e <= 1e-12}
+    assert not bad, bad
+
+
 @pytest.mark.gpu
 def test_gpu_full_storage_matches_oracle():
     """Every point of every field, halos included, on the golden case,

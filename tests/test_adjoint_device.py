@@ -2,8 +2,7 @@
 (tests/test_a2b_adjoint.py, test_halo_adjoint.py, test_pressure_adjoint.py,
 test_ray_adjoint.py, test_del2cubed_adjoint.py, test_tempadjust_adjoint.py):
 the gradients through their torch.autograd Functions on the GPU against the
-host builds of the same headers.  Marked gpu_pending until they have run on
-a GPU."""
+host builds of the same headers."""
 import ctypes
 import os
 import subprocess
@@ -13,7 +12,7 @@ import pytest
 
 import cases
 
-pytestmark = pytest.mark.gpu_pending
+pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 H = 3

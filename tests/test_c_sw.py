@@ -37,7 +37,7 @@ def _interior_mask(n, nz, h=3):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n,nz,seed", [(12, 6, 21), (24, 10, 4), (48, 5, 9)])
+@pytest.mark.parametrize("n,nz,seed", [(12, 6, 21), (24, 10, 4), (48, 5, 9), (12, 79, 6)])
 def test_gpu_matches_oracle(n, nz, seed):
     import gpu_runs
 

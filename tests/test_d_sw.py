@@ -41,7 +41,7 @@ def _compute_region(name, n, nz, h=3):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n,nz,seed", [(12, 8, 31), (24, 12, 2), (48, 6, 8)])
+@pytest.mark.parametrize("n,nz,seed", [(12, 8, 31), (24, 12, 2), (48, 6, 8), (12, 79, 7)])
 def test_gpu_matches_oracle(n, nz, seed):
     import gpu_runs
 

@@ -18,7 +18,7 @@ def _device_math():
     with _math.device_math():
         yield
 H = 3
-SIZES = [(12, 8, 3), (24, 16, 4)]
+SIZES = [(12, 8, 3), (24, 16, 4), (12, 79, 5)]
 
 
 def _state(n, nz, seed):
