@@ -71,6 +71,16 @@ CTX_SIGNATURES = {
     "fv3b_synchronize_vector_interfaces_adjoint": [P, P, ctypes.c_int, P],
     "fv3b_acoustics_setup": [P] * 6,
     "fv3b_acoustics": [P, P],
+    "fv3b_ppm_flux": [ctypes.c_int, ctypes.c_int, P, P, P] + [ctypes.c_int] * 6 + [P],
+    "fv3b_transport_create": [ctypes.c_int, P, P, ctypes.c_int, P],
+}
+
+# entry points whose first argument is a transport object (fv3b_transport*),
+# which belongs to the context it was created on
+TRANSPORT_SIGNATURES = {
+    "fv3b_transport_destroy": [],
+    "fv3b_fvtp2d": [P] * 10 + [P],
+    "fv3b_tracer_advection": [ctypes.c_int, P, P, P, P, P, P, D, P],
 }
 
 # entry points that return a pointer rather than a status
@@ -133,6 +143,10 @@ def lib(precision="f64"):
             fn = getattr(L, name)
             fn.argtypes = [ctypes.c_void_p] + args
             fn.restype = ctypes.c_int
+        for name, args in TRANSPORT_SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = [ctypes.c_void_p] + args
+            fn.restype = ctypes.c_int
         for name, args in PTR_SIGNATURES.items():
             fn = getattr(L, name)
             fn.argtypes = args
@@ -166,11 +180,21 @@ def call_ctx(name, ctx, *args):
         raise ERRORS.get(rc, RuntimeError)(f"{name} failed ({rc}): {msg}")
 
 
+def call_precision(name, precision, *args):
+    """Call entry point ``name`` of the ``precision`` build with its own
+    argument list; raise the reference's exception type on failure."""
+    L = lib(precision)
+    rc = getattr(L, name)(*args)
+    if rc != 0:
+        msg = L.fv3b_last_error().decode()
+        raise ERRORS.get(rc, RuntimeError)(f"{name} failed ({rc}): {msg}")
+
+
 def exported_symbols():
     return ["fv3b_last_error", "fv3b_version", "fv3b_launch_count", "fv3b_set_launch_shape", "fv3b_get_launch_shape",
             "fv3b_ctx_create", "fv3b_ctx_destroy"] + [
         k for k, v in SIGNATURES.items() if v is not None
-    ] + list(CTX_SIGNATURES) + list(PTR_SIGNATURES)
+    ] + list(CTX_SIGNATURES) + list(PTR_SIGNATURES) + list(TRANSPORT_SIGNATURES)
 
 
 def launch_count(precision="f64"):

@@ -124,6 +124,133 @@ __device__ __forceinline__ real ppm_flux(const Q& q, const A& dxa, real c, int p
   return c > RC(0.0) ? qm + fx1 * mask : q0 + fx1 * mask;
 }
 
+// ------------------------------------------------------------------ ord 8
+// The ord-8 limiter of tracer transport (hord = 8): xppm.py:85-266 and
+// ppm.py:22-36.  ppm.py:16-18
+constexpr real PPM_S11 = RC(11.0) / RC(14.0), PPM_S14 = RC(4.0) / RC(7.0), PPM_S15 = RC(3.0) / RC(14.0);
+
+// basic_operations.sign (basic_operations.py:34-40): |a|, negative unless b > 0
+__device__ __forceinline__ real sign_of(real a, real b) { return b > RC(0.0) ? fabs(a) : -fabs(a); }
+
+// dm_iord8plus (xppm.py:85-90) of the cell at offset o; the dm_left /
+// dm_right temporaries of bl_br_edges are this function of the neighbour
+template <typename Q>
+__device__ __forceinline__ real dm_ord8(const Q& q, int o) {
+  const real qm = q(o - 1), q0 = q(o), qp = q(o + 1);
+  const real xt = RC(0.25) * (qp - qm);
+  const real dqr = fmax(fmax(q0, qm), qp) - q0;
+  const real dql = q0 - fmin(fmin(q0, qm), qp);
+  return sign_of(fmin(fmin(fabs(xt), dqr), dql), xt);
+}
+
+// al_iord8plus (xppm.py:93-95): interface value left of cell o
+template <typename Q>
+__device__ __forceinline__ real al_ord8(const Q& q, int o) {
+  return RC(0.5) * (q(o - 1) + q(o)) + (RC(1.0) / RC(3.0)) * (dm_ord8(q, o - 1) - dm_ord8(q, o));
+}
+
+// xt_dxa_edge_0 / xt_dxa_edge_1 with xt_minmax (xppm.py:105-145), cell o
+template <typename Q, typename A>
+__device__ __forceinline__ real xt_dxa_edge0(const Q& q, const A& dxa, int o) {
+  const real qm = q(o - 1), q0 = q(o), q1 = q(o + 1), q2 = q(o + 2);
+  const real d0 = dxa(o), dm = dxa(o - 1), d1 = dxa(o + 1), d2 = dxa(o + 2);
+  const real xt = RC(0.5) * (((RC(2.0) * d0 + dm) * q0 - d0 * qm) / (dm + d0) +
+                             ((RC(2.0) * d1 + d2) * q1 - d1 * q2) / (d1 + d2));
+  const real minq = fmin(fmin(fmin(qm, q0), q1), q2);
+  const real maxq = fmax(fmax(fmax(qm, q0), q1), q2);
+  return fmin(fmax(xt, minq), maxq);
+}
+template <typename Q, typename A>
+__device__ __forceinline__ real xt_dxa_edge1(const Q& q, const A& dxa, int o) {
+  const real qm2 = q(o - 2), qm = q(o - 1), q0 = q(o), q1 = q(o + 1);
+  const real d0 = dxa(o), dm = dxa(o - 1), dm2 = dxa(o - 2), d1 = dxa(o + 1);
+  const real xt = RC(0.5) * (((RC(2.0) * dm + dm2) * qm - dm * qm2) / (dm2 + dm) +
+                             ((RC(2.0) * d0 + d1) * q0 - d0 * q1) / (d0 + d1));
+  const real minq = fmin(fmin(fmin(qm2, qm), q0), q1);
+  const real maxq = fmax(fmax(fmax(qm2, qm), q0), q1);
+  return fmin(fmax(xt, minq), maxq);
+}
+
+// Edge perturbations (bl, br) of the cell at offset o, absolute index p:
+// compute_blbr_ord8plus (xppm.py:250-266) = blbr_iord8 (98-102) away from
+// the tile edges; bl_br_edges (185-246) and the standard constraint
+// (pert_ppm_standard_constraint_fcn, ppm.py:22-36) on the three cells at
+// each edge.  The edge regions are tested last first, so that where two of
+// them meet the later one wins, as the reference's sequential regions do.
+template <typename Q, typename A>
+__device__ __forceinline__ void blbr_ord8(const Q& q, const A& dxa, int o, int p, int s, int e, real& bl,
+                                          real& br) {
+  const real q0 = q(o);
+  const real dm0 = dm_ord8(q, o);
+  const bool near_s = p >= s - 1 && p <= s + 1, near_e = p >= e - 1 && p <= e + 1;
+  if (!near_s && !near_e) {
+    const real xt = RC(2.0) * dm0;
+    bl = -RC(1.0) * sign_of(fmin(fabs(xt), fabs(al_ord8(q, o) - q0)), xt);
+    br = sign_of(fmin(fabs(xt), fabs(al_ord8(q, o + 1) - q0)), xt);
+    return;
+  }
+  real xbl, xbr;
+  if (p == e + 1) {
+    xbl = xt_dxa_edge1(q, dxa, o);
+    xbr = PPM_S11 * (q(o + 1) - q0) - PPM_S14 * dm_ord8(q, o + 1) + q0;
+  } else if (p == e) {
+    xbl = PPM_S15 * q0 + PPM_S11 * q(o - 1) + PPM_S14 * dm_ord8(q, o - 1);
+    xbr = xt_dxa_edge0(q, dxa, o);
+  } else if (p == e - 1) {
+    xbl = al_ord8(q, o);
+    xbr = PPM_S15 * q(o + 1) + PPM_S11 * q0 + PPM_S14 * dm0;
+  } else if (p == s + 1) {
+    xbl = PPM_S15 * q(o - 1) + PPM_S11 * q0 - PPM_S14 * dm0;
+    xbr = al_ord8(q, o + 1);
+  } else if (p == s) {
+    xbl = xt_dxa_edge1(q, dxa, o);
+    xbr = PPM_S15 * q0 + PPM_S11 * q(o + 1) - PPM_S14 * dm_ord8(q, o + 1);
+  } else {  // p == s - 1
+    xbl = PPM_S14 * dm_ord8(q, o - 1) + PPM_S11 * (q(o - 1) - q0) + q0;
+    xbr = xt_dxa_edge0(q, dxa, o);
+  }
+  real l = xbl - q0, r = xbr - q0;
+  if (l * r < RC(0.0)) {
+    const real da1 = l - r;
+    const real da2 = da1 * da1;
+    const real a6da = RC(3.0) * (l + r) * da1;
+    if (a6da < -da2)
+      r = -RC(2.0) * l;
+    else if (a6da > da2)
+      l = -RC(2.0) * r;
+  } else {
+    l = RC(0.0);
+    r = RC(0.0);
+  }
+  bl = l;
+  br = r;
+}
+
+// get_flux_ord8plus (xppm.py:75-82): mean of q advected through the
+// interface at offset 0 with the ord-8 perturbations of the upwind cell
+template <typename Q, typename A>
+__device__ __forceinline__ real ppm_flux8(const Q& q, const A& dxa, real c, int pos, int s, int e) {
+  real bl, br;
+  if (c > RC(0.0)) {
+    blbr_ord8(q, dxa, -1, pos - 1, s, e, bl, br);
+    const real b0 = bl + br;
+    return q(-1) + (RC(1.0) - c) * (br - c * b0);
+  }
+  blbr_ord8(q, dxa, 0, pos, s, e, bl, br);
+  const real b0 = bl + br;
+  return q(0) + (RC(1.0) + c) * (bl + c * b0);
+}
+
+// The PPM flux of order ORD8 ? 8 : mord.
+template <bool ORD8, typename Q, typename A>
+__device__ __forceinline__ real ppm_flux_ord(const Q& q, const A& dxa, real c, int pos, int s, int e, int mord) {
+  if constexpr (ORD8) {
+    return ppm_flux8(q, dxa, c, pos, s, e);
+  } else {
+    return ppm_flux(q, dxa, c, pos, s, e, mord);
+  }
+}
+
 // Scratch and options of one FiniteVolumeTransport call.
 struct FvTp2dArgs {
   const real* q_base;   // field, its cube-corner blocks holding their x copies
@@ -135,7 +262,7 @@ struct FvTp2dArgs {
   const real* y_unit;
   real* fx;
   real* fy;
-  int hord;
+  int hord;             // 5, 6, 7 (monotonic PPM) or 8 (ord-8 limiter)
   real* fx_mean;
   real* fy_mean;
   real* q_adv_x;
@@ -143,13 +270,14 @@ struct FvTp2dArgs {
 };
 
 // FiniteVolumeTransport.__call__ (fvtp2d.py:249-362) without the damping
-// step; three passes: inner PPM, q_i/q_j, outer PPM + final fluxes.
-inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a, cudaStream_t st) {
+// step; three passes: inner PPM, q_i/q_j, outer PPM + final fluxes.  Inner
+// and outer PPM have the same order here (the reference's hord = 10, inner
+// 8 and outer 10, fails its own compile_assert and is rejected).
+template <bool ORD8>
+inline cudaError_t fvtp2d_impl(const Dims d, const fv3b_metrics g, const FvTp2dArgs a, cudaStream_t st) {
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nk = d.nk;
   const int full = d.ni - 1;
-  const int ord_in = a.hord == 10 ? 8 : a.hord;
-  const int mord_in = ord_in < 0 ? -ord_in : ord_in;
-  const int mord_out = a.hord < 0 ? -a.hord : a.hord;
+  const int mord = a.hord < 0 ? -a.hord : a.hord;
   cudaError_t err;
   // inner PPM: fy_mean on [is-3, ie+4] x [js, je+1], fx_mean on [is, ie+1] x [js-3, je+4]
   err = launch_box(Box{s - 3, e + 5, js - 3, je + 5, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
@@ -157,14 +285,14 @@ inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a
     if (j >= js && j < je + 2) {
       auto dya = line2<1>(d, g.dya, t, i, j);
       if (i >= s && i <= e) {  // no cube-corner point on this line: plain reads
-        a.fy_mean[o] = ppm_flux(line3<1>(d, a.q_base, t, i, j, k), dya, a.cry[o], j, js, je, mord_in);
+        a.fy_mean[o] = ppm_flux_ord<ORD8>(line3<1>(d, a.q_base, t, i, j, k), dya, a.cry[o], j, js, je, mord);
       } else {
-        a.fy_mean[o] = ppm_flux(LineQY{d, a.q_base, t, i, j, k}, dya, a.cry[o], j, js, je, mord_in);
+        a.fy_mean[o] = ppm_flux_ord<ORD8>(LineQY{d, a.q_base, t, i, j, k}, dya, a.cry[o], j, js, je, mord);
       }
     }
     if (i >= s && i < e + 2) {
-      a.fx_mean[o] = ppm_flux(line3<0>(d, a.q_base, t, i, j, k), line2<0>(d, g.dxa, t, i, j), a.crx[o], i, s, e,
-                              mord_in);
+      a.fx_mean[o] = ppm_flux_ord<ORD8>(line3<0>(d, a.q_base, t, i, j, k), line2<0>(d, g.dxa, t, i, j), a.crx[o],
+                                        i, s, e, mord);
     }
   });
   if (err != cudaSuccess) return err;
@@ -191,22 +319,29 @@ inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a
   return launch_box(Box{s, e + 2, js, je + 2, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
     const idx_t o = idx3(d, t, i, j, k);
     if (j <= je) {
-      real xo = ppm_flux(line3<0>(d, a.q_adv_y, t, i, j, k), line2<0>(d, g.dxa, t, i, j), a.crx[o], i, s, e, mord_out);
+      real xo = ppm_flux_ord<ORD8>(line3<0>(d, a.q_adv_y, t, i, j, k), line2<0>(d, g.dxa, t, i, j), a.crx[o], i, s,
+                                   e, mord);
       a.fx[o] = RC(0.5) * (xo + a.fx_mean[o]) * a.x_unit[o];
     }
     if (i <= e) {
-      real yo = ppm_flux(line3<1>(d, a.q_adv_x, t, i, j, k), line2<1>(d, g.dya, t, i, j), a.cry[o], j, js, je, mord_out);
+      real yo = ppm_flux_ord<ORD8>(line3<1>(d, a.q_adv_x, t, i, j, k), line2<1>(d, g.dya, t, i, j), a.cry[o], j, js,
+                                   je, mord);
       a.fy[o] = RC(0.5) * (yo + a.fy_mean[o]) * a.y_unit[o];
     }
   });
 }
 
+// hord 5, 6, 7 or 8 (the caller rejects the rest)
+inline cudaError_t fvtp2d(const Dims d, const fv3b_metrics g, const FvTp2dArgs a, cudaStream_t st) {
+  return a.hord == 8 ? fvtp2d_impl<true>(d, g, a, st) : fvtp2d_impl<false>(d, g, a, st);
+}
+
 // The x half of CopyCornersXY in place (corners.py:64-117): only the 3 x 3
-// cube-corner blocks of q change; all npz+1 levels.
-inline cudaError_t copy_corners_x_inplace(const Dims d, real* q, cudaStream_t st) {
+// cube-corner blocks of q change; levels [0, nlev) (all npz+1 by default).
+inline cudaError_t copy_corners_x_inplace(const Dims d, real* q, cudaStream_t st, int nlev = -1) {
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
   // 4 corner blocks of 3 x 3 points
-  return launch_box(Box{0, 12, 0, 3, 0, d.nk}, st, [=] __device__(int t, int x, int y, int k) {
+  return launch_box(Box{0, 12, 0, 3, 0, nlev < 0 ? d.nk : nlev}, st, [=] __device__(int t, int x, int y, int k) {
     PT_SETUP(d, t, k);
     const int c = x / 3, a = x % 3;
     const int i = (c == 0 || c == 2) ? s - 3 + a : e + 1 + a;

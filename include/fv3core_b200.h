@@ -413,6 +413,66 @@ int fv3b_acoustics_setup(fv3b_ctx* ctx, const fv3b_acoustic_config* config, cons
  */
 int fv3b_acoustics(fv3b_ctx* ctx, const fv3b_dycore_state* state, void* stream);
 
+/*
+ * FiniteVolumeTransport as an object (fv3core/stencils/fvtp2d.py:151-247,
+ * constructor FiniteVolumeTransport(stencil_factory, grid_data,
+ * damping_coefficients, grid_type, hord, nord=None, damp_c=None)).  hord is
+ * the PPM order (5, 6, 7, or 8 for the ord-8 limiter of tracer transport);
+ * nord and damp_c are HOST per-level columns of n >= npz values (both NULL
+ * for no del-n damping), turned into the DelnFlux coefficients
+ * (damp_c * da_min)^(nord + 1) (delnflux.py:24-26, 907-962).  Allocates the
+ * device columns (cudaMalloc) and synchronises.  Rejects damp_c columns
+ * that are small only on some levels (FV3B_ERR_UNSUPPORTED), as DelnFlux
+ * does.  Lives until fv3b_transport_destroy; belongs to ctx.
+ */
+typedef struct fv3b_transport fv3b_transport;
+int fv3b_transport_create(fv3b_ctx* ctx, int hord, const double* nord, const double* damp_c, int n,
+                          fv3b_transport** out);
+int fv3b_transport_destroy(fv3b_transport* transport);
+
+/*
+ * FiniteVolumeTransport.__call__ (fv3core/stencils/fvtp2d.py:249-362):
+ * q_x_flux, q_y_flux = the Lin-Rood fluxes of q from the Courant numbers
+ * crx, cry and the area fluxes; x/y_mass_flux (NULL: the area fluxes) weight
+ * the final fluxes; mass (NULL allowed without damping) weights the del-n
+ * damping.  q's 3x3 cube-corner halo blocks are overwritten with their
+ * x-direction copies, as the reference's CopiedCorners base is
+ * (corners.py:64-117); its y-direction copies are read on the fly.
+ */
+int fv3b_fvtp2d(const fv3b_transport* transport, fv3b_real* q, const fv3b_real* crx, const fv3b_real* cry,
+                const fv3b_real* x_area_flux, const fv3b_real* y_area_flux, fv3b_real* q_x_flux,
+                fv3b_real* q_y_flux, const fv3b_real* x_mass_flux, const fv3b_real* y_mass_flux,
+                const fv3b_real* mass, void* stream);
+
+/*
+ * XPiecewiseParabolic.__call__ (axis 0; fv3core/stencils/xppm.py:283-347)
+ * and YPiecewiseParabolic.__call__ (axis 1; yppm.py): flux = the mean of q
+ * advected through each interface for Courant number c, order iord (5, 6, 7
+ * or 8), over the box [i0, i0+ni) x [j0, j0+nj) x [k0, k0+nk) (the
+ * reference's origin and domain).  The tile-edge rules apply at the tile's
+ * compute-domain edges, as the reference's i_start / i_end externals place
+ * them.  The box plus three points before and two after along the axis
+ * must lie inside the storage.  dxa / dya are the context's.
+ */
+int fv3b_ppm_flux(fv3b_ctx* ctx, int axis, int iord, const fv3b_real* q, const fv3b_real* c, fv3b_real* flux,
+                  int i0, int j0, int k0, int ni, int nj, int nk, void* stream);
+
+/*
+ * TracerAdvection.__call__ (fv3core/stencils/tracer_2d_1l.py:199-300),
+ * constructed with the given transport (hord_tr, no damping; fv_dynamics.py
+ * 301-309): area fluxes from the accumulated Courant numbers cxd, cyd; the
+ * fixed three sub-steps (cmax = 2), cxd, cyd, mfxd, mfyd scaled by 1/3 in
+ * place; each sub-step adjusts the pressure thickness by the mass-flux
+ * divergence and transports and re-weights every tracer, with tracer halo
+ * updates in between.  tracers: HOST array of ntracers device pointers
+ * (3-D fields), updated in place.  dp1 serves as one of the two pressure
+ * thickness buffers and holds the second sub-step's value afterwards, as
+ * the reference's does.  mdt is unused, as in the reference.
+ */
+int fv3b_tracer_advection(const fv3b_transport* transport, int ntracers, fv3b_real* const* tracers,
+                          fv3b_real* dp1, fv3b_real* mfxd, fv3b_real* mfyd, fv3b_real* cxd, fv3b_real* cyd,
+                          double mdt, void* stream);
+
 /* Device pointer of one of the substep temporaries by its reference name
  * ("gz", "zh", "pkc", "pk3", "ut", "vt", "divgd", "heat_source", "crx",
  * "cry", "xfx", "yfx", "delpc", "ptc", "ws3", "zs", "dp_ref"), or NULL. */

@@ -208,3 +208,40 @@ def resting_case(n=12, nz=8, n_split=2):
         mdt=37.5 * n_split, n_map=1, akap=C.KAPPA, n_split=n_split,
     )
     return case
+
+
+def tracer_case(n=12, nz=8, seed=61, ntracers=4, courant=0.6):
+    """Inputs of TracerAdvection after an acoustic loop: four tracers uniform
+    in [0, 1e-2), the pressure thickness dp1 of the baroclinic-wave state,
+    and accumulated Courant numbers and mass fluxes of a smooth flow (the
+    state's D-grid winds averaged to the C-grid interfaces, scaled to peak
+    Courant number ``courant``) with seeded 1e-3 relative noise."""
+    st = base_state(n, nz, seed)
+    g = grid_for(n)
+    rng = np.random.default_rng(seed + 1000)
+    shp = st["delp"].shape
+    u, v, dp = st["u"], st["v"], st["delp"]
+
+    def sh(a, di, dj):
+        out = np.zeros_like(a)
+        m = a.shape[1]
+        out[:, max(0, -di):m - max(0, di), max(0, -dj):m - max(0, dj)] = \
+            a[:, max(0, di):m - max(0, -di), max(0, dj):m - max(0, -dj)]
+        return out
+
+    # x-interface (i - 1/2, j) and y-interface (i, j - 1/2) winds
+    ux = 0.25 * (sh(u, -1, 0) + u + sh(u, -1, 1) + sh(u, 0, 1))
+    vy = 0.25 * (sh(v, 0, -1) + v + sh(v, 1, -1) + sh(v, 1, 0))
+    scale = courant / max(np.abs(ux).max(), np.abs(vy).max())
+    cx = scale * ux * (1.0 + 1e-3 * rng.standard_normal(shp))
+    cy = scale * vy * (1.0 + 1e-3 * rng.standard_normal(shp))
+    dxa, dya, dx, dy = (getattr(g, k)[:, :, :, None] for k in ("dxa", "dya", "dx", "dy"))
+    mfx = cx * 0.5 * (sh(dxa, -1, 0) + dxa) * dy * 0.5 * (sh(dp, -1, 0) + dp)
+    mfy = cy * 0.5 * (sh(dya, 0, -1) + dya) * dx * 0.5 * (sh(dp, 0, -1) + dp)
+    tracers = rng.uniform(0.0, 1.0e-2, size=(ntracers,) + shp)
+    tracers[..., nz] = 0.0
+    return {"tracers": tracers, "dp1": dp.copy(), "mfxd": mfx, "mfyd": mfy, "cxd": cx, "cyd": cy,
+            "mdt": 225.0}
+
+
+CASES["tracer_advection"] = tracer_case

@@ -180,12 +180,67 @@ def run_acoustics_compute(case, n, nz):
     return res, {"region": "compute domain (+1 on staggered axes)"}
 
 
+TRACER_NAMES = ("qvapor", "qliquid", "qrain", "qsnow")
+
+
+def run_tracer_advection(case, n, nz):
+    """Six TracerAdvection instances (one per tile, hord_tr = 8 transport)
+    stepping in lock step on threads, their tracer halo updates going
+    through ``ThreadComm``, as DynamicalCore._dyn calls them after the
+    acoustic loop (fv_dynamics.py:301-309, 544-557)."""
+    import threading
+
+    from fv3core.stencils.fvtp2d import FiniteVolumeTransport
+    from fv3core.stencils.tracer_2d_1l import TracerAdvection
+    from fv3core.utils.grid import quantity_wrap
+
+    grid = cases.grid_for(n)
+    exchange = rr._Exchange()
+    S = rr.storage
+    ntr = case["tracers"].shape[0]
+    dims = ("x", "y", "z")
+    runs = []
+    for t in range(6):
+        tr = rr.TileReference(grid, t, nz)
+        tr.activate()
+        tr.add_tracer_grid()
+        comm = rr.ThreadComm(t, n, 3, exchange)
+        transport = FiniteVolumeTransport(tr.stencil_factory, tr.grid_data, tr.damping_coefficients, 0, hord=8)
+        adv = TracerAdvection(tr.stencil_factory, transport, comm, ntr)
+        tracers = {TRACER_NAMES[q]: quantity_wrap(S(case["tracers"][q, t]), dims, tr.grid_indexing)
+                   for q in range(ntr)}
+        args = {k: S(case[k][t]) for k in ("dp1", "mfxd", "mfyd", "cxd", "cyd")}
+        runs.append((adv, tracers, args))
+    errors = []
+
+    def work(adv, tracers, args):
+        try:
+            adv(tracers, args["dp1"], args["mfxd"], args["mfyd"], args["cxd"], args["cyd"], case["mdt"])
+        except BaseException as exc:  # surfaced after join
+            errors.append(exc)
+            raise
+
+    threads = [threading.Thread(target=work, args=r) for r in runs]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    if errors:
+        raise errors[0]
+    out = {"tracers": np.stack([np.stack([np.asarray(r[1][TRACER_NAMES[q]].storage) for r in runs])
+                                for q in range(ntr)])}
+    for k in ("dp1", "mfxd", "mfyd", "cxd", "cyd"):
+        out[k] = np.stack([np.asarray(r[2][k]) for r in runs])
+    return out, {"region": "full storage"}
+
+
 RUNNERS = {
     "acoustics": (run_acoustics, dict(n=12, nz=8, seed=41)),
     "d_sw": (run_d_sw, dict(n=12, nz=8, seed=31)),
     "c_sw": (run_c_sw, dict(n=12, nz=6, seed=21)),
     "riem_solver_c": (run_riem_solver_c, dict(n=12, nz=16, seed=11)),
     "acoustics_c12_l79": (run_acoustics_compute, dict(n=12, nz=79, seed=7, n_split=1)),
+    "tracer_advection": (run_tracer_advection, dict(n=12, nz=8, seed=61)),
 }
 
 

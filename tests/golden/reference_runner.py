@@ -170,6 +170,29 @@ class TileReference:
         """Make this tile's legacy grid the global one (constructors read it)."""
         self.spec.grid = self.legacy
 
+    def add_tracer_grid(self):
+        """The legacy-grid members TracerAdvection reads
+        (tracer_2d_1l.py:143-200): metric terms, quantity_wrap and
+        get_halo_update_spec."""
+        import fv3gfs.util as fu
+
+        g, t, h, nz = self.grid, self.tile, self.grid.halo, self.nz
+        legacy = self.legacy
+        for name in ("dxa", "dya", "dx", "dy", "sin_sg1", "sin_sg2", "sin_sg3", "sin_sg4", "rarea"):
+            setattr(legacy, name, storage(getattr(g, name)[t], origin=(h, h)))
+        sizer = fu.SubtileGridSizer(g.n, g.n, nz, h)
+        gi = self.grid_indexing
+
+        def quantity_wrap(data, dims=(fu.X_DIM, fu.Y_DIM, fu.Z_DIM), units="Unknown"):
+            return fu.Quantity(data, dims=dims, units=units, origin=sizer.get_origin(dims),
+                               extent=sizer.get_extent(dims))
+
+        def get_halo_update_spec(shape, origin, halo_points, dims=(fu.X_DIM, fu.Y_DIM, fu.Z_DIM)):
+            return gi.get_quantity_halo_spec(shape, origin, dims=list(dims), n_halo=halo_points)
+
+        legacy.quantity_wrap = quantity_wrap
+        legacy.get_halo_update_spec = get_halo_update_spec
+
 
 # ---------------------------------------------------------------------------
 # Six tiles in lock step: a fake communicator whose halo updaters exchange

@@ -100,3 +100,34 @@ def run_acoustics(case, n, nz, precision="f64"):
     gd.close()
     return out
 
+
+
+def run_tracer_advection(case, n, nz, precision="f64"):
+    """The package's TracerAdvection (hord_tr = 8 transport) on a case of
+    ``cases.tracer_case``; returns the tracers and the in-place updated
+    dp1, mfxd, mfyd, cxd, cyd."""
+    import torch
+
+    from fv3core_b200.grid_data import GridData
+    from fv3core_b200.stencil import StencilConfig, StencilFactory
+    from fv3core_b200.stencils.fvtp2d import FiniteVolumeTransport
+    from fv3core_b200.stencils.tracer_2d_1l import TracerAdvection
+    from fv3core_b200.storage import to_device, to_host
+
+    gd = GridData(cases.grid_for(n), nz, precision=precision)
+    dtype = gd.grid_indexing.dtype
+    sf = StencilFactory(StencilConfig(), gd.grid_indexing)
+    try:
+        transport = FiniteVolumeTransport(sf, gd, gd, 0, hord=8)
+        ntr = case["tracers"].shape[0]
+        adv = TracerAdvection(sf, transport, None, ntr)
+        tracers = {f"q{q}": to_device(case["tracers"][q], dtype=dtype) for q in range(ntr)}
+        dev = {k: to_device(case[k], dtype=dtype) for k in ("dp1", "mfxd", "mfyd", "cxd", "cyd")}
+        adv(tracers, dev["dp1"], dev["mfxd"], dev["mfyd"], dev["cxd"], dev["cyd"], case["mdt"])
+        torch.cuda.synchronize()
+        out = {k: to_host(v) for k, v in dev.items()}
+        out["tracers"] = np.stack([to_host(tracers[f"q{q}"]) for q in range(ntr)])
+        transport.close()
+        return out
+    finally:
+        gd.close()

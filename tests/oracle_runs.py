@@ -71,3 +71,19 @@ def run_acoustics(case, n, nz):
     for name, arr in ad.tmp.items():
         out["tmp_" + name] = arr
     return out
+
+
+def run_tracer_advection(case, n, nz):
+    """The oracle's TracerAdvection (hord_tr = 8) over all six tiles; returns
+    the tracers and the in-place updated dp1, mfxd, mfyd, cxd, cyd."""
+    from oracle.tracer import TracerAdvection
+
+    g = cases.grid_for(n)
+    metrics = [cases.metric_namespace(n, t) for t in range(6)]
+    ntr = case["tracers"].shape[0]
+    adv = TracerAdvection(g, metrics, nz, ntr, hord=8)
+    out = {k: np.array(case[k], copy=True) for k in ("tracers", "dp1", "mfxd", "mfyd", "cxd", "cyd")}
+    with np.errstate(all="ignore"):
+        adv([out["tracers"][q] for q in range(ntr)], out["dp1"], out["mfxd"], out["mfyd"], out["cxd"],
+            out["cyd"], case["mdt"])
+    return out
