@@ -72,6 +72,10 @@ CTX_SIGNATURES = {
     "fv3b_acoustics_setup": [P] * 6,
     "fv3b_acoustics": [P, P],
     "fv3b_ppm_flux": [ctypes.c_int, ctypes.c_int, P, P, P] + [ctypes.c_int] * 6 + [P],
+    "fv3b_compute_preamble": [P] * 14 + [P],
+    "fv3b_post_remap": [P] * 4 + [ctypes.c_int, P],
+    "fv3b_adjust_negative_tracers": [P] * 11 + [ctypes.c_int, P],
+    "fv3b_cubed_to_latlon": [P] * 8 + [ctypes.c_int, P],
     "fv3b_transport_create": [ctypes.c_int, P, P, ctypes.c_int, P],
 }
 

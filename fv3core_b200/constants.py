@@ -19,3 +19,14 @@ CNST_0P20 = 0.2
 ZVIR = RVGAS / RDGAS - 1
 RGRAV = 1.0 / GRAV
 SDAY = 86400.0
+
+# moist thermodynamics of the step preamble and epilogue (the same file, 7-8, 21-37)
+HLV = 2.5e6  # latent heat of evaporation [J/kg]
+HLF = 3.3358e5  # latent heat of fusion [J/kg]
+CV_VAP = 3.0 * RVGAS
+C_ICE = 1972.0
+C_LIQ = 4.1855e3
+CP_VAP = 4.0 * RVGAS
+TICE = 273.16
+DC_ICE = C_LIQ - C_ICE
+LI0 = HLF - DC_ICE * TICE

@@ -270,6 +270,7 @@ class CubedSphereGrid:
         # A->B edge interpolation factors (fv3core/grid/geometry.py:604-714)
         self.edge_w, self.edge_e, self.edge_s, self.edge_n = self._edge_factors(C)
         self.a2b_extrap = self._a2b_extrap_ratios()
+        self._cubed_to_latlon(C, me, mn)
         # minimum areas over the six compute domains
         self.da_min = float(area[:, hs:he, hs:he].min())
         self.da_max = float(area[:, hs:he, hs:he].max())
@@ -367,6 +368,26 @@ class CubedSphereGrid:
                 e[:, j] = d2 / (d1 + d2)
             out.append(e)
         return out
+
+    def _cubed_to_latlon(self, C, me, mn):
+        """a11, a12, a21, a22 of the cell-centre winds' transformation to
+        longitude and latitude components (fv3core/grid/geometry.py:588-601):
+        z = projections of the local grid directions ec1 (x, towards the east
+        edge midpoint) and ec2 (y, towards the north edge midpoint) on the
+        local east and north unit vectors, divided by sin_sg5."""
+        _, _, east, north = lonlat_basis(C)
+        ec1 = _tangent(C, me)
+        ec2 = _tangent(C, mn)
+        z11 = np.sum(ec1 * east, axis=-1)
+        z12 = np.sum(ec1 * north, axis=-1)
+        z21 = np.sum(ec2 * east, axis=-1)
+        z22 = np.sum(ec2 * north, axis=-1)
+        s5 = self.sin_sg5[:, : C.shape[1], : C.shape[2]]
+        for name, val in (("a11", 0.5 * z22 / s5), ("a12", -0.5 * z12 / s5), ("a21", -0.5 * z21 / s5),
+                          ("a22", 0.5 * z11 / s5)):
+            out = np.zeros(self.shape2d)
+            out[:, : C.shape[1], : C.shape[2]] = val
+            setattr(self, name, out)
 
     # ------------------------------------------------------------------ helpers
     def wind_vectors(self):

@@ -28,6 +28,10 @@ METRIC_FIELDS = [
     "edge_w", "edge_e", "edge_s", "edge_n",
     "a2b_extrap",
 ]
+# 2-D fields on the device that are not part of the C ABI's metric struct:
+# the cubed-to-latlon coefficients (the reference keeps them on its legacy
+# grid, not in GridData), passed to fv3b_cubed_to_latlon directly
+EXTRA_FIELDS = ["a11", "a12", "a21", "a22"]
 
 
 class Metrics(ctypes.Structure):
@@ -48,7 +52,7 @@ class GridData:
         tdtype = self.grid_indexing.dtype
         self.device = device
         self.tensors = {}
-        for name in METRIC_FIELDS:
+        for name in METRIC_FIELDS + EXTRA_FIELDS:
             a = np.asarray(getattr(grid, name), dtype=np.float64)
             if a.ndim == 3 and name != "a2b_extrap":  # [6, i, j] -> [6, j, i]
                 t = torch.from_numpy(np.ascontiguousarray(a.transpose(0, 2, 1))).to(device=device, dtype=tdtype)

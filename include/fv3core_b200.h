@@ -473,6 +473,54 @@ int fv3b_tracer_advection(const fv3b_transport* transport, int ntracers, fv3b_re
                           fv3b_real* dp1, fv3b_real* mfxd, fv3b_real* mfyd, fv3b_real* cxd, fv3b_real* cyd,
                           double mdt, void* stream);
 
+/*
+ * compute_preamble of DynamicalCore.step_dynamics (fv3core/stencils/
+ * fv_dynamics.py:54-106): fv_setup with moist_phys and nwat = 6
+ * (moist_cv.py:197-228: cvm, q_con, dp1 = zvir * qvapor, cappa, pkz) followed
+ * by pt_adjust (fv_dynamics.py:32-34), in one pass over the compute domain
+ * and the npz layers.  Water species, delp, delz in; q_con, cvm, pkz,
+ * cappa, dp1 out; pt in and out.
+ */
+int fv3b_compute_preamble(fv3b_ctx* ctx, const fv3b_real* qvapor, const fv3b_real* qliquid, const fv3b_real* qrain,
+                          const fv3b_real* qsnow, const fv3b_real* qice, const fv3b_real* qgraupel,
+                          fv3b_real* q_con, fv3b_real* cvm, fv3b_real* pkz, fv3b_real* pt, fv3b_real* cappa,
+                          const fv3b_real* delp, const fv3b_real* delz, fv3b_real* dp1, void* stream);
+
+/*
+ * post_remap of DynamicalCore.step_dynamics (fv_dynamics.py:109-133) for the
+ * nonhydrostatic dynamics: set_omega (omga = delp / delz * w, fv_dynamics.py
+ * 37-39) and, when nf_omega > 0, the halo update of omga and nf_omega del-2
+ * passes (HyperdiffusionDamping) with coefficient 0.18 da_min.
+ */
+int fv3b_post_remap(fv3b_ctx* ctx, const fv3b_real* delp, const fv3b_real* delz, const fv3b_real* w,
+                    fv3b_real* omga, int nf_omega, void* stream);
+
+/*
+ * AdjustNegativeTracerMixingRatio.__call__ (fv3core/stencils/neg_adj3.py
+ * 293-372), the first half of wrapup (fv_dynamics.py:136-169): fix_neg_water,
+ * fillq on graupel and rain, fix_water_vapor_down and fix_neg_cloud on the
+ * compute-domain columns.  hydrostatic != 0 is rejected
+ * (FV3B_ERR_UNSUPPORTED), as the reference does.  peln is not read (the
+ * reference passes it and does not read it either).
+ */
+int fv3b_adjust_negative_tracers(fv3b_ctx* ctx, fv3b_real* qvapor, fv3b_real* qliquid, fv3b_real* qrain,
+                                 fv3b_real* qsnow, fv3b_real* qice, fv3b_real* qgraupel, fv3b_real* qcld,
+                                 fv3b_real* pt, const fv3b_real* delp, const fv3b_real* delz,
+                                 const fv3b_real* peln, int hydrostatic, void* stream);
+
+/*
+ * CubedToLatLon.__call__ (fv3core/stencils/c2l_ord.py:75-141), the second
+ * half of wrapup: D-grid winds u, v to A-grid winds ua, va in longitude /
+ * latitude components.  order 4: vector halo update of u, v, then
+ * ord4_transform on the compute domain; order 2: c2l_ord2 on the compute
+ * domain plus one halo row.  a11 .. a22: 2-D device fields of the
+ * transformation (the legacy grid's a11 .. a22, fv3core/grid/geometry.py
+ * 596-601).
+ */
+int fv3b_cubed_to_latlon(fv3b_ctx* ctx, fv3b_real* u, fv3b_real* v, const fv3b_real* a11, const fv3b_real* a12,
+                         const fv3b_real* a21, const fv3b_real* a22, fv3b_real* ua, fv3b_real* va, int order,
+                         void* stream);
+
 /* Device pointer of one of the substep temporaries by its reference name
  * ("gz", "zh", "pkc", "pk3", "ut", "vt", "divgd", "heat_source", "crx",
  * "cry", "xfx", "yfx", "delpc", "ptc", "ws3", "zs", "dp_ref"), or NULL. */

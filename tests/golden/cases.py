@@ -245,3 +245,34 @@ def tracer_case(n=12, nz=8, seed=61, ntracers=4, courant=0.6):
 
 
 CASES["tracer_advection"] = tracer_case
+
+
+WATER_NAMES = ("qvapor", "qliquid", "qrain", "qsnow", "qice", "qgraupel", "qcld")
+
+
+def fv_step_case(n=12, nz=8, seed=71):
+    """Inputs of the step preamble and epilogue: the baroclinic-wave state
+    with seven water species, uniform in [0, 1e-3), of which a seeded 20 %
+    of the points are made negative (down to -2e-4) so that the negative
+    tracer fixes act; the bottom level of qvapor stays non-negative (the
+    reference's borrowing from below reads a temporary it only writes on the
+    bottom level)."""
+    st = base_state(n, nz, seed)
+    rng = np.random.default_rng(seed + 1000)
+    shp = st["delp"].shape
+    case = {k: np.array(st[k], copy=True) for k in ("delp", "delz", "pt", "u", "v", "peln")}
+    for name in WATER_NAMES:
+        q = rng.uniform(0.0, 1.0e-3, shp)
+        neg = rng.random(shp) < 0.2
+        q = np.where(neg, -rng.uniform(0.0, 2.0e-4, shp), q)
+        if name == "qvapor":
+            q[..., nz - 1] = np.abs(q[..., nz - 1])
+        q[..., nz] = 0.0
+        case[name] = q
+    case["w"] = 0.1 * rng.standard_normal(shp)
+    for name in ("q_con", "cvm", "pkz", "cappa", "dp1", "omga", "ua", "va"):
+        case[name] = np.zeros(shp)
+    return case
+
+
+CASES["fv_step"] = fv_step_case

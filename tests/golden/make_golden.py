@@ -234,6 +234,87 @@ def run_tracer_advection(case, n, nz):
     return out, {"region": "full storage"}
 
 
+FV_STEP_FIELDS = cases.WATER_NAMES + ("q_con", "cvm", "pkz", "pt", "cappa", "delp", "delz", "dp1", "w", "omga",
+                                      "u", "v", "ua", "va", "peln")
+
+
+def run_fv_step(case, n, nz):
+    """The step preamble, post_remap and wrapup of DynamicalCore
+    (fv_dynamics.py:54-169) on six tiles in lock step on threads, with the
+    stencils built as DynamicalCore.__init__ builds them (fv_dynamics.py
+    320-392); the state after each phase is stored (prefixes pre_, post_,
+    wrap_)."""
+    import threading
+    import types
+
+    from fv3core.stencils import fv_dynamics as fvd
+    from fv3core.stencils import moist_cv
+    from fv3core.stencils.c2l_ord import CubedToLatLon
+    from fv3core.stencils.del2cubed import HyperdiffusionDamping
+    from fv3core.stencils.neg_adj3 import AdjustNegativeTracerMixingRatio
+    from fv3core.utils.grid import quantity_wrap
+
+    grid = cases.grid_for(n)
+    exchange = rr._Exchange()
+    S = rr.storage
+    config = types.SimpleNamespace(hydrostatic=False, rf_fast=True, tau=10.0, adiabatic=False, kord_tm=-9,
+                                   nf_omega=1, nwat=6, moist_phys=True)
+    runs = []
+    for t in range(6):
+        tr = rr.TileReference(grid, t, nz)
+        tr.activate()
+        tr.add_tracer_grid()
+        comm = rr.ThreadComm(t, n, 3, exchange)
+        sf, gi = tr.stencil_factory, tr.grid_indexing
+        fv_setup = sf.from_origin_domain(moist_cv.fv_setup, externals={"nwat": 6, "moist_phys": True},
+                                         origin=gi.origin_compute(), domain=gi.domain_compute())
+        pt_adjust = sf.from_origin_domain(fvd.pt_adjust, origin=gi.origin_compute(), domain=gi.domain_compute())
+        set_omega = sf.from_origin_domain(fvd.set_omega, origin=gi.origin_compute(), domain=gi.domain_compute())
+        hyper = HyperdiffusionDamping(sf, tr.damping_coefficients, tr.grid_data.rarea, config.nf_omega)
+        c2l = CubedToLatLon(sf, tr.grid_data, order=4)
+        adjust = AdjustNegativeTracerMixingRatio(sf, False, False)
+        spec = gi.get_quantity_halo_spec(gi.domain_full(add=(1, 1, 1)), gi.origin_compute(),
+                                         dims=["x", "y", "z"], n_halo=3)
+        omega_updater = comm.get_scalar_halo_updater([spec])
+        st = types.SimpleNamespace(**{k: S(case[k][t]) for k in FV_STEP_FIELDS})
+        st.consv_te = 0.0
+        st.do_adiabatic_init = False
+        st.omga_quantity = quantity_wrap(st.omga, ("x", "y", "z"), gi)
+        st.u_quantity = quantity_wrap(st.u, ("x", "y_interface", "z"), gi)
+        st.v_quantity = quantity_wrap(st.v, ("x_interface", "y", "z"), gi)
+        runs.append((st, comm, fv_setup, pt_adjust, set_omega, hyper, c2l, adjust, omega_updater, tr))
+    snaps = [dict() for _ in range(6)]
+    errors = []
+
+    def work(t, st, comm, fv_setup, pt_adjust, set_omega, hyper, c2l, adjust, omega_updater, tr):
+        try:
+            fvd.compute_preamble(st, False, config, fv_setup, pt_adjust)
+            snaps[t]["pre"] = {k: np.array(getattr(st, k)) for k in FV_STEP_FIELDS}
+            fvd.post_remap(st, False, config, hyper, set_omega, omega_updater, tr.damping_coefficients.da_min)
+            snaps[t]["post"] = {k: np.array(getattr(st, k)) for k in FV_STEP_FIELDS}
+            fvd.wrapup(st, comm, adjust, c2l, False)
+            snaps[t]["wrap"] = {k: np.array(getattr(st, k)) for k in FV_STEP_FIELDS}
+        except BaseException as exc:  # surfaced after join
+            errors.append(exc)
+            raise
+
+    threads = [threading.Thread(target=work, args=(t,) + r[:9] + (r[9],)) for t, r in enumerate(runs)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    if errors:
+        raise errors[0]
+    # the fields each phase writes
+    written = {"pre": ("q_con", "cvm", "pkz", "pt", "cappa", "dp1"), "post": ("omga",),
+               "wrap": cases.WATER_NAMES + ("pt", "u", "v", "ua", "va")}
+    out = {}
+    for phase, names in written.items():
+        for k in names:
+            out[f"{phase}_{k}"] = np.stack([snaps[t][phase][k] for t in range(6)])
+    return out, {"region": "full storage"}
+
+
 RUNNERS = {
     "acoustics": (run_acoustics, dict(n=12, nz=8, seed=41)),
     "d_sw": (run_d_sw, dict(n=12, nz=8, seed=31)),
@@ -241,6 +322,7 @@ RUNNERS = {
     "riem_solver_c": (run_riem_solver_c, dict(n=12, nz=16, seed=11)),
     "acoustics_c12_l79": (run_acoustics_compute, dict(n=12, nz=79, seed=7, n_split=1)),
     "tracer_advection": (run_tracer_advection, dict(n=12, nz=8, seed=61)),
+    "fv_step": (run_fv_step, dict(n=12, nz=8, seed=71)),
 }
 
 

@@ -192,6 +192,8 @@ class TileReference:
 
         legacy.quantity_wrap = quantity_wrap
         legacy.get_halo_update_spec = get_halo_update_spec
+        for name in ("a11", "a12", "a21", "a22"):
+            setattr(legacy, name, storage(getattr(g, name)[t], origin=(h, h)))
 
 
 # ---------------------------------------------------------------------------
@@ -251,6 +253,7 @@ class ThreadComm:
         self.n, self.h = n, h
         self.exchange = exchange
         self._uids = {}
+        self._vector_updaters = {}
         self.sync_gen = 0
 
     def uid_of(self, updater):
@@ -294,6 +297,18 @@ class ThreadComm:
                     for r in rows:
                         src = posts[r[3]][r[6]][qi]
                         dst.data[r[1], r[2], :nk] = r[7] * src[r[4], r[5], :nk]
+
+    def vector_halo_update(self, u_q, v_q, n_points):
+        """CubedSphereCommunicator.vector_halo_update: one blocking vector
+        exchange (as CubedToLatLon calls it)."""
+        from types import SimpleNamespace
+
+        nk = u_q.extent[-1]
+        key = ("vector_halo_update", n_points, nk)
+        if key not in self._vector_updaters:  # one updater per shape: keys stay unique
+            spec = SimpleNamespace(n_points=n_points, extent=(0, 0, nk))
+            self._vector_updaters[key] = _HaloUpdater(self, "vector", ([spec], [spec]))
+        self._vector_updaters[key].update([u_q], [v_q])
 
     def synchronize_vector_interfaces(self, u_q, v_q):
         from fv3core_b200 import halo_map as hm

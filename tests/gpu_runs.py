@@ -131,3 +131,47 @@ def run_tracer_advection(case, n, nz, precision="f64"):
         return out
     finally:
         gd.close()
+
+
+def run_fv_step(case, n, nz, precision="f64"):
+    """The package's compute_preamble, post_remap and wrapup on a case of
+    ``cases.fv_step_case``; returns the state after each phase (prefixes
+    pre_, post_, wrap_), as the oracle run does."""
+    import types
+
+    import torch
+
+    from fv3core_b200.grid_data import GridData
+    from fv3core_b200.halo import DeviceCubedSphereCommunicator, spec_for
+    from fv3core_b200.stencil import StencilConfig, StencilFactory
+    from fv3core_b200.stencils import fv_dynamics as fvd
+    from fv3core_b200.stencils.del2cubed import HyperdiffusionDamping
+    from fv3core_b200.storage import to_device, to_host
+
+    gd = GridData(cases.grid_for(n), nz, precision=precision)
+    dtype = gd.grid_indexing.dtype
+    sf = StencilFactory(StencilConfig(), gd.grid_indexing)
+    try:
+        config = types.SimpleNamespace(hydrostatic=False, rf_fast=True, tau=10.0, adiabatic=False, kord_tm=-9,
+                                       nf_omega=1)
+        comm = DeviceCubedSphereCommunicator(gd.grid_indexing)
+        st = types.SimpleNamespace(**{k: to_device(v, dtype=dtype) for k, v in case.items()})
+        st.consv_te, st.do_adiabatic_init = 0.0, False
+        out = {}
+
+        def snap(prefix, names):
+            torch.cuda.synchronize()
+            out.update({f"{prefix}_{k}": to_host(getattr(st, k)) for k in names})
+
+        fvd.compute_preamble(st, False, config, fvd.FvSetup(sf), fvd.PtAdjust(sf))
+        snap("pre", ("q_con", "cvm", "pkz", "pt", "cappa", "dp1"))
+        omega_updater = comm.get_scalar_halo_updater([spec_for(gd.grid_indexing, ("x", "y", "z"))])
+        fvd.post_remap(st, False, config, HyperdiffusionDamping(sf, gd, gd.rarea, config.nf_omega),
+                       fvd.SetOmega(sf), omega_updater, gd.da_min)
+        snap("post", ("omga",))
+        fvd.wrapup(st, comm, fvd.AdjustNegativeTracerMixingRatio(sf, False, False), fvd.CubedToLatLon(sf, gd, 4),
+                   False)
+        snap("wrap", cases.WATER_NAMES + ("pt", "u", "v", "ua", "va"))
+        return out
+    finally:
+        gd.close()

@@ -87,3 +87,42 @@ def run_tracer_advection(case, n, nz):
         adv([out["tracers"][q] for q in range(ntr)], out["dp1"], out["mfxd"], out["mfyd"], out["cxd"],
             out["cyd"], case["mdt"])
     return out
+
+
+def run_fv_step(case, n, nz):
+    """The oracle's step preamble, post_remap and wrapup (fv_dynamics.py
+    54-169) over all six tiles; returns the state after each phase
+    (prefixes pre_, post_, wrap_)."""
+    from oracle import fv_step as F
+    from oracle.dyn_core import del2cubed
+    from oracle.halo import HaloExchange
+
+    g = cases.grid_for(n)
+    t = Tile(n, nz)
+    st = {k: np.array(v, copy=True) for k, v in case.items()}
+    halo = HaloExchange(n, 3)
+    out = {}
+    with np.errstate(all="ignore"):
+        for tt in range(6):
+            F.fv_setup(t, *[st[k][tt] for k in ("qvapor", "qliquid", "qrain", "qsnow", "qice", "qgraupel", "q_con",
+                                                "cvm", "pkz", "pt", "cappa", "delp", "delz", "dp1")])
+            F.pt_adjust(t, st["pkz"][tt], st["dp1"][tt], st["q_con"][tt], st["pt"][tt])
+        out.update({f"pre_{k}": st[k].copy() for k in ("q_con", "cvm", "pkz", "pt", "cappa", "dp1")})
+        for tt in range(6):
+            F.set_omega(t, st["delp"][tt], st["delz"][tt], st["w"][tt], st["omga"][tt])
+        # nf_omega = 1: omega halo update, then one del-2 pass with 0.18 da_min
+        halo.scalar(st["omga"], nk=nz)
+        for tt in range(6):
+            ns = cases.metric_namespace(n, tt)
+            scr = {name: np.full((t.m, t.m, t.nk), np.nan) for name in ("q", "fx", "fy")}
+            del2cubed(t, ns, st["omga"][tt], 0.18 * g.da_min, 1, scr)
+        out["post_omga"] = st["omga"].copy()
+        for tt in range(6):
+            F.adjust_negative_tracers(t, *[st[k][tt] for k in cases.WATER_NAMES], st["pt"][tt], st["delp"][tt],
+                                      st["delz"][tt], st["peln"][tt])
+        halo.vector_d(st["u"], st["v"], nk=nz)
+        for tt in range(6):
+            F.cubed_to_latlon_ord4(t, st["u"][tt], st["v"][tt], g.dx[tt], g.dy[tt], g.a11[tt], g.a12[tt],
+                                   g.a21[tt], g.a22[tt], st["ua"][tt], st["va"][tt])
+        out.update({f"wrap_{k}": st[k].copy() for k in cases.WATER_NAMES + ("pt", "u", "v", "ua", "va")})
+    return out
