@@ -43,12 +43,24 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "C384 L79 acoustic-substep cell-levels/s"
-# DRAM bytes (read + write) per cell-level per substep that the kernels of
-# one AcousticDynamics call move, summed by ncu over every launch of one call
-# at C384 L79 (dram__bytes_read.sum + dram__bytes_write.sum); the compulsory
-# state traffic is 272 B (FP64) and 136 B (mixed).
-DRAM_BYTES_PER_CELL_LEVEL = {"f64": 4554.0, "f32": 2381.0}
 UNIT = "cell-levels/s"
+# The committed ncu summary of one call's DRAM traffic (every launch, one-pass
+# metrics dram__bytes_read.sum + dram__bytes_write.sum) of the current code.
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "acoustics_c128_l79_dram_traffic.md")
+
+
+def dram_bytes_per_cell_level():
+    """{"f32": B, "f64": B}: DRAM bytes per cell-level per substep, read from
+    the profile's line ``bytes per cell-level per substep: f32 X, f64 Y``
+    (None when the file or the line is missing)."""
+    import re
+
+    try:
+        text = open(TRAFFIC_PROFILE).read()
+    except OSError:
+        return None
+    m = re.search(r"bytes per cell-level per substep: f32 (\d+), f64 (\d+)", text)
+    return {"f32": float(m.group(1)), "f64": float(m.group(2))} if m else None
 
 
 def _env_rank():
@@ -205,6 +217,17 @@ def _max_rel(a, b, n, npz):
     return float((torch.abs(a - b) / torch.clamp(torch.abs(b), min=1e-30)).max())
 
 
+def _rel_stats(a, b, n, npz):
+    """(max, 99.9th percentile, count above 1e-4) of the relative difference
+    over the compute domain."""
+    import torch
+
+    a, b = _compute(a, n, npz).double(), _compute(b, n, npz).double()
+    r = (torch.abs(a - b) / torch.clamp(torch.abs(b), min=1e-30)).flatten()
+    q = torch.kthvalue(r.cpu(), max(1, int(0.999 * r.numel()))).values.item()
+    return {"max": float(r.max()), "p999": q, "above_1e-4": int((r > 1e-4).sum())}
+
+
 def _rms_rel(a, b, n, npz):
     """RMS of the difference over RMS of the reference, compute domain."""
     a, b = _compute(a, n, npz).double(), _compute(b, n, npz).double()
@@ -235,7 +258,6 @@ def run_cuda(args):
     precisions = {"both": ["f32", "f64"], "mixed": ["f32"], "f64": ["f64"]}[args.precision]
     problems = {p: build_problem(n, npz, n_split, 1234 + rank, precision=p, grid=grid, state0=state0)
                 for p in precisions}
-    del state0
 
     def barrier():
         if dist is not None:
@@ -255,11 +277,16 @@ def run_cuda(args):
         for k, t in initial[prec].items():
             getattr(state, k).copy_(t)
 
-    # error of the mixed build against FP64 after one call (one dynamics
-    # step's acoustic part) from the same initial state
-    # from the same state; and, to separate the build's own arithmetic
-    # error from the state's sensitivity to its inputs, FP64 started from
-    # the initial state rounded to FP32 (the mixed build's input)
+    # Error of the mixed build against FP64 after one call (one dynamics
+    # step's acoustic part) from the same state.  The driver's temporaries
+    # carry over between calls, as the reference's instance storages do
+    # (heat_source, which d_sw accumulates into, among them), so every
+    # compared run is the first call of its own AcousticDynamics.  Beside
+    # it: FP64 started from the state rounded to FP32 (the mixed build's
+    # input), the mixed build against that run (both start from identical
+    # numbers, only the arithmetic differs), FP64's response to input
+    # perturbations of relative size eps, and what the carry-over alone does
+    # (a second FP64 call from the same state).
     mixed_error = None
     if len(precisions) == 2:
         fields = ("delp", "pt", "delz", "q_con")
@@ -270,19 +297,51 @@ def run_cuda(args):
         ref = {k: getattr(s64, k).clone() for k in fields + ("u", "v", "w")}
         mixed = {k: _max_rel(getattr(s32, k), ref[k], n, npz) for k in fields}
         mixed_rms = {k: _rms_rel(getattr(s32, k), ref[k], n, npz) for k in fields + ("u", "v", "w")}
-        for k, t in initial["f64"].items():
-            getattr(s64, k).copy_(t.float())
+        reset("f64")
         problems["f64"][1](s64)
         barrier()
-        floor = {k: _max_rel(getattr(s64, k), ref[k], n, npz) for k in fields}
-        arith = {k: _max_rel(getattr(s32, k), getattr(s64, k), n, npz) for k in fields}
+        carry = {k: _max_rel(getattr(s64, k), ref[k], n, npz) for k in fields}
+
+        def first_call_f64(make_input):
+            """One FP64 call on a fresh AcousticDynamics from make_input(k, t)
+            applied to every initial field; returns the fresh state."""
+            gd2, ad2, st2 = build_problem(n, npz, n_split, 1234 + rank, precision="f64", grid=grid, state0=state0)
+            for k, t in initial["f64"].items():
+                getattr(st2, k).copy_(make_input(k, t))
+            ad2(st2)
+            barrier()
+            return gd2, st2
+
+        gd2, st2 = first_call_f64(lambda k, t: t.float().double())
+        floor = {k: _max_rel(getattr(st2, k), ref[k], n, npz) for k in fields}
+        arith = {k: _max_rel(getattr(s32, k), getattr(st2, k), n, npz) for k in fields}
+        gd2.close()
+        del gd2, st2
+        gen = torch.Generator(device="cuda").manual_seed(99)
+        response = {}
+        for eps in (6e-8, 6e-10, 6e-12):
+            def perturbed(k, t, eps=eps):
+                r = torch.rand(t.shape, device=t.device, dtype=t.dtype, generator=gen) * 2.0 - 1.0
+                return t * (1.0 + eps * r)
+
+            gd2, st2 = first_call_f64(perturbed)
+            response[f"{eps:.0e}"] = {k: _rel_stats(getattr(st2, k), ref[k], n, npz) for k in ("delp", "pt")}
+            gd2.close()
+            del gd2, st2
         del ref
         mixed_error = {
             "mixed_vs_fp64": mixed, "mixed_vs_fp64_rms": mixed_rms, "fp64_from_fp32_rounded_input_vs_fp64": floor,
             "mixed_vs_fp64_from_same_input": arith,
-            "after": "one AcousticDynamics call (n_split acoustic substeps) from the same state; max relative "
-                     "error over the compute domain (rms: RMS difference over RMS of the FP64 field)",
+            "fp64_second_call_vs_first": carry,
+            "fp64_response_to_input_perturbation": {
+                "per_eps": response,
+                "stats": "max relative change, its 99.9th percentile, and the number of compute points above 1e-4",
+            },
+            "after": "one AcousticDynamics call (n_split acoustic substeps) from the same state, each compared run "
+                     "the first call of its own AcousticDynamics; max relative error over the compute domain "
+                     "(rms: RMS difference over RMS of the FP64 field)",
         }
+    del state0
 
     results = {}
     for prec in precisions:
@@ -372,19 +431,23 @@ def run_cuda(args):
     e2e_seq_ms, e2e_ms = vals[-2], vals[-1]
     peak, peak_kind = _measured_peak()
 
+    per_cell = dram_bytes_per_cell_level()
+
     def roof(prec):
         width = 4 if prec == "f32" else 8
         sec = results[prec]["ms"] * 1e-3
         achieved = 34 * width * cells * n_split / sec / 1e9
-        traffic = DRAM_BYTES_PER_CELL_LEVEL[prec] * cells * n_split
-        return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_source": peak_kind,
-                "scope": f"whole AcousticDynamics call: {34 * width} B compulsory traffic per cell-level per "
-                         "substep (34 field transfers at the stored width)",
-                "traffic_note": f"DRAM bytes read + written per call, {DRAM_BYTES_PER_CELL_LEVEL[prec]:.0f} B per "
-                                "cell-level per substep from ncu over one call's launches at C384 L79 "
-                                "(profiles/acoustics_c384_l79_dram_traffic.md)",
-                "dram_gbs_at_traffic": traffic / sec / 1e9}
+        r = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+             "traffic": None, "peak_source": peak_kind,
+             "scope": f"whole AcousticDynamics call: {34 * width} B compulsory traffic per cell-level per "
+                      "substep (34 field transfers at the stored width)"}
+        if per_cell is not None:
+            traffic = per_cell[prec] * cells * n_split
+            r.update(traffic=traffic, dram_gbs_at_traffic=traffic / sec / 1e9,
+                     traffic_note=f"DRAM bytes read + written per call: {per_cell[prec]:.0f} B per cell-level per "
+                                  "substep (ncu, every launch of one call at C128 L79, the current code) times "
+                                  "this call's cell-levels and substeps")
+        return r
 
     ms = results[head]["ms"]
     value = world * cells * n_split / (ms * 1e-3)

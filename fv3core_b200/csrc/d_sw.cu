@@ -657,24 +657,33 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, real* delpc, real* delp, real* ptc, real
         }
       }));
     }
-    // get_delpc second computation + damping (k < kz); copy_computeplus (k >= kz)
+    // get_delpc second computation (k < kz); copy_computeplus (k >= kz)
     FV3B_CHECK(launch_box(Box{s, e + 2, js, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
       PT_SETUP(d, t, k);
       if (k < kz) {
         real dpc = F3(v_contra_dxc, i, j - 1) - F3(v_contra_dxc, i, j) + F3(u_contra_dyc, i - 1, j) -
                      F3(u_contra_dyc, i, j);
-        dpc = F2(g.rarea_c, i, j) * dpc;
-        W3(delpc, i, j) = dpc;
+        W3(delpc, i, j) = F2(g.rarea_c, i, j) * dpc;
+      } else {
+        W3(delpc, i, j) = F3(divgd, i, j);
+      }
+    }));
+    // damping (divergence_damping.py:94-107) on k < kz.  It overwrites
+    // v_contra_dxc, which the launch above reads one row down, so it is a
+    // launch of its own: in one launch a block could read a row another
+    // block has already overwritten.
+    if (kz > 0) {
+      FV3B_CHECK(launch_box(Box{s, e + 2, js, je + 2, 0, kz}, st, [=] __device__(int t, int i, int j, int k) {
+        PT_SETUP(d, t, k);
+        const real dpc = F3(delpc, i, j);
         real delpcdt = dpc * dt;
         real mintmp = fmin(RC(0.2), dddmp * fabs(delpcdt));
         real damp = da_min_c * fmax(col_d2_divg[k], mintmp);
         real vort = damp * dpc;
         W3(v_contra_dxc, i, j) = vort;
         W3(tmp_ke, i, j) = F3(tmp_ke, i, j) + vort;
-      } else {
-        W3(delpc, i, j) = F3(divgd, i, j);
-      }
-    }));
+      }));
+    }
     for (int n = 0; n < nn; ++n) {
       const int nt = nn - n - 1;
       const bool fillc = n + 1 != nn;

@@ -186,6 +186,24 @@ def acoustics_case(n=12, nz=8, seed=41, n_split=2):
 
 
 CASES["acoustics"] = acoustics_case
+
+
+def smooth_acoustics_case(n=48, nz=79, n_split=6):
+    """The baroclinic-wave state without seeded noise and without tracers
+    (dry), w and the surface w at zero: a state smooth at the grid scale."""
+    st = baroclinic_state(grid_for(n), nz, seed=0, noise=0.0, ntracers=0)
+    shp = st["delp"].shape
+    case = {name: np.array(st[name], copy=True) for name in ACOUSTIC_STATE if name in st}
+    case["w"] = np.zeros(shp)
+    case["wsd"] = np.zeros(shp[:3])
+    for name in ("omga", "ua", "va", "uc", "vc", "mfxd", "mfyd", "cxd", "cyd", "diss_estd"):
+        case[name] = np.zeros(shp)
+    case.update(
+        ak=np.asarray(st["ak"], dtype=np.float64), bk=np.asarray(st["bk"], dtype=np.float64),
+        pfull=np.asarray(st["pfull"], dtype=np.float64), ptop=st["ptop"], ks=st["ks"],
+        mdt=37.5 * n_split, n_map=1, akap=C.KAPPA, n_split=n_split,
+    )
+    return case
 # the parity case of the plain FP64 method: C12 L79, one acoustic substep of
 # dt_acoustic = 225 / 6 s (n_split = 1, mdt = 37.5 s)
 CASES["acoustics_c12_l79"] = acoustics_case
