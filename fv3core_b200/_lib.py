@@ -77,6 +77,8 @@ CTX_SIGNATURES = {
     "fv3b_adjust_negative_tracers": [P] * 11 + [ctypes.c_int, P],
     "fv3b_cubed_to_latlon": [P] * 8 + [ctypes.c_int, P],
     "fv3b_transport_create": [ctypes.c_int, P, P, ctypes.c_int, P],
+    "fv3b_remap_setup": [P, P],
+    "fv3b_lagrangian_to_eulerian": [P, P, D, D, D, ctypes.c_int, P],
 }
 
 # entry points whose first argument is a transport object (fv3b_transport*),
@@ -116,6 +118,18 @@ DYCORE_FIELDS = ("u", "v", "w", "delz", "delp", "pt", "pe", "pk", "phis", "wsd",
 class DycoreState(ctypes.Structure):
     _fields_ = [(n, P) for n in DYCORE_FIELDS] + [("mdt", D), ("akap", D), ("ptop", D), ("n_map", I32),
                                                   ("ks", I32)]
+
+
+REMAP_TRACERS = ("qvapor", "qliquid", "qrain", "qice", "qsnow", "qgraupel", "qo3mr", "qsgs_tke")
+REMAP_FIELDS = ("pt", "delp", "delz", "peln", "u", "v", "w", "ua", "va", "cappa", "q_con", "pkz", "pk", "pe", "ps")
+
+
+class RemapConfig(ctypes.Structure):
+    _fields_ = [(n, I32) for n in ("kord_tm", "kord_tr", "kord_wz", "kord_mt", "fill", "reserved")]
+
+
+class RemapFields(ctypes.Structure):
+    _fields_ = [("tracers", P * 8)] + [(n, P) for n in REMAP_FIELDS] + [("wsd", P)]
 
 
 def lib(precision="f64"):

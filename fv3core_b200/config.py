@@ -105,3 +105,52 @@ def baroclinic_acoustic_config(n_split=6, k_split=1):
         riemann=RiemannConfig(p_fac=0.05, a_imp=1.0, use_logp=False, beta=0.0),
         d_grid_shallow_water=baroclinic_dsw_config(),
     )
+
+
+@dataclasses.dataclass(frozen=True)
+class SatAdjustConfig:
+    """The fast saturation adjustment's namelist (fv3core/_config.py:85-110);
+    carried by RemappingConfig.  The adjustment itself is not run here:
+    LagrangianToEulerian rejects do_sat_adj."""
+
+    hydrostatic: bool
+    rad_snow: bool
+    rad_rain: bool
+    rad_graupel: bool
+    tintqs: bool
+    sat_adj0: float
+    ql_gen: float
+    qs_mlt: float
+    ql0_max: float
+    t_sub: float
+    qi_gen: float
+    qi_lim: float
+    qi0_max: float
+    dw_ocean: float
+    dw_land: float
+    icloud_f: int
+    cld_min: float
+    tau_i2s: float
+    tau_v2l: float
+    tau_r2g: float
+    tau_l2r: float
+    tau_l2v: float
+    tau_imlt: float
+    tau_smlt: float
+
+
+@dataclasses.dataclass(frozen=True)
+class RemappingConfig:
+    """fv3core/_config.py:113-125."""
+
+    fill: bool
+    kord_tm: int
+    kord_tr: int
+    kord_wz: int
+    kord_mt: int
+    do_sat_adj: bool
+    sat_adjust: SatAdjustConfig
+
+    @property
+    def hydrostatic(self) -> bool:
+        return self.sat_adjust.hydrostatic

@@ -45,8 +45,10 @@ extern "C" int fv3b_ctx_destroy(fv3b_ctx* ctx) {
   fv3b_acoustics_release(ctx);
   cudaError_t e = cudaFree(ctx->ws_base);
   cudaError_t e2 = cudaFree(ctx->col);
+  cudaError_t e3 = cudaFree(ctx->remap_akbk);
   delete ctx;
   if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = e3;
   FV3B_CHECK(e);
   return FV3B_OK;
 }

@@ -60,6 +60,10 @@ struct fv3b_ctx {
   int dzd_hord_tm = 0;
   fv3b::RayState ray;
   fv3b::AcousticState* acoustic = nullptr;
+  // LagrangianToEulerian: ak and bk in FP64 on the device (2 x MAXLEV),
+  // set by fv3b_remap_setup
+  double* remap_akbk = nullptr;
+  int remap_nlev = 0;
 };
 
 namespace fv3b {

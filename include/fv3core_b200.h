@@ -521,6 +521,50 @@ int fv3b_cubed_to_latlon(fv3b_ctx* ctx, fv3b_real* u, fv3b_real* v, const fv3b_r
                          const fv3b_real* a21, const fv3b_real* a22, fv3b_real* ua, fv3b_real* va, int order,
                          void* stream);
 
+/*
+ * LagrangianToEulerian.__init__ (fv3core/stencils/remapping.py:210-414):
+ * keeps the hybrid coordinate ak, bk (HOST arrays of npz+1 values) on the
+ * device in FP64.  Allocates (cudaMalloc) on the first call for a context
+ * and synchronises.
+ */
+int fv3b_remap_setup(fv3b_ctx* ctx, const double* ak, const double* bk);
+
+/*
+ * RemappingConfig (fv3core/_config.py:114-125) without the saturation
+ * adjustment: the PPM remapping orders (|kord| <= 10; kord_tm < 0, as the
+ * reference requires) and fill (0/1, negative-tracer filling after the
+ * tracer remap).
+ */
+typedef struct fv3b_remap_config {
+  int32_t kord_tm, kord_tr, kord_wz, kord_mt, fill, reserved;
+} fv3b_remap_config;
+
+/*
+ * The fields LagrangianToEulerian.__call__ reads and writes, as device
+ * pointers: the eight remapped tracers in the reference's order (qvapor,
+ * qliquid, qrain, qice, qsnow, qgraupel, qo3mr, qsgs_tke;
+ * fv3core/utils/gt4py_utils.py:26-36), the 3-D state fields, ps (2-D,
+ * written) and wsd (2-D, the bottom boundary value of w).
+ */
+typedef struct fv3b_remap_fields {
+  fv3b_real* tracers[8];
+  fv3b_real *pt, *delp, *delz, *peln, *u, *v, *w, *ua, *va, *cappa, *q_con, *pkz, *pk, *pe, *ps;
+  const fv3b_real* wsd;
+} fv3b_remap_fields;
+
+/*
+ * LagrangianToEulerian.__call__ (fv3core/stencils/remapping.py:416-628)
+ * with do_sat_adj false: moist pt and the delz adjustment, the Eulerian
+ * pressures ak + bk ps, the PPM remapping (remap_profile.py cs_profile,
+ * map_single.py) of pt in log pressure, of the tracers (then fillz) and of
+ * w, delz, u and v, moist pkz, and the last-step pt conversion (last_step 1)
+ * or the division by pkz (last_step 0).  One thread per column; the column
+ * work arrays and the arithmetic are FP64 in both builds.  Requires
+ * fv3b_remap_setup.
+ */
+int fv3b_lagrangian_to_eulerian(fv3b_ctx* ctx, const fv3b_remap_fields* fields, const fv3b_remap_config* config,
+                                double ptop, double akap, double zvir, int last_step, void* stream);
+
 /* Device pointer of one of the substep temporaries by its reference name
  * ("gz", "zh", "pkc", "pk3", "ut", "vt", "divgd", "heat_source", "crx",
  * "cry", "xfx", "yfx", "delpc", "ptc", "ws3", "zs", "dp_ref"), or NULL. */

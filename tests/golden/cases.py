@@ -294,3 +294,86 @@ def fv_step_case(n=12, nz=8, seed=71):
 
 
 CASES["fv_step"] = fv_step_case
+
+
+# Tracers of the remapping step, in the reference's order (utils.tracer_variables,
+# the first NQ = 8 are remapped by MapNTracer); qcld is remapped only by the
+# saturation adjustment, which this case leaves out.
+REMAP_TRACERS = ("qvapor", "qliquid", "qrain", "qice", "qsnow", "qgraupel", "qo3mr", "qsgs_tke")
+# Remapping namelist of the baroclinic-wave configuration
+# (examples/wrapped/config/baroclinic.yml in the reference), without the
+# saturation adjustment.
+REMAP_CONFIG = dict(fill=True, kord_tm=-9, kord_tr=9, kord_wz=9, kord_mt=9, do_sat_adj=False)
+# fast saturation adjustment namelist (baroclinic.yml values, the reference's
+# Namelist defaults for the rest)
+SAT_ADJUST_CONFIG = dict(
+    hydrostatic=False, rad_snow=True, rad_rain=True, rad_graupel=True, tintqs=False, sat_adj0=0.9, ql_gen=1.0e-3,
+    qs_mlt=1.0e-6, ql0_max=2.0e-3, t_sub=184.0, qi_gen=1.82e-6, qi_lim=1.0, qi0_max=1.0e-4, dw_ocean=0.1,
+    dw_land=0.15, icloud_f=0, cld_min=0.05, tau_i2s=1000.0, tau_v2l=90.0, tau_r2g=900.0, tau_l2r=900.0,
+    tau_l2v=300.0, tau_imlt=600.0, tau_smlt=900.0,
+)
+REMAP_STATE = ("pt", "delp", "delz", "peln", "u", "v", "w", "ua", "va", "cappa", "q_con", "pkz", "pk", "pe",
+               "ps", "te0_2d", "wsd")
+
+
+def remap_case(n=12, nz=8, seed=81, kord=(-9, 9, 9, 9)):
+    """Inputs of LagrangianToEulerian: the baroclinic-wave state whose layer
+    thicknesses are perturbed by a seeded factor in [0.7, 1.3] at every
+    point (halo included), so that the Lagrangian surfaces pe (ptop plus the
+    running sum of delp) leave the Eulerian ak + bk ps levels, some target
+    layers spanning three source layers; peln, pk and
+    the hydrostatic delz follow from pe.  Eight tracers uniform in
+    [0, 1e-3), of which a seeded 3 % of the points are negative (down to
+    -1e-4) so that the negative-value filling acts; w and the bottom w
+    boundary wsd are seeded noise.  ``kord`` gives (kord_tm, kord_tr,
+    kord_wz, kord_mt)."""
+    st = base_state(n, nz, seed)
+    rng = np.random.default_rng(seed + 1000)
+    shp = st["delp"].shape
+    ptop = st["ptop"]
+    delp = st["delp"][..., :nz] * rng.uniform(0.7, 1.3, shp[:3] + (nz,))
+    pe = np.empty(shp)
+    pe[..., 0] = ptop
+    pe[..., 1:] = ptop + np.cumsum(delp, axis=-1)
+    pe_col = st["pe"][0, 0, 0, :]
+    ratio = np.log(pe[..., 1:] / pe[..., :-1]) / np.log(pe_col[1:] / pe_col[:-1])
+    case = {k: np.array(st[k], copy=True) for k in ("pt", "u", "v", "cappa", "q_con", "pkz", "phis")}
+    case["delp"] = np.zeros(shp)
+    case["delp"][..., :nz] = delp
+    case["delz"] = np.zeros(shp)
+    case["delz"][..., :nz] = st["delz"][..., :nz] * ratio
+    case["pe"] = pe
+    case["peln"] = np.log(pe)
+    case["pk"] = np.exp(C.KAPPA * case["peln"])
+    case["w"] = 0.1 * rng.standard_normal(shp)
+    case["wsd"] = 0.05 * rng.standard_normal(shp[:3])
+    case["ps"] = np.zeros(shp[:3])
+    case["te0_2d"] = np.zeros(shp[:3])
+    case["ua"] = np.zeros(shp)
+    case["va"] = np.zeros(shp)
+    for name in REMAP_TRACERS:
+        q = rng.uniform(0.0, 1.0e-3, shp)
+        neg = rng.random(shp) < 0.03
+        q = np.where(neg, -rng.uniform(0.0, 1.0e-4, shp), q)
+        q[..., nz] = 0.0
+        case[name] = q
+    case["qcld"] = np.zeros(shp)
+    case["dp1"] = np.zeros(shp)
+    case["omga"] = np.zeros(shp)
+    case["ak"], case["bk"], case["pfull"] = st["ak"], st["bk"], st["pfull"]
+    case["ptop"] = ptop
+    case["mdt"] = 225.0
+    case["kord"] = np.array(kord)
+    return case
+
+
+def remap_config(case):
+    """The remapping namelist of a remap case (its kord values)."""
+    kord_tm, kord_tr, kord_wz, kord_mt = (int(x) for x in case["kord"])
+    return dict(REMAP_CONFIG, kord_tm=kord_tm, kord_tr=kord_tr, kord_wz=kord_wz, kord_mt=kord_mt)
+
+
+CASES["remap"] = remap_case
+# the profile's other limiters: kord 10 (ext5 / ext6 tests) and kord 8
+CASES["remap_kord10"] = functools.partial(remap_case, kord=(-10, 10, 10, 10))
+CASES["remap_kord8"] = functools.partial(remap_case, kord=(-8, 8, 8, 8))

@@ -182,6 +182,20 @@ class _Stmt:
         self.block = block
 
 
+class _Loop:
+    """A ``while`` loop: ``body`` starts with the statement that evaluates the
+    loop test into ``test``; ``active`` is the mask under which the body runs
+    (the enclosing condition and the test)."""
+
+    __slots__ = ("body", "active", "comp", "block", "idx")
+
+    def __init__(self, body, active, comp, block):
+        self.body = body
+        self.active = active
+        self.comp = comp
+        self.block = block
+
+
 class _Comp:
     def __init__(self, order):
         self.order = order
@@ -192,6 +206,8 @@ def _expr_reads(e, out):
     tag = e[0]
     if tag == "f":
         out.append((e[1], e[2][0], e[2][1]))
+        if not isinstance(e[2][2], int):
+            _expr_reads(e[2][2][1], out)
     elif tag in ("bin", "cmp"):
         _expr_reads(e[2], out)
         _expr_reads(e[3], out)
@@ -421,9 +437,14 @@ class _Lowering:
     def offset_of(self, sl, env, globs, b):
         if isinstance(sl, ast.Tuple):
             vals = []
-            for x in sl.elts:
+            for n, x in enumerate(sl.elts):
                 e = self.lower_expr(x, env, globs, None)
                 if e[0] != "c":
+                    # a vertical offset read from a field (map_single's
+                    # ``q[0, 0, lev]``): a per-column gather along k
+                    if n == 2 and len(sl.elts) == 3 and self.axes_of(b) == "IJK":
+                        vals.append(("dyn", e))
+                        continue
                     raise SyntaxError("non-constant offset")
                 vals.append(int(e[1]))
         else:
@@ -629,6 +650,24 @@ class _Lowering:
                 r2 = self.lower_body(node.orelse, env, globs, ctx_f, in_function)
             if r1 is not None or r2 is not None:
                 raise SyntaxError("return inside a field-dependent if")
+            return None
+        if isinstance(node, ast.While):
+            if node.orelse:
+                raise SyntaxError("while ... else")
+            outer = self.cur_block
+            loop = _Loop([], None, self.cur_comp, outer)
+            self.cur_block = (outer[0], loop.body)
+            cname = self.fresh("wcond")
+            self.emit(cname, self.lower_expr(node.test, env, globs, ctx), ctx)
+            cref = ("f", cname, (0, 0, 0))
+            ctx_t = dict(ctx)
+            ctx_t["cond"] = cref if ctx["cond"] is None else ("bool", "and", [ctx["cond"], cref])
+            loop.active = ctx_t["cond"]
+            r = self.lower_body(node.body, env, globs, ctx_t, in_function)
+            self.cur_block = outer
+            if r is not None:
+                raise SyntaxError("return inside a while loop")
+            outer[1].append(loop)
             return None
         if isinstance(node, ast.With):
             return self.lower_with(node, env, globs, ctx, in_function)
@@ -870,19 +909,28 @@ class StencilObject:
         self.comps = low.comps
         self.temps = set(low.temps)
         stmts = []
+
+        def collect(items, ci):
+            for s in items:
+                if isinstance(s, _Loop):
+                    s.comp = ci
+                    collect(s.body, ci)
+                    s.idx = s.body[0].idx
+                    continue
+                s.comp = ci
+                s.idx = len(stmts)
+                reads = []
+                _expr_reads(s.expr, reads)
+                if s.cond is not None:
+                    _expr_reads(s.cond, reads)
+                if s.cond is not None or s.regions is not None:
+                    reads.append((s.target, 0, 0))
+                s.reads = reads
+                stmts.append(s)
+
         for ci, comp in enumerate(self.comps):
             for bi, (iv, blk) in enumerate(comp.blocks):
-                for s in blk:
-                    s.comp = ci
-                    s.idx = len(stmts)
-                    reads = []
-                    _expr_reads(s.expr, reads)
-                    if s.cond is not None:
-                        _expr_reads(s.cond, reads)
-                    if s.cond is not None or s.regions is not None:
-                        reads.append((s.target, 0, 0))
-                    s.reads = reads
-                    stmts.append(s)
+                collect(blk, ci)
         self.stmts = stmts
         written = {s.target for s in stmts}
         read = set()
@@ -1021,7 +1069,7 @@ class _Executor:
                     if k1 <= k0:
                         continue
                     for s in stmts:
-                        self.exec_stmt(s, k0, k1)
+                        self.exec_item(s, k0, k1)
             else:
                 ranges = [(self.k_range(iv), stmts) for iv, stmts in comp.blocks]
                 ks = range(self.nk) if comp.order == FORWARD else range(self.nk - 1, -1, -1)
@@ -1029,11 +1077,28 @@ class _Executor:
                     for (k0, k1), stmts in ranges:
                         if k0 <= k < k1:
                             for s in stmts:
-                                self.exec_stmt(s, k, k + 1)
+                                self.exec_item(s, k, k + 1)
+
+    def exec_item(self, s, k0, k1):
+        if not isinstance(s, _Loop):
+            self.exec_stmt(s, k0, k1)
+            return
+        # the numpy backend's masked loop: run the body while the test holds
+        # at any point of the box (bounded by the column length)
+        box = self.boxes[s.body[0].idx]
+        for _ in range(self.nk + 2 * self.kpad + 1):
+            self.exec_stmt(s.body[0], k0, k1)
+            if box is None or not np.any(_truth(self.ev(s.active, box, k0, k1))):
+                return
+            for b in s.body[1:]:
+                self.exec_item(b, k0, k1)
+        raise RuntimeError("gtscript shim: while loop did not end")
 
     def read(self, name, off, box, k0, k1):
         i0, i1, j0, j1 = box
         di, dj, dk = off
+        if not isinstance(dk, int):
+            return self.read_dyn(name, (di, dj), dk[1], box, k0, k1)
         if name in self.temps:
             p, kp = self.pad, self.kpad
             return _take(
@@ -1055,6 +1120,27 @@ class _Executor:
         if axes == "J":
             return _take(arr, (o[0] + j0 + dj,), (j1 - j0,))[None, :, None]
         raise ValueError(axes)
+
+    def read_dyn(self, name, dij, dk_expr, box, k0, k1):
+        """field[i + di, j + dj, k + dk(i, j, k)] for an integer field dk."""
+        i0, i1, j0, j1 = box
+        di, dj = dij
+        shape = (i1 - i0, j1 - j0, k1 - k0)
+        dk = np.broadcast_to(np.asarray(self.ev(dk_expr, box, k0, k1)), shape).astype(np.int64)
+        kk = np.arange(k0, k1)[None, None, :] + dk
+        if name in self.temps:
+            p, kp = self.pad, self.kpad
+            arr = self.temps[name]
+            plane = arr[i0 + di + p : i1 + di + p, j0 + dj + p : j1 + dj + p, :]
+            kidx = kk + kp
+        else:
+            arr = self.arrays[name]
+            o = self.origins[name]
+            plane = arr[o[0] + i0 + di : o[0] + i1 + di, o[1] + j0 + dj : o[1] + j1 + dj, :]
+            kidx = kk + o[2]
+        ok = (kidx >= 0) & (kidx < plane.shape[2])
+        out = np.take_along_axis(plane, np.clip(kidx, 0, plane.shape[2] - 1), axis=2).astype(np.float64)
+        return np.where(ok, out, np.nan)
 
     def ev(self, e, box, k0, k1):
         tag = e[0]

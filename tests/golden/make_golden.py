@@ -315,6 +315,44 @@ def run_fv_step(case, n, nz):
     return out, {"region": "full storage"}
 
 
+REMAP_FIELDS = cases.REMAP_TRACERS + ("pt", "delp", "delz", "peln", "u", "v", "w", "ua", "va", "cappa", "q_con",
+                                      "pkz", "pk", "pe", "ps")
+
+
+def run_remap(case, n, nz):
+    """LagrangianToEulerian (remapping.py:205-628) tile by tile, built and
+    called as DynamicalCore builds and calls it (fv_dynamics.py:380-386,
+    483-519), on the last k_split step (last_step, no adiabatic init,
+    consv_te 0); the fields it writes, over the compute domain and the
+    extra row of the D-grid winds."""
+    import fv3core._config as spec
+    from fv3core.stencils.remapping import LagrangianToEulerian
+
+    config = spec.RemappingConfig(sat_adjust=spec.SatAdjustConfig(**cases.SAT_ADJUST_CONFIG),
+                                  **cases.remap_config(case))
+    grid = cases.grid_for(n)
+    S = rr.storage
+    out = {k: [] for k in REMAP_FIELDS}
+    for t in range(6):
+        tr = rr.TileReference(grid, t, nz)
+        tr.activate()
+        l2e = LagrangianToEulerian(tr.stencil_factory, config, tr.grid_data.area_64, len(cases.REMAP_TRACERS),
+                                   case["pfull"])
+        tracers = {k: S(case[k][t]) for k in cases.REMAP_TRACERS}
+        st = {k: S(case[k][t]) for k in ("pt", "delp", "delz", "peln", "u", "v", "w", "ua", "va", "cappa",
+                                         "q_con", "qcld", "pkz", "pk", "pe", "omga", "dp1")}
+        for k in ("phis", "te0_2d", "ps", "wsd"):
+            st[k] = S(case[k][t], origin=(3, 3))
+        l2e(tracers, st["pt"], st["delp"], st["delz"], st["peln"], st["u"], st["v"], st["w"], st["ua"], st["va"],
+            st["cappa"], st["q_con"], st["qcld"], st["pkz"], st["pk"], st["pe"], st["phis"], st["te0_2d"],
+            st["ps"], st["wsd"], st["omga"], case["ak"], case["bk"], case["pfull"], st["dp1"], case["ptop"],
+            cases.C.KAPPA, cases.C.ZVIR, True, 0.0, case["mdt"], case["mdt"], False, len(cases.REMAP_TRACERS))
+        box = (slice(3, 3 + n + 1), slice(3, 3 + n + 1))
+        for k in REMAP_FIELDS:
+            out[k].append(np.array(tracers[k] if k in tracers else st[k])[box])
+    return {k: np.stack(v) for k, v in out.items()}, {"region": "storage [3, 3 + n + 1) in i and j"}
+
+
 RUNNERS = {
     "acoustics": (run_acoustics, dict(n=12, nz=8, seed=41)),
     "d_sw": (run_d_sw, dict(n=12, nz=8, seed=31)),
@@ -323,6 +361,9 @@ RUNNERS = {
     "acoustics_c12_l79": (run_acoustics_compute, dict(n=12, nz=79, seed=7, n_split=1)),
     "tracer_advection": (run_tracer_advection, dict(n=12, nz=8, seed=61)),
     "fv_step": (run_fv_step, dict(n=12, nz=8, seed=71)),
+    "remap": (run_remap, dict(n=4, nz=79, seed=81)),
+    "remap_kord10": (run_remap, dict(n=4, nz=30, seed=83)),
+    "remap_kord8": (run_remap, dict(n=4, nz=30, seed=85)),
 }
 
 

@@ -175,3 +175,36 @@ def run_fv_step(case, n, nz, precision="f64"):
         return out
     finally:
         gd.close()
+
+
+def run_remap(case, n, nz, precision="f64"):
+    """The package's LagrangianToEulerian on a case of ``cases.remap_case``
+    (last step, no adiabatic init, consv_te 0); returns the remapped fields
+    over the full storage."""
+    import torch
+
+    from fv3core_b200 import constants as C
+    from fv3core_b200.config import RemappingConfig, SatAdjustConfig
+    from fv3core_b200.grid_data import GridData
+    from fv3core_b200.stencil import StencilConfig, StencilFactory
+    from fv3core_b200.stencils.remapping import LagrangianToEulerian
+    from fv3core_b200.storage import to_device, to_host
+
+    gd = GridData(cases.grid_for(n), nz, precision=precision)
+    dtype = gd.grid_indexing.dtype
+    sf = StencilFactory(StencilConfig(), gd.grid_indexing)
+    try:
+        config = RemappingConfig(sat_adjust=SatAdjustConfig(**cases.SAT_ADJUST_CONFIG), **cases.remap_config(case))
+        l2e = LagrangianToEulerian(sf, config, None, len(cases.REMAP_TRACERS), case["pfull"])
+        dev = {k: to_device(case[k], dtype=dtype) for k in cases.REMAP_TRACERS + cases.REMAP_STATE
+               + ("qcld", "omga", "dp1", "phis")}
+        tracers = {k: dev[k] for k in cases.REMAP_TRACERS}
+        d = dev
+        l2e(tracers, d["pt"], d["delp"], d["delz"], d["peln"], d["u"], d["v"], d["w"], d["ua"], d["va"],
+            d["cappa"], d["q_con"], d["qcld"], d["pkz"], d["pk"], d["pe"], d["phis"], d["te0_2d"], d["ps"],
+            d["wsd"], d["omga"], case["ak"], case["bk"], case["pfull"], d["dp1"], case["ptop"], C.KAPPA, C.ZVIR,
+            True, 0.0, case["mdt"], case["mdt"], False, len(cases.REMAP_TRACERS))
+        torch.cuda.synchronize()
+        return {k: to_host(dev[k]) for k in cases.REMAP_TRACERS + cases.REMAP_STATE}
+    finally:
+        gd.close()

@@ -2,6 +2,7 @@
 import numpy as np
 
 import cases
+from fv3core_b200 import constants as C
 from oracle._util import Tile
 
 
@@ -125,4 +126,25 @@ def run_fv_step(case, n, nz):
             F.cubed_to_latlon_ord4(t, st["u"][tt], st["v"][tt], g.dx[tt], g.dy[tt], g.a11[tt], g.a12[tt],
                                    g.a21[tt], g.a22[tt], st["ua"][tt], st["va"][tt])
         out.update({f"wrap_{k}": st[k].copy() for k in cases.WATER_NAMES + ("pt", "u", "v", "ua", "va")})
+    return out
+
+
+def run_remap(case, n, nz):
+    """The oracle's LagrangianToEulerian (remapping.py:416-628, no saturation
+    adjustment) tile by tile; returns the remapped fields over the full
+    storage."""
+    from oracle import remapping as R
+
+    t = Tile(n, nz)
+    st = {k: np.array(v, copy=True) for k, v in case.items() if isinstance(v, np.ndarray)}
+    out = {}
+    with np.errstate(all="ignore"):
+        for tt in range(6):
+            tracers = {k: st[k][tt] for k in cases.REMAP_TRACERS}
+            fields = {k: st[k][tt] for k in cases.REMAP_STATE}
+            R.lagrangian_to_eulerian(t, tracers, fields, case["ak"], case["bk"], case["ptop"], C.KAPPA, C.ZVIR,
+                                     True, **{k: v for k, v in cases.remap_config(case).items()
+                                              if k != "do_sat_adj"})
+    for k in cases.REMAP_TRACERS + cases.REMAP_STATE:
+        out[k] = st[k]
     return out
