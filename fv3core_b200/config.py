@@ -154,3 +154,137 @@ class RemappingConfig:
     @property
     def hydrostatic(self) -> bool:
         return self.sat_adjust.hydrostatic
+
+
+@dataclasses.dataclass
+class DynamicalCoreConfig:
+    """fv3core/_config.py:214-430: the dynamical core's namelist, with the
+    reference's defaults (NamelistDefaults, _config.py:14-65) and the same
+    derived configurations."""
+
+    dt_atmos: int
+    a_imp: float
+    beta: float
+    consv_te: bool
+    d2_bg: float
+    d2_bg_k1: float
+    d2_bg_k2: float
+    d4_bg: float
+    d_con: float
+    d_ext: float
+    dddmp: float
+    delt_max: float
+    do_sat_adj: bool
+    do_vort_damp: bool
+    fill: bool
+    hord_dp: int
+    hord_mt: int
+    hord_tm: int
+    hord_tr: int
+    hord_vt: int
+    hydrostatic: bool
+    k_split: int
+    ke_bg: float
+    kord_mt: int
+    kord_tm: int
+    kord_tr: int
+    kord_wz: int
+    n_split: int
+    nord: int
+    npx: int
+    npy: int
+    npz: int
+    ntiles: int
+    nwat: int
+    p_fac: float
+    rf_cutoff: float
+    tau: float
+    vtdm4: float
+    z_tracer: bool
+    do_qa: bool
+    layout: tuple = (1, 1)
+    grid_type: int = 0
+    do_f3d: bool = False
+    inline_q: bool = False
+    do_skeb: bool = False
+    use_logp: bool = False
+    moist_phys: bool = True
+    check_negative: bool = False
+    tau_r2g: float = 900.0
+    tau_smlt: float = 900.0
+    tau_g2r: float = 600.0
+    tau_imlt: float = 600.0
+    tau_i2s: float = 1000.0
+    tau_l2r: float = 900.0
+    tau_g2v: float = 900.0
+    tau_v2g: float = 21600.0
+    sat_adj0: float = 0.90
+    ql_gen: float = 1.0e-3
+    ql_mlt: float = 2.0e-3
+    qs_mlt: float = 1.0e-6
+    ql0_max: float = 2.0e-3
+    t_sub: float = 184.0
+    qi_gen: float = 1.82e-6
+    qi_lim: float = 1.0
+    qi0_max: float = 1.0e-4
+    rad_snow: bool = True
+    rad_rain: bool = True
+    rad_graupel: bool = True
+    tintqs: bool = False
+    dw_ocean: float = 0.10
+    dw_land: float = 0.20
+    icloud_f: int = 0
+    cld_min: float = 0.05
+    tau_l2v: float = 300.0
+    tau_v2l: float = 150.0
+    c2l_ord: int = 4
+    regional: bool = False
+    m_split: int = 0
+    convert_ke: bool = False
+    breed_vortex_inline: bool = False
+    use_old_omega: bool = True
+    rf_fast: bool = False
+    p_ref: float = 1e5
+    adiabatic: bool = False
+    nf_omega: int = 1
+    fv_sg_adj: int = -1
+    n_sponge: int = 1
+
+    @property
+    def riemann(self) -> RiemannConfig:
+        return RiemannConfig(p_fac=self.p_fac, a_imp=self.a_imp, use_logp=self.use_logp, beta=self.beta)
+
+    @property
+    def d_grid_shallow_water(self) -> DGridShallowWaterLagrangianDynamicsConfig:
+        return DGridShallowWaterLagrangianDynamicsConfig(
+            dddmp=self.dddmp, d2_bg=self.d2_bg, d2_bg_k1=self.d2_bg_k1, d2_bg_k2=self.d2_bg_k2, d4_bg=self.d4_bg,
+            ke_bg=self.ke_bg, nord=self.nord, n_sponge=self.n_sponge, grid_type=self.grid_type, d_ext=self.d_ext,
+            inline_q=self.inline_q, hord_dp=self.hord_dp, hord_tm=self.hord_tm, hord_mt=self.hord_mt,
+            hord_vt=self.hord_vt, do_f3d=self.do_f3d, do_skeb=self.do_skeb, d_con=self.d_con, vtdm4=self.vtdm4,
+            do_vort_damp=self.do_vort_damp, hydrostatic=self.hydrostatic, convert_ke=self.convert_ke,
+        )
+
+    @property
+    def acoustic_dynamics(self) -> AcousticDynamicsConfig:
+        return AcousticDynamicsConfig(
+            tau=self.tau, k_split=self.k_split, n_split=self.n_split, m_split=self.m_split,
+            delt_max=self.delt_max, rf_fast=self.rf_fast, rf_cutoff=self.rf_cutoff,
+            breed_vortex_inline=self.breed_vortex_inline, use_old_omega=self.use_old_omega, riemann=self.riemann,
+            d_grid_shallow_water=self.d_grid_shallow_water,
+        )
+
+    @property
+    def sat_adjust(self) -> SatAdjustConfig:
+        return SatAdjustConfig(
+            hydrostatic=self.hydrostatic, rad_snow=self.rad_snow, rad_rain=self.rad_rain,
+            rad_graupel=self.rad_graupel, tintqs=self.tintqs, sat_adj0=self.sat_adj0, ql_gen=self.ql_gen,
+            qs_mlt=self.qs_mlt, ql0_max=self.ql0_max, t_sub=self.t_sub, qi_gen=self.qi_gen, qi_lim=self.qi_lim,
+            qi0_max=self.qi0_max, dw_ocean=self.dw_ocean, dw_land=self.dw_land, icloud_f=self.icloud_f,
+            cld_min=self.cld_min, tau_i2s=self.tau_i2s, tau_v2l=self.tau_v2l, tau_r2g=self.tau_r2g,
+            tau_l2r=self.tau_l2r, tau_l2v=self.tau_l2v, tau_imlt=self.tau_imlt, tau_smlt=self.tau_smlt,
+        )
+
+    @property
+    def remapping(self) -> RemappingConfig:
+        return RemappingConfig(fill=self.fill, kord_tm=self.kord_tm, kord_tr=self.kord_tr, kord_wz=self.kord_wz,
+                               kord_mt=self.kord_mt, do_sat_adj=self.do_sat_adj, sat_adjust=self.sat_adjust)

@@ -377,3 +377,54 @@ CASES["remap"] = remap_case
 # the profile's other limiters: kord 10 (ext5 / ext6 tests) and kord 8
 CASES["remap_kord10"] = functools.partial(remap_case, kord=(-10, 10, 10, 10))
 CASES["remap_kord8"] = functools.partial(remap_case, kord=(-8, 8, 8, 8))
+
+
+# the water species and tracers of DynamicalCore's state: the eight it
+# advects and remaps (NQ = 8) and qcld
+STEP_TRACERS = REMAP_TRACERS + ("qcld",)
+
+
+def step_case(n=12, nz=12, seed=101, n_split=2):
+    """Inputs of DynamicalCore.step_dynamics (one k_split step of
+    dt_atmos = 225 s, n_split acoustic substeps): the acoustics case's
+    baroclinic-wave state with its potential temperature turned back into a
+    temperature (pt pkz, step_dynamics converts it in its preamble), water
+    vapour uniform in [1e-4, 1e-2), the other species in [0, 1e-5) with a
+    seeded 2 % of negative points (down to -1e-6), cloud fraction in
+    [0, 0.5)."""
+    case = acoustics_case(n, nz, seed, n_split)
+    rng = np.random.default_rng(seed + 2000)
+    shp = case["delp"].shape
+    case["pt"] = case["pt"] * case["pkz"]
+    for name in STEP_TRACERS:
+        if name == "qvapor":
+            q = rng.uniform(1.0e-4, 1.0e-2, shp)
+        elif name == "qcld":
+            q = rng.uniform(0.0, 0.5, shp)
+        else:
+            q = rng.uniform(0.0, 1.0e-5, shp)
+            neg = rng.random(shp) < 0.02
+            q = np.where(neg, -rng.uniform(0.0, 1.0e-6, shp), q)
+        q[..., nz] = 0.0
+        case[name] = q
+    case["ps"] = np.array(case["pe"][..., nz], copy=True)
+    case["mdt"] = 225.0
+    case["dt_atmos"] = 225.0
+    return case
+
+
+CASES["step"] = step_case
+
+
+def dycore_namelist(n, nz, n_split):
+    """DynamicalCoreConfig values of the baroclinic-wave configuration
+    (examples/wrapped/config/baroclinic.yml in the reference) on a C``n``
+    L``nz`` grid, without the saturation adjustment."""
+    nl = dict(DSW_CONFIG)
+    nl.update({k: v for k, v in ACOUSTIC_CONFIG.items()})
+    nl.update(RIEMANN_CONFIG)
+    nl.update({k: v for k, v in REMAP_CONFIG.items()})
+    nl.update(SAT_ADJUST_CONFIG)
+    nl.update(dt_atmos=225, consv_te=False, hord_tr=8, z_tracer=True, nwat=6, npx=n + 1, npy=n + 1, npz=nz,
+              ntiles=6, do_qa=True, n_split=n_split, moist_phys=True, c2l_ord=4, p_ref=1e5, nf_omega=1)
+    return nl

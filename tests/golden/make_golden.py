@@ -353,6 +353,136 @@ def run_remap(case, n, nz):
     return {k: np.stack(v) for k, v in out.items()}, {"region": "storage [3, 3 + n + 1) in i and j"}
 
 
+
+STEP_OUT = {"u": (0, 1, 0), "v": (1, 0, 0), "w": (0, 0, 0), "delz": (0, 0, 0), "delp": (0, 0, 0), "pt": (0, 0, 0),
+            "pe": (0, 0, 1), "pk": (0, 0, 1), "peln": (0, 0, 1), "pkz": (0, 0, 0), "q_con": (0, 0, 0),
+            "cappa": (0, 0, 0), "omga": (0, 0, 0), "ua": (0, 0, 0), "va": (0, 0, 0)}
+
+
+def run_step(case, n, nz):
+    """DynamicalCore.step_dynamics (fv_dynamics.py:395-557) for one k_split
+    step, composed as DynamicalCore._compute composes it from the
+    reference's own classes and functions (built as DynamicalCore.__init__
+    builds them, fv_dynamics.py:252-394): compute_preamble, then _dyn (the
+    dp1 copy, AcousticDynamics, TracerAdvection of the eight tracers),
+    LagrangianToEulerian, post_remap and wrapup; six tiles in lock step on
+    threads.  DynamicalCore's own temporaries (te_2d, te0_2d, wsd, cappa,
+    dp1, cvm, gz) start at zero.  Stored: the prognostic state on the
+    compute domain (+1 on the staggered axes and interfaces) and ps."""
+    import threading
+    import types
+
+    import fv3core._config as spec
+    from fv3core.stencils import fv_dynamics as fvd
+    from fv3core.stencils import moist_cv
+    from fv3core.stencils.c2l_ord import CubedToLatLon
+    from fv3core.stencils.del2cubed import HyperdiffusionDamping
+    from fv3core.stencils.dyn_core import AcousticDynamics
+    from fv3core.stencils.fvtp2d import FiniteVolumeTransport
+    from fv3core.stencils.neg_adj3 import AdjustNegativeTracerMixingRatio
+    from fv3core.stencils.remapping import LagrangianToEulerian
+    from fv3core.stencils.tracer_2d_1l import TracerAdvection
+    from fv3core.utils.grid import quantity_wrap
+
+    grid = cases.grid_for(n)
+    exchange = rr._Exchange()
+    S = rr.storage
+    acfg = spec.AcousticDynamicsConfig(
+        **{**cases.ACOUSTIC_CONFIG, "n_split": int(case["n_split"])},
+        riemann=spec.RiemannConfig(**cases.RIEMANN_CONFIG),
+        d_grid_shallow_water=spec.DGridShallowWaterLagrangianDynamicsConfig(**cases.DSW_CONFIG),
+    )
+    rcfg = spec.RemappingConfig(sat_adjust=spec.SatAdjustConfig(**cases.SAT_ADJUST_CONFIG), **cases.REMAP_CONFIG)
+    config = types.SimpleNamespace(hydrostatic=False, rf_fast=True, tau=10.0, adiabatic=False, kord_tm=-9,
+                                   nf_omega=1, nwat=6, moist_phys=True)
+    nq = len(cases.REMAP_TRACERS)
+    dims3 = ("x", "y", "z")
+    runs = []
+    for t in range(6):
+        tr = rr.TileReference(grid, t, nz)
+        tr.activate()
+        tr.add_tracer_grid()
+        comm = rr.ThreadComm(t, n, 3, exchange)
+        sf, gi = tr.stencil_factory, tr.grid_indexing
+        ak, bk, pfull = (S(case[k], origin=(0,)) for k in ("ak", "bk", "pfull"))
+        phis = S(case["phis"][t], origin=(0, 0))
+        o = types.SimpleNamespace()
+        o.fv_setup = sf.from_origin_domain(moist_cv.fv_setup, externals={"nwat": 6, "moist_phys": True},
+                                           origin=gi.origin_compute(), domain=gi.domain_compute())
+        o.pt_adjust = sf.from_origin_domain(fvd.pt_adjust, origin=gi.origin_compute(), domain=gi.domain_compute())
+        o.set_omega = sf.from_origin_domain(fvd.set_omega, origin=gi.origin_compute(), domain=gi.domain_compute())
+        o.ad = AcousticDynamics(comm, sf, tr.grid_data, tr.damping_coefficients, 0, False, False, acfg, ak, bk,
+                                pfull, phis)
+        transport = FiniteVolumeTransport(sf, tr.grid_data, tr.damping_coefficients, 0, hord=8)
+        o.adv = TracerAdvection(sf, transport, comm, nq)
+        o.l2e = LagrangianToEulerian(sf, rcfg, tr.grid_data.area_64, nq, np.asarray(pfull))
+        o.hyper = HyperdiffusionDamping(sf, tr.damping_coefficients, tr.grid_data.rarea, config.nf_omega)
+        o.c2l = CubedToLatLon(sf, tr.grid_data, order=4)
+        o.adjust = AdjustNegativeTracerMixingRatio(sf, False, False)
+        spec_o = gi.get_quantity_halo_spec(gi.domain_full(add=(1, 1, 1)), gi.origin_compute(), dims=list(dims3),
+                                           n_halo=3)
+        o.omega_updater = comm.get_scalar_halo_updater([spec_o])
+        st = types.SimpleNamespace()
+        for name in tuple(cases.ACOUSTIC_STATE) + cases.STEP_TRACERS + ("ps",):
+            arr = case[name][t]
+            setattr(st, name, S(arr, origin=(3, 3) if arr.ndim == 2 else (3, 3, 0)))
+        # DynamicalCore's temporaries (fvdyn_temporaries, fv_dynamics.py:172-190)
+        m = case["delp"].shape[1]
+        for name in ("te_2d", "te0_2d", "wsd"):
+            setattr(st, name, S(np.zeros((m, m)), origin=(3, 3)))
+        for name in ("cappa", "dp1", "cvm"):
+            setattr(st, name, S(np.zeros((m, m, nz + 1))))
+        for name, dims in ACOUSTIC_DIMS.items():
+            setattr(st, name + "_quantity", quantity_wrap(getattr(st, name), dims, gi))
+        st.omga_quantity = quantity_wrap(st.omga, dims3, gi)
+        o.tracers = {k: quantity_wrap(getattr(st, k), dims3, gi) for k in cases.REMAP_TRACERS}
+        st.ak, st.bk, st.pfull = ak, bk, pfull
+        st.consv_te, st.do_adiabatic_init, st.bdt = 0.0, False, float(case["dt_atmos"])
+        st.mdt, st.n_split, st.k_split, st.ptop, st.ks = float(case["dt_atmos"]), int(case["n_split"]), 1, \
+            case["ptop"], case["ks"]
+        st.akap = cases.C.KAPPA
+        st.qcld_quantity = quantity_wrap(st.qcld, dims3, gi)
+        runs.append((t, o, st, comm, tr))
+    errors = []
+
+    def work(t, o, st, comm, tr):
+        try:
+            fvd.compute_preamble(st, False, config, o.fv_setup, o.pt_adjust)
+            st.n_map = 1
+            # _dyn (fv_dynamics.py:535-557): dp1 = delp, the acoustic loop,
+            # then the tracers with the accumulated fluxes
+            st.dp1[:, :, :nz] = st.delp[:, :, :nz]
+            o.ad(st)
+            o.adv(o.tracers, st.dp1, st.mfxd, st.mfyd, st.cxd, st.cyd, st.mdt)
+            o.l2e({k: q.storage for k, q in o.tracers.items()}, st.pt, st.delp, st.delz, st.peln, st.u, st.v,
+                  st.w, st.ua, st.va, st.cappa, st.q_con, st.qcld, st.pkz, st.pk, st.pe, st.phis, st.te0_2d,
+                  st.ps, st.wsd, st.omga, st.ak, st.bk, st.pfull, st.dp1, st.ptop, cases.C.KAPPA, cases.C.ZVIR,
+                  True, st.consv_te, st.bdt / st.k_split, st.bdt, st.do_adiabatic_init, nq)
+            fvd.post_remap(st, False, config, o.hyper, o.set_omega, o.omega_updater,
+                           tr.damping_coefficients.da_min)
+            fvd.wrapup(st, comm, o.adjust, o.c2l, False)
+        except BaseException as exc:  # surfaced after join
+            errors.append(exc)
+            raise
+
+    threads = [threading.Thread(target=work, args=r) for r in runs]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    if errors:
+        raise errors[0]
+    h = 3
+    out = {}
+    for name, (di, dj, dk) in STEP_OUT.items():
+        out[name] = np.stack([np.asarray(getattr(r[2], name)) for r in runs])[:, h:h + n + di, h:h + n + dj,
+                                                                             :nz + dk]
+    for name in cases.STEP_TRACERS:
+        out[name] = np.stack([np.asarray(getattr(r[2], name)) for r in runs])[:, h:h + n, h:h + n, :nz]
+    out["ps"] = np.stack([np.asarray(r[2].ps) for r in runs])[:, h:h + n, h:h + n]
+    return out, {"region": "compute domain (+1 on staggered axes and interfaces)"}
+
+
 RUNNERS = {
     "acoustics": (run_acoustics, dict(n=12, nz=8, seed=41)),
     "d_sw": (run_d_sw, dict(n=12, nz=8, seed=31)),
@@ -364,6 +494,7 @@ RUNNERS = {
     "remap": (run_remap, dict(n=4, nz=79, seed=81)),
     "remap_kord10": (run_remap, dict(n=4, nz=30, seed=83)),
     "remap_kord8": (run_remap, dict(n=4, nz=30, seed=85)),
+    "step": (run_step, dict(n=12, nz=12, seed=101)),
 }
 
 

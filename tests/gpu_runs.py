@@ -208,3 +208,38 @@ def run_remap(case, n, nz, precision="f64"):
         return {k: to_host(dev[k]) for k in cases.REMAP_TRACERS + cases.REMAP_STATE}
     finally:
         gd.close()
+
+
+def run_step(case, n, nz, precision="f64", steps=1):
+    """The package's DynamicalCore.step_dynamics on a case of
+    ``cases.step_case`` (``steps`` steps of dt_atmos); returns the full
+    storages of the state."""
+    import torch
+
+    from fv3core_b200.config import DynamicalCoreConfig
+    from fv3core_b200.grid_data import GridData
+    from fv3core_b200.stencil import StencilConfig, StencilFactory
+    from fv3core_b200.stencils.fv_dynamics import DynamicalCore
+    from fv3core_b200.storage import to_device, to_host
+
+    gd = GridData(cases.grid_for(n), nz, precision=precision)
+    dtype = gd.grid_indexing.dtype
+    sf = StencilFactory(StencilConfig(), gd.grid_indexing)
+    try:
+        config = DynamicalCoreConfig(**cases.dycore_namelist(n, nz, int(case["n_split"])))
+        phis = to_device(case["phis"], dtype=dtype)
+        core = DynamicalCore(None, gd, sf, gd, config, case["ak"], case["bk"], phis)
+        names = tuple(cases.ACOUSTIC_STATE) + cases.STEP_TRACERS + ("ps",)
+        state = {k: to_device(case[k], dtype=dtype) for k in names if k not in ("phis",)}
+        state["phis"] = phis
+        for _ in range(steps):
+            core.step_dynamics(state, False, False, float(case["dt_atmos"]), case["ptop"], int(case["n_split"]),
+                               case["ks"])
+        torch.cuda.synchronize()
+        out = {k: to_host(v) for k, v in state.items()}
+        # cappa is not a step_dynamics argument: the step keeps it in
+        # DynamicalCore's own temporary, as the reference does
+        out["cappa"] = to_host(core._temporaries["cappa"])
+        return out
+    finally:
+        gd.close()

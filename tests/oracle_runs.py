@@ -148,3 +148,69 @@ def run_remap(case, n, nz):
     for k in cases.REMAP_TRACERS + cases.REMAP_STATE:
         out[k] = st[k]
     return out
+
+
+def run_step(case, n, nz, steps=1):
+    """The oracle's DynamicalCore.step_dynamics for one k_split step
+    (fv_dynamics.py:430-557): compute_preamble, dp1 = delp, AcousticDynamics,
+    TracerAdvection of the eight tracers, LagrangianToEulerian, post_remap
+    (set_omega, omega halo, del-2 filter) and wrapup (neg_adj3, halo,
+    cubed-to-latlon); DynamicalCore's temporaries (cappa, dp1, cvm, wsd,
+    te_2d, te0_2d) start at zero and, like the acoustic driver's, persist
+    from one of ``steps`` steps to the next.  Returns the full storages."""
+    from oracle.dyn_core import AcousticDynamics
+    from oracle.halo import HaloExchange
+    from oracle.tracer import TracerAdvection
+
+    g = cases.grid_for(n)
+    t = Tile(n, nz)
+    m = t.m
+    metrics = [cases.metric_namespace(n, tt) for tt in range(6)]
+    st = {k: (np.array(v, copy=True) if isinstance(v, np.ndarray) else v) for k, v in case.items()}
+    for name in ("te_2d", "te0_2d", "wsd"):
+        st[name] = np.zeros((6, m, m))
+    for name in ("cappa", "dp1", "cvm"):
+        st[name] = np.zeros((6, m, m, nz + 1))
+    bdt = float(case["dt_atmos"])
+    st.update(mdt=bdt, n_map=1, akap=C.KAPPA)
+    cfg = {**cases.ACOUSTIC_CONFIG, **cases.RIEMANN_CONFIG, "n_split": int(case["n_split"]),
+           "dsw": cases.DSW_CONFIG}
+    ad = AcousticDynamics(g, metrics, cfg, case["ak"], case["bk"], case["pfull"], case["phis"], nz)
+    adv = TracerAdvection(g, metrics, nz, len(cases.REMAP_TRACERS), hord=8)
+    halo = HaloExchange(n, 3)
+    with np.errstate(all="ignore"):
+        for _ in range(steps):
+            _oracle_step(st, case, n, nz, t, g, metrics, ad, adv, halo, bdt)
+    return st
+
+
+def _oracle_step(st, case, n, nz, t, g, metrics, ad, adv, halo, bdt):
+    from oracle import fv_step as F
+    from oracle import remapping as R
+    from oracle.dyn_core import del2cubed
+
+    for tt in range(6):
+        F.fv_setup(t, *[st[k][tt] for k in ("qvapor", "qliquid", "qrain", "qsnow", "qice", "qgraupel", "q_con",
+                                            "cvm", "pkz", "pt", "cappa", "delp", "delz", "dp1")])
+        F.pt_adjust(t, st["pkz"][tt], st["dp1"][tt], st["q_con"][tt], st["pt"][tt])
+    st["dp1"][..., :nz] = st["delp"][..., :nz]
+    ad(st)
+    adv([st[q] for q in cases.REMAP_TRACERS], st["dp1"], st["mfxd"], st["mfyd"], st["cxd"], st["cyd"], bdt)
+    for tt in range(6):
+        R.lagrangian_to_eulerian(t, {k: st[k][tt] for k in cases.REMAP_TRACERS},
+                                 {k: st[k][tt] for k in cases.REMAP_STATE}, case["ak"], case["bk"], case["ptop"],
+                                 C.KAPPA, C.ZVIR, True,
+                                 **{k: v for k, v in cases.REMAP_CONFIG.items() if k != "do_sat_adj"})
+    for tt in range(6):
+        F.set_omega(t, st["delp"][tt], st["delz"][tt], st["w"][tt], st["omga"][tt])
+    halo.scalar(st["omga"], nk=nz)
+    for tt in range(6):
+        scr = {name: np.full((t.m, t.m, t.nk), np.nan) for name in ("q", "fx", "fy")}
+        del2cubed(t, metrics[tt], st["omga"][tt], 0.18 * g.da_min, 1, scr)
+    for tt in range(6):
+        F.adjust_negative_tracers(t, *[st[k][tt] for k in cases.WATER_NAMES], st["pt"][tt], st["delp"][tt],
+                                  st["delz"][tt], st["peln"][tt])
+    halo.vector_d(st["u"], st["v"], nk=nz)
+    for tt in range(6):
+        F.cubed_to_latlon_ord4(t, st["u"][tt], st["v"][tt], g.dx[tt], g.dy[tt], g.a11[tt], g.a12[tt],
+                               g.a21[tt], g.a22[tt], st["ua"][tt], st["va"][tt])
