@@ -341,7 +341,6 @@ def run_cuda(args):
                      "the first call of its own AcousticDynamics; max relative error over the compute domain "
                      "(rms: RMS difference over RMS of the FP64 field)",
         }
-    del state0
 
     results = {}
     for prec in precisions:
@@ -484,12 +483,192 @@ def run_cuda(args):
         line["mixed_error_vs_fp64"] = mixed_error
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(1, args.cpu_n, args.cpu_npz)
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     for gd, _, _ in problems.values():
         gd.close()
+    del problems, initial, state, host, ad
+    torch.cuda.empty_cache()
+    if world == 1 and args.step_n > 0:
+        line["step_dynamics"] = run_step_section(args, state0, grid, local)
+    del state0
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------- full dynamics step
+STEP_FIELDS = ("qvapor", "qliquid", "qrain", "qice", "qsnow", "qgraupel", "qo3mr", "qsgs_tke", "qcld", "pt", "delp",
+               "delz", "peln", "u", "v", "w", "ua", "va", "uc", "vc", "q_con", "pe", "pk", "pkz", "ps", "omga",
+               "mfxd", "mfyd", "cxd", "cyd", "diss_estd")
+# compulsory field transfers per cell-level of one step (k_split 1): the
+# acoustic call's 34 per substep, the tracer advection's 8 tracers read and
+# written plus its 5 shared fluxes (one sub-cycle), the remapping's 21
+# fields read and written, the preamble's 15, post_remap's 6 and wrapup's 23
+STEP_TRANSFERS_NON_ACOUSTIC = 8 * 2 + 5 + 21 * 2 + 15 + 6 + 23
+
+
+def step_problem(n, npz, n_split, precision, st0, grid):
+    """GridData, DynamicalCore (baroclinic namelist) and device state for a
+    step_state ``st0``."""
+    import torch
+
+    from fv3core_b200.config import baroclinic_config
+    from fv3core_b200.grid_data import GridData
+    from fv3core_b200.stencil import StencilConfig, StencilFactory
+    from fv3core_b200.stencils.fv_dynamics import DynamicalCore
+    from fv3core_b200.storage import to_device
+
+    gd = GridData(grid, npz, precision=precision)
+    dtype = gd.grid_indexing.dtype
+    sf = StencilFactory(StencilConfig(), gd.grid_indexing)
+    phis = to_device(st0["phis"], dtype=dtype)
+    core = DynamicalCore(None, gd, sf, gd, baroclinic_config(n, npz, n_split), st0["ak"], st0["bk"], phis)
+    state = {k: to_device(st0[k], dtype=dtype) for k in STEP_FIELDS}
+    state["phis"] = phis
+    torch.cuda.synchronize()
+    return gd, core, state
+
+
+def _oracle_step_worker(n, npz, n_split, q):
+    """One bounded sample of the step on the host: one oracle step_dynamics
+    at C{n} L{npz}; returns (cell-levels, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import cases
+    import oracle_runs
+
+    case = cases.step_case(n, npz, 5, n_split)
+    t0 = time.perf_counter()
+    oracle_runs.run_step(case, n, npz)
+    q.put((6 * n * n * npz, time.perf_counter() - t0))
+
+
+def step_cpu_sample(n, npz, n_split):
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_oracle_step_worker, args=(n, npz, n_split, q))
+    p.start()
+    cells, sec = q.get()
+    p.join()
+    return {"value": cells / sec, "unit": "cell-levels/s (one dynamics step)", "cores": 1, "kind": "port",
+            "sample": f"one step_dynamics (n_split {n_split}) of C{n} L{npz}, numpy FP64 oracle on one core: "
+                      f"{sec:.1f} s"}
+
+
+def run_step_section(args, state0, grid384, local):
+    """BASELINE configurations of the whole dynamics step: the plain FP64
+    (and mixed) DynamicalCore.step_dynamics at C``step_n`` L79 — time per
+    step, roofline, the oracle step on the host — and the mixed build's
+    error against FP64 after 1 and ``error_steps`` steps at C384 L79."""
+    import torch
+
+    from fv3core_b200 import _lib
+    from fv3core_b200.grid import CubedSphereGrid
+    from fv3core_b200.initial_state import step_state
+
+    n, npz, n_split = args.step_n, args.npz, args.n_split
+    stream = torch.cuda.current_stream()
+    cells = 6 * n * n * npz
+    grid = CubedSphereGrid(n, 3)
+    st0 = step_state(grid, npz, seed=4321)
+    out = {"metric": f"C{n} L{npz} step_dynamics cell-levels/s", "unit": "cell-levels/s",
+           "config": {"workload": f"DynamicalCore.step_dynamics C{n} L{npz}, k_split 1, n_split {n_split}, "
+                                  "dt_atmos 225 s, nonhydrostatic, d_ext 0, nord 3, hord_tr 8, kord 9, 8 advected "
+                                  "tracers + qcld, no saturation adjustment (do_sat_adj not built)",
+                      "n": n, "npz": npz, "n_split": n_split, "cell_levels": cells,
+                      "reset": "every step restarts from the initial state (device copy outside the events)"}}
+    peak, peak_kind = _measured_peak()
+    for prec in ("f64", "f32"):
+        gd, core, state = step_problem(n, npz, n_split, prec, st0, grid)
+        initial = {k: v.clone() for k, v in state.items()}
+
+        def step():
+            core.step_dynamics(state, False, False, 225.0, st0["ptop"], n_split, st0["ks"])
+
+        def reset():
+            for k, v in initial.items():
+                state[k].copy_(v)
+
+        for _ in range(args.warmup):
+            reset()
+            step()
+        torch.cuda.synchronize()
+        launches0 = _lib.launch_count(prec)
+        events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(args.steps)]
+        with ClockSampler(local) as clk:
+            torch.cuda.synchronize()
+            torch.cuda.nvtx.range_push("step_timed_" + prec)
+            for a, b in events:
+                reset()
+                a.record(stream)
+                step()
+                b.record(stream)
+            torch.cuda.nvtx.range_pop()
+            torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in events) / args.steps
+        launches = (_lib.launch_count(prec) - launches0) // args.steps
+        width = 8 if prec == "f64" else 4
+        transfers = 34 * n_split + STEP_TRANSFERS_NON_ACOUSTIC
+        achieved = transfers * width * cells / (ms * 1e-3) / 1e9
+        h = 3
+        finite = all(bool(torch.isfinite(state[k][:, :npz, h:h + n, h:h + n]).all()) for k in
+                     ("u", "v", "w", "delp", "pt", "delz", "qvapor"))
+        r = {"value": cells / (ms * 1e-3), "ms_per_step": ms,
+             "cell_level_substeps_per_s": cells * n_split / (ms * 1e-3), "gpu_launches_per_step": launches,
+             "clocks": clk.summary(), "finite": finite,
+             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                          "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                          "scope": f"whole step: {transfers} compulsory field transfers of {width} B per "
+                                   "cell-level (34 per acoustic substep, 107 for the tracer advection, "
+                                   "remapping, preamble and epilogue)"}}
+        out["fp64" if prec == "f64" else "mixed"] = r
+        del initial, state, core
+        gd.close()
+    out["value"] = out["fp64"]["value"]
+    out["mixed_speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = step_cpu_sample(12, npz, n_split)
+
+    # mixed against FP64 after 1 and error_steps dynamics steps at C384 L79
+    if args.error_steps > 0 and state0 is not None:
+        ne = grid384.n
+        st384 = step_state(grid384, npz, base=state0)
+        snaps = {}
+        keep = ("delp", "pt", "delz", "u", "v", "w", "qvapor")
+        h = 3
+        for prec in ("f64", "f32"):
+            gd, core, state = step_problem(ne, npz, n_split, prec, st384, grid384)
+            for s in range(1, args.error_steps + 1):
+                core.step_dynamics(state, False, False, 225.0, st384["ptop"], n_split, st384["ks"])
+                if s in (1, args.error_steps):
+                    snaps[(prec, s)] = {k: state[k][:, :npz, h:h + ne, h:h + ne].double().cpu() for k in keep}
+            del state, core
+            gd.close()
+        del st384
+        err = {}
+        for s in sorted({1, args.error_steps}):
+            a64, a32 = snaps[("f64", s)], snaps[("f32", s)]
+            entry = {}
+            for k in keep:
+                d = (a32[k] - a64[k]).abs()
+                scale = a64[k].abs()
+                with torch.no_grad():
+                    rel = d / scale.clamp_min(1e-6 * float(scale.max()))
+                entry[k] = {"max_rel": float(rel.max()), "max_abs_over_max": float(d.max() / scale.max()),
+                            "rms_rel": float(torch.sqrt((d * d).mean() / (a64[k] * a64[k]).mean())),
+                            "finite": bool(torch.isfinite(a32[k]).all() and torch.isfinite(a64[k]).all())}
+            err[f"after_{s}_steps"] = entry
+        out["mixed_error_vs_fp64"] = {
+            "grid": f"C{ne} L{npz}", "n_split": n_split, "per_field": err,
+            "metric": "max over the compute domain of |mixed - fp64| / max(|fp64|, 1e-6 max|fp64|) (max_rel; "
+                      "points near zero dominate it for the winds and the tracers), of |mixed - fp64| / max|fp64| "
+                      "(max_abs_over_max), and the RMS difference over the RMS of the FP64 field; both runs from "
+                      "the same baroclinic-wave state",
+        }
+    return out
 
 
 # ----------------------------------------------------------------------------- CPU oracle
@@ -803,6 +982,10 @@ def main():
     ap.add_argument("--ref-n", type=int, default=24, help="resolution of the reference arm's per-worker sample")
     ap.add_argument("--ref-max-workers", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--step-n", type=int, default=128,
+                    help="resolution of the full-step measurement (0: skip the step section)")
+    ap.add_argument("--error-steps", type=int, default=10,
+                    help="dynamics steps of the mixed-vs-FP64 comparison at the headline resolution (0: skip)")
     ap.add_argument("--workload", choices=["acoustics", "ensemble", "adjoint"], default="acoustics",
                     help="ensemble: the mixed-resolution ensemble with CUDA-graph steps; adjoint: the "
                          "RiemannSolver3 adjoint's cost")

@@ -112,6 +112,8 @@ def baroclinic_state(grid: CubedSphereGrid, nz, seed=0, noise=1.0e-3, ntracers=4
         out[..., : a3.shape[-1]] = a3
         return out
 
+    for name, q_ in (("qvapor", qv), ("qliquid", ql), ("qrain", qr), ("qice", qi)):
+        st[name] = full(q_)
     st["delp"] = full(delp)
     st["pt"] = full(pt)
     st["delz"] = full(delz)
@@ -155,7 +157,8 @@ def baroclinic_state(grid: CubedSphereGrid, nz, seed=0, noise=1.0e-3, ntracers=4
     st["ks"] = int(ks)
     # ---- make halos consistent with the neighbouring tiles
     tc = scalar_table(n, h, 1, 1, h)
-    for name in ("delp", "pt", "delz", "q_con", "cappa", "pkz", "pe", "peln", "pk"):
+    for name in ("delp", "pt", "delz", "q_con", "cappa", "pkz", "pe", "peln", "pk", "qvapor", "qliquid", "qrain",
+                 "qice"):
         apply_scalar_table(st[name], tc)
     apply_scalar_table(st["phis"], tc)
     apply_vector_tables(st["u"], st["v"], vector_tables(n, h, (1, 0), (0, 1), h))
@@ -181,4 +184,26 @@ def resting_state(grid: CubedSphereGrid, nz, temperature=280.0):
         st[name][..., :nz] = col
     for name in ("u", "v", "w", "phis"):
         st[name][...] = 0.0
+    return st
+
+
+STEP_TRACERS = ("qvapor", "qliquid", "qrain", "qice", "qsnow", "qgraupel", "qo3mr", "qsgs_tke", "qcld")
+
+
+def step_state(grid: CubedSphereGrid, nz, seed=0, noise=1.0e-3, base=None):
+    """The baroclinic-wave state in the form DynamicalCore.step_dynamics
+    takes it: ``baroclinic_state`` with its four seeded water species, the
+    other species and the cloud fraction at zero, pt back as temperature
+    (the step's preamble converts it, fv_dynamics.py:32-34, whose inverse is
+    applied here) and the surface pressure ps."""
+    st = baroclinic_state(grid, nz, seed=seed, noise=noise)
+    shape3 = st["delp"].shape
+    for name in STEP_TRACERS:
+        if name not in st:
+            st[name] = np.zeros(shape3)
+    dp1 = C.ZVIR * st["qvapor"]
+    with np.errstate(all="ignore"):
+        t = st["pt"] * st["pkz"] / ((1.0 + dp1) * (1.0 - st["q_con"]))
+    st["pt"] = np.where(np.isfinite(t), t, 0.0)
+    st["ps"] = np.array(st["pe"][..., nz], copy=True)
     return st
