@@ -288,7 +288,7 @@ def run_cuda(args):
     # perturbations of relative size eps, and what the carry-over alone does
     # (a second FP64 call from the same state).
     mixed_error = None
-    if len(precisions) == 2:
+    if len(precisions) == 2 and not args.no_error_analysis:
         fields = ("delp", "pt", "delz", "q_con")
         s32, s64 = problems["f32"][2], problems["f64"][2]
         problems["f32"][1](s32)
@@ -982,6 +982,8 @@ def main():
     ap.add_argument("--ref-n", type=int, default=24, help="resolution of the reference arm's per-worker sample")
     ap.add_argument("--ref-max-workers", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-error-analysis", action="store_true",
+                    help="skip the mixed-vs-FP64 error analysis of the acoustic call")
     ap.add_argument("--step-n", type=int, default=128,
                     help="resolution of the full-step measurement (0: skip the step section)")
     ap.add_argument("--error-steps", type=int, default=10,

@@ -58,6 +58,49 @@ cudaError_t launch_box(const Box& b, cudaStream_t s, F f) {
   return cudaGetLastError();
 }
 
+// A box launch whose thread order along i puts the columns [a0, a1) first,
+// padded to a whole number of thread-block rows, and the box's other
+// columns after them.  Stencils whose edge columns take a longer code path
+// (the PPM boundary formulas, the cube-corner reads) then keep those
+// columns out of the warps that run the interior path; every point still
+// computes what it computes under launch_box.
+template <typename F>
+__global__ void box_kernel_split(Box b, int a0, int nint, int nint_pad, F f) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = b.j0 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int nkb = b.k1 - b.k0;
+  const int t = blockIdx.z / nkb;
+  const int k = b.k0 + blockIdx.z % nkb;
+  int i;
+  if (x < nint_pad) {
+    if (x >= nint) return;
+    i = a0 + x;
+  } else {
+    const int e = x - nint_pad, nleft = a0 - b.i0;
+    i = e < nleft ? b.i0 + e : a0 + nint + (e - nleft);
+    if (i >= b.i1) return;
+  }
+  if (j < b.j1) f(t, i, j, k);
+}
+
+template <typename F>
+cudaError_t launch_box_split(const Box& b, int a0, int a1, cudaStream_t s, F f) {
+  int ni = b.i1 - b.i0, nj = b.j1 - b.j0, nk = b.k1 - b.k0;
+  if (ni <= 0 || nj <= 0 || nk <= 0) return cudaSuccess;
+  a0 = a0 < b.i0 ? b.i0 : a0;
+  a1 = a1 > b.i1 ? b.i1 : a1;
+  if (a1 <= a0) return launch_box(b, s, f);
+  const LaunchShape& ls = launch_shape();
+  const int nint = a1 - a0;
+  const int nint_pad = (nint + ls.box_x - 1) / ls.box_x * ls.box_x;
+  const int nx = nint_pad + (ni - nint);
+  dim3 block(ls.box_x, ls.box_y, 1);
+  dim3 grid((nx + ls.box_x - 1) / ls.box_x, (nj + ls.box_y - 1) / ls.box_y, 6 * nk);
+  box_kernel_split<<<grid, block, 0, s>>>(b, a0, nint, nint_pad, f);
+  note_launch();
+  return cudaGetLastError();
+}
+
 // Launch f(t, i, j) over the columns of a 2-D box (all six tiles).
 template <typename F>
 __global__ void column_kernel(int i0, int i1, int j0, int j1, F f) {

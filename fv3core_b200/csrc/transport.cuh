@@ -279,12 +279,16 @@ inline cudaError_t fvtp2d_impl(const Dims d, const fv3b_metrics g, const FvTp2dA
   const int full = d.ni - 1;
   const int mord = a.hord < 0 ? -a.hord : a.hord;
   cudaError_t err;
-  // inner PPM: fy_mean on [is-3, ie+4] x [js, je+1], fx_mean on [is, ie+1] x [js-3, je+4]
-  err = launch_box(Box{s - 3, e + 5, js - 3, je + 5, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
+  // inner PPM: fy_mean on [is-3, ie+4] x [js, je+1], fx_mean on [is, ie+1] x [js-3, je+4];
+  // columns [is+3, ie-2] (both fluxes on the interior path) in warps of their own
+  err = launch_box_split(Box{s - 3, e + 5, js - 3, je + 5, 0, nk}, s + 3, e - 1, st,
+                         [=] __device__(int t, int i, int j, int k) {
     const idx_t o = idx3(d, t, i, j, k);
     if (j >= js && j < je + 2) {
       auto dya = line2<1>(d, g.dya, t, i, j);
-      if (i >= s && i <= e) {  // no cube-corner point on this line: plain reads
+      // the line reads rows j-3 .. j+2; a read can fall in a cube-corner
+      // block only from a halo column within three rows of a tile edge
+      if ((i >= s && i <= e) || (j >= js + 3 && j <= je - 2)) {  // plain reads
         a.fy_mean[o] = ppm_flux_ord<ORD8>(line3<1>(d, a.q_base, t, i, j, k), dya, a.cry[o], j, js, je, mord);
       } else {
         a.fy_mean[o] = ppm_flux_ord<ORD8>(LineQY{d, a.q_base, t, i, j, k}, dya, a.cry[o], j, js, je, mord);
@@ -315,8 +319,10 @@ inline cudaError_t fvtp2d_impl(const Dims d, const fv3b_metrics g, const FvTp2dA
     }
   });
   if (err != cudaSuccess) return err;
-  // outer PPM and final_fluxes (fvtp2d.py:63-93) on [is, ie+1] x [js, je+1]
-  return launch_box(Box{s, e + 2, js, je + 2, 0, nk}, st, [=] __device__(int t, int i, int j, int k) {
+  // outer PPM and final_fluxes (fvtp2d.py:63-93) on [is, ie+1] x [js, je+1],
+  // the interior-path columns [is+3, ie-2] in warps of their own
+  return launch_box_split(Box{s, e + 2, js, je + 2, 0, nk}, s + 3, e - 1, st,
+                          [=] __device__(int t, int i, int j, int k) {
     const idx_t o = idx3(d, t, i, j, k);
     if (j <= je) {
       real xo = ppm_flux_ord<ORD8>(line3<0>(d, a.q_adv_y, t, i, j, k), line2<0>(d, g.dxa, t, i, j), a.crx[o], i, s,
