@@ -78,7 +78,7 @@ CTX_SIGNATURES = {
     "fv3b_cubed_to_latlon": [P] * 8 + [ctypes.c_int, P],
     "fv3b_transport_create": [ctypes.c_int, P, P, ctypes.c_int, P],
     "fv3b_remap_setup": [P, P],
-    "fv3b_lagrangian_to_eulerian": [P, P, D, D, D, ctypes.c_int, P],
+    "fv3b_lagrangian_to_eulerian": [P, P, P, D, D, D, D, ctypes.c_int, ctypes.c_int, P],
 }
 
 # entry points whose first argument is a transport object (fv3b_transport*),
@@ -129,7 +129,18 @@ class RemapConfig(ctypes.Structure):
 
 
 class RemapFields(ctypes.Structure):
-    _fields_ = [("tracers", P * 8)] + [(n, P) for n in REMAP_FIELDS] + [("wsd", P)]
+    _fields_ = [("tracers", P * 8)] + [(n, P) for n in REMAP_FIELDS] + [("wsd", P), ("qcld", P), ("dp1", P),
+                                                                          ("hs", P)]
+
+
+SAT_ADJUST_DOUBLES = ("sat_adj0", "ql_gen", "qs_mlt", "ql0_max", "t_sub", "qi_gen", "qi_lim", "qi0_max", "dw_ocean",
+                      "dw_land", "cld_min", "tau_i2s", "tau_v2l", "tau_r2g", "tau_l2r", "tau_l2v", "tau_imlt",
+                      "tau_smlt")
+SAT_ADJUST_INTS = ("icloud_f", "rad_snow", "rad_rain", "rad_graupel", "tintqs", "hydrostatic")
+
+
+class SatAdjustConfig(ctypes.Structure):
+    _fields_ = [(n, D) for n in SAT_ADJUST_DOUBLES] + [(n, I32) for n in SAT_ADJUST_INTS]
 
 
 def lib(precision="f64"):

@@ -290,13 +290,13 @@ class DynamicalCoreConfig:
                                kord_mt=self.kord_mt, do_sat_adj=self.do_sat_adj, sat_adjust=self.sat_adjust)
 
 
-def baroclinic_config(npx, npz, n_split=6, dt_atmos=225, k_split=1):
+def baroclinic_config(npx, npz, n_split=6, dt_atmos=225, k_split=1, do_sat_adj=True):
     """The DynamicalCoreConfig of the reference's baroclinic-wave example
     (examples/wrapped/config/baroclinic.yml) on a C``npx`` L``npz`` grid,
-    with the fast saturation adjustment off (do_sat_adj, not built here)."""
+    the fast saturation adjustment on as there."""
     return DynamicalCoreConfig(
         dt_atmos=dt_atmos, a_imp=1.0, beta=0.0, consv_te=False, d2_bg=0.0, d2_bg_k1=0.2, d2_bg_k2=0.1,
-        d4_bg=0.15, d_con=1.0, d_ext=0.0, dddmp=0.5, delt_max=0.002, do_sat_adj=False, do_vort_damp=True,
+        d4_bg=0.15, d_con=1.0, d_ext=0.0, dddmp=0.5, delt_max=0.002, do_sat_adj=do_sat_adj, do_vort_damp=True,
         fill=True, hord_dp=6, hord_mt=6, hord_tm=6, hord_tr=8, hord_vt=6, hydrostatic=False, k_split=k_split,
         ke_bg=0.0, kord_mt=9, kord_tm=-9, kord_tr=9, kord_wz=9, n_split=n_split, nord=3, npx=npx + 1,
         npy=npx + 1, npz=npz, ntiles=6, nwat=6, p_fac=0.05, rf_cutoff=3000.0, tau=10.0, vtdm4=0.06,

@@ -84,8 +84,10 @@ extern "C" int fv3b_c_sw(fv3b_ctx* ctx, real* delp, real* pt, const real* u, con
     if (corner_x(d, i, j, true, -RC(1.0), RC(1.0), RC(1.0), -RC(1.0), r)) W3(utmp, i, j) = r.mult * F3(vtmp, i + r.di, j + r.dj);
     if (corner_x(d, i, j, false, -RC(1.0), RC(1.0), RC(1.0), -RC(1.0), r)) W3(ua, i, j) = r.mult * F3(va, i + r.di, j + r.dj);
   }));
-  // ut_main + east_west_edges (d2a2c_vect.py:45-93, 263-273)
-  FV3B_CHECK(launch_box(Box{s - 3, e + 4, js - 1, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+  // ut_main + east_west_edges (d2a2c_vect.py:45-93, 263-273); the ut_main
+  // columns in warps of their own
+  FV3B_CHECK(launch_box_split(Box{s - 3, e + 4, js - 1, je + 2, 0, nz}, s + 2, e, st,
+                              [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
     real cu = F2(g.cosa_u, i, j), ru = F2(g.rsin_u, i, j);
     if (i >= s + 2 && i <= e - 1) {

@@ -551,7 +551,9 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, real* delpc, real* delp, real* ptc, real
   // kinetic_energy_update_part_1 + part_2 (d_sw.py:198-246, 566-603; xtp_u.py, ytp_v.py)
   {
     const int mord = cfg.hord_mt < 0 ? -cfg.hord_mt : cfg.hord_mt;
-    FV3B_CHECK(launch_box(Box{s, e + 2, js, je + 2, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+    // the columns whose x-advection takes the interior PPM path in warps of their own
+    FV3B_CHECK(launch_box_split(Box{s, e + 2, js, je + 2, 0, nz}, s + 3, e - 1, st,
+                                [=] __device__(int t, int i, int j, int k) {
       PT_SETUP(d, t, k);
       real ub_cov = RC(0.5) * (F3(uc, i, j - 1) + F3(uc, i, j));
       real vb_cov = RC(0.5) * (F3(vc, i - 1, j) + F3(vc, i, j));

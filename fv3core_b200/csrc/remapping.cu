@@ -19,7 +19,8 @@
 //   3. each tracer remapped (kord_tr, the sixth kord 9, iv 0), then fillz;
 //   4. w (kord_wz, iv -2, bottom value wsd);
 //   5. delz (kord_wz, iv 1), then delz = -delz dp2;
-//   6. moist pkz, then the last-step pt conversion (or pt / pkz);
+//   6. moist pkz, then (do_sat_adj) the fast saturation adjustment on levels
+//      [kmp, npz), then the last-step pt conversion (or pt / pkz);
 //   7. u on pressures averaged to the D-grid y faces (kord_mt, iv -1);
 //   8. v on pressures averaged to the x faces;
 //   9. update_ua and copy_from_below (ua, the interior pe).
@@ -32,6 +33,7 @@
 
 #include "ctx.cuh"
 #include "fmath.h"
+#include "sat_adjust.cuh"
 #include "stencil.cuh"
 
 using namespace fv3b;
@@ -678,8 +680,9 @@ extern "C" int fv3b_remap_setup(fv3b_ctx* ctx, const double* ak, const double* b
 }
 
 extern "C" int fv3b_lagrangian_to_eulerian(fv3b_ctx* ctx, const fv3b_remap_fields* fields,
-                                           const fv3b_remap_config* config, double ptop, double akap,
-                                           double zvir, int last_step, void* stream) {
+                                           const fv3b_remap_config* config, const fv3b_sat_adjust_config* sat,
+                                           double ptop, double akap, double zvir, double mdt, int kmp,
+                                           int last_step, void* stream) {
   FV3B_REQUIRE(ctx && fields && config, "fv3b_lagrangian_to_eulerian: null argument");
   const fv3b_remap_fields& f = *fields;
   for (int n = 0; n < NTRACER; ++n) FV3B_REQUIRE(f.tracers[n], "fv3b_lagrangian_to_eulerian: null tracer");
@@ -693,6 +696,12 @@ extern "C" int fv3b_lagrangian_to_eulerian(fv3b_ctx* ctx, const fv3b_remap_field
                    kord_ok(config->kord_mt),
                "fv3b_lagrangian_to_eulerian: |kord| must be in 1..10");
   FV3B_REQUIRE(ctx->d.nz >= 5, "fv3b_lagrangian_to_eulerian: need npz >= 5");
+  if (sat) {
+    FV3B_REQUIRE(f.qcld && f.hs, "fv3b_lagrangian_to_eulerian: the saturation adjustment needs qcld and hs");
+    FV3B_REQUIRE(!sat->hydrostatic, "fv3b_lagrangian_to_eulerian: hydrostatic is not implemented");
+    FV3B_REQUIRE(kmp >= 0 && kmp < ctx->d.nz, "fv3b_lagrangian_to_eulerian: kmp out of range");
+    FV3B_REQUIRE(mdt > 0.0, "fv3b_lagrangian_to_eulerian: mdt must be positive");
+  }
   const Dims d = ctx->d;
   cudaStream_t st = (cudaStream_t)stream;
   RemapArgs a;
@@ -745,11 +754,80 @@ extern "C" int fv3b_lagrangian_to_eulerian(fv3b_ctx* ctx, const fv3b_remap_field
   FV3B_CHECK(launch_remap<MapW>(a, s, e + 1, js, je + 1, st));
   FV3B_CHECK(launch_remap<MapDelz>(a, s, e + 1, js, je + 1, st));
   // 6. moist_cv_pkz (moist_cv.py:171-194), then moist_pt_last_step (139-162,
-  // levels 0..npz, dtmp 0) or adjust_divide_stencil
+  // levels 0..npz, dtmp 0) or adjust_divide_stencil; with the saturation
+  // adjustment between them, three launches instead of one
+  const bool do_sat = sat != nullptr;
+  if (do_sat) {
+    FV3B_CHECK(launch_box(Box{s, e + 1, js, je + 1, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
+      PT_SETUP(d, t, k);
+      const real qvk = F3(qv, i, j);
+      const real ql = F3(qlq, i, j) + F3(qr, i, j);
+      const real qs = F3(qi, i, j) + F3(qsn, i, j) + F3(qg, i, j);
+      const real gz = ql + qs;
+      const real cvm = (RC(1.0) - (qvk + gz)) * cv_air + qvk * cv_vap + ql * c_liq + qs * c_ice;
+      W3(f.q_con, i, j) = gz;
+      const real cappa = rdgas / (rdgas + cvm / (RC(1.0) + zv * qvk));
+      W3(f.cappa, i, j) = cappa;
+      W3(f.pkz, i, j) = static_cast<real>(
+          fm::fm_exp(cappa * fm::fm_log(rdg * F3(f.delp, i, j) / F3(f.delz, i, j) * F3(f.pt, i, j))));
+    }));
+    // SatAdjust3d.__call__ (saturation_adjustment.py:970-1024): the per-call
+    // factors on the host, with the C library's exp (as Python's math.exp)
+    satadj::Params prm;
+    prm.cfg = *sat;
+    prm.mdt = mdt;
+    prm.sdt = 0.5 * mdt;
+    prm.zvir = zvir;
+    prm.fac_i2s = 1.0 - exp(-mdt / sat->tau_i2s);
+    prm.fac_v2l = 1.0 - exp(-prm.sdt / sat->tau_v2l);
+    prm.fac_r2g = 1.0 - exp(-mdt / sat->tau_r2g);
+    prm.fac_l2r = 1.0 - exp(-mdt / sat->tau_l2r);
+    const double fac_l2v = 1.0 - exp(-prm.sdt / sat->tau_l2v);
+    prm.fac_l2v = fac_l2v < sat->sat_adj0 ? fac_l2v : sat->sat_adj0;
+    prm.fac_imlt = 1.0 - exp(-prm.sdt / sat->tau_imlt);
+    prm.fac_smlt = 1.0 - exp(-mdt / sat->tau_smlt);
+    prm.c_air = CV_AIR_D;
+    prm.c_vap = CV_VAP_D;
+    prm.d0_vap = prm.c_vap - C_LIQ_D;
+    prm.lv00 = satadj::HLV - prm.d0_vap * satadj::TICE;
+    prm.last_step = last_step;
+    const real* area = ctx->m.area;
+    FV3B_CHECK(launch_box(Box{s, e + 1, js, je + 1, kmp, nz}, st, [=] __device__(int t, int i, int j, int k) {
+      const idx_t o = idx3(d, t, i, j, k), o2 = idx2(d, t, i, j);
+      satadj::Point P;
+      P.qv = qv[o];
+      P.ql = qlq[o];
+      P.qi = qi[o];
+      P.qr = qr[o];
+      P.qs = qsn[o];
+      P.qg = qg[o];
+      P.cappa = f.cappa[o];
+      P.pt = f.pt[o];
+      P.dp = f.delp[o];
+      P.delz = f.delz[o];
+      P.qa = f.qcld[o];
+      P.area = area[o2];
+      P.hs = f.hs[o2];
+      P.pkz = f.pkz[o];
+      P.q_con = f.q_con[o];
+      satadj::sat_adjust_point(P, prm);
+      qv[o] = static_cast<real>(P.qv);
+      qlq[o] = static_cast<real>(P.ql);
+      qi[o] = static_cast<real>(P.qi);
+      qr[o] = static_cast<real>(P.qr);
+      qsn[o] = static_cast<real>(P.qs);
+      qg[o] = static_cast<real>(P.qg);
+      f.cappa[o] = static_cast<real>(P.cappa);
+      f.pt[o] = static_cast<real>(P.pt);
+      f.q_con[o] = static_cast<real>(P.q_con);
+      f.qcld[o] = static_cast<real>(P.qa);
+      f.pkz[o] = static_cast<real>(P.pkz);
+    }));
+  }
   FV3B_CHECK(launch_box(Box{s, e + 1, js, je + 1, 0, nz + 1}, st, [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
     const real qvk = F3(qv, i, j);
-    if (k < nz) {
+    if (k < nz && !do_sat) {
       const real ql = F3(qlq, i, j) + F3(qr, i, j);
       const real qs = F3(qi, i, j) + F3(qsn, i, j) + F3(qg, i, j);
       const real gz = ql + qs;

@@ -14,10 +14,11 @@ CONSV_MIN = 0.001  # remapping.py:30
 class LagrangianToEulerian:
     """Fortran Lagrangian_to_Eulerian (remapping.py:205-628).
 
-    ``config`` is a RemappingConfig; ``area_64`` and ``pfull`` are taken as
-    the reference takes them (the saturation adjustment, the only user of
-    area_64 and of the pfull-derived kmp, is not built: do_sat_adj is
-    rejected).  Rejects what the reference rejects: kord_tm >= 0 and
+    ``config`` is a RemappingConfig; with do_sat_adj the fast saturation
+    adjustment runs after the remaps on the levels from kmp (the first
+    level whose reference pressure ``pfull`` exceeds 10 hPa) down, with the
+    grid's cell areas (``area_64`` is taken for the signature; the context
+    holds the areas).  Rejects what the reference rejects: kord_tm >= 0 and
     hydrostatic."""
 
     def __init__(self, stencil_factory, config, area_64, nq, pfull):
@@ -25,8 +26,6 @@ class LagrangianToEulerian:
             raise NotImplementedError("map ppm, untested mode where kord_tm >= 0")
         if config.hydrostatic:
             raise NotImplementedError("Hydrostatic is not implemented")
-        if config.do_sat_adj:
-            raise NotImplementedError("the fast saturation adjustment (do_sat_adj=True) is not built")
         for name in ("kord_tm", "kord_tr", "kord_wz", "kord_mt"):
             if abs(getattr(config, name)) > 10:
                 raise AssertionError(f"kord {getattr(config, name)} not implemented.")
@@ -43,6 +42,11 @@ class LagrangianToEulerian:
         self._config = _lib.RemapConfig(int(config.kord_tm), int(config.kord_tr), int(config.kord_wz),
                                         int(config.kord_mt), int(bool(config.fill)), 0)
         self._akbk = None
+        self._sat = None
+        if config.do_sat_adj:
+            sa = config.sat_adjust
+            self._sat = _lib.SatAdjustConfig(*([float(getattr(sa, n)) for n in _lib.SAT_ADJUST_DOUBLES]
+                                               + [int(getattr(sa, n)) for n in _lib.SAT_ADJUST_INTS]))
         # kmp (remapping.py:396-400): the first level below 10 hPa
         self.kmp = npz - 1
         for k in range(self._pfull.shape[0]):
@@ -65,10 +69,10 @@ class LagrangianToEulerian:
         """remapping.py:416-628.  ``tracers`` maps the tracer names
         (qvapor, qliquid, qrain, qice, qsnow, qgraupel, qo3mr, qsgs_tke) to
         device fields; every other field is a device field in the library's
-        layout (hs, te0_2d, ps, wsd 2-D).  q_cld, hs, te0_2d, omga, dp1,
-        mdt and bdt feed only the saturation adjustment and the omega
-        remap, neither of which runs (as in the reference with do_sat_adj
-        false)."""
+        layout (hs, te0_2d, ps, wsd 2-D).  q_cld, hs, dp1 and mdt feed the
+        saturation adjustment (do_sat_adj); te0_2d, omga and bdt only the
+        total-energy fixer and the omega remap, which the reference does not
+        run either (consv_te 0, do_omega off)."""
         if last_step and not do_adiabatic_init:
             if consv_te > CONSV_MIN:
                 raise NotImplementedError("We do not support consv_te > 0.001 because that would trigger an "
@@ -89,5 +93,12 @@ class LagrangianToEulerian:
             setattr(f, name, check_field(t, gi, "3d", name))
         f.ps = check_field(ps, gi, "2d", "ps")
         f.wsd = check_field(wsd, gi, "2d", "wsd")
+        sat = None
+        if self._sat is not None:
+            f.qcld = check_field(q_cld, gi, "3d", "q_cld")
+            f.dp1 = check_field(dp1, gi, "3d", "dp1")
+            f.hs = check_field(hs, gi, "2d", "hs")
+            sat = ctypes.addressof(self._sat)
         _lib.call_ctx("fv3b_lagrangian_to_eulerian", self._ctx, ctypes.addressof(f), ctypes.addressof(self._config),
-                      float(ptop), float(akap), float(zvir), int(bool(last_step)), stream_ptr())
+                      sat, float(ptop), float(akap), float(zvir), float(mdt), int(self.kmp), int(bool(last_step)),
+                      stream_ptr())

@@ -550,20 +550,39 @@ typedef struct fv3b_remap_fields {
   fv3b_real* tracers[8];
   fv3b_real *pt, *delp, *delz, *peln, *u, *v, *w, *ua, *va, *cappa, *q_con, *pkz, *pk, *pe, *ps;
   const fv3b_real* wsd;
+  /* read only by the saturation adjustment: the cloud fraction (written),
+   * dp1 (the reference passes it as the total-energy field) and the surface
+   * geopotential hs (2-D) */
+  fv3b_real *qcld, *dp1;
+  const fv3b_real* hs;
 } fv3b_remap_fields;
 
 /*
- * LagrangianToEulerian.__call__ (fv3core/stencils/remapping.py:416-628)
- * with do_sat_adj false: moist pt and the delz adjustment, the Eulerian
- * pressures ak + bk ps, the PPM remapping (remap_profile.py cs_profile,
- * map_single.py) of pt in log pressure, of the tracers (then fillz) and of
- * w, delz, u and v, moist pkz, and the last-step pt conversion (last_step 1)
- * or the division by pkz (last_step 0).  One thread per column; the column
- * work arrays and the arithmetic are FP64 in both builds.  Requires
+ * SatAdjustConfig (fv3core/_config.py:85-110): the fast saturation
+ * adjustment's namelist.  Flags are 0/1; hydrostatic must be 0.
+ */
+typedef struct fv3b_sat_adjust_config {
+  double sat_adj0, ql_gen, qs_mlt, ql0_max, t_sub, qi_gen, qi_lim, qi0_max, dw_ocean, dw_land, cld_min;
+  double tau_i2s, tau_v2l, tau_r2g, tau_l2r, tau_l2v, tau_imlt, tau_smlt;
+  int32_t icloud_f, rad_snow, rad_rain, rad_graupel, tintqs, hydrostatic;
+} fv3b_sat_adjust_config;
+
+/*
+ * LagrangianToEulerian.__call__ (fv3core/stencils/remapping.py:416-628):
+ * moist pt and the delz adjustment, the Eulerian pressures ak + bk ps, the
+ * PPM remapping (remap_profile.py cs_profile, map_single.py) of pt in log
+ * pressure, of the tracers (then fillz) and of w, delz, u and v, moist pkz,
+ * the fast saturation adjustment when ``sat`` is not NULL (do_sat_adj;
+ * SatAdjust3d, saturation_adjustment.py:544-1024, on levels [kmp, npz),
+ * remapping time step mdt, without the total-energy fixer: consv_te 0),
+ * and the last-step pt conversion (last_step 1) or the division by pkz
+ * (last_step 0).  The remaps run one thread per column, the adjustment one
+ * thread per point; both compute in FP64 in both builds.  Requires
  * fv3b_remap_setup.
  */
 int fv3b_lagrangian_to_eulerian(fv3b_ctx* ctx, const fv3b_remap_fields* fields, const fv3b_remap_config* config,
-                                double ptop, double akap, double zvir, int last_step, void* stream);
+                                const fv3b_sat_adjust_config* sat, double ptop, double akap, double zvir,
+                                double mdt, int kmp, int last_step, void* stream);
 
 /* Device pointer of one of the substep temporaries by its reference name
  * ("gz", "zh", "pkc", "pk3", "ut", "vt", "divgd", "heat_source", "crx",

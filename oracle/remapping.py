@@ -457,15 +457,27 @@ def _set_cappa(qv, cvm, r_vir):
     return C.RDGAS / (C.RDGAS + cvm / (1.0 + r_vir * qv))
 
 
+def kmp_of(pfull, npz):
+    """The saturation adjustment's top level (remapping.py:396-400): the
+    first level whose reference pressure exceeds 10 hPa."""
+    for k in range(len(pfull)):
+        if pfull[k] > 10.0e2:
+            return k
+    return npz - 1
+
+
 def lagrangian_to_eulerian(t: Tile, tracers, st, ak, bk, ptop, akap, zvir, last_step, kord_tm=-9, kord_tr=9,
-                           kord_wz=9, kord_mt=9, fill=True):
+                           kord_wz=9, kord_mt=9, fill=True, sat_adjust=None):
     """LagrangianToEulerian.__call__ (remapping.py:416-628) on one tile,
     without the saturation adjustment (do_sat_adj False).  ``tracers`` maps
     the eight remapped tracer names, in the reference's order
     (qvapor, qliquid, qrain, qice, qsnow, qgraupel, qo3mr, qsgs_tke), to
     their storages; ``st`` holds pt, delp, delz, peln, u, v, w, ua, va,
     cappa, q_con, pkz, pk, pe, ps (2-D) and wsd (2-D).  Every field is
-    updated in place."""
+    updated in place.  ``sat_adjust`` (do_sat_adj): a dict with the
+    SatAdjustConfig values (``cfg``), ``area``, ``hs`` (2-D), ``dp1``,
+    ``qcld``, ``pfull`` and ``mdt``; the adjustment then runs after the
+    remaps (remapping.py:570-589), with no total-energy fixer (consv_te 0)."""
     nz = t.nz
     s, e, js, je = t.isc, t.iec, t.jsc, t.jec
     pe = st["pe"]
@@ -562,6 +574,16 @@ def lagrangian_to_eulerian(t: Tile, tracers, st, ak, bk, ptop, akap, zvir, last_
         ua[I, je + 1, 0:nz - 1] = pe2[I, je, 1:nz]
         # copy_from_below (194-196): pe[k] = ua[k - 1] on the compute domain
         pe[I, J, 1:nz] = ua[I, J, 0:nz - 1]
+        if sat_adjust is not None:
+            from .sat_adjust import sat_adjust_3d
+
+            sa = sat_adjust
+            fields = {"te": sa["dp1"], "qvapor": q["qvapor"], "qliquid": q["qliquid"], "qice": q["qice"],
+                      "qrain": q["qrain"], "qsnow": q["qsnow"], "qgraupel": q["qgraupel"], "qcld": sa["qcld"],
+                      "peln": peln, "delp": delp, "delz": delz, "q_con": st["q_con"], "pt": pt, "pkz": st["pkz"],
+                      "cappa": st["cappa"]}
+            sat_adjust_3d(t, fields, sa["cfg"], sa["area"], sa["hs"], zvir, sa["mdt"], False, last_step,
+                          kmp_of(sa["pfull"], nz))
         if last_step:
             # moist_pt_last_step (moist_cv.py:139-162), dtmp = 0, levels 0..npz
             Kx = slice(0, nz + 1)

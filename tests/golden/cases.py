@@ -316,7 +316,7 @@ REMAP_STATE = ("pt", "delp", "delz", "peln", "u", "v", "w", "ua", "va", "cappa",
                "ps", "te0_2d", "wsd")
 
 
-def remap_case(n=12, nz=8, seed=81, kord=(-9, 9, 9, 9)):
+def remap_case(n=12, nz=8, seed=81, kord=(-9, 9, 9, 9), sat_adj=False):
     """Inputs of LagrangianToEulerian: the baroclinic-wave state whose layer
     thicknesses are perturbed by a seeded factor in [0.7, 1.3] at every
     point (halo included), so that the Lagrangian surfaces pe (ptop plus the
@@ -326,7 +326,8 @@ def remap_case(n=12, nz=8, seed=81, kord=(-9, 9, 9, 9)):
     [0, 1e-3), of which a seeded 3 % of the points are negative (down to
     -1e-4) so that the negative-value filling acts; w and the bottom w
     boundary wsd are seeded noise.  ``kord`` gives (kord_tm, kord_tr,
-    kord_wz, kord_mt)."""
+    kord_wz, kord_mt); ``sat_adj`` turns on the fast saturation adjustment
+    (cloud fraction qcld then seeded in [0, 1))."""
     st = base_state(n, nz, seed)
     rng = np.random.default_rng(seed + 1000)
     shp = st["delp"].shape
@@ -357,26 +358,30 @@ def remap_case(n=12, nz=8, seed=81, kord=(-9, 9, 9, 9)):
         q = np.where(neg, -rng.uniform(0.0, 1.0e-4, shp), q)
         q[..., nz] = 0.0
         case[name] = q
-    case["qcld"] = np.zeros(shp)
+    case["qcld"] = rng.uniform(0.0, 1.0, shp) if sat_adj else np.zeros(shp)
     case["dp1"] = np.zeros(shp)
     case["omga"] = np.zeros(shp)
     case["ak"], case["bk"], case["pfull"] = st["ak"], st["bk"], st["pfull"]
     case["ptop"] = ptop
     case["mdt"] = 225.0
     case["kord"] = np.array(kord)
+    case["do_sat_adj"] = np.array(bool(sat_adj))
     return case
 
 
 def remap_config(case):
     """The remapping namelist of a remap case (its kord values)."""
     kord_tm, kord_tr, kord_wz, kord_mt = (int(x) for x in case["kord"])
-    return dict(REMAP_CONFIG, kord_tm=kord_tm, kord_tr=kord_tr, kord_wz=kord_wz, kord_mt=kord_mt)
+    return dict(REMAP_CONFIG, kord_tm=kord_tm, kord_tr=kord_tr, kord_wz=kord_wz, kord_mt=kord_mt,
+                do_sat_adj=bool(case.get("do_sat_adj", False)))
 
 
 CASES["remap"] = remap_case
 # the profile's other limiters: kord 10 (ext5 / ext6 tests) and kord 8
 CASES["remap_kord10"] = functools.partial(remap_case, kord=(-10, 10, 10, 10))
 CASES["remap_kord8"] = functools.partial(remap_case, kord=(-8, 8, 8, 8))
+# the baroclinic namelist's remapping with the fast saturation adjustment
+CASES["remap_satadj"] = functools.partial(remap_case, sat_adj=True)
 
 
 # the water species and tracers of DynamicalCore's state: the eight it
@@ -384,14 +389,15 @@ CASES["remap_kord8"] = functools.partial(remap_case, kord=(-8, 8, 8, 8))
 STEP_TRACERS = REMAP_TRACERS + ("qcld",)
 
 
-def step_case(n=12, nz=12, seed=101, n_split=2):
+def step_case(n=12, nz=12, seed=101, n_split=2, sat_adj=False):
     """Inputs of DynamicalCore.step_dynamics (one k_split step of
     dt_atmos = 225 s, n_split acoustic substeps): the acoustics case's
     baroclinic-wave state with its potential temperature turned back into a
     temperature (pt pkz, step_dynamics converts it in its preamble), water
     vapour uniform in [1e-4, 1e-2), the other species in [0, 1e-5) with a
     seeded 2 % of negative points (down to -1e-6), cloud fraction in
-    [0, 0.5)."""
+    [0, 0.5); ``sat_adj`` turns on the remapping's fast saturation
+    adjustment."""
     case = acoustics_case(n, nz, seed, n_split)
     rng = np.random.default_rng(seed + 2000)
     shp = case["delp"].shape
@@ -410,13 +416,15 @@ def step_case(n=12, nz=12, seed=101, n_split=2):
     case["ps"] = np.array(case["pe"][..., nz], copy=True)
     case["mdt"] = 225.0
     case["dt_atmos"] = 225.0
+    case["do_sat_adj"] = np.array(bool(sat_adj))
     return case
 
 
 CASES["step"] = step_case
+CASES["step_satadj"] = functools.partial(step_case, sat_adj=True)
 
 
-def dycore_namelist(n, nz, n_split):
+def dycore_namelist(n, nz, n_split, sat_adj=False):
     """DynamicalCoreConfig values of the baroclinic-wave configuration
     (examples/wrapped/config/baroclinic.yml in the reference) on a C``n``
     L``nz`` grid, without the saturation adjustment."""
@@ -426,5 +434,6 @@ def dycore_namelist(n, nz, n_split):
     nl.update({k: v for k, v in REMAP_CONFIG.items()})
     nl.update(SAT_ADJUST_CONFIG)
     nl.update(dt_atmos=225, consv_te=False, hord_tr=8, z_tracer=True, nwat=6, npx=n + 1, npy=n + 1, npz=nz,
-              ntiles=6, do_qa=True, n_split=n_split, moist_phys=True, c2l_ord=4, p_ref=1e5, nf_omega=1)
+              ntiles=6, do_qa=True, n_split=n_split, moist_phys=True, c2l_ord=4, p_ref=1e5, nf_omega=1,
+              do_sat_adj=bool(sat_adj))
     return nl

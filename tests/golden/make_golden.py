@@ -316,7 +316,7 @@ def run_fv_step(case, n, nz):
 
 
 REMAP_FIELDS = cases.REMAP_TRACERS + ("pt", "delp", "delz", "peln", "u", "v", "w", "ua", "va", "cappa", "q_con",
-                                      "pkz", "pk", "pe", "ps")
+                                      "pkz", "pk", "pe", "ps", "qcld")
 
 
 def run_remap(case, n, nz):
@@ -392,7 +392,8 @@ def run_step(case, n, nz):
         riemann=spec.RiemannConfig(**cases.RIEMANN_CONFIG),
         d_grid_shallow_water=spec.DGridShallowWaterLagrangianDynamicsConfig(**cases.DSW_CONFIG),
     )
-    rcfg = spec.RemappingConfig(sat_adjust=spec.SatAdjustConfig(**cases.SAT_ADJUST_CONFIG), **cases.REMAP_CONFIG)
+    rcfg = spec.RemappingConfig(sat_adjust=spec.SatAdjustConfig(**cases.SAT_ADJUST_CONFIG),
+                                **dict(cases.REMAP_CONFIG, do_sat_adj=bool(case["do_sat_adj"])))
     config = types.SimpleNamespace(hydrostatic=False, rf_fast=True, tau=10.0, adiabatic=False, kord_tm=-9,
                                    nf_omega=1, nwat=6, moist_phys=True)
     nq = len(cases.REMAP_TRACERS)
@@ -494,7 +495,9 @@ RUNNERS = {
     "remap": (run_remap, dict(n=4, nz=79, seed=81)),
     "remap_kord10": (run_remap, dict(n=4, nz=30, seed=83)),
     "remap_kord8": (run_remap, dict(n=4, nz=30, seed=85)),
+    "remap_satadj": (run_remap, dict(n=4, nz=79, seed=87)),
     "step": (run_step, dict(n=12, nz=12, seed=101)),
+    "step_satadj": (run_step, dict(n=12, nz=12, seed=103)),
 }
 
 

@@ -205,7 +205,7 @@ def run_remap(case, n, nz, precision="f64"):
             d["wsd"], d["omga"], case["ak"], case["bk"], case["pfull"], d["dp1"], case["ptop"], C.KAPPA, C.ZVIR,
             True, 0.0, case["mdt"], case["mdt"], False, len(cases.REMAP_TRACERS))
         torch.cuda.synchronize()
-        return {k: to_host(dev[k]) for k in cases.REMAP_TRACERS + cases.REMAP_STATE}
+        return {k: to_host(dev[k]) for k in cases.REMAP_TRACERS + cases.REMAP_STATE + ("qcld",)}
     finally:
         gd.close()
 
@@ -226,7 +226,8 @@ def run_step(case, n, nz, precision="f64", steps=1):
     dtype = gd.grid_indexing.dtype
     sf = StencilFactory(StencilConfig(), gd.grid_indexing)
     try:
-        config = DynamicalCoreConfig(**cases.dycore_namelist(n, nz, int(case["n_split"])))
+        config = DynamicalCoreConfig(**cases.dycore_namelist(n, nz, int(case["n_split"]),
+                                                             bool(case.get("do_sat_adj", False))))
         phis = to_device(case["phis"], dtype=dtype)
         core = DynamicalCore(None, gd, sf, gd, config, case["ak"], case["bk"], phis)
         names = tuple(cases.ACOUSTIC_STATE) + cases.STEP_TRACERS + ("ps",)

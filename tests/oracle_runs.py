@@ -138,14 +138,20 @@ def run_remap(case, n, nz):
     t = Tile(n, nz)
     st = {k: np.array(v, copy=True) for k, v in case.items() if isinstance(v, np.ndarray)}
     out = {}
+    cfg = cases.remap_config(case)
+    g = cases.grid_for(n)
     with np.errstate(all="ignore"):
         for tt in range(6):
             tracers = {k: st[k][tt] for k in cases.REMAP_TRACERS}
             fields = {k: st[k][tt] for k in cases.REMAP_STATE}
+            sa = None
+            if cfg["do_sat_adj"]:
+                sa = {"cfg": cases.SAT_ADJUST_CONFIG, "area": g.area[tt], "hs": st["phis"][tt], "dp1": st["dp1"][tt],
+                      "qcld": st["qcld"][tt], "pfull": case["pfull"], "mdt": case["mdt"]}
             R.lagrangian_to_eulerian(t, tracers, fields, case["ak"], case["bk"], case["ptop"], C.KAPPA, C.ZVIR,
-                                     True, **{k: v for k, v in cases.remap_config(case).items()
-                                              if k != "do_sat_adj"})
-    for k in cases.REMAP_TRACERS + cases.REMAP_STATE:
+                                     True, sat_adjust=sa,
+                                     **{k: v for k, v in cfg.items() if k != "do_sat_adj"})
+    for k in cases.REMAP_TRACERS + cases.REMAP_STATE + ("qcld",):
         out[k] = st[k]
     return out
 
@@ -197,9 +203,13 @@ def _oracle_step(st, case, n, nz, t, g, metrics, ad, adv, halo, bdt):
     ad(st)
     adv([st[q] for q in cases.REMAP_TRACERS], st["dp1"], st["mfxd"], st["mfyd"], st["cxd"], st["cyd"], bdt)
     for tt in range(6):
+        sa = None
+        if bool(case.get("do_sat_adj", False)):
+            sa = {"cfg": cases.SAT_ADJUST_CONFIG, "area": g.area[tt], "hs": st["phis"][tt], "dp1": st["dp1"][tt],
+                  "qcld": st["qcld"][tt], "pfull": case["pfull"], "mdt": bdt}
         R.lagrangian_to_eulerian(t, {k: st[k][tt] for k in cases.REMAP_TRACERS},
                                  {k: st[k][tt] for k in cases.REMAP_STATE}, case["ak"], case["bk"], case["ptop"],
-                                 C.KAPPA, C.ZVIR, True,
+                                 C.KAPPA, C.ZVIR, True, sat_adjust=sa,
                                  **{k: v for k, v in cases.REMAP_CONFIG.items() if k != "do_sat_adj"})
     for tt in range(6):
         F.set_omega(t, st["delp"][tt], st["delz"][tt], st["w"][tt], st["omga"][tt])

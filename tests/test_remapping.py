@@ -15,9 +15,15 @@ from metrics import max_rel_err, parity_err
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 H = 3
-GOLDENS = ("remap", "remap_kord10", "remap_kord8")
+GOLDENS = ("remap", "remap_kord10", "remap_kord8", "remap_satadj")
 OUT = cases.REMAP_TRACERS + ("pt", "delp", "delz", "peln", "u", "v", "w", "ua", "va", "cappa", "q_con", "pkz",
                              "pk", "pe", "ps")
+
+
+def _out(g):
+    """The fields a golden stores (the cloud fraction with the saturation
+    adjustment)."""
+    return OUT + (("qcld",) if "qcld" in g.files else ())
 
 
 def _golden(name):
@@ -37,7 +43,7 @@ def test_oracle_matches_reference_golden(name):
     every level, bit for bit."""
     g, n, nz, case = _golden(name)
     out = oracle_runs.run_remap(case, n, nz)
-    for k in OUT:
+    for k in _out(g):
         assert np.array_equal(_box(out[k], n), g[k], equal_nan=True), k
 
 
@@ -103,9 +109,6 @@ def test_dropin_rejects_what_the_reference_rejects():
     with pytest.raises(NotImplementedError, match="Hydrostatic"):
         hsat = SatAdjustConfig(**dict(cases.SAT_ADJUST_CONFIG, hydrostatic=True))
         LagrangianToEulerian(sf, RemappingConfig(sat_adjust=hsat, **base), None, 8, np.ones(79))
-    with pytest.raises(NotImplementedError, match="saturation"):
-        LagrangianToEulerian(sf, RemappingConfig(sat_adjust=sat, **dict(base, do_sat_adj=True)), None, 8,
-                             np.ones(79))
     with pytest.raises(AssertionError, match="kord"):
         LagrangianToEulerian(sf, RemappingConfig(sat_adjust=sat, **dict(base, kord_tr=11)), None, 8, np.ones(79))
 
@@ -118,17 +121,21 @@ def _cmp(a, b, n, nz, extra=0):
 
 # Points where the kord-10 limiter switches (ext5 / ext6 are discontinuous
 # in the profile) after a last-place difference of the moist pt
-# conversion's exp / log between numpy and the kernels' own functions: the
-# oracle shows the same points with either set of functions
+# conversion's exp / log between numpy and the kernels' own functions, and,
+# with the saturation adjustment, single points where a species is a small
+# difference of terms carrying the saturation tables' exp / log (qliquid
+# 1.0e-12, qsnow 4.4e-12 between the two sets of functions): the oracle
+# shows the same points with either set of functions
 # (test_kord10_switch_comes_from_the_transcendentals), and the GPU matches
 # the oracle bit for bit with the kernels' functions (test_gpu_matches_oracle).
-SWITCHED = {"remap_kord10": {"pt": 1e-5, "pkz": 1e-5}}
+SWITCHED = {"remap_kord10": {"pt": 1e-5, "pkz": 1e-5}, "remap_satadj": {"qliquid": 1e-11, "qsnow": 5e-11}}
 
 
 def test_kord10_switch_comes_from_the_transcendentals():
     """The oracle with numpy's exp / log against the oracle with the
     kernels' own: identical to 1e-12 except at two kord-10 points where the
-    limiter switches (2.7e-6 in pt), none for kord 9 and 8."""
+    limiter switches (2.7e-6 in pt) and single points of two species with
+    the saturation adjustment, none for kord 9 and 8."""
     from oracle import _math
 
     for name in GOLDENS:
@@ -136,7 +143,7 @@ def test_kord10_switch_comes_from_the_transcendentals():
         a = oracle_runs.run_remap(case, n, nz)
         with _math.device_math():
             b = oracle_runs.run_remap(case, n, nz)
-        for k in OUT:
+        for k in _out(g):
             x, y = _box(a[k], n)[..., :nz], _box(b[k], n)[..., :nz]
             d = np.abs(x - y) / np.maximum(np.abs(y), 1e-300)
             bound = SWITCHED.get(name, {}).get(k, 1e-12)
@@ -155,7 +162,7 @@ def test_gpu_matches_reference_golden(name):
     g, n, nz, case = _golden(name)
     gpu = gpu_runs.run_remap(case, n, nz)
     bad = {}
-    for k in OUT:
+    for k in _out(g):
         a, b = _box(gpu[k], n), g[k]
         bound = SWITCHED.get(name, {}).get(k, 1e-12)
         e = (parity_err(a, b), max_rel_err(a, b))
@@ -166,20 +173,23 @@ def test_gpu_matches_reference_golden(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n,nz,seed,kord", [(4, 79, 81, (-9, 9, 9, 9)), (24, 79, 92, (-9, 9, 9, 9)),
-                                            (12, 63, 93, (-10, 10, 10, 10)), (12, 40, 94, (-8, 8, 8, 8))])
-def test_gpu_matches_oracle(n, nz, seed, kord):
+@pytest.mark.parametrize("n,nz,seed,kord,sat", [(4, 79, 81, (-9, 9, 9, 9), False), (24, 79, 92, (-9, 9, 9, 9), False),
+                                                (12, 63, 93, (-10, 10, 10, 10), False),
+                                                (12, 40, 94, (-8, 8, 8, 8), False),
+                                                (12, 79, 95, (-9, 9, 9, 9), True)])
+def test_gpu_matches_oracle(n, nz, seed, kord, sat):
     """Bit for bit against the oracle running the kernels' exp/log, on the
-    remapped region of every field."""
+    remapped region of every field (the last case with the fast saturation
+    adjustment)."""
     import gpu_runs
     from oracle import _math
 
-    case = cases.remap_case(n, nz, seed, kord=kord)
+    case = cases.remap_case(n, nz, seed, kord=kord, sat_adj=sat)
     with _math.device_math():
         ref = oracle_runs.run_remap(case, n, nz)
     gpu = gpu_runs.run_remap(case, n, nz)
     bad = {}
-    for k in OUT:
+    for k in OUT + ("qcld",):
         a, b = _cmp(gpu[k], ref[k], n, nz, extra=1)
         if not np.array_equal(a, b, equal_nan=True):
             d = np.abs(a - b)

@@ -27,14 +27,22 @@ FIELDS = list(STEP_OUT) + list(cases.STEP_TRACERS) + ["ps"]
 # u 1.6e-10, v 1.2e-10, w 1.8e-8, omga 8.2e-11, va 3.2e-9 (6.1e-9),
 # qo3mr 1.3e-12 (4e-14); every other field below 3e-14), the acoustic
 # substeps' amplification of last-place differences into the winds.
+# With the saturation adjustment (step_satadj) the species that are small
+# differences of terms carrying its saturation tables' exp / log are added
+# (floors qliquid 1.1e-11, qrain 2.0e-12, q_con 3.4e-13, qsnow 5.0e-13,
+# qice 3.2e-13, qcld 1.6e-13).
 STEP_BOUNDS = {"u": (1e-8, 1e-8), "v": (1e-8, 1e-8), "w": (5e-7, 5e-7), "omga": (3e-9, 3e-9),
                "va": (1e-7, 2e-7), "qo3mr": (5e-11, 1e-12)}
+BOUNDS = {"step": STEP_BOUNDS,
+          "step_satadj": dict(STEP_BOUNDS, qliquid=(3e-10, 3e-10), qrain=(6e-11, 6e-11), q_con=(1e-11, 1e-11),
+                              qsnow=(1e-11, 1e-11), qice=(1e-11, 1e-11), qcld=(1e-11, 1e-11))}
+GOLDENS = tuple(BOUNDS)
 
 
-def _golden():
-    g = np.load(os.path.join(HERE, "golden", "step.npz"))
+def _golden(name="step"):
+    g = np.load(os.path.join(HERE, "golden", f"{name}.npz"))
     n, nz, seed = int(g["arg_n"]), int(g["arg_nz"]), int(g["arg_seed"])
-    return g, n, nz, cases.step_case(n, nz, seed)
+    return g, n, nz, cases.CASES[name](n=n, nz=nz, seed=seed)
 
 
 def _region(a, name, n, nz):
@@ -43,26 +51,29 @@ def _region(a, name, n, nz):
     return a[sl] if name == "ps" else a[sl + (slice(0, nz + dk),)]
 
 
-def test_oracle_matches_reference_golden():
-    """Every stored point of every field, bit for bit."""
-    g, n, nz, case = _golden()
+@pytest.mark.parametrize("name", GOLDENS)
+def test_oracle_matches_reference_golden(name):
+    """Every stored point of every field, bit for bit (the second golden
+    with the remapping's fast saturation adjustment)."""
+    g, n, nz, case = _golden(name)
     out = oracle_runs.run_step(case, n, nz)
     for k in FIELDS:
         assert np.array_equal(_region(out[k], k, n, nz), g[k], equal_nan=True), k
 
 
-def test_conditioning_of_the_step():
-    """The floors behind STEP_BOUNDS: the oracle with numpy's exp/log/pow
+@pytest.mark.parametrize("name", GOLDENS)
+def test_conditioning_of_the_step(name):
+    """The floors behind BOUNDS: the oracle with numpy's exp/log/pow
     against the oracle with the kernels' own."""
     from oracle import _math
 
-    g, n, nz, case = _golden()
+    g, n, nz, case = _golden(name)
     a = oracle_runs.run_step(case, n, nz)
     with _math.device_math():
         b = oracle_runs.run_step(case, n, nz)
     for k in FIELDS:
         x, y = _region(a[k], k, n, nz), _region(b[k], k, n, nz)
-        bp, bc = STEP_BOUNDS.get(k, (1e-12, 1e-12))
+        bp, bc = BOUNDS[name].get(k, (1e-12, 1e-12))
         assert parity_err(x, y) <= bp / 10 and max_rel_err(x, y) <= bc / 10, (k, parity_err(x, y))
 
 
@@ -82,34 +93,36 @@ def test_golden_step_moves_every_field():
 
 
 @pytest.mark.gpu
-def test_gpu_step_matches_reference_golden():
+@pytest.mark.parametrize("name", GOLDENS)
+def test_gpu_step_matches_reference_golden(name):
     """The CUDA DynamicalCore against the reference's own output, both
-    metrics, every stored point, within STEP_BOUNDS (1e-12 where not
-    listed)."""
+    metrics, every stored point, within BOUNDS (1e-12 where not listed)."""
     import gpu_runs
 
-    g, n, nz, case = _golden()
+    g, n, nz, case = _golden(name)
     gpu = gpu_runs.run_step(case, n, nz)
     bad = {}
     for k in FIELDS:
         a = _region(gpu[k], k, n, nz)
         e = (parity_err(a, g[k]), max_rel_err(a, g[k]))
-        bp, bc = STEP_BOUNDS.get(k, (1e-12, 1e-12))
+        bp, bc = BOUNDS[name].get(k, (1e-12, 1e-12))
         if not (e[0] <= bp and e[1] <= bc):
             bad[k] = e
     assert not bad, bad
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n,nz,seed,n_split", [(12, 12, 101, 2), (12, 79, 102, 6)])
-def test_gpu_step_matches_oracle(n, nz, seed, n_split):
+@pytest.mark.parametrize("n,nz,seed,n_split,sat", [(12, 12, 101, 2, False), (12, 79, 102, 6, False),
+                                                   (12, 79, 104, 6, True)])
+def test_gpu_step_matches_oracle(n, nz, seed, n_split, sat):
     """1e-12 on every field (parity metric) against the oracle with the
     kernels' exp/log/pow; at C12 L79 the step of the baroclinic namelist
-    (dt_atmos 225 s, n_split 6)."""
+    (dt_atmos 225 s, n_split 6), without and with the fast saturation
+    adjustment."""
     import gpu_runs
     from oracle import _math
 
-    case = cases.step_case(n, nz, seed, n_split)
+    case = cases.step_case(n, nz, seed, n_split, sat_adj=sat)
     with _math.device_math():
         ref = oracle_runs.run_step(case, n, nz)
     gpu = gpu_runs.run_step(case, n, nz)
