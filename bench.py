@@ -503,8 +503,9 @@ STEP_FIELDS = ("qvapor", "qliquid", "qrain", "qice", "qsnow", "qgraupel", "qo3mr
 # compulsory field transfers per cell-level of one step (k_split 1): the
 # acoustic call's 34 per substep, the tracer advection's 8 tracers read and
 # written plus its 5 shared fluxes (one sub-cycle), the remapping's 21
-# fields read and written, the preamble's 15, post_remap's 6 and wrapup's 23
-STEP_TRANSFERS_NON_ACOUSTIC = 8 * 2 + 5 + 21 * 2 + 15 + 6 + 23
+# fields read and written, the saturation adjustment's 13 read and 11
+# written, the preamble's 15, post_remap's 6 and wrapup's 23
+STEP_TRANSFERS_NON_ACOUSTIC = 8 * 2 + 5 + 21 * 2 + 13 + 11 + 15 + 6 + 23
 
 
 def step_problem(n, npz, n_split, precision, st0, grid):
@@ -537,7 +538,7 @@ def _oracle_step_worker(n, npz, n_split, q):
     import cases
     import oracle_runs
 
-    case = cases.step_case(n, npz, 5, n_split)
+    case = cases.step_case(n, npz, 5, n_split, sat_adj=True)
     t0 = time.perf_counter()
     oracle_runs.run_step(case, n, npz)
     q.put((6 * n * n * npz, time.perf_counter() - t0))
@@ -576,7 +577,7 @@ def run_step_section(args, state0, grid384, local):
     out = {"metric": f"C{n} L{npz} step_dynamics cell-levels/s", "unit": "cell-levels/s",
            "config": {"workload": f"DynamicalCore.step_dynamics C{n} L{npz}, k_split 1, n_split {n_split}, "
                                   "dt_atmos 225 s, nonhydrostatic, d_ext 0, nord 3, hord_tr 8, kord 9, 8 advected "
-                                  "tracers + qcld, no saturation adjustment (do_sat_adj not built)",
+                                  "tracers + qcld, fast saturation adjustment (do_sat_adj)",
                       "n": n, "npz": npz, "n_split": n_split, "cell_levels": cells,
                       "reset": "every step restarts from the initial state (device copy outside the events)"}}
     peak, peak_kind = _measured_peak()
@@ -622,8 +623,9 @@ def run_step_section(args, state0, grid384, local):
              "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                           "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
                           "scope": f"whole step: {transfers} compulsory field transfers of {width} B per "
-                                   "cell-level (34 per acoustic substep, 107 for the tracer advection, "
-                                   "remapping, preamble and epilogue)"}}
+                                   f"cell-level (34 per acoustic substep, {STEP_TRANSFERS_NON_ACOUSTIC} for the "
+                                   "tracer advection, remapping with the saturation adjustment, preamble and "
+                                   "epilogue)"}}
         out["fp64" if prec == "f64" else "mixed"] = r
         del initial, state, core
         gd.close()
