@@ -29,6 +29,7 @@ __device__ __forceinline__ int corner_j6(const Dims& d, int x) { return x < 3 ? 
 extern "C" int fv3b_c_sw(fv3b_ctx* ctx, real* delp, real* pt, const real* u, const real* v, real* w,
                          real* uc, real* vc, real* ua, real* va, real* ut, real* vt, real* divgd,
                          real* omga, double dt2_in, int nord, real* delpc, real* ptc, void* stream) {
+  FV3B_TILES(ctx);
   // the build's precision inside the kernels (the same value in FP64 builds)
   const real dt2 = static_cast<real>(dt2_in);
   FV3B_REQUIRE(ctx && delp && pt && u && v && w && uc && vc && ua && va && ut && vt && divgd && omga && delpc && ptc,

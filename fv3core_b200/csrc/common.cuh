@@ -46,13 +46,26 @@ struct LaunchShape {
 };
 const LaunchShape& launch_shape();
 
+// Tile slots of the calling entry point's arrays (6, or 6 x members of a
+// batched context), a per-host-thread setting that TileScope sets from the
+// context for the duration of a call; the launch helpers size their grids
+// by it, so one launch covers every member.
+int& tile_slots();
+struct TileScope {
+  int saved;
+  explicit TileScope(int nt) : saved(tile_slots()) { tile_slots() = nt; }
+  ~TileScope() { tile_slots() = saved; }
+  TileScope(const TileScope&) = delete;
+  TileScope& operator=(const TileScope&) = delete;
+};
+
 template <typename F>
 cudaError_t launch_box(const Box& b, cudaStream_t s, F f) {
   int ni = b.i1 - b.i0, nj = b.j1 - b.j0, nk = b.k1 - b.k0;
   if (ni <= 0 || nj <= 0 || nk <= 0) return cudaSuccess;
   const LaunchShape& ls = launch_shape();
   dim3 block(ls.box_x, ls.box_y, 1);
-  dim3 grid((ni + ls.box_x - 1) / ls.box_x, (nj + ls.box_y - 1) / ls.box_y, 6 * nk);
+  dim3 grid((ni + ls.box_x - 1) / ls.box_x, (nj + ls.box_y - 1) / ls.box_y, tile_slots() * nk);
   box_kernel<<<grid, block, 0, s>>>(b, f);
   note_launch();
   return cudaGetLastError();
@@ -95,7 +108,7 @@ cudaError_t launch_box_split(const Box& b, int a0, int a1, cudaStream_t s, F f) 
   const int nint_pad = (nint + ls.box_x - 1) / ls.box_x * ls.box_x;
   const int nx = nint_pad + (ni - nint);
   dim3 block(ls.box_x, ls.box_y, 1);
-  dim3 grid((nx + ls.box_x - 1) / ls.box_x, (nj + ls.box_y - 1) / ls.box_y, 6 * nk);
+  dim3 grid((nx + ls.box_x - 1) / ls.box_x, (nj + ls.box_y - 1) / ls.box_y, tile_slots() * nk);
   box_kernel_split<<<grid, block, 0, s>>>(b, a0, nint, nint_pad, f);
   note_launch();
   return cudaGetLastError();
@@ -119,7 +132,7 @@ cudaError_t launch_columns(int i0, int i1, int j0, int j1, cudaStream_t s, F f, 
   if (block <= 0) block = launch_shape().col;
   int ncol = (i1 - i0) * (j1 - j0);
   if (ncol <= 0) return cudaSuccess;
-  dim3 grid((ncol + block - 1) / block, 6, 1);
+  dim3 grid((ncol + block - 1) / block, tile_slots(), 1);
   column_kernel<<<grid, block, 0, s>>>(i0, i1, j0, j1, f);
   note_launch();
   return cudaGetLastError();
@@ -138,6 +151,10 @@ void set_last_error_msg(const char* msg);
       return FV3B_ERR_CUDA;                               \
     }                                                     \
   } while (0)
+
+// every entry point that takes a context starts with this: its launches
+// cover the context's tile slots
+#define FV3B_TILES(ctx) const ::fv3b::TileScope _fv3b_tiles((ctx) ? (ctx)->d.nt : 6)
 
 #define FV3B_REQUIRE(cond, msg)                           \
   do {                                                    \

@@ -315,6 +315,7 @@ inline double max_(double a, double b) { return a > b ? a : b; }
 }  // namespace
 
 extern "C" int fv3b_d_sw_setup(fv3b_ctx* ctx, const fv3b_dsw_config* cfg) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && cfg, "fv3b_d_sw_setup: null argument");
   if (cfg->grid_type >= 3 || cfg->inline_q || cfg->d_ext > 0.0) {
     set_last_error_msg("fv3b_d_sw_setup: grid_type >= 3, inline_q and d_ext > 0 are not implemented");
@@ -447,6 +448,7 @@ extern "C" int fv3b_d_sw(fv3b_ctx* ctx, real* delpc, real* delp, real* ptc, real
                          real* mfx, real* mfy, real* cx, real* cy, real* crx, real* cry, real* xfx,
                          real* yfx, real* q_con, const real* zh, real* heat_source, real* diss_est,
                          double dt_in, void* stream) {
+  FV3B_TILES(ctx);
   // the build's precision inside the kernels (the same value in FP64 builds)
   const real dt = static_cast<real>(dt_in);
   FV3B_REQUIRE(ctx && delpc && delp && ptc && pt && u && v && w && uc && vc && ua && va && divgd && mfx && mfy &&

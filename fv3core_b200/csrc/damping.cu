@@ -42,6 +42,7 @@ constexpr real RDG = -RDGAS / GRAV;
 // prefixes [0, k_rf) and [0, k_nudge).
 extern "C" int fv3b_ray_fast(fv3b_ctx* ctx, real* u, real* v, real* w, const double* dp, const double* pfull,
                              double dt, double ptop, double rf_cutoff, double tau, int hydrostatic, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && u && v && w && dp && pfull, "fv3b_ray_fast: null argument");
   const Dims d = ctx->d;
   const int nz = d.nz;
@@ -125,6 +126,7 @@ extern "C" int fv3b_ray_fast(fv3b_ctx* ctx, real* u, real* v, real* w, const dou
 extern "C" int fv3b_ray_fast_adjoint(fv3b_ctx* ctx, real* gu, real* gv, real* gw, const double* dp,
                                      const double* pfull, double dt, double ptop, double rf_cutoff, double tau,
                                      int hydrostatic, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && gu && gv && gw && dp && pfull, "fv3b_ray_fast_adjoint: null argument");
   const Dims d = ctx->d;
   const RayState& rs = ctx->ray;
@@ -153,6 +155,7 @@ extern "C" int fv3b_ray_fast_adjoint(fv3b_ctx* ctx, real* gu, real* gv, real* gw
 // copies of its scratch q (copy_corners_x before the x fluxes, _y before
 // the y fluxes and the copy back) are reads through the corner rules.
 extern "C" int fv3b_del2cubed(fv3b_ctx* ctx, real* qdel, double cd_in, int nmax, void* stream) {
+  FV3B_TILES(ctx);
   // the build's precision inside the kernels (the same value in FP64 builds)
   const real cd = static_cast<real>(cd_in);
   FV3B_REQUIRE(ctx && qdel, "fv3b_del2cubed: null argument");
@@ -225,6 +228,7 @@ extern "C" int fv3b_del2cubed(fv3b_ctx* ctx, real* qdel, double cd_in, int nmax,
 // (del2cubed_adjoint.h), each scattering every point's cotangent onto the
 // inputs it read (atomic adds) in the workspace, then copied back.
 extern "C" int fv3b_del2cubed_adjoint(fv3b_ctx* ctx, real* gq, double cd_in, int nmax, void* stream) {
+  FV3B_TILES(ctx);
   const real cd = static_cast<real>(cd_in);
   FV3B_REQUIRE(ctx && gq, "fv3b_del2cubed_adjoint: null argument");
   const Dims d = ctx->d;
@@ -235,7 +239,7 @@ extern "C" int fv3b_del2cubed_adjoint(fv3b_ctx* ctx, real* gq, double cd_in, int
   const int ntimes = nmax < 3 ? nmax : 3;
   for (int n = ntimes - 1; n >= 0; --n) {
     const int nt = ntimes - (n + 1);
-    FV3B_CHECK(cudaMemsetAsync(nxt, 0, sizeof(real) * (size_t)6 * d.st, st));
+    FV3B_CHECK(cudaMemsetAsync(nxt, 0, sizeof(real) * (size_t)d.nt * d.st, st));
     FV3B_CHECK(launch_box(Box{0, d.ni, 0, d.nj, 0, nz}, st, [=] __device__(int t, int i, int j, int k) {
       const idx_t o = idx3(d, t, i, j, k);
       if (i == full || j == full) {
@@ -258,6 +262,7 @@ extern "C" int fv3b_del2cubed_adjoint(fv3b_ctx* ctx, real* gq, double cd_in, int
 extern "C" int fv3b_pkz_tempadjust(fv3b_ctx* ctx, const real* delp, const real* delz, const real* cappa,
                                    const real* heat_source, real* pt, real* pkz, double delt_time_factor_in,
                                    int nk_heat, void* stream) {
+  FV3B_TILES(ctx);
   // the build's precision inside the kernels (the same value in FP64 builds)
   const real delt_time_factor = static_cast<real>(delt_time_factor_in);
   FV3B_REQUIRE(ctx && delp && delz && cappa && heat_source && pt && pkz, "fv3b_pkz_tempadjust: null argument");
@@ -289,13 +294,14 @@ extern "C" int fv3b_pkz_tempadjust_adjoint(fv3b_ctx* ctx, const real* delp, cons
                                            const real* heat_source, const real* pt, real* g_pt, real* g_pkz,
                                            real* g_delp, real* g_delz, real* g_heat, double delt_time_factor_in,
                                            int nk_heat, void* stream) {
+  FV3B_TILES(ctx);
   const real delt_time_factor = static_cast<real>(delt_time_factor_in);
   FV3B_REQUIRE(ctx && delp && delz && cappa && heat_source && pt && g_pt && g_pkz && g_delp && g_delz && g_heat,
                "fv3b_pkz_tempadjust_adjoint: null argument");
   const Dims d = ctx->d;
   FV3B_REQUIRE(nk_heat >= 0 && nk_heat <= d.nz, "fv3b_pkz_tempadjust_adjoint: nk_heat out of range");
   cudaStream_t st = (cudaStream_t)stream;
-  const size_t bytes = sizeof(real) * (size_t)6 * d.st;
+  const size_t bytes = sizeof(real) * (size_t)d.nt * d.st;
   FV3B_CHECK(cudaMemsetAsync(g_delp, 0, bytes, st));
   FV3B_CHECK(cudaMemsetAsync(g_delz, 0, bytes, st));
   FV3B_CHECK(cudaMemsetAsync(g_heat, 0, bytes, st));

@@ -44,6 +44,10 @@ using idx_t = int;
 struct Dims {
   int n, h, nz;
   int ni, nj, nk;
+  // tile slots of the arrays: 6 for one cube, 6 x members for an ensemble
+  // of same-resolution members kept in one allocation (member m owns tiles
+  // 6m .. 6m+5)
+  int nt;
   idx_t sj, sk, st;  // 3-D strides (i stride is 1)
   idx_t st2;         // 2-D tile stride (j stride is ni)
   int isc, iec, jsc, jec;  // compute domain (inclusive), storage indices
@@ -63,6 +67,7 @@ inline Dims make_dims(const fv3b_grid_dims* g) {
   d.ni = d.n + 2 * d.h + 1;
   d.nj = d.ni;
   d.nk = d.nz + 1;
+  d.nt = 6;
   d.sj = d.ni;
   d.sk = d.ni * d.nj;
   d.st = d.sk * d.nk;

@@ -65,6 +65,7 @@ using namespace fv3b;
 
 extern "C" int fv3b_acoustics_setup(fv3b_ctx* ctx, const fv3b_acoustic_config* config, const fv3b_dsw_config* dsw,
                                     const double* ak, const double* bk, const double* pfull, const real* phis) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && config && dsw && ak && bk && pfull && phis, "fv3b_acoustics_setup: null argument");
   FV3B_REQUIRE(dsw->d_ext == 0.0, "fv3b_acoustics_setup: d_ext != 0 is not implemented");
   FV3B_REQUIRE(!dsw->hydrostatic, "fv3b_acoustics_setup: only the nonhydrostatic dynamics are implemented");
@@ -78,7 +79,7 @@ extern "C" int fv3b_acoustics_setup(fv3b_ctx* ctx, const fv3b_acoustic_config* c
   if (a == nullptr) {
     a = new (std::nothrow) AcousticState();
     FV3B_REQUIRE(a != nullptr, "fv3b_acoustics_setup: out of host memory");
-    const size_t n3 = (size_t)d.st * 6, n2 = (size_t)d.st2 * 6;
+    const size_t n3 = (size_t)d.st * d.nt, n2 = (size_t)d.st2 * d.nt;
     cudaError_t e = cudaMalloc((void**)&a->base, sizeof(real) * (n3 * N_TMP3 + 2 * n2));
     if (e != cudaSuccess) {
       delete a;
@@ -102,7 +103,7 @@ extern "C" int fv3b_acoustics_setup(fv3b_ctx* ctx, const fv3b_acoustic_config* c
   a->do_del2cubed = a->nk_heat != 0 && dsw->d_con > 1.0e-5;
   a->cd = 0.2 * ctx->m.da_min;
   // temporaries: zero, gz and pk3 at HUGE_R (dyn_core.py:333-336)
-  const size_t n3 = (size_t)d.st * 6, n2 = (size_t)d.st2 * 6;
+  const size_t n3 = (size_t)d.st * d.nt, n2 = (size_t)d.st2 * d.nt;
   FV3B_CHECK(cudaMemset(a->base, 0, sizeof(real) * (n3 * N_TMP3 + 2 * n2)));
   FV3B_CHECK(fill(a->tmp[T_GZ], (long long)n3, HUGE_R, 0));
   FV3B_CHECK(fill(a->tmp[T_PK3], (long long)n3, HUGE_R, 0));
@@ -141,6 +142,7 @@ void fv3b_acoustics_release(fv3b_ctx* ctx) {
   } while (0)
 
 extern "C" int fv3b_acoustics(fv3b_ctx* ctx, const fv3b_dycore_state* S, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && S, "fv3b_acoustics: null argument");
   FV3B_REQUIRE(ctx->acoustic, "fv3b_acoustics: call fv3b_acoustics_setup first");
   AcousticState* a = ctx->acoustic;

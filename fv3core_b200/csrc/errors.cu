@@ -20,6 +20,11 @@ void set_last_error(const char* where, cudaError_t e) {
 void set_last_error_msg(const char* msg) { snprintf(g_last_error, sizeof(g_last_error), "%s", msg); }
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
+int& tile_slots() {
+  thread_local int slots = 6;
+  return slots;
+}
+
 namespace {
 LaunchShape g_shape;
 }

@@ -224,6 +224,7 @@ extern "C" int fv3b_compute_preamble(fv3b_ctx* ctx, const real* qvapor, const re
                                      const real* qsnow, const real* qice, const real* qgraupel, real* q_con,
                                      real* cvm, real* pkz, real* pt, real* cappa, const real* delp,
                                      const real* delz, real* dp1, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && qvapor && qliquid && qrain && qsnow && qice && qgraupel && q_con && cvm && pkz && pt && cappa &&
                    delp && delz && dp1,
                "fv3b_compute_preamble: null argument");
@@ -257,6 +258,7 @@ extern "C" int fv3b_compute_preamble(fv3b_ctx* ctx, const real* qvapor, const re
 
 extern "C" int fv3b_post_remap(fv3b_ctx* ctx, const real* delp, const real* delz, const real* w, real* omga,
                                int nf_omega, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && delp && delz && w && omga, "fv3b_post_remap: null argument");
   FV3B_REQUIRE(nf_omega >= 0, "fv3b_post_remap: nf_omega must be >= 0");
   const Dims d = ctx->d;
@@ -278,6 +280,7 @@ extern "C" int fv3b_post_remap(fv3b_ctx* ctx, const real* delp, const real* delz
 extern "C" int fv3b_adjust_negative_tracers(fv3b_ctx* ctx, real* qvapor, real* qliquid, real* qrain, real* qsnow,
                                             real* qice, real* qgraupel, real* qcld, real* pt, const real* delp,
                                             const real* delz, const real* peln, int hydrostatic, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && qvapor && qliquid && qrain && qsnow && qice && qgraupel && qcld && pt && delp && delz && peln,
                "fv3b_adjust_negative_tracers: null argument");
   if (hydrostatic) {
@@ -325,6 +328,7 @@ extern "C" int fv3b_adjust_negative_tracers(fv3b_ctx* ctx, real* qvapor, real* q
 
 extern "C" int fv3b_cubed_to_latlon(fv3b_ctx* ctx, real* u, real* v, const real* a11, const real* a12,
                                     const real* a21, const real* a22, real* ua, real* va, int order, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && u && v && a11 && a12 && a21 && a22 && ua && va, "fv3b_cubed_to_latlon: null argument");
   FV3B_REQUIRE(order == 2 || order == 4, "fv3b_cubed_to_latlon: order must be 2 or 4");
   const Dims d = ctx->d;

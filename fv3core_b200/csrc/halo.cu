@@ -70,7 +70,7 @@ __global__ void interface_sync_kernel(Dims d, real* u, real* v, int nlev) {
 cudaError_t halo_scalars(const Dims& d, real* const* fields, int nfields, int stagger, int n_halo, int nlev,
                          cudaStream_t st) {
   const int nc = halo_candidates(d, n_halo);
-  dim3 grid((nc + HALO_BLOCK - 1) / HALO_BLOCK, 6);
+  dim3 grid((nc + HALO_BLOCK - 1) / HALO_BLOCK, d.nt);
   for (int f0 = 0; f0 < nfields; f0 += 4) {
     FieldSet fs;
     fs.n = nfields - f0 < 4 ? nfields - f0 : 4;
@@ -85,14 +85,14 @@ cudaError_t halo_scalars(const Dims& d, real* const* fields, int nfields, int st
 
 cudaError_t halo_vector(const Dims& d, real* x, real* y, bool cgrid, int nlev, cudaStream_t st) {
   const int nc = halo_candidates(d, d.h);
-  dim3 grid((nc + HALO_BLOCK - 1) / HALO_BLOCK, 12);
+  dim3 grid((nc + HALO_BLOCK - 1) / HALO_BLOCK, 2 * d.nt);
   halo_vector_kernel<<<grid, HALO_BLOCK, 0, st>>>(d, x, y, cgrid ? 1 : 0, nlev);
   note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t sync_vector_interfaces(const Dims& d, real* u, real* v, int nlev, cudaStream_t st) {
-  dim3 grid((d.n + HALO_BLOCK - 1) / HALO_BLOCK, 12);
+  dim3 grid((d.n + HALO_BLOCK - 1) / HALO_BLOCK, 2 * d.nt);
   interface_sync_kernel<<<grid, HALO_BLOCK, 0, st>>>(d, u, v, nlev);
   note_launch();
   return cudaGetLastError();
@@ -107,6 +107,7 @@ using namespace fv3b;
 // corners (X_INTERFACE, Y_INTERFACE); n_halo rows; nlev levels.
 extern "C" int fv3b_halo_update_scalar(fv3b_ctx* ctx, real* field, int stagger, int n_halo, int nlev,
                                        void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && field, "fv3b_halo_update_scalar: null argument");
   FV3B_REQUIRE(stagger == 0 || stagger == 1, "fv3b_halo_update_scalar: stagger must be 0 or 1");
   FV3B_REQUIRE(n_halo >= 1 && n_halo <= ctx->d.h, "fv3b_halo_update_scalar: n_halo out of range");
@@ -118,6 +119,7 @@ extern "C" int fv3b_halo_update_scalar(fv3b_ctx* ctx, real* field, int stagger, 
 // Vector HaloUpdater.update: grid 0 = D-grid winds (u, v), 1 = C-grid winds
 // (uc, vc); full halo width.
 extern "C" int fv3b_halo_update_vector(fv3b_ctx* ctx, real* x, real* y, int grid, int nlev, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && x && y, "fv3b_halo_update_vector: null argument");
   FV3B_REQUIRE(grid == 0 || grid == 1, "fv3b_halo_update_vector: grid must be 0 (D) or 1 (C)");
   FV3B_REQUIRE(nlev >= 1 && nlev <= ctx->d.nk, "fv3b_halo_update_vector: nlev out of range");
@@ -127,6 +129,7 @@ extern "C" int fv3b_halo_update_vector(fv3b_ctx* ctx, real* x, real* y, int grid
 
 // CubedSphereCommunicator.synchronize_vector_interfaces for D-grid winds.
 extern "C" int fv3b_synchronize_vector_interfaces(fv3b_ctx* ctx, real* u, real* v, int nlev, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && u && v, "fv3b_synchronize_vector_interfaces: null argument");
   FV3B_REQUIRE(nlev >= 1 && nlev <= ctx->d.nk, "fv3b_synchronize_vector_interfaces: nlev out of range");
   FV3B_CHECK(sync_vector_interfaces(ctx->d, u, v, nlev, (cudaStream_t)stream));

@@ -25,22 +25,26 @@ namespace fv3b {
 
 enum HaloEdge { EDGE_W = 0, EDGE_E = 1, EDGE_S = 2, EDGE_N = 3 };
 
+// Tile slot t belongs to cube t / 6 (one cube, or one member of a batched
+// ensemble); its neighbours are tiles of the same cube.
 __host__ __device__ __forceinline__ void edge_neighbor(int t, int edge, int& t2, int& e2, bool& rev) {
-  if (t % 2 == 0) {
+  const int tl = t % 6, base = t - tl;
+  if (tl % 2 == 0) {
     switch (edge) {
-      case EDGE_E: t2 = (t + 1) % 6; e2 = EDGE_W; rev = false; break;
-      case EDGE_N: t2 = (t + 2) % 6; e2 = EDGE_W; rev = true; break;
-      case EDGE_W: t2 = (t + 4) % 6; e2 = EDGE_N; rev = true; break;
-      default: t2 = (t + 5) % 6; e2 = EDGE_N; rev = false; break;
+      case EDGE_E: t2 = (tl + 1) % 6; e2 = EDGE_W; rev = false; break;
+      case EDGE_N: t2 = (tl + 2) % 6; e2 = EDGE_W; rev = true; break;
+      case EDGE_W: t2 = (tl + 4) % 6; e2 = EDGE_N; rev = true; break;
+      default: t2 = (tl + 5) % 6; e2 = EDGE_N; rev = false; break;
     }
   } else {
     switch (edge) {
-      case EDGE_E: t2 = (t + 2) % 6; e2 = EDGE_S; rev = true; break;
-      case EDGE_N: t2 = (t + 1) % 6; e2 = EDGE_S; rev = false; break;
-      case EDGE_W: t2 = (t + 5) % 6; e2 = EDGE_E; rev = false; break;
-      default: t2 = (t + 4) % 6; e2 = EDGE_E; rev = true; break;
+      case EDGE_E: t2 = (tl + 2) % 6; e2 = EDGE_S; rev = true; break;
+      case EDGE_N: t2 = (tl + 1) % 6; e2 = EDGE_S; rev = false; break;
+      case EDGE_W: t2 = (tl + 5) % 6; e2 = EDGE_E; rev = false; break;
+      default: t2 = (tl + 4) % 6; e2 = EDGE_E; rev = true; break;
     }
   }
+  t2 += base;
 }
 
 // axis (0 = x, 1 = y) normal to an edge, and the sign of the inward normal

@@ -47,7 +47,7 @@ __global__ void interface_sync_adjoint_kernel(Dims d, real* gu, real* gv, int nl
 }
 
 cudaError_t halo_adjoint(const Dims& d, const HaloAdjArgs& a, cudaStream_t st) {
-  dim3 grid((halo_candidates(d, a.n_halo) + HALO_ADJ_BLOCK - 1) / HALO_ADJ_BLOCK, 6 * a.ncomp);
+  dim3 grid((halo_candidates(d, a.n_halo) + HALO_ADJ_BLOCK - 1) / HALO_ADJ_BLOCK, d.nt * a.ncomp);
   for (int zero = 0; zero < 2; ++zero) {
     halo_adjoint_kernel<<<grid, HALO_ADJ_BLOCK, 0, st>>>(d, a, zero);
     note_launch();
@@ -65,6 +65,7 @@ using namespace fv3b;
 // field and is turned, in place, into that of the field before the update.
 extern "C" int fv3b_halo_update_scalar_adjoint(fv3b_ctx* ctx, real* g, int stagger, int n_halo, int nlev,
                                                void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && g, "fv3b_halo_update_scalar_adjoint: null argument");
   FV3B_REQUIRE(stagger == 0 || stagger == 1, "fv3b_halo_update_scalar_adjoint: stagger must be 0 or 1");
   FV3B_REQUIRE(n_halo >= 1 && n_halo <= ctx->d.h, "fv3b_halo_update_scalar_adjoint: n_halo out of range");
@@ -77,6 +78,7 @@ extern "C" int fv3b_halo_update_scalar_adjoint(fv3b_ctx* ctx, real* g, int stagg
 // Adjoint of fv3b_halo_update_vector (grid 0 = D, 1 = C), in place on gx, gy.
 extern "C" int fv3b_halo_update_vector_adjoint(fv3b_ctx* ctx, real* gx, real* gy, int grid, int nlev,
                                                void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && gx && gy, "fv3b_halo_update_vector_adjoint: null argument");
   FV3B_REQUIRE(grid == 0 || grid == 1, "fv3b_halo_update_vector_adjoint: grid must be 0 (D) or 1 (C)");
   FV3B_REQUIRE(nlev >= 1 && nlev <= ctx->d.nk, "fv3b_halo_update_vector_adjoint: nlev out of range");
@@ -89,10 +91,11 @@ extern "C" int fv3b_halo_update_vector_adjoint(fv3b_ctx* ctx, real* gx, real* gy
 // Adjoint of fv3b_synchronize_vector_interfaces, in place on gu, gv.
 extern "C" int fv3b_synchronize_vector_interfaces_adjoint(fv3b_ctx* ctx, real* gu, real* gv, int nlev,
                                                           void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && gu && gv, "fv3b_synchronize_vector_interfaces_adjoint: null argument");
   FV3B_REQUIRE(nlev >= 1 && nlev <= ctx->d.nk, "fv3b_synchronize_vector_interfaces_adjoint: nlev out of range");
   const Dims d = ctx->d;
-  dim3 grid((d.n + HALO_ADJ_BLOCK - 1) / HALO_ADJ_BLOCK, 12);
+  dim3 grid((d.n + HALO_ADJ_BLOCK - 1) / HALO_ADJ_BLOCK, 2 * d.nt);
   for (int zero = 0; zero < 2; ++zero) {
     interface_sync_adjoint_kernel<<<grid, HALO_ADJ_BLOCK, 0, (cudaStream_t)stream>>>(d, gu, gv, nlev, zero);
     note_launch();

@@ -20,7 +20,7 @@ namespace {
 cudaError_t a2b_transpose(const Dims d, const adj::A2BGrid<real> g, const real* gout, real* gin, real* gqx,
                           real* gqy, real* gedges, int k0, int k1, cudaStream_t st) {
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, n = d.n;
-  const size_t bytes = sizeof(real) * (size_t)6 * d.st;
+  const size_t bytes = sizeof(real) * (size_t)d.nt * d.st;
   cudaError_t err;
   if ((err = cudaMemsetAsync(gqx, 0, bytes, st)) != cudaSuccess) return err;
   if ((err = cudaMemsetAsync(gqy, 0, bytes, st)) != cudaSuccess) return err;
@@ -57,6 +57,7 @@ extern "C" int fv3b_nh_p_grad_adjoint(fv3b_ctx* ctx, const real* pp, const real*
                                       const real* ggz, const real* gpk3, real* g_u, real* g_v, real* g_pp,
                                       real* g_gz, real* g_pk3, real* g_delp, double dt_in, double ptop, double akap,
                                       void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && pp && gz && pk3 && delp && gu && gv && gpp && ggz && gpk3 && g_u && g_v && g_pp && g_gz &&
                    g_pk3 && g_delp,
                "fv3b_nh_p_grad_adjoint: null argument");

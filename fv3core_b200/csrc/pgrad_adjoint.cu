@@ -10,6 +10,7 @@ using namespace fv3b;
 extern "C" int fv3b_p_grad_c_adjoint(fv3b_ctx* ctx, const real* delpc, const real* pkc, const real* gz,
                                      const real* gu, const real* gv, real* g_delpc, real* g_pkc, real* g_gz,
                                      double dt2_in, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && delpc && pkc && gz && gu && gv && g_delpc && g_pkc && g_gz,
                "fv3b_p_grad_c_adjoint: null argument");
   const real dt2 = static_cast<real>(dt2_in);

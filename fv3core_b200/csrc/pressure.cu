@@ -16,6 +16,7 @@ using namespace fv3b;
 // p_grad_c_stencil, nonhydrostatic (wk = delpc), on [is, ie+1] x [js, je+1].
 extern "C" int fv3b_p_grad_c(fv3b_ctx* ctx, real* uc, real* vc, const real* delpc, const real* pkc,
                              const real* gz, double dt2_in, void* stream) {
+  FV3B_TILES(ctx);
   // the build's precision inside the kernels (the same value in FP64 builds)
   const real dt2 = static_cast<real>(dt2_in);
   FV3B_REQUIRE(ctx && uc && vc && delpc && pkc && gz, "fv3b_p_grad_c: null argument");
@@ -42,6 +43,7 @@ extern "C" int fv3b_p_grad_c(fv3b_ctx* ctx, real* uc, real* vc, const real* delp
 // wind update: level 0 of pp and pk3 is read as its new value (0, ptop^akap).
 extern "C" int fv3b_nh_p_grad(fv3b_ctx* ctx, real* u, real* v, real* pp, real* gz, real* pk3,
                               real* delp, double dt_in, double ptop, double akap, void* stream) {
+  FV3B_TILES(ctx);
   // the build's precision inside the kernels (the same value in FP64 builds)
   const real dt = static_cast<real>(dt_in);
   FV3B_REQUIRE(ctx && u && v && pp && gz && pk3 && delp, "fv3b_nh_p_grad: null argument");
@@ -98,6 +100,7 @@ extern "C" int fv3b_nh_p_grad(fv3b_ctx* ctx, real* u, real* v, real* pp, real* g
 // edge_pe (pe_halo.py:6-33): interface pressure on the one-cell ring around
 // the compute domain, summed from ptop.
 extern "C" int fv3b_edge_pe(fv3b_ctx* ctx, real* pe, const real* delp, double ptop, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && pe && delp, "fv3b_edge_pe: null argument");
   const Dims d = ctx->d;
   cudaStream_t st = (cudaStream_t)stream;
@@ -120,6 +123,7 @@ extern "C" int fv3b_edge_pe(fv3b_ctx* ctx, real* pe, const real* delp, double pt
 // levels 1..npz.
 extern "C" int fv3b_pk3_halo(fv3b_ctx* ctx, real* pk3, const real* delp, double ptop, double akap,
                              void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && pk3 && delp, "fv3b_pk3_halo: null argument");
   const Dims d = ctx->d;
   cudaStream_t st = (cudaStream_t)stream;

@@ -8,11 +8,12 @@
 using namespace fv3b;
 
 extern "C" int fv3b_edge_pe_adjoint(fv3b_ctx* ctx, real* g_pe, real* g_delp, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && g_pe && g_delp, "fv3b_edge_pe_adjoint: null argument");
   const Dims d = ctx->d;
   cudaStream_t st = (cudaStream_t)stream;
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nk = d.nk;
-  FV3B_CHECK(cudaMemsetAsync(g_delp, 0, sizeof(real) * (size_t)6 * d.st, st));
+  FV3B_CHECK(cudaMemsetAsync(g_delp, 0, sizeof(real) * (size_t)d.nt * d.st, st));
   FV3B_CHECK(launch_columns(s - 1, e + 2, js - 1, je + 2, st, [=] __device__(int t, int i, int j) {
     if (i >= s && i <= e && j >= js && j <= je) return;
     const idx_t o = idx3(d, t, i, j, 0);
@@ -23,12 +24,13 @@ extern "C" int fv3b_edge_pe_adjoint(fv3b_ctx* ctx, real* g_pe, real* g_delp, voi
 
 extern "C" int fv3b_pk3_halo_adjoint(fv3b_ctx* ctx, const real* delp, real* g_pk3, real* g_delp, double ptop,
                                      double akap, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && delp && g_pk3 && g_delp, "fv3b_pk3_halo_adjoint: null argument");
   const Dims d = ctx->d;
   FV3B_REQUIRE(d.nk <= 128, "fv3b_pk3_halo_adjoint: npz must be at most 127");
   cudaStream_t st = (cudaStream_t)stream;
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec, nk = d.nk;
-  FV3B_CHECK(cudaMemsetAsync(g_delp, 0, sizeof(real) * (size_t)6 * d.st, st));
+  FV3B_CHECK(cudaMemsetAsync(g_delp, 0, sizeof(real) * (size_t)d.nt * d.st, st));
   FV3B_CHECK(launch_columns(s - 2, e + 3, js - 2, je + 3, st, [=] __device__(int t, int i, int j) {
     if (i >= s && i <= e && j >= js && j <= je) return;
     const idx_t o = idx3(d, t, i, j, 0);

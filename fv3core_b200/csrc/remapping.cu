@@ -552,7 +552,7 @@ template <int NK>
 cudaError_t launch_tracers_nk(const RemapArgs& a, int i0, int i1, int j0, int j1, cudaStream_t s) {
   const int block = launch_shape().col;
   const int ncol = (i1 - i0) * (j1 - j0);
-  dim3 grid((ncol + block - 1) / block, 6, NTRACER);
+  dim3 grid((ncol + block - 1) / block, tile_slots(), NTRACER);
   tracer_kernel<NK><<<grid, block, 0, s>>>(a, i0, i1, j0, j1);
   note_launch();
   return cudaGetLastError();
@@ -661,6 +661,7 @@ bool kord_ok(int kord) { return kord >= -10 && kord <= 10 && kord != 0; }
 }  // namespace
 
 extern "C" int fv3b_remap_setup(fv3b_ctx* ctx, const double* ak, const double* bk) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && ak && bk, "fv3b_remap_setup: null argument");
   const int nlev = ctx->d.nz + 1;
   FV3B_REQUIRE(nlev <= MAXLEV, "fv3b_remap_setup: npz out of range");
@@ -683,6 +684,7 @@ extern "C" int fv3b_lagrangian_to_eulerian(fv3b_ctx* ctx, const fv3b_remap_field
                                            const fv3b_remap_config* config, const fv3b_sat_adjust_config* sat,
                                            double ptop, double akap, double zvir, double mdt, int kmp,
                                            int last_step, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && fields && config, "fv3b_lagrangian_to_eulerian: null argument");
   const fv3b_remap_fields& f = *fields;
   for (int n = 0; n < NTRACER; ++n) FV3B_REQUIRE(f.tracers[n], "fv3b_lagrangian_to_eulerian: null tracer");

@@ -48,6 +48,7 @@ struct fv3b_transport {
 
 extern "C" int fv3b_transport_create(fv3b_ctx* ctx, int hord, const double* nord, const double* damp_c, int n,
                                      fv3b_transport** out) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && out, "fv3b_transport_create: null argument");
   FV3B_REQUIRE(hord_supported(hord), "fv3b_transport_create: hord must be 5, 6, 7 or 8");
   FV3B_REQUIRE((nord == nullptr) == (damp_c == nullptr),
@@ -155,6 +156,7 @@ cudaError_t launch_ppm_box(const Dims d, const real* dxa, const Box b, const rea
 extern "C" int fv3b_fvtp2d(const fv3b_transport* tr, real* q, const real* crx, const real* cry,
                            const real* x_area_flux, const real* y_area_flux, real* q_x_flux, real* q_y_flux,
                            const real* x_mass_flux, const real* y_mass_flux, const real* mass, void* stream) {
+  FV3B_TILES((tr ? tr->ctx : nullptr));
   FV3B_REQUIRE(tr && q && crx && cry && x_area_flux && y_area_flux && q_x_flux && q_y_flux,
                "fv3b_fvtp2d: null argument");
   // fvtp2d.py:289-296
@@ -170,6 +172,7 @@ extern "C" int fv3b_fvtp2d(const fv3b_transport* tr, real* q, const real* crx, c
 // each interface of the box along the axis.
 extern "C" int fv3b_ppm_flux(fv3b_ctx* ctx, int axis, int iord, const real* q, const real* c, real* flux, int i0,
                              int j0, int k0, int ni, int nj, int nk, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && q && c && flux, "fv3b_ppm_flux: null argument");
   FV3B_REQUIRE(axis == 0 || axis == 1, "fv3b_ppm_flux: axis must be 0 (x) or 1 (y)");
   FV3B_REQUIRE(hord_supported(iord), "fv3b_ppm_flux: iord must be 5, 6, 7 or 8");
@@ -204,6 +207,7 @@ extern "C" int fv3b_ppm_flux(fv3b_ctx* ctx, int axis, int iord, const real* q, c
 // TracerAdvection.__call__ (tracer_2d_1l.py:199-300).
 extern "C" int fv3b_tracer_advection(const fv3b_transport* tr, int ntracers, real* const* tracers, real* dp1,
                                      real* mfxd, real* mfyd, real* cxd, real* cyd, double mdt, void* stream) {
+  FV3B_TILES((tr ? tr->ctx : nullptr));
   (void)mdt;  // unused by the reference as well
   FV3B_REQUIRE(tr && dp1 && mfxd && mfyd && cxd && cyd && (ntracers == 0 || tracers),
                "fv3b_tracer_advection: null argument");

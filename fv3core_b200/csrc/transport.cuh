@@ -567,7 +567,7 @@ inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const real*
     const int lo = nmax - p;
     DelnIterArgs a{d, g, col, out_x(p - 1), out_y(p - 1), out_x(p), out_y(p), cb,
                    lo, s - lo, e + 2 + lo, js - lo, je + 2 + lo, nz, p == nmax};
-    const dim3 grid((a.i1 - a.i0 + DELN_TX - 1) / DELN_TX, (a.j1 - a.j0 + DELN_TY - 1) / DELN_TY, 6 * nz);
+    const dim3 grid((a.i1 - a.i0 + DELN_TX - 1) / DELN_TX, (a.j1 - a.j0 + DELN_TY - 1) / DELN_TY, tile_slots() * nz);
     deln_iter_kernel<<<grid, dim3(DELN_TX, DELN_TY, 1), 0, st>>>(a);
     note_launch();
     cudaError_t err = cudaGetLastError();

@@ -40,6 +40,7 @@ __device__ __forceinline__ real p_weighted(const real* dp0, int k, int nk, real 
 // UpdateGeopotentialHeightOnCGrid.__call__ (updatedzc.py:123-163).
 extern "C" int fv3b_update_dz_c(fv3b_ctx* ctx, const real* dp_ref, const real* zs, const real* ut,
                                 const real* vt, real* gz, real* ws, double dt_in, void* stream) {
+  FV3B_TILES(ctx);
   // the build's precision inside the kernels (the same value in FP64 builds)
   const real dt = static_cast<real>(dt_in);
   FV3B_REQUIRE(ctx && dp_ref && zs && ut && vt && gz && ws, "fv3b_update_dz_c: null argument");
@@ -105,6 +106,7 @@ extern "C" int fv3b_update_dz_c(fv3b_ctx* ctx, const real* dp_ref, const real* z
 // UpdateHeightOnDGrid.__init__ (updatedzd.py:189-320): the cubic-spline
 // constants of cubic_spline_interpolation_constants (121-145) from dp0.
 extern "C" int fv3b_update_dz_d_setup(fv3b_ctx* ctx, const double* dp_ref_host, int hord_tm) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && dp_ref_host, "fv3b_update_dz_d_setup: null argument");
   FV3B_REQUIRE(ctx->dsw.ready, "fv3b_update_dz_d_setup: call fv3b_d_sw_setup first (column namelist)");
   const int nk = ctx->d.nk;
@@ -130,6 +132,7 @@ extern "C" int fv3b_update_dz_d_setup(fv3b_ctx* ctx, const double* dp_ref_host, 
 // UpdateHeightOnDGrid.__call__ (updatedzd.py:323-393).
 extern "C" int fv3b_update_dz_d(fv3b_ctx* ctx, const real* zs, real* zh, const real* crx, const real* cry,
                                 const real* xfx, const real* yfx, real* wsd, double dt_in, void* stream) {
+  FV3B_TILES(ctx);
   // the build's precision inside the kernels (the same value in FP64 builds)
   const real dt = static_cast<real>(dt_in);
   FV3B_REQUIRE(ctx && zs && zh && crx && cry && xfx && yfx && wsd, "fv3b_update_dz_d: null argument");

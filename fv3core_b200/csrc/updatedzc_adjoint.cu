@@ -14,6 +14,7 @@ using namespace fv3b;
 extern "C" int fv3b_update_dz_c_adjoint(fv3b_ctx* ctx, const real* dp_ref, const real* ut, const real* vt,
                                         const real* gz, const real* g_gz_out, const real* g_ws, real* g_gz,
                                         real* g_ut, real* g_vt, double dt_in, void* stream) {
+  FV3B_TILES(ctx);
   FV3B_REQUIRE(ctx && dp_ref && ut && vt && gz && g_gz_out && g_ws && g_gz && g_ut && g_vt,
                "fv3b_update_dz_c_adjoint: null argument");
   const Dims d = ctx->d;

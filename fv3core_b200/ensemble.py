@@ -1,10 +1,14 @@
 """Ensembles of independent cubed-sphere states advanced together.
 
-Each member is a full AcousticDynamics problem (its own grid, context and
-state) at its own resolution.  ``step`` enqueues one AcousticDynamics call
-(n_split acoustic substeps) per member, eagerly; ``capture`` records the
-whole ensemble step, every member's launches, in one CUDA graph, so a step
-costs one graph launch instead of ~1000 kernel launches per member.
+The members of one resolution form a ``MemberGroup``: their states live in
+one batched context (``GridData(members=M)``, fv3b_ctx_create_batched), so
+every kernel of an AcousticDynamics call advances all of them in one launch
+(the grid's tile dimension covers 6 x M tile slots; halo updates stay
+within a member).  An ensemble at mixed resolutions is one group per
+resolution, and a step is one AcousticDynamics call per group.  ``capture``
+records a whole ensemble step in one CUDA graph.  ``Member`` (one context
+per member, one call per member) is the unbatched form, kept for
+comparison.
 """
 import types
 
@@ -61,17 +65,70 @@ class Member:
         self.grid_data.close()
 
 
-class Ensemble:
-    """members: iterable of (n, npz, seed)."""
+class MemberGroup:
+    """Members of one resolution (n, npz), one seed each, in one batched
+    context: every kernel of a step covers all of them."""
 
-    def __init__(self, members, precision="f64", n_split=6):
+    def __init__(self, n, npz, seeds, precision="f64", n_split=6, mdt=225.0, noise=1.0e-3, grid=None):
+        self.n, self.npz, self.seeds = n, npz, list(seeds)
+        grid = CubedSphereGrid(n, 3) if grid is None else grid
+        states = [baroclinic_state(grid, npz, seed=s, noise=noise) for s in self.seeds]
+        st0 = states[0]
+        self.grid_data = GridData(grid, npz, precision=precision, members=len(self.seeds))
+        gi = self.grid_data.grid_indexing
+        state = types.SimpleNamespace()
+        for name in _lib.DYCORE_FIELDS:
+            parts = [st[name] if name in st else np.zeros(st["phis"].shape if name == "wsd" else st["delp"].shape)
+                     for st in states]
+            setattr(state, name, to_device(np.concatenate(parts, axis=0), dtype=gi.dtype))
+        state.mdt, state.n_map, state.akap = mdt, 1, 287.05 / 1004.6
+        state.ptop, state.ks = st0["ptop"], st0["ks"]
+        self.state = state
+        self.dynamics = AcousticDynamics(
+            DeviceCubedSphereCommunicator(gi), StencilFactory(StencilConfig(), gi), self.grid_data, self.grid_data,
+            0, False, False, baroclinic_acoustic_config(n_split=n_split), st0["ak"], st0["bk"], st0["pfull"],
+            state.phis,
+        )
+        self.cell_levels = len(self.seeds) * 6 * n * n * npz
+        self._initial = None
+
+    def member_field(self, name, m):
+        """Member m's tiles of a state field (a view)."""
+        return getattr(self.state, name)[6 * m:6 * m + 6]
+
+    keep_initial = Member.keep_initial
+    reset = Member.reset
+    step = Member.step
+    close = Member.close
+
+
+class Ensemble:
+    """members: iterable of (n, npz, seed).  ``batched`` (default): the
+    members of each resolution share one batched context (MemberGroup), in
+    the order in which their resolutions first appear; otherwise one context
+    per member."""
+
+    def __init__(self, members, precision="f64", n_split=6, batched=True):
         self.n_split = n_split
         grids = {}
-        self.members = []
+        members = list(members)
         for n, npz, seed in members:
             if n not in grids:
                 grids[n] = CubedSphereGrid(n, 3)
-            self.members.append(Member(n, npz, seed, precision, n_split, grid=grids[n]))
+        self.members = []
+        if batched:
+            order = []
+            seeds = {}
+            for n, npz, seed in members:
+                if (n, npz) not in seeds:
+                    order.append((n, npz))
+                    seeds[(n, npz)] = []
+                seeds[(n, npz)].append(seed)
+            for n, npz in order:
+                self.members.append(MemberGroup(n, npz, seeds[(n, npz)], precision, n_split, grid=grids[n]))
+        else:
+            for n, npz, seed in members:
+                self.members.append(Member(n, npz, seed, precision, n_split, grid=grids[n]))
 
     @property
     def cell_levels(self):

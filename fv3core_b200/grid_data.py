@@ -43,17 +43,26 @@ class Metrics(ctypes.Structure):
 
 
 class GridData:
-    """All metric terms of an n x n cube on the GPU, plus the stage context."""
+    """All metric terms of an n x n cube on the GPU, plus the stage context.
 
-    def __init__(self, grid: CubedSphereGrid, npz: int, device="cuda", precision="f64"):
+    ``members`` > 1 makes the context of an ensemble of that many cubes of
+    this grid advanced together (fv3b_ctx_create_batched): every field then
+    holds 6 x members tile slots, and the metric terms are repeated for each
+    member."""
+
+    def __init__(self, grid: CubedSphereGrid, npz: int, device="cuda", precision="f64", members=1):
         self.grid = grid
         self.precision = precision
-        self.grid_indexing = GridIndexing((grid.n, grid.n, npz), grid.halo, precision=precision)
+        self.members = int(members)
+        self.grid_indexing = GridIndexing((grid.n, grid.n, npz), grid.halo, precision=precision,
+                                          members=self.members)
         tdtype = self.grid_indexing.dtype
         self.device = device
         self.tensors = {}
         for name in METRIC_FIELDS + EXTRA_FIELDS:
             a = np.asarray(getattr(grid, name), dtype=np.float64)
+            if self.members > 1:  # the same metric terms for every member
+                a = np.concatenate([a] * self.members, axis=0)
             if a.ndim == 3 and name != "a2b_extrap":  # [6, i, j] -> [6, j, i]
                 t = torch.from_numpy(np.ascontiguousarray(a.transpose(0, 2, 1))).to(device=device, dtype=tdtype)
             else:  # edge factors [6, n+1], corner ratios [6, 4, 3]
@@ -70,12 +79,13 @@ class GridData:
         self._metrics = m
         self._dims = self.grid_indexing.dims()
         L = _lib.lib(precision)
-        L.fv3b_ctx_create.argtypes = [ctypes.POINTER(_lib.GridDims), ctypes.POINTER(Metrics), ctypes.POINTER(ctypes.c_void_p)]
-        L.fv3b_ctx_create.restype = ctypes.c_int
+        L.fv3b_ctx_create_batched.argtypes = [ctypes.POINTER(_lib.GridDims), ctypes.POINTER(Metrics), ctypes.c_int,
+                                              ctypes.POINTER(ctypes.c_void_p)]
+        L.fv3b_ctx_create_batched.restype = ctypes.c_int
         L.fv3b_ctx_destroy.argtypes = [ctypes.c_void_p]
         L.fv3b_ctx_destroy.restype = ctypes.c_int
         ctx = ctypes.c_void_p()
-        rc = L.fv3b_ctx_create(ctypes.byref(self._dims), ctypes.byref(m), ctypes.byref(ctx))
+        rc = L.fv3b_ctx_create_batched(ctypes.byref(self._dims), ctypes.byref(m), self.members, ctypes.byref(ctx))
         if rc != 0:
             raise RuntimeError(f"fv3b_ctx_create failed ({rc}): {L.fv3b_last_error().decode()}")
         self.ctx = ctx

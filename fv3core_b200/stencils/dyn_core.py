@@ -73,7 +73,8 @@ class AcousticDynamics:
             raise KeyError(name)
         ptr = _lib.lib(self._gi.precision).fv3b_acoustics_temporary(self._ctx, name.encode())
         m, _, nk = self._gi.max_shape
-        shape = {"ws3": (6, m, m), "zs": (6, m, m), "dp_ref": (nk,)}.get(name, (6, nk, m, m))
+        nt = self._gi.ntiles
+        shape = {"ws3": (nt, m, m), "zs": (nt, m, m), "dp_ref": (nk,)}.get(name, (nt, nk, m, m))
 
         class _View:
             __cuda_array_interface__ = {"shape": shape, "typestr": "<f4" if self._gi.precision == "f32" else "<f8",

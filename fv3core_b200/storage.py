@@ -17,8 +17,11 @@ class GridIndexing:
     for all six tiles of an n x n x npz cube."""
 
     def __init__(self, domain, n_halo=3, south_edge=True, north_edge=True, west_edge=True, east_edge=True,
-                 precision="f64"):
+                 precision="f64", members=1):
         self.domain = tuple(int(x) for x in domain)
+        # cubes held in every array: 1, or the members of a batched ensemble
+        # (member m owns tile slots 6m .. 6m+5)
+        self.members = int(members)
         self.n_halo = int(n_halo)
         if self.domain[0] != self.domain[1]:
             raise ValueError("cube tiles must be square")
@@ -30,6 +33,10 @@ class GridIndexing:
         self.context = None
         # "f64" (FP64 fields) or "f32" (the mixed-precision build's FP32 fields)
         self.precision = precision
+
+    @property
+    def ntiles(self):
+        return 6 * self.members
 
     @property
     def dtype(self):
@@ -66,10 +73,11 @@ class GridIndexing:
 def empty(gi: GridIndexing, kind="3d", device="cuda", dtype=None):
     m, _, nk = gi.max_shape
     dtype = gi.dtype if dtype is None else dtype
+    nt = gi.ntiles
     if kind == "3d":
-        t = torch.empty((6, nk, m, m), device=device, dtype=dtype)
+        t = torch.empty((nt, nk, m, m), device=device, dtype=dtype)
     elif kind == "2d":
-        t = torch.empty((6, m, m), device=device, dtype=dtype)
+        t = torch.empty((nt, m, m), device=device, dtype=dtype)
     elif kind == "1d":
         t = torch.empty((nk,), device=device, dtype=dtype)
     else:
@@ -111,7 +119,8 @@ def as_reference_view(t: torch.Tensor) -> torch.Tensor:
 
 def check_field(t, gi, kind, name):
     m, _, nk = gi.max_shape
-    want = {"3d": (6, nk, m, m), "2d": (6, m, m), "1d": (nk,)}[kind]
+    nt = gi.ntiles
+    want = {"3d": (nt, nk, m, m), "2d": (nt, m, m), "1d": (nk,)}[kind]
     if not isinstance(t, torch.Tensor):
         raise TypeError(f"{name}: expected a torch tensor in device layout, got {type(t).__name__}")
     if tuple(t.shape) != want or not t.is_contiguous():

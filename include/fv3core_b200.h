@@ -90,6 +90,19 @@ typedef struct fv3b_ctx fv3b_ctx;
 
 /* Allocates the workspace (cudaMalloc) on the current device. */
 int fv3b_ctx_create(const fv3b_grid_dims* dims, const fv3b_metrics* metrics, fv3b_ctx** out);
+
+/*
+ * A context for an ensemble of `members` cubes of the same grid, advanced
+ * together: every array of the context's calls holds 6 x members tile slots
+ * (member m owns tiles 6m .. 6m+5, i.e. fields fv3b_real[6 x members][npz+1]
+ * [n+2h+1][n+2h+1]), including the metric terms, which the caller repeats
+ * for every member.  Each stage call then advances all members in one
+ * launch per kernel; halo updates stay within a member.  The reference has
+ * no counterpart (it runs one cube per process); it replaces running
+ * members one at a time.  The adjoint entry
+ * points serve single cubes only.
+ */
+int fv3b_ctx_create_batched(const fv3b_grid_dims* dims, const fv3b_metrics* metrics, int members, fv3b_ctx** out);
 int fv3b_ctx_destroy(fv3b_ctx* ctx);
 
 /*

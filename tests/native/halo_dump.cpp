@@ -22,6 +22,16 @@ static void dump(const fv3b::Dims& d, const char* kind, const int sx[2], const i
 
 int main(int argc, char** argv) {
   int n = argc > 1 ? atoi(argv[1]) : 12;
+  if (argc > 2) {  // "edges": the tile connectivity of 24 tile slots (four batched cubes)
+    for (int t = 0; t < 24; ++t)
+      for (int edge = 0; edge < 4; ++edge) {
+        int t2, e2;
+        bool rev;
+        fv3b::edge_neighbor(t, edge, t2, e2, rev);
+        printf("edge %d %d %d %d %d\n", t, edge, t2, e2, rev ? 1 : 0);
+      }
+    return 0;
+  }
   fv3b_grid_dims g{n, 3, 8, 0};
   fv3b::Dims d = fv3b::make_dims(&g);
   const int centre[2] = {1, 1}, corner[2] = {0, 0};
