@@ -760,11 +760,15 @@ def _parse_members(spec):
 
 
 def run_ensemble(args):
-    """Ensemble of seed-perturbed members at mixed resolutions, one
-    AcousticDynamics call per member per step: eager launches against one
-    CUDA graph of the whole ensemble step, optionally after the launch-shape
-    autotuner.  Each step first returns every member to its initial state
-    (a device-to-device copy, inside both timings)."""
+    """Ensemble of seed-perturbed members at mixed resolutions (BASELINE
+    configuration 4): the members of each resolution batched in one context,
+    so every kernel of an AcousticDynamics call advances all of them in one
+    launch, one CUDA graph per ensemble step, optionally after the
+    launch-shape autotuner; against the same members one at a time (one
+    context and one call per member), eager and as one graph.  Each step
+    first returns every member to its initial state (a device-to-device
+    copy, inside every timing).  The two forms run in turn, so one ensemble
+    is on the device at a time."""
     import torch
 
     from fv3core_b200 import _lib, autotune
@@ -781,22 +785,13 @@ def run_ensemble(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     prec = "f64" if args.precision == "f64" else "f32"
     spec = _parse_members(args.members)
-    ens = Ensemble([(n, npz, 1000 * rank + q) for q, (n, npz) in enumerate(spec)], precision=prec,
-                   n_split=args.n_split)
-    ens.step()  # the first call uploads per-level factors
-    ens.keep_initial()
+    members = [(n, npz, 1000 * rank + q) for q, (n, npz) in enumerate(spec)]
     stream = torch.cuda.current_stream()
 
     def barrier():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
-
-    shape = _lib.get_launch_shape(prec)
-    tuned = None
-    if args.autotune:
-        shape, timings = autotune.tune(lambda: ens.step(reset=True), precision=prec, repeats=1)
-        tuned = {"x".join(map(str, k)): round(v, 3) for k, v in timings.items()}
 
     def timed(run):
         for _ in range(args.warmup):
@@ -811,32 +806,56 @@ def run_ensemble(args):
                 run()
             b.record(stream)
             barrier()
-        return a.elapsed_time(b) / args.steps, _lib.launch_count(prec) - l0, clk.summary()
+        return a.elapsed_time(b) / args.steps, (_lib.launch_count(prec) - l0) // args.steps, clk.summary()
 
-    eager_ms, eager_launches, _ = timed(lambda: ens.step(reset=True))
-    graph = ens.capture(reset=True)
-    graph_ms, _, clocks = timed(graph.replay)
-    graph_launches = eager_launches  # the graph replays the same kernels
-    eager_ms, graph_ms = max_over_ranks([eager_ms, graph_ms], dist)
-    cells = ens.cell_levels * args.n_split * world
+    results = {}
+    shape = _lib.get_launch_shape(prec)
+    tuned = None
+    cell_levels = None
+    for mode in ("one_at_a_time", "batched"):
+        ens = Ensemble(members, precision=prec, n_split=args.n_split, batched=(mode == "batched"))
+        cell_levels = ens.cell_levels
+        ens.step()  # the first call uploads per-level factors
+        ens.keep_initial()
+        if mode == "batched" and args.autotune:
+            shape, timings = autotune.tune(lambda: ens.step(reset=True), precision=prec, repeats=1)
+            tuned = {"x".join(map(str, k)): round(v, 3) for k, v in timings.items()}
+        eager_ms, eager_launches, _ = timed(lambda: ens.step(reset=True))
+        graph = ens.capture(reset=True)
+        graph_ms, _, clocks = timed(graph.replay)
+        results[mode] = {"eager_ms": eager_ms, "graph_ms": graph_ms, "launches": eager_launches, "clocks": clocks,
+                         "contexts": len(ens.members)}
+        del graph
+        ens.close()
+        torch.cuda.empty_cache()
+    vals = max_over_ranks([results[m][k] for m in ("one_at_a_time", "batched") for k in ("eager_ms", "graph_ms")],
+                          dist)
+    results["one_at_a_time"]["eager_ms"], results["one_at_a_time"]["graph_ms"] = vals[0], vals[1]
+    results["batched"]["eager_ms"], results["batched"]["graph_ms"] = vals[2], vals[3]
+    cells = cell_levels * args.n_split * world
+    bt, one = results["batched"], results["one_at_a_time"]
     line = {
-        "metric": "ensemble acoustic-substep cell-levels/s", "value": cells / (graph_ms * 1e-3),
+        "metric": "ensemble acoustic-substep cell-levels/s", "value": cells / (bt["graph_ms"] * 1e-3),
         "unit": "cell-levels/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": graph_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": bt["graph_ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "mixed: f32 fields and arithmetic, f64 column solves" if prec == "f32" else "f64",
         "data": "synthetic (seeded baroclinic-wave states, one seed per member)",
-        "config": {"workload": f"ensemble {args.members} (count x n x npz), n_split={args.n_split}, one CUDA "
-                               "graph per ensemble step; each step resets the members to their initial state",
-                   "members": len(spec), "cell_levels": ens.cell_levels, "launch_shape": list(shape),
-                   "autotune_ms": tuned, "l2": "inputs larger than L2 in total; no flush"},
-        "clocks": clocks, "gpu_launches": graph_launches,
-        "eager": {"value": cells / (eager_ms * 1e-3), "ms_per_step": eager_ms},
-        "graph_speedup_vs_eager": eager_ms / graph_ms,
+        "config": {"workload": f"ensemble {args.members} (count x n x npz), n_split={args.n_split}: the members of "
+                               "each resolution batched in one context (one launch per kernel per resolution), "
+                               "one CUDA graph per ensemble step; each step resets the members to their initial "
+                               "state",
+                   "members": len(spec), "batched_contexts": bt["contexts"], "cell_levels": cell_levels,
+                   "launch_shape": list(shape), "autotune_ms": tuned, "l2": "inputs larger than L2 in total; no flush"},
+        "clocks": bt["clocks"], "gpu_launches": bt["launches"],
+        "batched_eager": {"value": cells / (bt["eager_ms"] * 1e-3), "ms_per_step": bt["eager_ms"]},
+        "one_at_a_time": {"value": cells / (one["eager_ms"] * 1e-3), "ms_per_step": one["eager_ms"],
+                          "gpu_launches": one["launches"], "contexts": one["contexts"],
+                          "graph": {"value": cells / (one["graph_ms"] * 1e-3), "ms_per_step": one["graph_ms"]}},
+        "batched_speedup_vs_one_at_a_time": one["eager_ms"] / bt["graph_ms"],
+        "graph_speedup_vs_eager": bt["eager_ms"] / bt["graph_ms"],
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
-    del graph
-    ens.close()
     if dist is not None:
         dist.destroy_process_group()
 
