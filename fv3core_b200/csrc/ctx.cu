@@ -59,9 +59,11 @@ extern "C" int fv3b_ctx_destroy(fv3b_ctx* ctx) {
   cudaError_t e = cudaFree(ctx->ws_base);
   cudaError_t e2 = cudaFree(ctx->col);
   cudaError_t e3 = cudaFree(ctx->remap_akbk);
+  cudaError_t e4 = cudaFree(ctx->sat_tables);
   delete ctx;
   if (e == cudaSuccess) e = e2;
   if (e == cudaSuccess) e = e3;
+  if (e == cudaSuccess) e = e4;
   FV3B_CHECK(e);
   return FV3B_OK;
 }

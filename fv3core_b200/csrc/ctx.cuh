@@ -64,6 +64,9 @@ struct fv3b_ctx {
   // set by fv3b_remap_setup
   double* remap_akbk = nullptr;
   int remap_nlev = 0;
+  // the saturation adjustment's tables (es and its differences over water
+  // and ice), [4][2624] doubles, filled by fv3b_remap_setup
+  double* sat_tables = nullptr;
 };
 
 namespace fv3b {

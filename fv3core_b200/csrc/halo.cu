@@ -1,7 +1,8 @@
 // Device halo updates of the six-tile array (see halo.cuh for the
-// geometry).  One thread per (tile, edge-halo point), looping over the
-// levels, so each thread decodes its source once; up to four fields of the
-// same staggering share a launch.
+// geometry).  One thread per (tile, edge-halo point, level): the copies of
+// all levels go out at once instead of one level after another (the copies
+// are small, so their latency, not their bytes, sets a launch's time); up
+// to four fields of the same staggering share a launch.
 #include "ctx.cuh"
 #include "halo.cuh"
 #include "halo_ops.cuh"
@@ -16,25 +17,25 @@ struct FieldSet {
   int n;
 };
 
-__global__ void halo_scalar_kernel(Dims d, FieldSet fs, int sx, int sy, int n_halo, int nlev) {
+__global__ void halo_scalar_kernel(Dims d, FieldSet fs, int sx, int sy, int n_halo) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  const int t = blockIdx.y;
+  const int t = blockIdx.y, k = blockIdx.z;
   if (p >= halo_candidates(d, n_halo)) return;
   int i, j;
   if (!halo_point(d, p, sx, sy, n_halo, i, j)) return;
   const int sxo[2] = {sx, sx}, syo[2] = {sy, sy};
   HaloSource src;
   if (!halo_source(d, t, i, j, 0, sxo, syo, n_halo, src)) return;
-  const idx_t dst = idx3(d, t, i, j, 0), from = idx3(d, src.t, src.i, src.j, 0);
+  const idx_t dst = idx3(d, t, i, j, k), from = idx3(d, src.t, src.i, src.j, k);
   for (int q = 0; q < fs.n; ++q) {
     real* f = fs.f[q];
-    for (int k = 0; k < nlev; ++k) f[dst + k * d.sk] = f[from + k * d.sk];
+    f[dst] = f[from];
   }
 }
 
-__global__ void halo_vector_kernel(Dims d, real* x, real* y, int cgrid, int nlev) {
+__global__ void halo_vector_kernel(Dims d, real* x, real* y, int cgrid) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  const int t = blockIdx.y >> 1, comp = blockIdx.y & 1;
+  const int t = blockIdx.y >> 1, comp = blockIdx.y & 1, k = blockIdx.z;
   const int n_halo = d.h;
   if (p >= halo_candidates(d, n_halo)) return;
   // D grid: x (u) on (centre, interface), y (v) on (interface, centre);
@@ -48,13 +49,12 @@ __global__ void halo_vector_kernel(Dims d, real* x, real* y, int cgrid, int nlev
   real* dstf = comp == 0 ? x : y;
   const real* srcf = src.comp == 0 ? x : y;
   const real sign = (real)src.sign;
-  const idx_t dst = idx3(d, t, i, j, 0), from = idx3(d, src.t, src.i, src.j, 0);
-  for (int k = 0; k < nlev; ++k) dstf[dst + k * d.sk] = sign * srcf[from + k * d.sk];
+  dstf[idx3(d, t, i, j, k)] = sign * srcf[idx3(d, src.t, src.i, src.j, k)];
 }
 
-__global__ void interface_sync_kernel(Dims d, real* u, real* v, int nlev) {
+__global__ void interface_sync_kernel(Dims d, real* u, real* v) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
-  const int t = blockIdx.y >> 1, comp = blockIdx.y & 1;
+  const int t = blockIdx.y >> 1, comp = blockIdx.y & 1, k = blockIdx.z;
   if (a >= d.n) return;
   HaloSource dst;
   interface_sync_target(d, t, comp == 0 ? EDGE_S : EDGE_W, a, dst);
@@ -62,20 +62,20 @@ __global__ void interface_sync_kernel(Dims d, real* u, real* v, int nlev) {
   const real* srcf = comp == 0 ? u : v;
   real* dstf = dst.comp == 0 ? u : v;
   const real sign = (real)dst.sign;
-  const idx_t from = idx3(d, t, si, sj, 0), to = idx3(d, dst.t, dst.i, dst.j, 0);
-  for (int k = 0; k < nlev; ++k) dstf[to + k * d.sk] = sign * srcf[from + k * d.sk];
+  dstf[idx3(d, dst.t, dst.i, dst.j, k)] = sign * srcf[idx3(d, t, si, sj, k)];
 }
 }  // namespace
 
 cudaError_t halo_scalars(const Dims& d, real* const* fields, int nfields, int stagger, int n_halo, int nlev,
                          cudaStream_t st) {
   const int nc = halo_candidates(d, n_halo);
-  dim3 grid((nc + HALO_BLOCK - 1) / HALO_BLOCK, d.nt);
+  if (nlev <= 0) return cudaSuccess;
+  dim3 grid((nc + HALO_BLOCK - 1) / HALO_BLOCK, d.nt, nlev);
   for (int f0 = 0; f0 < nfields; f0 += 4) {
     FieldSet fs;
     fs.n = nfields - f0 < 4 ? nfields - f0 : 4;
     for (int q = 0; q < fs.n; ++q) fs.f[q] = fields[f0 + q];
-    halo_scalar_kernel<<<grid, HALO_BLOCK, 0, st>>>(d, fs, stagger, stagger, n_halo, nlev);
+    halo_scalar_kernel<<<grid, HALO_BLOCK, 0, st>>>(d, fs, stagger, stagger, n_halo);
     note_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -85,15 +85,17 @@ cudaError_t halo_scalars(const Dims& d, real* const* fields, int nfields, int st
 
 cudaError_t halo_vector(const Dims& d, real* x, real* y, bool cgrid, int nlev, cudaStream_t st) {
   const int nc = halo_candidates(d, d.h);
-  dim3 grid((nc + HALO_BLOCK - 1) / HALO_BLOCK, 2 * d.nt);
-  halo_vector_kernel<<<grid, HALO_BLOCK, 0, st>>>(d, x, y, cgrid ? 1 : 0, nlev);
+  if (nlev <= 0) return cudaSuccess;
+  dim3 grid((nc + HALO_BLOCK - 1) / HALO_BLOCK, 2 * d.nt, nlev);
+  halo_vector_kernel<<<grid, HALO_BLOCK, 0, st>>>(d, x, y, cgrid ? 1 : 0);
   note_launch();
   return cudaGetLastError();
 }
 
 cudaError_t sync_vector_interfaces(const Dims& d, real* u, real* v, int nlev, cudaStream_t st) {
-  dim3 grid((d.n + HALO_BLOCK - 1) / HALO_BLOCK, 2 * d.nt);
-  interface_sync_kernel<<<grid, HALO_BLOCK, 0, st>>>(d, u, v, nlev);
+  if (nlev <= 0) return cudaSuccess;
+  dim3 grid((d.n + HALO_BLOCK - 1) / HALO_BLOCK, 2 * d.nt, nlev);
+  interface_sync_kernel<<<grid, HALO_BLOCK, 0, st>>>(d, u, v);
   note_launch();
   return cudaGetLastError();
 }

@@ -676,6 +676,16 @@ extern "C" int fv3b_remap_setup(fv3b_ctx* ctx, const double* ak, const double* b
   }
   cudaError_t e = cudaMemcpy(ctx->remap_akbk, host, sizeof(host), cudaMemcpyHostToDevice);
   FV3B_CHECK(e);
+  if (ctx->sat_tables == nullptr) {
+    e = cudaMalloc((void**)&ctx->sat_tables, sizeof(double) * 4 * satadj::TAB_N);
+    FV3B_CHECK(e);
+    satadj::sat_tables_kernel<<<(satadj::TAB_N + 127) / 128, 128>>>(ctx->sat_tables);
+    note_launch();
+    e = cudaGetLastError();
+    FV3B_CHECK(e);
+    e = cudaDeviceSynchronize();
+    FV3B_CHECK(e);
+  }
   ctx->remap_nlev = nlev;
   return FV3B_OK;
 }
@@ -794,6 +804,7 @@ extern "C" int fv3b_lagrangian_to_eulerian(fv3b_ctx* ctx, const fv3b_remap_field
     prm.lv00 = satadj::HLV - prm.d0_vap * satadj::TICE;
     prm.last_step = last_step;
     const real* area = ctx->m.area;
+    const double* tb = ctx->sat_tables;
     FV3B_CHECK(launch_box(Box{s, e + 1, js, je + 1, kmp, nz}, st, [=] __device__(int t, int i, int j, int k) {
       const idx_t o = idx3(d, t, i, j, k), o2 = idx2(d, t, i, j);
       satadj::Point P;
@@ -812,7 +823,7 @@ extern "C" int fv3b_lagrangian_to_eulerian(fv3b_ctx* ctx, const fv3b_remap_field
       P.hs = f.hs[o2];
       P.pkz = f.pkz[o];
       P.q_con = f.q_con[o];
-      satadj::sat_adjust_point(P, prm);
+      satadj::sat_adjust_point(P, prm, tb);
       qv[o] = static_cast<real>(P.qv);
       qlq[o] = static_cast<real>(P.ql);
       qi[o] = static_cast<real>(P.qi);

@@ -4,10 +4,13 @@
 //
 // Every point is independent, so the adjustment is one FP64 function of a
 // point's values (sat_adjust_point), called by one thread per point.  The
-// saturation tables (es over ice / water, their differences) are evaluated
-// from a point's table index on the fly, as the reference does
-// (qs_table2_fn, qs_tablew_fn, des2_table, desw_table), with the library's
-// exp and log (fmath.h).  Statement order, branch structure and the
+// saturation tables (es over ice / water and their differences,
+// qs_table2_fn, qs_tablew_fn, des2_table, desw_table) are functions of an
+// integer table index; the reference evaluates them on the fly, here they
+// are evaluated once per context by the same device functions (the
+// library's exp and log, fmath.h) into a table of every index a point can
+// reach (-1 .. 2622), so each lookup returns the value the reference
+// computes.  Statement order, branch structure and the
 // association of every expression follow the reference, so FP64 results
 // agree with the oracle bit for bit.  Nonhydrostatic only (the caller
 // rejects hydrostatic); the total-energy fixer (consv_te) is off, as in
@@ -94,6 +97,27 @@ __device__ double desw(double i) {
   return des;
 }
 
+// the precomputed tables: [4][TAB_N] doubles, index i at offset i + 1
+constexpr int TAB_N = 2624;  // indices -1 .. 2622
+enum { TAB_W = 0, TAB_2 = 1, DES_W = 2, DES_2 = 3 };
+
+__device__ __forceinline__ double tab_at(const double* tab, int which, double i) {
+  int ii = (int)i + 1;
+  ii = ii < 0 ? 0 : (ii > TAB_N - 1 ? TAB_N - 1 : ii);
+  return tab[which * TAB_N + ii];
+}
+
+// fills the tables: one thread per index
+__global__ void sat_tables_kernel(double* tab) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= TAB_N) return;
+  const double i = (double)(x - 1);
+  tab[TAB_W * TAB_N + x] = qs_tablew(i);
+  tab[TAB_2 * TAB_N + x] = qs_table2(i);
+  tab[DES_W * TAB_N + x] = desw(i);
+  tab[DES_2 * TAB_N + x] = des2(i);
+}
+
 // ap1_for_wqs2 (454-457)
 __device__ __forceinline__ double ap1_of(double ta) {
   const double ap1 = 10.0 * dim(ta, TMIN) + 1.0;
@@ -102,15 +126,16 @@ __device__ __forceinline__ double ap1_of(double ta) {
 
 // wqs2_fn_w / wqs2_fn_2 with wqsat_and_dqdt (487-519)
 template <bool WATER>
-__device__ void wqs2(double ta, double den, double& wqsat, double& dqdt) {
+__device__ void wqs2(const double* tb, double ta, double den, double& wqsat, double& dqdt) {
   const double ap1 = ap1_of(ta);
   const double it = floor(ap1);
   const double it2 = floor(ap1 - 0.5);
   const double it2_p1 = it2 + 1;
-  const double tab = WATER ? qs_tablew(it) : qs_table2(it);
-  const double des = WATER ? desw(it) : des2(it);
-  const double des_2 = WATER ? desw(it2) : des2(it2);
-  const double des_p1 = WATER ? desw(it2_p1) : des2(it2_p1);
+  const int T = WATER ? TAB_W : TAB_2, D = WATER ? DES_W : DES_2;
+  const double tab = tab_at(tb, T, it);
+  const double des = tab_at(tb, D, it);
+  const double des_2 = tab_at(tb, D, it2);
+  const double des_p1 = tab_at(tb, D, it2_p1);
   const double es = tab + (ap1 - it) * des;
   const double denom = RVGAS * ta * den;
   wqsat = es / denom;
@@ -144,7 +169,7 @@ struct Point {
 };
 
 // satadjust (544-932), nonhydrostatic, consv_te off
-__device__ void sat_adjust_point(Point& P, const Params& p) {
+__device__ void sat_adjust_point(Point& P, const Params& p, const double* tb) {
   const fv3b_sat_adjust_config& c = p.cfg;
   double qv = P.qv, ql = P.ql, qi = P.qi, qr = P.qr, qs = P.qs, qg = P.qg;
   double q_liq = ql + qr;
@@ -208,7 +233,7 @@ __device__ void sat_adjust_point(Point& P, const Params& p) {
     }
   }
   double wqsat, dq2dt;
-  wqs2<true>(pt1, den, wqsat, dq2dt);
+  wqs2<true>(tb, pt1, den, wqsat, dq2dt);
   lat(pt1, cvm, p.lv00, p.d0_vap, lhl, lhi, lcp2, icp2);
   double diff_ice = dim(TICE, pt1) / 48.0;
   double dimmin = dmin(1.0, diff_ice);
@@ -232,7 +257,7 @@ __device__ void sat_adjust_point(Point& P, const Params& p) {
   dimmin = dmin(1.0, diff_ice);
   tcp3 = lcp2 + icp2 * dimmin;
   if (p.last_step) {
-    wqs2<true>(pt1, den, wqsat, dq2dt);
+    wqs2<true>(tb, pt1, den, wqsat, dq2dt);
     dq0 = (qv - wqsat) / (1.0 + tcp3 * dq2dt);
     if (dq0 > 0) {
       src = dq0;
@@ -322,7 +347,7 @@ __device__ void sat_adjust_point(Point& P, const Params& p) {
     ql = ql - sink;
   }
   double iqs2, dqsdt;
-  wqs2<false>(pt1, den, iqs2, dqsdt);
+  wqs2<false>(tb, pt1, den, iqs2, dqsdt);
   const double expsubl = fm::fm_exp(0.875 * fm::fm_log(qi * den));
   lat(pt1, cvm, p.lv00, p.d0_vap, lhl, lhi, lcp2, icp2);
   const double tcp2 = lcp2 + icp2;
@@ -394,8 +419,8 @@ __device__ void sat_adjust_point(Point& P, const Params& p) {
     const double tin = c.tintqs ? pt1 : pt1 - (lcp2 * q_cond + icp2 * q_sol);
     const double ap1 = ap1_of(tin);
     const double it = floor(ap1);
-    const double wqs1 = (qs_tablew(it) + (ap1 - it) * desw(it)) / (RVGAS * tin * den);
-    const double iqs1 = (qs_table2(it) + (ap1 - it) * des2(it)) / (RVGAS * tin * den);
+    const double wqs1 = (tab_at(tb, TAB_W, it) + (ap1 - it) * tab_at(tb, DES_W, it)) / (RVGAS * tin * den);
+    const double iqs1 = (tab_at(tb, TAB_2, it) + (ap1 - it) * tab_at(tb, DES_2, it)) / (RVGAS * tin * den);
     double qstar;
     if (tin < T_WFR) {
       qstar = iqs1;

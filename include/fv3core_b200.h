@@ -537,8 +537,10 @@ int fv3b_cubed_to_latlon(fv3b_ctx* ctx, fv3b_real* u, fv3b_real* v, const fv3b_r
 /*
  * LagrangianToEulerian.__init__ (fv3core/stencils/remapping.py:210-414):
  * keeps the hybrid coordinate ak, bk (HOST arrays of npz+1 values) on the
- * device in FP64.  Allocates (cudaMalloc) on the first call for a context
- * and synchronises.
+ * device in FP64, and on the first call fills the saturation adjustment's
+ * tables (saturation vapour pressure over water and ice and their
+ * differences at every table index, 84 KB).  Allocates (cudaMalloc) on the
+ * first call for a context and synchronises.
  */
 int fv3b_remap_setup(fv3b_ctx* ctx, const double* ak, const double* bk);
 
