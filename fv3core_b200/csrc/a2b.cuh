@@ -123,8 +123,10 @@ inline cudaError_t a2b_ord4(const Dims d, const fv3b_metrics g, real* qin, real*
     W3(edges, i, j) = v;
   });
   if (err != cudaSuccess) return err;
-  // ppm_volume_mean_x on [is, ie+1] x [js-2, je+2], _y on [is-2, ie+2] x [js, je+1]
-  err = launch_box(Box{s - 2, e + 3, js - 2, je + 3, k0, k1}, st, [=] __device__(int t, int i, int j, int k) {
+  // ppm_volume_mean_x on [is, ie+1] x [js-2, je+2], _y on [is-2, ie+2] x [js, je+1];
+  // the columns of the interior formula (is+2 .. ie-1) in warps of their own
+  err = launch_box_split(Box{s - 2, e + 3, js - 2, je + 3, k0, k1}, s + 2, e, st,
+                         [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
     idx_t b = idx3(d, t, i, j, k);
     idx_t b2 = idx2(d, t, i, j);
@@ -140,8 +142,10 @@ inline cudaError_t a2b_ord4(const Dims d, const fv3b_metrics g, real* qin, real*
     }
   });
   if (err != cudaSuccess) return err;
-  // a2b_interpolation (a2b_ord4.py:286-310) on interior cell corners
-  err = launch_box(Box{s + 1, e + 1, js + 1, je + 1, k0, k1}, st, [=] __device__(int t, int i, int j, int k) {
+  // a2b_interpolation (a2b_ord4.py:286-310) on interior cell corners, the
+  // columns without the edge corrections (is+2 .. ie-1) in warps of their own
+  err = launch_box_split(Box{s + 1, e + 1, js + 1, je + 1, k0, k1}, s + 2, e, st,
+                         [=] __device__(int t, int i, int j, int k) {
     PT_SETUP(d, t, k);
     real qxx = A2 * (F3(qx, i, j - 2) + F3(qx, i, j + 1)) + A1 * (F3(qx, i, j - 1) + F3(qx, i, j));
     real qyy = A2 * (F3(qy, i - 2, j) + F3(qy, i + 1, j)) + A1 * (F3(qy, i - 1, j) + F3(qy, i, j));
