@@ -15,7 +15,7 @@
 
 namespace fv3b {
 
-__device__ __forceinline__ bool copy_corner_x(const Dims& d, int i, int j, int& si, int& sj) {
+__host__ __device__ __forceinline__ bool copy_corner_x(const Dims& d, int i, int j, int& si, int& sj) {
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
   if (i >= s - 3 && i <= s - 1) {
     int a = i - s;
@@ -29,7 +29,7 @@ __device__ __forceinline__ bool copy_corner_x(const Dims& d, int i, int j, int& 
   return false;
 }
 
-__device__ __forceinline__ bool copy_corner_y(const Dims& d, int i, int j, int& si, int& sj) {
+__host__ __device__ __forceinline__ bool copy_corner_y(const Dims& d, int i, int j, int& si, int& sj) {
   const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
   if (i >= s - 3 && i <= s - 1) {
     int a = i - s;

@@ -8,6 +8,10 @@
 // parameter); the statement order of the reference is kept so that FP64
 // results agree to rounding.
 #pragma once
+#include <algorithm>
+#include <map>
+#include <mutex>
+
 #include "corners.cuh"
 #include "ctx.cuh"
 #include "stencil.cuh"
@@ -514,6 +518,261 @@ static __global__ void __launch_bounds__(DELN_TX* DELN_TY) deln_iter_kernel(cons
   }
 }
 
+// ------------------------------------------------------------ fused chain
+// The whole del-n chain of one level (passes 0 .. NMAX, NMAX = 1 or 2) for
+// one tile of the final fluxes, every pass in shared memory: q is read once
+// and only the final fluxes (or their combine into fx, fy) are written,
+// where the pass-by-pass form reads and writes two flux fields per pass.
+//
+// The window is the tile widened by NMAX + 1 points (low sides) and NMAX
+// (high sides) and is one warp wide, so a thread keeps one window column
+// and the same rows through every pass, with the metric terms of its
+// points in registers.  Pass p is computed on the tile widened by NMAX - p
+// points (what the next pass reads), its d2 on the points those fluxes
+// read.  A pass writes only inside its own region, as the reference's does,
+// into one of two flux sets that alternate as the global buffers do, so the
+// points the final combine reads outside the final region hold the value
+// of pass NMAX - 2 there, as the buffer does in the pass-by-pass form (for
+// NMAX = 1 no pass of the chain writes them: the buffer is read).
+//
+// Most tiles lie inside every pass's region and away from the cube
+// corners: they take the path without region tests.  The others test the
+// region per point and map the d2 reads of corner points to their copy
+// sources inside the window; a pass-0 source outside the window is damp q
+// read from q.  deln_window_ok checks on the host, for the grid at hand,
+// that every later-pass source lies inside the window; where it does not,
+// the chain runs pass by pass.  Levels with nord = 0 take their single pass
+// here.  Same operations in the same order as the pass-by-pass form, so the
+// results are the same numbers.
+constexpr int CHAIN_TY = 16, CHAIN_BY = 8;
+
+template <int NMAX>
+struct DelnTile {
+  static constexpr int TX = 32 - 2 * NMAX - 1;            // output columns
+  static constexpr int WY = CHAIN_TY + 2 * NMAX + 1;       // window rows
+  static constexpr int R = (WY + CHAIN_BY - 1) / CHAIN_BY;  // window rows per thread
+};
+
+struct DelnChainArgs {
+  Dims d;
+  fv3b_metrics g;
+  DelnCol col;
+  const real* q;
+  real* fx2;  // final fluxes; with a combine, the final-pass buffer
+  real* fy2;
+  DelnCombine cb;
+  int mass_weighted;
+  int nlev;
+};
+
+template <int NMAX>
+static __global__ void __launch_bounds__(32 * CHAIN_BY) deln_chain_kernel(const DelnChainArgs a) {
+  using G = DelnTile<NMAX>;
+  constexpr int TX = G::TX, WY = G::WY, R = G::R, WN = 32 * WY;
+  __shared__ real sd2[WN];
+  __shared__ real sfx[2][WN];
+  __shared__ real sfy[2][WN];
+  const Dims& d = a.d;
+  const int t = blockIdx.z / a.nlev, k = blockIdx.z % a.nlev;
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
+  const int i0 = s + blockIdx.x * TX, j0 = js + blockIdx.y * CHAIN_TY;
+  const int wi0 = i0 - NMAX - 1, wj0 = j0 - NMAX - 1;
+  const int x = threadIdx.x, ty = threadIdx.y;
+  const int i = wi0 + x;
+  const idx_t b3 = t * d.st + k * d.sk, b2 = t * d.st2;
+  const int nk_ = nord_at(a.col.nord, k);
+  const real damp = a.col.damp[k];
+  const real* q = a.q;
+  const bool mw = a.mass_weighted != 0;
+  const bool out_col = x >= NMAX + 1 && x < NMAX + 1 + TX && i < e + 2;
+  if (nk_ == 0) {
+    // one pass on the compute-domain faces, combined now if asked
+    if (!out_col) return;
+    auto D2 = [&](int ii, int jj) {
+      const real qv = q[b3 + jj * d.sj + ii];
+      return mw ? qv : damp * qv;
+    };
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int y = ty + r * CHAIN_BY, j = wj0 + y;
+      if (y >= NMAX + 1 && y < NMAX + 1 + CHAIN_TY && j < je + 2)
+        deln_flux_point(d, a.g, t, i, j, k, NMAX, 0, true, a.fx2, a.fy2, D2, a.cb, a.col.damp);
+    }
+    return;
+  }
+  const int i1 = min(i0 + TX, e + 2), j1 = min(j0 + CHAIN_TY, je + 2);
+  // inside every region, no corner point, the window inside the arrays
+  const bool slow = i1 == e + 2 || j1 == je + 2 ||
+                    ((i0 - NMAX <= s || i1 - 1 + NMAX >= e + 1) && (j0 - NMAX <= js || j1 - 1 + NMAX >= je + 1));
+  real m_ra[R], m_dv[R], m_du[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int y = ty + r * CHAIN_BY, jj = wj0 + y;
+    const bool ok = y < WY && i < d.ni && jj < d.nj;
+    const idx_t o2 = b2 + jj * d.sj + i;
+    m_ra[r] = ok ? a.g.rarea[o2] : RC(0.0);
+    m_dv[r] = ok ? a.g.del6_v[o2] : RC(0.0);
+    m_du[r] = ok ? a.g.del6_u[o2] : RC(0.0);
+    if (y < WY) {
+      real v = RC(0.0);
+      if (ok) {
+        const real qv = q[b3 + jj * d.sj + i];
+        v = mw ? qv : damp * qv;
+      }
+      sd2[y * 32 + x] = v;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int p = 0; p <= NMAX; ++p) {
+    if (p > 0) {
+      // d2 of pass p from the fluxes of pass p - 1, window shrunk by p
+      const int ps = (NMAX - p + 1) & 1;
+      if (x >= p && x < 32 - p) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int y = ty + r * CHAIN_BY;
+          if (y >= p && y < WY - p) {
+            const int c = y * 32 + x;
+            real v = RC(0.0);
+            if (!slow || (i + 1 < d.ni && wj0 + y + 1 < d.nj))
+              v = (sfx[ps][c] - sfx[ps][c + 1] + sfy[ps][c] - sfy[ps][c + 32]) * m_ra[r] * a.col.rscale;
+            sd2[c] = v;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // fluxes of pass p, window shrunk by p + 1 on the low sides and p on the high sides
+    const int set = (NMAX - p) & 1, lo = NMAX - p;
+    if (x >= p + 1 && x < 32 - p) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int y = ty + r * CHAIN_BY;
+        if (!(y >= p + 1 && y < WY - p)) continue;
+        const int c = y * 32 + x;
+        const real d2c = sd2[c];
+        if (!slow) {
+          const real vx = m_dv[r] * (sd2[c - 1] - d2c);
+          const real vy = m_du[r] * (sd2[c - 32] - d2c);
+          sfx[set][c] = p == 0 ? vx : -vx;
+          sfy[set][c] = p == 0 ? vy : -vy;
+          continue;
+        }
+        const int j = wj0 + y;
+        const bool fx_in = i >= s - lo && i < e + 2 + lo && j >= js - lo && j < je + 1 + lo;
+        const bool fy_in = i >= s - lo && i < e + 1 + lo && j >= js - lo && j < je + 2 + lo;
+        const bool corners = (i <= s || i >= e + 1) && (j <= js || j >= je + 1);
+        // d2 of this pass at storage point (ii, jj)
+        auto d2w = [&](int ii, int jj) -> real {
+          const int xx = ii - wi0, yy = jj - wj0;
+          if (p == 0 && (xx < 0 || xx >= 32 || yy < 0 || yy >= WY)) {
+            const real qv = q[b3 + jj * d.sj + ii];
+            return mw ? qv : damp * qv;
+          }
+          return sd2[yy * 32 + xx];
+        };
+        if (fx_in) {
+          int ai = i - 1, aj = j, bi = i, bj = j;
+          if (corners) {
+            int si, sj;
+            if (copy_corner_x(d, i - 1, j, si, sj)) ai = si, aj = sj;
+            if (copy_corner_x(d, i, j, si, sj)) bi = si, bj = sj;
+          }
+          const real vx = m_dv[r] * (d2w(ai, aj) - d2w(bi, bj));
+          sfx[set][c] = p == 0 ? vx : -vx;
+        }
+        if (fy_in) {
+          int ai = i, aj = j - 1, bi = i, bj = j;
+          if (corners) {
+            int si, sj;
+            if (copy_corner_y(d, i, j - 1, si, sj)) ai = si, aj = sj;
+            if (copy_corner_y(d, i, j, si, sj)) bi = si, bj = sj;
+          }
+          const real vy = m_du[r] * (d2w(ai, aj) - d2w(bi, bj));
+          sfy[set][c] = p == 0 ? vy : -vy;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (!out_col) return;
+  PT_SETUP(d, t, k);
+  const DelnCombine& cb = a.cb;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int y = ty + r * CHAIN_BY, j = wj0 + y;
+    if (!(y >= NMAX + 1 && y < NMAX + 1 + CHAIN_TY && j < je + 2)) continue;
+    const int c = y * 32 + x;
+    const bool fx_in = j < je + 1, fy_in = i < e + 1;  // the final region (i >= is, j >= js hold)
+    if (cb.fx == nullptr) {
+      if (fx_in) W3(a.fx2, i, j) = sfx[0][c];
+      if (fy_in) W3(a.fy2, i, j) = sfy[0][c];
+      continue;
+    }
+    const real fx2 = (fx_in || NMAX >= 2) ? sfx[0][c] : F3(a.fx2, i, j);
+    const real fy2 = (fy_in || NMAX >= 2) ? sfy[0][c] : F3(a.fy2, i, j);
+    if (cb.mass == nullptr) {
+      W3(cb.fx, i, j) = F3(cb.fx, i, j) + fx2;
+      W3(cb.fy, i, j) = F3(cb.fy, i, j) + fy2;
+    } else {
+      W3(cb.fx, i, j) = F3(cb.fx, i, j) + RC(0.5) * damp * (F3(cb.mass, i - 1, j) + F3(cb.mass, i, j)) * fx2;
+      W3(cb.fy, i, j) = F3(cb.fy, i, j) + RC(0.5) * damp * (F3(cb.mass, i, j - 1) + F3(cb.mass, i, j)) * fy2;
+    }
+  }
+}
+
+// Whether every d2 read of the fused chain's later passes (p >= 1) at a
+// corner point, mapped to its copy source, lies inside the tile's window
+// and reads fluxes of the pass before inside that pass's region: an
+// enumeration over the tiles that hold corner points (the other reads lie
+// inside by construction).  Results cached per (n, halo, nmax).
+template <int NMAX>
+inline bool deln_window_ok_impl(const Dims& d) {
+  using G = DelnTile<NMAX>;
+  const int s = d.isc, e = d.iec, js = d.jsc, je = d.jec;
+  auto fxr = [&](int lo, int i, int j) { return i >= s - lo && i < e + 2 + lo && j >= js - lo && j < je + 1 + lo; };
+  auto fyr = [&](int lo, int i, int j) { return i >= s - lo && i < e + 1 + lo && j >= js - lo && j < je + 2 + lo; };
+  for (int i0 = s; i0 < e + 2; i0 += G::TX)
+    for (int j0 = js; j0 < je + 2; j0 += CHAIN_TY) {
+      const int i1 = std::min(i0 + G::TX, e + 2), j1 = std::min(j0 + CHAIN_TY, je + 2);
+      const int wi0 = i0 - NMAX - 1, wj0 = j0 - NMAX - 1;
+      for (int p = 1; p <= NMAX; ++p) {
+        const int lo = NMAX - p;
+        for (int i = i0 - lo; i < i1 + lo; ++i)
+          for (int j = j0 - lo; j < j1 + lo; ++j) {
+            if (!((i <= s || i >= e + 1) && (j <= js || j >= je + 1))) continue;
+            for (int kind = 0; kind < 2; ++kind) {
+              if (!(kind == 0 ? fxr(lo, i, j) : fyr(lo, i, j))) continue;
+              const int pts[2][2] = {{kind == 0 ? i - 1 : i, kind == 0 ? j : j - 1}, {i, j}};
+              for (const auto& pt : pts) {
+                int ii = pt[0], jj = pt[1], si, sj;
+                if (kind == 0 ? copy_corner_x(d, ii, jj, si, sj) : copy_corner_y(d, ii, jj, si, sj)) ii = si, jj = sj;
+                const int xx = ii - wi0, yy = jj - wj0;
+                if (xx < p || xx >= 32 - p || yy < p || yy >= G::WY - p) return false;
+                if (!(fxr(lo + 1, ii, jj) && fxr(lo + 1, ii + 1, jj) && fyr(lo + 1, ii, jj) &&
+                      fyr(lo + 1, ii, jj + 1)))
+                  return false;
+              }
+            }
+          }
+      }
+    }
+  return true;
+}
+
+inline bool deln_window_ok(const Dims& d, int nmax) {
+  static std::mutex mu;
+  static std::map<long long, bool> cache;
+  const long long key = ((long long)d.n * 64 + d.h) * 4 + nmax;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  const bool ok = d.h >= 3 && (nmax == 1 ? deln_window_ok_impl<1>(d) : deln_window_ok_impl<2>(d));
+  cache[key] = ok;
+  return ok;
+}
+
 // DelnFluxNoSG.__call__ (delnflux.py:1156-1207): del-n diffusive fluxes of q
 // into fx2/fy2.  Corner copies of d2 are applied on read (a point of a
 // corner block reads its copy source), which gives the values the reference
@@ -538,6 +797,18 @@ inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const real*
   // pass p writes (fx2, fy2) when nmax - p is even, so the last pass does
   auto out_x = [&](int p) { return ((nmax - p) % 2 == 0) ? fx2 : ax; };
   auto out_y = [&](int p) { return ((nmax - p) % 2 == 0) ? fy2 : ay; };
+  if ((nmax == 1 || nmax == 2) && deln_window_ok(d, nmax)) {
+    DelnChainArgs a{d, g, col, q, fx2, fy2, cb, mass_weighted ? 1 : 0, nz};
+    const int len = e + 2 - s;
+    const int tx = nmax == 1 ? DelnTile<1>::TX : DelnTile<2>::TX;
+    const dim3 grid((len + tx - 1) / tx, (len + CHAIN_TY - 1) / CHAIN_TY, tile_slots() * nz);
+    if (nmax == 1)
+      deln_chain_kernel<1><<<grid, dim3(32, CHAIN_BY, 1), 0, st>>>(a);
+    else
+      deln_chain_kernel<2><<<grid, dim3(32, CHAIN_BY, 1), 0, st>>>(a);
+    note_launch();
+    return cudaGetLastError();
+  }
   // first pass: d2 = damp * q (d2_damp_interval) or q (copy_stencil_interval)
   {
     const int lo = nmax;
@@ -567,8 +838,8 @@ inline cudaError_t delnflux_nosg(const Dims d, const fv3b_metrics g, const real*
     const int lo = nmax - p;
     DelnIterArgs a{d, g, col, out_x(p - 1), out_y(p - 1), out_x(p), out_y(p), cb,
                    lo, s - lo, e + 2 + lo, js - lo, je + 2 + lo, nz, p == nmax};
-    const dim3 grid((a.i1 - a.i0 + DELN_TX - 1) / DELN_TX, (a.j1 - a.j0 + DELN_TY - 1) / DELN_TY, tile_slots() * nz);
-    deln_iter_kernel<<<grid, dim3(DELN_TX, DELN_TY, 1), 0, st>>>(a);
+    const dim3 grid((a.i1 - a.i0 + DELN_TX - 1) / DELN_TX, (a.j1 - a.j0 + CHAIN_TY - 1) / CHAIN_TY, tile_slots() * nz);
+    deln_iter_kernel<<<grid, dim3(DELN_TX, CHAIN_TY, 1), 0, st>>>(a);
     note_launch();
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return err;

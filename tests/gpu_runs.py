@@ -38,7 +38,10 @@ DSW_ARGS = ["delpc", "delp", "ptc", "pt", "u", "v", "w", "uc", "vc", "ua", "va",
             "cx", "cy", "crx", "cry", "xfx", "yfx", "q_con", "zh", "heat_source", "diss_est"]
 
 
-def run_d_sw(case, n, nz):
+def run_d_sw(case, n, nz, overrides=None):
+    """``overrides``: namelist values replacing the baroclinic ones."""
+    import dataclasses
+
     import torch
 
     from fv3core_b200.config import baroclinic_dsw_config
@@ -46,7 +49,8 @@ def run_d_sw(case, n, nz):
     from fv3core_b200.storage import to_device, to_host
 
     gd, sf = device_grid(n, nz)
-    dsw = DGridShallowWaterLagrangianDynamics(sf, gd, gd, None, False, False, baroclinic_dsw_config())
+    config = dataclasses.replace(baroclinic_dsw_config(), **(overrides or {}))
+    dsw = DGridShallowWaterLagrangianDynamics(sf, gd, gd, None, False, False, config)
     dev = {k: to_device(case[k]) for k in DSW_ARGS}
     dsw(*[dev[k] for k in DSW_ARGS], case["dt"])
     torch.cuda.synchronize()

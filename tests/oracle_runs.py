@@ -40,18 +40,20 @@ DSW_ARGS = ["delpc", "delp", "ptc", "pt", "u", "v", "w", "uc", "vc", "ua", "va",
             "cx", "cy", "crx", "cry", "xfx", "yfx", "q_con", "zh", "heat_source", "diss_est"]
 
 
-def run_d_sw(case, n, nz, states=None):
+def run_d_sw(case, n, nz, states=None, overrides=None):
+    """``overrides``: namelist values replacing those of cases.DSW_CONFIG."""
     from oracle.d_sw import DSWState, d_sw
 
+    config = {**cases.DSW_CONFIG, **(overrides or {})}
     out = {k: np.array(case[k], copy=True) for k in DSW_ARGS}
     g = cases.grid_for(n)
     for t in range(6):
         T = Tile(n, nz)
         ns = cases.metric_namespace(n, t)
-        st = DSWState(T, ns, cases.DSW_CONFIG) if states is None else states[t]
+        st = DSWState(T, ns, config) if states is None else states[t]
         arrs = {k: out[k][t] for k in DSW_ARGS}
         with np.errstate(all="ignore"):
-            d_sw(T, ns, g.f0[t], st, cases.DSW_CONFIG, *[arrs[k] for k in DSW_ARGS], case["dt"])
+            d_sw(T, ns, g.f0[t], st, config, *[arrs[k] for k in DSW_ARGS], case["dt"])
     return out
 
 

@@ -52,3 +52,21 @@ def test_gpu_matches_oracle(n, nz, seed):
         sl = _compute_region(k, n, nz)
         err = parity_err(gpu[k][sl], ref[k][sl])
         assert err <= 1e-12, (k, err)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nord", [0, 1])
+def test_gpu_matches_oracle_other_nord(nord):
+    """nord 1 takes the del-n chains with one pass after the first (nmax =
+    1), nord 0 the single-pass chains; C48 so that the chains run both in
+    the fused tiles and in the cube-corner tiles."""
+    import gpu_runs
+
+    n, nz, seed = 48, 6, 9
+    case = cases.d_sw_case(n, nz, seed)
+    ref = oracle_runs.run_d_sw(case, n, nz, overrides={"nord": nord})
+    gpu = gpu_runs.run_d_sw(case, n, nz, overrides={"nord": nord})
+    for k in OUT:
+        sl = _compute_region(k, n, nz)
+        err = parity_err(gpu[k][sl], ref[k][sl])
+        assert err <= 1e-12, (k, err)
