@@ -10,6 +10,7 @@
 #include <math.h>
 
 #include "dims.h"
+#include "fmath.h"
 
 namespace fv3b {
 namespace adj {
@@ -66,17 +67,22 @@ __host__ __device__ inline bool operator<(Dual<R> a, R b) { return a.v < b; }
 
 template <class R>
 __host__ __device__ inline Dual<R> dabs(Dual<R> a) { return a.v < R(0) ? -a : a; }
+// exp, log and pow are the library's own (fmath.h), the functions the
+// forward kernels evaluate, so value-driven branches and derivatives are
+// taken at the forward's values
 template <class R>
 __host__ __device__ inline Dual<R> dexp(Dual<R> a) {
-  const R e = exp(a.v);
+  const R e = static_cast<R>(fm::fm_exp(static_cast<double>(a.v)));
   return {e, e * a.d};
 }
 template <class R>
-__host__ __device__ inline Dual<R> dlog(Dual<R> a) { return {log(a.v), a.d / a.v}; }
+__host__ __device__ inline Dual<R> dlog(Dual<R> a) {
+  return {static_cast<R>(fm::fm_log(static_cast<double>(a.v))), a.d / a.v};
+}
 // a^b for a constant exponent b
 template <class R>
 __host__ __device__ inline Dual<R> dpow(Dual<R> a, R b) {
-  const R p = pow(a.v, b);
+  const R p = static_cast<R>(fm::fm_pow(static_cast<double>(a.v), static_cast<double>(b)));
   return {p, b * p / a.v * a.d};
 }
 

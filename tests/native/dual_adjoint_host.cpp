@@ -95,16 +95,15 @@ extern "C" void uzc_dual_scatter_host(int n, int halo, int npz, const double* dp
     for (int k = 0; k < d.nk; ++k)
       for (int j = d.jsc - 1; j <= d.jec + 1; ++j)
         for (int i = d.isc - 1; i <= d.iec + 1; ++i) {
-          // candidates: gz within two points (corner copies included), the
-          // fluxes' four layers at i, i+1 (ut) and j, j+1 (vt)
+          // candidates, the stencil's read set: gz within two points of the
+          // point's own level (corner copies included), the fluxes' four
+          // layers at i, i+1 (ut) and j, j+1 (vt)
           auto cands = [&](int m, idx_t& c) {
-            if (m < 25 * d.nk) {
-              const int ii = i - 2 + (m / d.nk) % 5, jj = j - 2 + m / (5 * d.nk), kk = m % d.nk;
-              if (kk != k) c = -1;
-              else c = fv3b::idx3(d, t, ii, jj, kk);
+            if (m < 25) {
+              c = fv3b::idx3(d, t, i - 2 + m % 5, j - 2 + m / 5, k);
               return true;
             }
-            m -= 25 * d.nk;
+            m -= 25;
             if (m >= 16) return false;
             const int a = 1 + m / 8, side = (m / 4) % 2, kk = k - 2 + m % 4;
             if (kk < 0 || kk >= d.nk) {
@@ -122,4 +121,27 @@ extern "C" void uzc_dual_scatter_host(int n, int halo, int npz, const double* dp
           auto add = [&](idx_t c, double v) { out[c / S][c % S] += v; };
           fv3b::adj::dual_point_adjoint<double>(f, cands, g_new[fv3b::idx3(d, t, i, j, k)], add);
         }
+}
+
+// A nonlinear column function with the transcendentals the column solvers
+// use: f(x) = pow(exp(0.3 log x) + x, 1.7) / log(1 + x), value and
+// derivative by duals at x[m], for a comparison with finite differences of
+// the same fmath functions.
+extern "C" void dual_transcendental_host(int n, const double* x, double* value, double* deriv) {
+  using fv3b::adj::dexp;
+  using fv3b::adj::dlog;
+  using fv3b::adj::dpow;
+  for (int m = 0; m < n; ++m) {
+    const D a(x[m], 1.0);
+    const D f = dpow(dexp(dlog(a) * D(0.3)) + a, 1.7) / dlog(a + D(1.0));
+    value[m] = f.v;
+    deriv[m] = f.d;
+  }
+}
+
+// The same function on plain doubles with the fmath functions.
+extern "C" void plain_transcendental_host(int n, const double* x, double* value) {
+  using namespace fv3b::fm;
+  for (int m = 0; m < n; ++m)
+    value[m] = fm_pow(fm_exp(fm_log(x[m]) * 0.3) + x[m], 1.7) / fm_log(x[m] + 1.0);
 }

@@ -83,3 +83,26 @@ def test_dual_scheme_on_update_dz_c(tmp_path_factory, thin):
     for name in ("gz", "ut", "vt"):
         b = hand_out[name]
         assert np.max(np.abs(mine[name] - b)) <= 1e-12 * np.max(np.abs(b)), name
+
+
+def test_dual_transcendentals_match_finite_differences(tmp_path_factory):
+    """dexp, dlog and dpow are the library's fmath functions with their
+    derivatives: a nonlinear column function's dual value equals the plain
+    fmath evaluation bit for bit, and its derivative agrees with central
+    differences of that evaluation (step 1e-6 relative, bound 1e-7)."""
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    lib = _build(tmp_path_factory, "dual_adjoint_host")
+    x = np.random.default_rng(5).uniform(0.05, 40.0, 64)
+    n = x.size
+    value, deriv, plain = np.empty(n), np.empty(n), np.empty(n)
+    lib.dual_transcendental_host(ctypes.c_int(n), _ptr(x), _ptr(value), _ptr(deriv))
+    lib.plain_transcendental_host(ctypes.c_int(n), _ptr(x), _ptr(plain))
+    np.testing.assert_array_equal(value, plain)
+    h = 1e-6 * x
+    fp, fm = np.empty(n), np.empty(n)
+    xp, xm = x + h, x - h
+    lib.plain_transcendental_host(ctypes.c_int(n), _ptr(xp), _ptr(fp))
+    lib.plain_transcendental_host(ctypes.c_int(n), _ptr(xm), _ptr(fm))
+    fd = (fp - fm) / (xp - xm)
+    assert np.max(np.abs(fd - deriv) / np.abs(deriv)) < 1e-7
