@@ -221,7 +221,7 @@ def call_precision(name, precision, *args):
 
 def exported_symbols():
     return ["fv3b_last_error", "fv3b_version", "fv3b_launch_count", "fv3b_set_launch_shape", "fv3b_get_launch_shape",
-            "fv3b_ctx_create", "fv3b_ctx_create_batched", "fv3b_ctx_destroy"] + [
+            "fv3b_ctx_create", "fv3b_ctx_create_batched", "fv3b_ctx_destroy", "fv3b_generate_grid"] + [
         k for k, v in SIGNATURES.items() if v is not None
     ] + list(CTX_SIGNATURES) + list(PTR_SIGNATURES) + list(TRANSPORT_SIGNATURES)
 

@@ -60,6 +60,15 @@ class GridData:
         self.device = device
         self.tensors = {}
         for name in METRIC_FIELDS + EXTRA_FIELDS:
+            if getattr(grid, "layout", "ij") == "ji":
+                # generated on the device (grid_device.DeviceGrid): FP64
+                # tensors already in the kernels' layout
+                t = getattr(grid, name).to(device=device, dtype=tdtype)
+                if self.members > 1:
+                    t = t.repeat(self.members, *([1] * (t.dim() - 1)))
+                self.tensors[name] = t.contiguous()
+                setattr(self, name, self.tensors[name])
+                continue
             a = np.asarray(getattr(grid, name), dtype=np.float64)
             if self.members > 1:  # the same metric terms for every member
                 a = np.concatenate([a] * self.members, axis=0)

@@ -605,6 +605,38 @@ int fv3b_lagrangian_to_eulerian(fv3b_ctx* ctx, const fv3b_remap_fields* fields, 
 fv3b_real* fv3b_acoustics_temporary(fv3b_ctx* ctx, const char* name);
 
 /*
+ * fv3b_generate_grid: the metric terms of one cube generated on the device,
+ * in place of MetricTerms (fv3core/grid/generation.py:66-2137, with
+ * gnomonic.py and geometry.py), which the reference computes on the host,
+ * one MPI rank per sub-tile, with halo updates between its steps.  Each
+ * output value is a closed-form function of the equiangular gnomonic cube
+ * (no halo update, no intermediate array, nothing allocated); the values
+ * are those of the package's host generator (fv3core_b200/grid.py) to
+ * rounding.  Outputs, all FP64 device arrays the caller allocates:
+ *   field[f]: FV3B_GRID_NFIELDS 2-D fields, each [6][m][m] with i fastest,
+ *     m = n + 2*halo + 1, in this order: dx dy dxa dya dxc dyc rdx rdy rdxa
+ *     rdya rdxc rdyc area rarea area_c rarea_c sin_sg1..5 cos_sg1..5 cosa
+ *     sina rsina cosa_u cosa_v cosa_s sina_u sina_v rsin_u rsin_v rsin2
+ *     del6_u del6_v divg_u divg_v fC f0 agrid1 agrid2 bgrid1 bgrid2 a11 a12
+ *     a21 a22;
+ *   edge[e]: the A->B edge weights edge_w, edge_e, edge_s, edge_n, [6][n+1];
+ *   a2b_extrap: a2b_ord4's cube-corner extrapolation ratios, [6][4][3];
+ *   scalars: da_min, da_max (cell areas over the compute domain), da_min_c,
+ *     da_max_c (dual cells over the compute corners), [4].
+ * radius in m, omega in 1/s (Coriolis fC, f0).  Needs 1 <= halo <= 8 and
+ * 2*halo <= n <= 4096.  Kernels run on `stream`; the call returns before
+ * they finish.
+ */
+#define FV3B_GRID_NFIELDS 51
+typedef struct {
+  double* field[FV3B_GRID_NFIELDS];
+  double* edge[4];
+  double* a2b_extrap;
+  double* scalars;
+} fv3b_grid_fields;
+int fv3b_generate_grid(int n, int halo, double radius, double omega, const fv3b_grid_fields* out, void* stream);
+
+/*
  * fv3b_del2cubed_noalloc: no reference counterpart.  The same filter as
  * fv3b_del2cubed (HyperdiffusionDamping, fv3core/stencils/del2cubed.py:152-181)
  * for callers that cannot let the library allocate device memory: it takes
