@@ -88,8 +88,8 @@ __global__ void grid_extremes_kernel(gg::Grid g, double* scalars) {
 }  // namespace fv3b
 
 // MetricTerms (fv3core/grid/generation.py:66) for one cube, on the device.
-extern "C" int fv3b_generate_grid(int n, int halo, double radius, double omega, const fv3b_grid_fields* out,
-                                  void* stream) {
+extern "C" int fv3b_generate_grid(int n, int halo, int lattice, double radius, double omega,
+                                  const fv3b_grid_fields* out, void* stream) {
   using namespace fv3b;
   FV3B_REQUIRE(out != nullptr && out->a2b_extrap != nullptr && out->scalars != nullptr,
                "fv3b_generate_grid: null output");
@@ -98,6 +98,7 @@ extern "C" int fv3b_generate_grid(int n, int halo, double radius, double omega, 
   FV3B_REQUIRE(halo >= 1 && halo <= 8 && n >= 2 * halo && n <= 4096,
                "fv3b_generate_grid: need 1 <= halo <= 8 and 2 * halo <= n <= 4096");
   FV3B_REQUIRE(radius > 0.0, "fv3b_generate_grid: radius must be positive");
+  FV3B_REQUIRE(lattice == 0 || lattice == 1, "fv3b_generate_grid: lattice must be 0 (equiangular) or 1 (equidistant)");
   static_assert(FV3B_GRID_NFIELDS == gg::GF_COUNT, "field list of the header and of grid_gen.h differ");
   fv3b_grid_dims gd{n, halo, 1, 0};
   gg::Grid g;
@@ -105,6 +106,7 @@ extern "C" int fv3b_generate_grid(int n, int halo, double radius, double omega, 
   g.n = n;
   g.h = halo;
   g.m = n + 2 * halo + 1;
+  g.lattice = lattice;
   g.radius = radius;
   g.omega = omega;
   GridOut o;

@@ -67,15 +67,30 @@ GG_HD void face_frame(int t, V3& c, V3& ex, V3& ey) {
 struct Grid {
   Dims d;         // n, h and the index helpers of the halo map
   int n, h, m;    // m = n + 2h + 1 corner points per axis
+  int lattice;    // 0 equiangular, 1 equal spacing along the edges (gnomonic_ed)
   double radius;
   double omega;
 };
 
-// unit vector of lattice point (a, b) (offsets from the first compute
-// corner) of face t: c + tan(alpha) ex + tan(beta) ey, normalised
-GG_HD V3 face_point(const Grid& g, int t, int a, int b) {
+// face coordinate (1 at the face's edges) of lattice line a (offset from
+// the first compute line): tan of equally spaced angles from the face
+// centre (equiangular), or sqrt(2) tan of latitudes equally spaced along
+// the edge meridian over [-asin(1/sqrt(3)), asin(1/sqrt(3))] (the
+// reference's gnomonic_ed, fv3core/grid/global_setup.py:42-85)
+GG_HD double face_coordinate(const Grid& g, int a) {
+  if (g.lattice == 1) {
+    const double alpha = asin(pow(3.0, -0.5));
+    const double dely = 2.0 * alpha / g.n;
+    return sqrt(2.0) * tan(-alpha + a * dely);
+  }
   const double dal = 0.5 * PI / g.n;
-  const double ta = tan(-0.25 * PI + a * dal), tb = tan(-0.25 * PI + b * dal);
+  return tan(-0.25 * PI + a * dal);
+}
+
+// unit vector of lattice point (a, b) (offsets from the first compute
+// corner) of face t: c + u(a) ex + u(b) ey, normalised
+GG_HD V3 face_point(const Grid& g, int t, int a, int b) {
+  const double ta = face_coordinate(g, a), tb = face_coordinate(g, b);
   V3 c, ex, ey;
   face_frame(t, c, ex, ey);
   const V3 p = {(c.x + ta * ex.x) + tb * ey.x, (c.y + ta * ex.y) + tb * ey.y, (c.z + ta * ex.z) + tb * ey.z};

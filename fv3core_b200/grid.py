@@ -9,9 +9,12 @@ for all six tiles at once, with halos.
 
 Construction (our own, from the standard FV3 cube geometry):
 
-* Cell corners of each face are the gnomonic projection of an equiangular
-  (alpha, beta) lattice on [-pi/4, pi/4]^2; faces are oriented so that the
-  tile connectivity is the FV3 one in ``halo_map``.
+* Cell corners of each face are the gnomonic projection of a lattice of
+  face coordinates (``face_coordinates``): by default equiangular (alpha,
+  beta on [-pi/4, pi/4]^2); ``lattice="equidistant"`` gives the reference's
+  gnomonic_ed (grid_type 0), whose edge points are equally spaced along the
+  edges.  Faces are oriented so that the tile connectivity is the FV3 one in
+  ``halo_map`` (tile 0 as the reference's first tile).
 * Halo corner points come from the neighbouring tile through the same halo
   gather as the dynamics (as the reference fills them with a halo update);
   the 3x3 blocks beyond two tile edges, which have no neighbour, extend the
@@ -40,14 +43,39 @@ _FACES = [
 ]
 
 
-def _face_points(tile, alpha, beta):
+def _face_points(tile, ua, ub):
+    """Unit vectors c + ua ex + ub ey of face ``tile`` for face coordinates
+    ua, ub (1 at the face's edges)."""
     c, ex, ey = (np.asarray(v, dtype=np.float64) for v in _FACES[tile])
     p = (
         c[None, None, :]
-        + np.tan(alpha)[:, :, None] * ex[None, None, :]
-        + np.tan(beta)[:, :, None] * ey[None, None, :]
+        + ua[:, :, None] * ex[None, None, :]
+        + ub[:, :, None] * ey[None, None, :]
     )
     return p / np.linalg.norm(p, axis=-1, keepdims=True)
+
+
+LATTICES = ("equiangular", "equidistant")
+
+
+def face_coordinates(n, halo, lattice="equiangular"):
+    """Face coordinate (1 at the face's edges) of the lattice lines -halo ..
+    n + halo.  ``equiangular``: tan of equally spaced angles from the face
+    centre, -pi/4 .. pi/4 over the face.  ``equidistant``: the reference's
+    gnomonic_ed (grid_type 0, fv3core/grid/global_setup.py:42-85), whose
+    edge points are equally spaced along the edge great circles (latitudes
+    -a .. a along the edge meridian, a = asin(1/sqrt(3))); on the face plane
+    that is sqrt(2) tan of those latitudes.  The halo lines continue the same
+    spacing."""
+    idx = np.arange(-halo, n + halo + 1)
+    if lattice == "equiangular":
+        dal = 0.5 * np.pi / n
+        return np.tan(-0.25 * np.pi + idx * dal)
+    if lattice == "equidistant":
+        alpha = np.arcsin(3 ** -0.5)
+        dely = 2.0 * alpha / n
+        return np.sqrt(2.0) * np.tan(-alpha + idx * dely)
+    raise ValueError(f"lattice must be one of {LATTICES}, got {lattice!r}")
 
 
 def _normalize(p):
@@ -98,10 +126,11 @@ class CubedSphereGrid:
     ``max_shape`` (``stencil.py:357-367``): ``[6, n+2h+1, n+2h+1]`` with the
     compute domain starting at index ``h``."""
 
-    def __init__(self, n, halo=3, radius=constants.RADIUS):
+    def __init__(self, n, halo=3, radius=constants.RADIUS, lattice="equiangular"):
         self.n = n
         self.halo = h = halo
         self.radius = radius
+        self.lattice = lattice
         m = n + 2 * h + 1
         self.shape2d = (N_TILES, m, m)
         self._build_corners()
@@ -111,13 +140,11 @@ class CubedSphereGrid:
     def _build_corners(self):
         n, h = self.n, self.halo
         m = n + 2 * h + 1
-        dal = 0.5 * np.pi / n
-        idx = np.arange(-h, n + h + 1)
-        a1 = -0.25 * np.pi + idx * dal
-        alpha, beta = np.meshgrid(a1, a1, indexing="ij")
+        u1 = face_coordinates(n, h, self.lattice)
+        ua, ub = np.meshgrid(u1, u1, indexing="ij")
         P = np.empty((N_TILES, m, m, 3))
         for t in range(N_TILES):
-            P[t] = _face_points(t, alpha, beta)
+            P[t] = _face_points(t, ua, ub)
         # snap each point to its exact cube-symmetric value: rebuild the halo
         # edge ring from the neighbour tiles so that shared points coincide
         for t in range(N_TILES):

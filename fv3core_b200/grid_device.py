@@ -14,6 +14,7 @@ import ctypes
 import torch
 
 from . import _lib, constants
+from .grid import LATTICES
 
 # the order of fv3b_grid_fields.field (include/fv3core_b200.h)
 GRID_FIELD_NAMES = [
@@ -31,13 +32,25 @@ GRID_FIELD_NAMES = [
 EDGE_NAMES = ["edge_w", "edge_e", "edge_s", "edge_n"]
 
 
+def bind():
+    """The FP64 library with fv3b_generate_grid's argument types set (the
+    generator writes FP64 in both builds)."""
+    L = _lib.lib("f64")
+    L.fv3b_generate_grid.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                     ctypes.POINTER(GridFields), ctypes.c_void_p]
+    L.fv3b_generate_grid.restype = ctypes.c_int
+    return L
+
+
 class GridFields(ctypes.Structure):
     _fields_ = [("field", ctypes.c_void_p * len(GRID_FIELD_NAMES)), ("edge", ctypes.c_void_p * 4),
                 ("a2b_extrap", ctypes.c_void_p), ("scalars", ctypes.c_void_p)]
 
 
 class DeviceGrid:
-    """Metric terms of an n x n cube (halo ``halo``) generated on ``device``.
+    """Metric terms of an n x n cube (halo ``halo``) generated on ``device``,
+    on the equiangular lattice or the reference's gnomonic_ed one
+    (``lattice``, as for ``CubedSphereGrid``).
 
     Attributes: the 2-D fields of ``GRID_FIELD_NAMES`` ([6, m, m] FP64 tensors
     indexed [tile, j, i], m = n + 2 halo + 1), ``edge_w`` .. ``edge_n``,
@@ -47,8 +60,11 @@ class DeviceGrid:
 
     layout = "ji"
 
-    def __init__(self, n, halo=3, radius=constants.RADIUS, omega=constants.OMEGA, device="cuda"):
-        self.n, self.halo, self.radius = int(n), int(halo), float(radius)
+    def __init__(self, n, halo=3, radius=constants.RADIUS, omega=constants.OMEGA, device="cuda",
+                 lattice="equiangular"):
+        if lattice not in LATTICES:
+            raise ValueError(f"lattice must be one of {LATTICES}, got {lattice!r}")
+        self.n, self.halo, self.radius, self.lattice = int(n), int(halo), float(radius), lattice
         m = self.n + 2 * self.halo + 1
         dev = torch.device(device)
         kw = dict(dtype=torch.float64, device=dev)
@@ -65,14 +81,11 @@ class DeviceGrid:
         scalars = torch.empty(4, **kw)
         out.a2b_extrap = self.a2b_extrap.data_ptr()
         out.scalars = scalars.data_ptr()
-        L = _lib.lib("f64")
-        L.fv3b_generate_grid.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
-                                         ctypes.POINTER(GridFields), ctypes.c_void_p]
-        L.fv3b_generate_grid.restype = ctypes.c_int
+        L = bind()
         with torch.cuda.device(dev):
             stream = torch.cuda.current_stream().cuda_stream
-            rc = L.fv3b_generate_grid(self.n, self.halo, self.radius, float(omega), ctypes.byref(out),
-                                      ctypes.c_void_p(stream))
+            rc = L.fv3b_generate_grid(self.n, self.halo, LATTICES.index(lattice), self.radius, float(omega),
+                                      ctypes.byref(out), ctypes.c_void_p(stream))
             if rc != 0:
                 raise RuntimeError(f"fv3b_generate_grid failed ({rc}): {L.fv3b_last_error().decode()}")
             self.da_min, self.da_max, self.da_min_c, self.da_max_c = (float(v) for v in scalars.cpu())

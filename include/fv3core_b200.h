@@ -623,7 +623,10 @@ fv3b_real* fv3b_acoustics_temporary(fv3b_ctx* ctx, const char* name);
  *   a2b_extrap: a2b_ord4's cube-corner extrapolation ratios, [6][4][3];
  *   scalars: da_min, da_max (cell areas over the compute domain), da_min_c,
  *     da_max_c (dual cells over the compute corners), [4].
- * radius in m, omega in 1/s (Coriolis fC, f0).  Needs 1 <= halo <= 8 and
+ * lattice: 0 for the equiangular lattice (the package's default grid), 1
+ * for the reference's gnomonic_ed (grid_type 0: edge points equally spaced
+ * along the edges, fv3core/grid/global_setup.py:42-85).  radius in m,
+ * omega in 1/s (Coriolis fC, f0).  Needs 1 <= halo <= 8 and
  * 2*halo <= n <= 4096.  Kernels run on `stream`; the call returns before
  * they finish.
  */
@@ -634,7 +637,8 @@ typedef struct {
   double* a2b_extrap;
   double* scalars;
 } fv3b_grid_fields;
-int fv3b_generate_grid(int n, int halo, double radius, double omega, const fv3b_grid_fields* out, void* stream);
+int fv3b_generate_grid(int n, int halo, int lattice, double radius, double omega, const fv3b_grid_fields* out,
+                       void* stream);
 
 /*
  * fv3b_del2cubed_noalloc: no reference counterpart.  The same filter as

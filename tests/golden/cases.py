@@ -437,3 +437,12 @@ def dycore_namelist(n, nz, n_split, sat_adj=False):
               ntiles=6, do_qa=True, n_split=n_split, moist_phys=True, c2l_ord=4, p_ref=1e5, nf_omega=1,
               do_sat_adj=bool(sat_adj))
     return nl
+
+
+def gnomonic_case(n=12, nz=1, seed=0):
+    """The reference's grid_type 0 face takes no inputs but its size."""
+    return {}
+
+
+CASES["gnomonic_ed_c12"] = gnomonic_case
+CASES["gnomonic_ed_c48"] = gnomonic_case

@@ -484,6 +484,35 @@ def run_step(case, n, nz):
     return out, {"region": "compute domain (+1 on staggered axes and interfaces)"}
 
 
+def run_gnomonic_ed(case, n, nz):
+    """The reference's grid_type 0 face (gnomonic_grid with
+    global_gnomonic_ed, fv3core/grid/global_setup.py:15-85: corner lon/lat of
+    the first tile's compute domain before rotation) and its own metric
+    functions on it (gnomonic.py: great_circle_distance_along_axis for dx,
+    dy; get_area; lon_lat_corner_to_cell_center).  fv3core.grid's package
+    init needs fv3gfs-util's partitioner, which is absent, so the three
+    modules load without it."""
+    import types
+
+    if "fv3core.grid" not in sys.modules:
+        pkg = types.ModuleType("fv3core.grid")
+        pkg.__path__ = [os.path.join(rr.reference_root(), "fv3core", "grid")]
+        sys.modules["fv3core.grid"] = pkg
+    from fv3core.grid import gnomonic as gn
+    from fv3core.grid.global_setup import gnomonic_grid
+    from fv3core.utils.global_constants import RADIUS
+
+    lon = np.zeros((n + 1, n + 1))
+    lat = np.zeros((n + 1, n + 1))
+    gnomonic_grid(0, lon, lat, np)
+    dx = gn.great_circle_distance_along_axis(lon, lat, RADIUS, np, axis=0)
+    dy = gn.great_circle_distance_along_axis(lon, lat, RADIUS, np, axis=1)
+    area = gn.get_area(lon, lat, RADIUS, np)
+    lon_a, lat_a = gn.lon_lat_corner_to_cell_center(lon, lat, np)
+    outputs = dict(lon=lon, lat=lat, dx=dx, dy=dy, area=area, lon_a=lon_a, lat_a=lat_a)
+    return outputs, {"radius": RADIUS}
+
+
 RUNNERS = {
     "acoustics": (run_acoustics, dict(n=12, nz=8, seed=41)),
     "d_sw": (run_d_sw, dict(n=12, nz=8, seed=31)),
@@ -498,6 +527,8 @@ RUNNERS = {
     "remap_satadj": (run_remap, dict(n=4, nz=79, seed=87)),
     "step": (run_step, dict(n=12, nz=12, seed=101)),
     "step_satadj": (run_step, dict(n=12, nz=12, seed=103)),
+    "gnomonic_ed_c12": (run_gnomonic_ed, dict(n=12, nz=1, seed=0)),
+    "gnomonic_ed_c48": (run_gnomonic_ed, dict(n=48, nz=1, seed=0)),
 }
 
 

@@ -6,8 +6,8 @@
 
 #include "../../fv3core_b200/csrc/grid_gen.h"
 
-extern "C" void grid_gen_host(int n, int h, double radius, double omega, double* fields, double* edges, double* a2b,
-                              double* scalars) {
+extern "C" void grid_gen_host(int n, int h, int lattice, double radius, double omega, double* fields, double* edges,
+                              double* a2b, double* scalars) {
   using namespace fv3b;
   fv3b_grid_dims gd{n, h, 1, 0};
   gg::Grid g;
@@ -15,6 +15,7 @@ extern "C" void grid_gen_host(int n, int h, double radius, double omega, double*
   g.n = n;
   g.h = h;
   g.m = n + 2 * h + 1;
+  g.lattice = lattice;
   g.radius = radius;
   g.omega = omega;
   const long long mm = (long long)g.m * g.m;

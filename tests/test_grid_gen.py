@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from fv3core_b200 import constants
-from fv3core_b200.grid import CubedSphereGrid
+from fv3core_b200.grid import LATTICES, CubedSphereGrid
 from fv3core_b200.grid_device import EDGE_NAMES, GRID_FIELD_NAMES
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -32,14 +32,14 @@ def host_lib(tmp_path_factory):
     return ctypes.CDLL(so)
 
 
-def _host_fields(lib, n, h=3):
+def _host_fields(lib, n, h=3, lattice=0):
     m = n + 2 * h + 1
     F = np.zeros((len(GRID_FIELD_NAMES), 6, m, m))
     E = np.zeros((4, 6, n + 1))
     A = np.zeros(72)
     S = np.zeros(4)
-    lib.grid_gen_host(n, h, ctypes.c_double(constants.RADIUS), ctypes.c_double(constants.OMEGA), _ptr(F), _ptr(E),
-                      _ptr(A), _ptr(S))
+    lib.grid_gen_host(n, h, lattice, ctypes.c_double(constants.RADIUS), ctypes.c_double(constants.OMEGA), _ptr(F),
+                      _ptr(E), _ptr(A), _ptr(S))
     return F, E, A.reshape(6, 4, 3), S
 
 
@@ -96,15 +96,16 @@ def test_field_order_matches_the_header():
     assert f"#define FV3B_GRID_NFIELDS {len(GRID_FIELD_NAMES)}" in hdr
 
 
+@pytest.mark.parametrize("lattice", ["equiangular", "equidistant"])
 @pytest.mark.parametrize("n", [7, 12, 48])
-def test_host_build_matches_numpy_generator(host_lib, n):
+def test_host_build_matches_numpy_generator(host_lib, n, lattice):
     """Every field of the point functions, compiled for the host, equals the
-    numpy generator's to rounding: 1e-13 of the field's largest magnitude
-    (measured 4e-16), the A->B edge weights and the area extremes to 1e-13
-    relative, a2b_ord4's corner ratios (a difference quotient of two close
-    distances) to 1e-12 relative."""
-    F, E, A, S = _host_fields(host_lib, n)
-    g = CubedSphereGrid(n, 3)
+    numpy generator's to rounding, on both lattices: 1e-13 of the field's
+    largest magnitude (measured 4e-16), the A->B edge weights and the area
+    extremes to 1e-13 relative, a2b_ord4's corner ratios (a difference
+    quotient of two close distances) to 1e-12 relative."""
+    F, E, A, S = _host_fields(host_lib, n, lattice=LATTICES.index(lattice))
+    g = CubedSphereGrid(n, 3, lattice=lattice)
     for k, name in enumerate(GRID_FIELD_NAMES):
         assert _field_err(F[k], np.asarray(getattr(g, name))) <= 1e-13, name
     for e, name in enumerate(EDGE_NAMES):
@@ -113,6 +114,55 @@ def test_host_build_matches_numpy_generator(host_lib, n):
     assert np.max(np.abs(A - g.a2b_extrap) / np.abs(g.a2b_extrap)) <= 1e-12
     ref = np.array([g.da_min, g.da_max, g.da_min_c, g.da_max_c])
     assert np.max(np.abs(S - ref) / ref) <= 1e-13
+
+
+@pytest.mark.parametrize("n", [12, 48])
+def test_equidistant_lattice_is_the_reference_grid_type_0(n):
+    """The equidistant lattice is the reference's grid_type 0 (gnomonic_ed):
+    tile 0's compute-domain corners, their lengths, the cell areas and the
+    cell-centre latitudes against the reference's own face and metric
+    functions (tests/golden/gnomonic_ed_c*.npz, made by make_golden.py):
+    corners to 1e-14, lengths to 1e-13 relative, areas to 1e-11 relative
+    (the reference's area sums four spherical angles, good to 1e-12 by its
+    own account: 2e-12 here at C48), centre latitudes to 1e-14.  The
+    equiangular lattice differs from it by up to 20 % in lengths."""
+    d = np.load(os.path.join(ROOT, "tests", "golden", f"gnomonic_ed_c{n}.npz"))
+    h = 3
+    lon, lat = d["lon"], d["lat"]
+    ref_corners = np.stack([np.cos(lat) * np.cos(lon), np.cos(lat) * np.sin(lon), np.sin(lat)], axis=-1)
+    for lattice, agrees in (("equidistant", True), ("equiangular", False)):
+        g = CubedSphereGrid(n, h, lattice=lattice)
+        dx = np.asarray(g.dx)[0, h:h + n, h:h + n + 1]
+        rel = np.max(np.abs(dx / d["dx"] - 1.0))
+        if not agrees:
+            assert rel > 0.1
+            continue
+        assert np.max(np.abs(g.corners[0, h:h + n + 1, h:h + n + 1] - ref_corners)) <= 1e-14
+        assert rel <= 1e-13
+        assert np.max(np.abs(np.asarray(g.dy)[0, h:h + n + 1, h:h + n] / d["dy"] - 1.0)) <= 1e-13
+        assert np.max(np.abs(np.asarray(g.area)[0, h:h + n, h:h + n] / d["area"] - 1.0)) <= 1e-11
+        assert np.max(np.abs(np.asarray(g.lat_a)[0, h:h + n, h:h + n] - d["lat_a"])) <= 1e-14
+
+
+def test_entry_point_rejects_bad_arguments_without_gpu():
+    """fv3b_generate_grid checks its arguments before any CUDA call, in the
+    order of the Python binding: a bad halo, lattice or radius each comes
+    back as FV3B_ERR_ARGUMENT naming it."""
+    from fv3core_b200 import _lib
+    from fv3core_b200.grid_device import GridFields, bind
+
+    L = bind()
+    out = GridFields()
+    for k in range(len(GRID_FIELD_NAMES)):
+        out.field[k] = 16
+    for e in range(4):
+        out.edge[e] = 16
+    out.a2b_extrap = out.scalars = 16
+    for args, word in (((12, 99, 0, 6.4e6), "halo"), ((12, 3, 5, 6.4e6), "lattice"), ((12, 3, 1, -1.0), "radius")):
+        rc = L.fv3b_generate_grid(*args, 7.3e-5, ctypes.byref(out), None)
+        assert rc == 1, args
+        assert word in L.fv3b_last_error().decode(), args
+    assert _lib.exported_symbols().count("fv3b_generate_grid") == 1
 
 
 @pytest.mark.gpu
