@@ -510,6 +510,20 @@ def run_gnomonic_ed(case, n, nz):
     area = gn.get_area(lon, lat, RADIUS, np)
     lon_a, lat_a = gn.lon_lat_corner_to_cell_center(lon, lat, np)
     outputs = dict(lon=lon, lat=lat, dx=dx, dy=dy, area=area, lon_a=lon_a, lat_a=lat_a)
+    # the angles of calculate_supergrid_cos_sin (geometry.py:163-215) at the
+    # four edge midpoints of each cell, and the corner angle of
+    # _calculate_more_trig_terms (geometry.py:326-352), with the
+    # reference's spherical_cos and midpoints
+    P = gn.lon_lat_to_xyz(lon, lat, np)
+    A = gn.lon_lat_to_xyz(lon_a, lat_a, np)
+    mid = gn.xyz_midpoint
+    outputs["cos_sg1"] = gn.spherical_cos(mid(P[:-1, :-1], P[:-1, 1:]), A, P[:-1, 1:], np)
+    outputs["cos_sg2"] = gn.spherical_cos(mid(P[:-1, :-1], P[1:, :-1]), P[1:, :-1], A, np)
+    outputs["cos_sg3"] = gn.spherical_cos(mid(P[1:, :-1], P[1:, 1:]), A, P[1:, :-1], np)
+    outputs["cos_sg4"] = gn.spherical_cos(mid(P[:-1, 1:], P[1:, 1:]), P[:-1, 1:], A, np)
+    sg6 = gn.spherical_cos(P[:-1, :-1], P[1:, :-1], P[:-1, 1:], np)
+    sg8 = gn.spherical_cos(P[1:, 1:], P[1:, :-1], P[:-1, 1:], np)
+    outputs["cosa_interior"] = 0.5 * (sg8[:-1, :-1] + sg6[1:, 1:])
     return outputs, {"radius": RADIUS}
 
 

@@ -124,8 +124,10 @@ def test_equidistant_lattice_is_the_reference_grid_type_0(n):
     functions (tests/golden/gnomonic_ed_c*.npz, made by make_golden.py):
     corners to 1e-14, lengths to 1e-13 relative, areas to 1e-11 relative
     (the reference's area sums four spherical angles, good to 1e-12 by its
-    own account: 2e-12 here at C48), centre latitudes to 1e-14.  The
-    equiangular lattice differs from it by up to 20 % in lengths."""
+    own account: 2e-12 here at C48), centre latitudes to 1e-14, and the
+    angles at the edge midpoints (cos_sg1..4) and the interior corners
+    (cosa) to 1e-12 (measured 8e-14; the reference goes through lon/lat).
+    The equiangular lattice differs from it by up to 20 % in lengths."""
     d = np.load(os.path.join(ROOT, "tests", "golden", f"gnomonic_ed_c{n}.npz"))
     h = 3
     lon, lat = d["lon"], d["lat"]
@@ -142,6 +144,10 @@ def test_equidistant_lattice_is_the_reference_grid_type_0(n):
         assert np.max(np.abs(np.asarray(g.dy)[0, h:h + n + 1, h:h + n] / d["dy"] - 1.0)) <= 1e-13
         assert np.max(np.abs(np.asarray(g.area)[0, h:h + n, h:h + n] / d["area"] - 1.0)) <= 1e-11
         assert np.max(np.abs(np.asarray(g.lat_a)[0, h:h + n, h:h + n] - d["lat_a"])) <= 1e-14
+        for k in range(1, 5):
+            cs = np.asarray(getattr(g, f"cos_sg{k}"))[0, h:h + n, h:h + n]
+            assert np.max(np.abs(cs - d[f"cos_sg{k}"])) <= 1e-12, k
+        assert np.max(np.abs(np.asarray(g.cosa)[0, h + 1:h + n, h + 1:h + n] - d["cosa_interior"])) <= 1e-12
 
 
 def test_entry_point_rejects_bad_arguments_without_gpu():
