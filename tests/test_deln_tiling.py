@@ -118,3 +118,35 @@ def test_fused_chain_reads_every_small_grid():
         for nmax in (1, 2):
             problems, _, _ = _check(n, nmax)
             assert not problems, (n, nmax, problems[:3])
+
+
+def test_host_check_agrees_with_the_enumeration(tmp_path):
+    """The library's own host check (deln_window_ok, compiled with nvcc for
+    the host) accepts every grid with the 3-point halo that the enumeration
+    above accepts (cube sizes 4 to 200), so the fused kernel serves them;
+    with a 2-point halo it declines, and the chain runs pass by pass."""
+    import os
+    import shutil
+    import subprocess
+
+    nvcc = shutil.which("nvcc") or ("/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else None)
+    if nvcc is None:
+        pytest.skip("no nvcc")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "deln_window_dump")
+    subprocess.check_call([nvcc, "-std=c++17", "--expt-extended-lambda", "-O1", "-gencode",
+                           "arch=compute_100a,code=sm_100a", "-o", exe,
+                           os.path.join(root, "tests", "native", "deln_window_dump.cu")])
+    ok = {}
+    for line in subprocess.check_output([exe], text=True).split("\n"):
+        if line:
+            n, h, nmax, v = (int(x) for x in line.split())
+            ok[(n, h, nmax)] = bool(v)
+    for n in range(4, 201):
+        for nmax in (1, 2):
+            assert ok[(n, 3, nmax)], (n, nmax)
+            assert not ok[(n, 2, nmax)], (n, nmax)
+    for n in list(range(4, 41)) + [96, 128, 192]:
+        for nmax in (1, 2):
+            problems, _, _ = _check(n, nmax)
+            assert not problems and ok[(n, 3, nmax)], (n, nmax)
