@@ -18,9 +18,19 @@ from fv3core_b200.initial_state import baroclinic_state
 HALO = 3
 
 
+# Face lattice of the cases' grid: the package's equiangular default, or
+# "equidistant" (the reference's grid_type 0) for the fixtures made on the
+# reference's own grid
+LATTICE = "equiangular"
+
+
 @functools.lru_cache(maxsize=8)
+def _grid(n, lattice):
+    return CubedSphereGrid(n, HALO, lattice=lattice)
+
+
 def grid_for(n):
-    return CubedSphereGrid(n, HALO)
+    return _grid(n, LATTICE)
 
 
 def base_state(n, nz, seed):
@@ -207,6 +217,7 @@ def smooth_acoustics_case(n=48, nz=79, n_split=6):
 # the parity case of the plain FP64 method: C12 L79, one acoustic substep of
 # dt_acoustic = 225 / 6 s (n_split = 1, mdt = 37.5 s)
 CASES["acoustics_c12_l79"] = acoustics_case
+CASES["acoustics_c12_l79_ed"] = acoustics_case
 
 
 def resting_case(n=12, nz=8, n_split=2):

@@ -541,6 +541,8 @@ RUNNERS = {
     "remap_satadj": (run_remap, dict(n=4, nz=79, seed=87)),
     "step": (run_step, dict(n=12, nz=12, seed=101)),
     "step_satadj": (run_step, dict(n=12, nz=12, seed=103)),
+    # BASELINE's plain FP64 case on the reference's own grid (grid_type 0)
+    "acoustics_c12_l79_ed": (run_acoustics_compute, dict(n=12, nz=79, seed=7, n_split=1, lattice="equidistant")),
     "gnomonic_ed_c12": (run_gnomonic_ed, dict(n=12, nz=1, seed=0)),
     "gnomonic_ed_c48": (run_gnomonic_ed, dict(n=48, nz=1, seed=0)),
 }
@@ -551,8 +553,12 @@ def main(names):
     for name in names or list(RUNNERS):
         fn, kw = RUNNERS[name]
         t0 = time.time()
+        kw = dict(kw)
+        cases.LATTICE = kw.pop("lattice", "equiangular")
         case = cases.CASES[name](**kw)
         outputs, meta = fn(case, kw["n"], kw["nz"])
+        meta["lattice"] = cases.LATTICE
+        cases.LATTICE = "equiangular"
         path = os.path.join(HERE, f"{name}.npz")
         np.savez_compressed(path, **outputs, **{f"meta_{k}": v for k, v in meta.items()}, **{f"arg_{k}": v for k, v in kw.items()})
         print(f"{name}: {time.time() - t0:.1f}s -> {path} ({os.path.getsize(path) / 1e3:.0f} kB)")

@@ -134,6 +134,22 @@ def test_oracle_matches_reference_golden_c12_l79():
         assert _same(v, g[k]), k
 
 
+def test_oracle_matches_reference_golden_c12_l79_on_the_reference_grid(monkeypatch):
+    """The same case on the reference's own grid (grid_type 0, the
+    equidistant lattice, which tests/test_grid_gen.py pins to the
+    reference's grid functions): the oracle reproduces the reference's
+    substep bit for bit there too."""
+    path = os.path.join(HERE, "golden", "acoustics_c12_l79_ed.npz")
+    g = np.load(path)
+    assert str(g["meta_lattice"]) == "equidistant"
+    monkeypatch.setattr(cases, "LATTICE", "equidistant")
+    n, nz, seed, n_split = (int(g["arg_" + k]) for k in ("n", "nz", "seed", "n_split"))
+    case = cases.acoustics_case(n, nz, seed, n_split=n_split)
+    out = _golden_fields(oracle_runs.run_acoustics(case, n, nz), g, n, nz)
+    for k, v in out.items():
+        assert _same(v, g[k]), k
+
+
 # Bounds of the CUDA path against the reference's own arithmetic (numpy's
 # exp/log/power) on the C12 L79 substep.  The oracle with numpy's
 # transcendentals and the oracle with the kernels' own (both within 1 ulp)
