@@ -559,7 +559,7 @@ def step_cpu_sample(n, npz, n_split):
 
 
 def run_step_section(args, state0, grid384, local):
-    """BASELINE configurations of the whole dynamics step: the plain FP64
+    """The whole dynamics step: the plain FP64
     (and mixed) DynamicalCore.step_dynamics at C``step_n`` L79 — time per
     step, roofline, the oracle step on the host — and the mixed build's
     error against FP64 after 1 and ``error_steps`` steps at C384 L79."""
@@ -760,8 +760,8 @@ def _parse_members(spec):
 
 
 def run_ensemble(args):
-    """Ensemble of seed-perturbed members at mixed resolutions (BASELINE
-    configuration 4): the members of each resolution batched in one context,
+    """Ensemble of seed-perturbed members at mixed resolutions (16 x C48 L79,
+    8 x C96 L79, 4 x C192 L63 by default): the members of each resolution batched in one context,
     so every kernel of an AcousticDynamics call advances all of them in one
     launch, one CUDA graph per ensemble step, optionally after the
     launch-shape autotuner; against the same members one at a time (one

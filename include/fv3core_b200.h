@@ -99,7 +99,7 @@ int fv3b_ctx_create(const fv3b_grid_dims* dims, const fv3b_metrics* metrics, fv3
  * for every member.  Each stage call then advances all members in one
  * launch per kernel; halo updates stay within a member.  The reference has
  * no counterpart (it runs one cube per process); it replaces running
- * members one at a time.  The adjoint entry
+ * members one at a time, one context each.  The adjoint entry
  * points serve single cubes only.
  */
 int fv3b_ctx_create_batched(const fv3b_grid_dims* dims, const fv3b_metrics* metrics, int members, fv3b_ctx** out);

@@ -541,7 +541,7 @@ RUNNERS = {
     "remap_satadj": (run_remap, dict(n=4, nz=79, seed=87)),
     "step": (run_step, dict(n=12, nz=12, seed=101)),
     "step_satadj": (run_step, dict(n=12, nz=12, seed=103)),
-    # BASELINE's plain FP64 case on the reference's own grid (grid_type 0)
+    # the plain FP64 C12 L79 substep on the reference's own grid (grid_type 0)
     "acoustics_c12_l79_ed": (run_acoustics_compute, dict(n=12, nz=79, seed=7, n_split=1, lattice="equidistant")),
     "gnomonic_ed_c12": (run_gnomonic_ed, dict(n=12, nz=1, seed=0)),
     "gnomonic_ed_c48": (run_gnomonic_ed, dict(n=48, nz=1, seed=0)),
